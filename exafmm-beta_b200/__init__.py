@@ -1,0 +1,285 @@
+"""Python binding of the B200 Laplace FMM engine (ctypes over include/exafmm_b200.h).
+
+The engine itself is C++/CUDA (libexafmm_b200.so next to this file); this
+module only marshals arrays.  There is no CPU fallback: if the shared library
+is missing or no CUDA device is usable, the calls raise.
+
+Typical use mirrors examples/fmm.cxx::
+
+    fmm = Fmm(P=10, theta=0.4, ncrit=64)
+    fmm.set_bodies(xyzq)          # (n, 4) float64: x, y, z, charge
+    fmm.solve()                   # getBounds, buildTree, upward, traverse, downward
+    trg = fmm.results()           # (n, 4): potential, grad x, grad y, grad z
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libexafmm_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "exafmm_b200.h")
+
+FP64 = 0
+MIXED = 1
+
+_c_int, _c_ll, _c_double, _vp = ctypes.c_int, ctypes.c_longlong, ctypes.c_double, ctypes.c_void_p
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile libexafmm_b200.so for sm_100a (nvcc cross-compiles without a GPU)."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-j8", "-C", os.path.join(HERE, "csrc")], check=True)
+    return LIB_PATH
+
+
+def exported_symbols() -> list[str]:
+    """Every function declared in include/exafmm_b200.h."""
+    import re
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(exafmm_[a-z0-9_]+)\s*\(", text)))
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: run build() (or __graft_entry__.build())")
+    L = ctypes.CDLL(LIB_PATH)
+    sig = {
+        "exafmm_create": (_c_int, [ctypes.POINTER(_vp), _c_int, _c_double, _c_int, _c_int, _c_int, _c_double,
+                                   _c_int, _c_int]),
+        "exafmm_destroy": (_c_int, [_vp]),
+        "exafmm_last_error": (ctypes.c_char_p, [_vp]),
+        "exafmm_create_error": (ctypes.c_char_p, []),
+        "exafmm_kernel_error": (ctypes.c_char_p, []),
+        "exafmm_set_bodies": (_c_int, [_vp, _vp, _c_ll]),
+        "exafmm_set_bodies_device": (_c_int, [_vp, _vp, _c_ll]),
+        "exafmm_get_bounds": (_c_int, [_vp, _vp]),
+        "exafmm_build_tree": (_c_int, [_vp, _vp]),
+        "exafmm_upward": (_c_int, [_vp]),
+        "exafmm_traverse": (_c_int, [_vp]),
+        "exafmm_downward": (_c_int, [_vp]),
+        "exafmm_solve": (_c_int, [_vp]),
+        "exafmm_get_results": (_c_int, [_vp, _vp]),
+        "exafmm_get_results_device": (_c_int, [_vp, _vp]),
+        "exafmm_tree_info": (_c_int, [_vp, ctypes.POINTER(_c_ll), ctypes.POINTER(_c_int), ctypes.POINTER(_c_ll),
+                                      ctypes.POINTER(_c_ll)]),
+        "exafmm_get_cells": (_c_int, [_vp, _vp, _vp]),
+        "exafmm_get_perm": (_c_int, [_vp, _vp]),
+        "exafmm_get_lists": (_c_int, [_vp, _vp, _vp]),
+        "exafmm_get_expansions": (_c_int, [_vp, _vp, _vp]),
+        "exafmm_stream": (_vp, [_vp]),
+        "exafmm_phase_times": (_c_int, [_vp, _vp]),
+        "exafmm_direct": (_c_int, [_vp, _c_ll, _vp, _c_ll, _c_int, _c_double, _c_double, _vp]),
+        "exafmm_kernel_p2m": (_c_int, [_c_int, _vp, _c_ll, _vp, _vp]),
+        "exafmm_kernel_m2m": (_c_int, [_c_int, _vp, _c_int, _vp, _vp, _vp]),
+        "exafmm_kernel_m2l": (_c_int, [_c_int, _vp, _vp, _vp, _vp, _vp]),
+        "exafmm_kernel_l2l": (_c_int, [_c_int, _vp, _vp, _vp, _vp]),
+        "exafmm_kernel_l2p": (_c_int, [_c_int, _vp, _vp, _c_ll, _vp, _vp]),
+        "exafmm_kernel_p2p": (_c_int, [_c_ll, _vp, _c_ll, _vp, _vp, _vp]),
+        "exafmm_drift": (_c_double, [_c_double, _c_ll, _c_int]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+def _f64(a, shape_last=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if shape_last is not None:
+        assert a.shape[-1] == shape_last
+    return a
+
+
+def _c128(a):
+    return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+class FmmError(RuntimeError):
+    pass
+
+
+class Fmm:
+    """One solve context (a CUDA stream plus every device buffer of a solve)."""
+
+    def __init__(self, P=10, theta=0.4, ncrit=64, nspawn=5000, images=0, cycle=2 * np.pi, precision=FP64,
+                 device=-1):
+        L = lib()
+        h = _vp()
+        if L.exafmm_create(ctypes.byref(h), P, theta, ncrit, nspawn, images, cycle, precision, device) != 0:
+            raise FmmError(L.exafmm_create_error().decode())
+        self._h = h
+        self.P, self.theta, self.ncrit, self.nspawn, self.images, self.cycle = P, theta, ncrit, nspawn, images, cycle
+        self.precision = precision
+        self.n = 0
+
+    def _check(self, rc):
+        if rc != 0:
+            raise FmmError(lib().exafmm_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().exafmm_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- solve steps (examples/fmm.cxx:163-179) ----
+    def set_bodies(self, xyzq):
+        xyzq = _f64(xyzq, 4)
+        self.n = len(xyzq)
+        self._check(lib().exafmm_set_bodies(self._h, _p(xyzq), self.n))
+
+    def set_bodies_device(self, ptr: int, n: int):
+        self.n = n
+        self._check(lib().exafmm_set_bodies_device(self._h, _vp(ptr), n))
+
+    def get_bounds(self) -> np.ndarray:
+        b = np.zeros(6)
+        self._check(lib().exafmm_get_bounds(self._h, _p(b)))
+        return b
+
+    def build_tree(self, bounds=None):
+        b = None if bounds is None else _f64(bounds)
+        self._check(lib().exafmm_build_tree(self._h, _p(b)))
+
+    def upward(self):
+        self._check(lib().exafmm_upward(self._h))
+
+    def traverse(self):
+        self._check(lib().exafmm_traverse(self._h))
+
+    def downward(self):
+        self._check(lib().exafmm_downward(self._h))
+
+    def solve(self):
+        self._check(lib().exafmm_solve(self._h))
+
+    def results(self) -> np.ndarray:
+        out = np.zeros((self.n, 4))
+        self._check(lib().exafmm_get_results(self._h, _p(out)))
+        return out
+
+    def results_device(self, ptr: int):
+        self._check(lib().exafmm_get_results_device(self._h, _vp(ptr)))
+
+    # ---- inspection ----
+    def info(self) -> dict:
+        nc, nm, npp, d = _c_ll(), _c_ll(), _c_ll(), _c_int()
+        self._check(lib().exafmm_tree_info(self._h, ctypes.byref(nc), ctypes.byref(d), ctypes.byref(nm),
+                                           ctypes.byref(npp)))
+        return {"ncells": nc.value, "depth": d.value, "n_m2l": nm.value, "n_p2p": npp.value}
+
+    def cells(self):
+        nc = self.info()["ncells"]
+        ints = np.zeros((nc, 5), dtype=np.int32)
+        reals = np.zeros((nc, 4))
+        self._check(lib().exafmm_get_cells(self._h, _p(ints), _p(reals)))
+        return ints, reals
+
+    def perm(self) -> np.ndarray:
+        p = np.zeros(self.n, dtype=np.int32)
+        self._check(lib().exafmm_get_perm(self._h, _p(p)))
+        return p
+
+    def lists(self):
+        i = self.info()
+        m2l = np.zeros((max(i["n_m2l"], 0), 3), dtype=np.int32)
+        p2p = np.zeros((max(i["n_p2p"], 0), 3), dtype=np.int32)
+        self._check(lib().exafmm_get_lists(self._h, _p(m2l), _p(p2p)))
+        return m2l, p2p
+
+    def expansions(self):
+        nc = self.info()["ncells"]
+        nt = self.P * (self.P + 1) // 2
+        M = np.zeros((nc, nt), dtype=np.complex128)
+        L = np.zeros((nc, nt), dtype=np.complex128)
+        self._check(lib().exafmm_get_expansions(self._h, _p(M), _p(L)))
+        return M, L
+
+    def stream(self) -> int:
+        return lib().exafmm_stream(self._h) or 0
+
+    def phase_times(self) -> dict:
+        t = np.zeros(7)
+        self._check(lib().exafmm_phase_times(self._h, _p(t)))
+        return dict(zip(["bounds", "tree", "upward", "lists", "m2l_p2p", "downward", "total"], t.tolist()))
+
+
+# ---- free functions: direct sum and per-operator forms ----
+def _kcheck(rc):
+    if rc != 0:
+        raise FmmError(lib().exafmm_kernel_error().decode())
+
+
+def direct(targets, sources, images=0, theta=0.4, cycle=2 * np.pi, trg=None) -> np.ndarray:
+    t, s = _f64(targets, 4), _f64(sources, 4)
+    out = np.zeros((len(t), 4)) if trg is None else _f64(trg).copy()
+    _kcheck(lib().exafmm_direct(_p(t), len(t), _p(s), len(s), images, theta, cycle, _p(out)))
+    return out
+
+
+def p2m(P, X, xyzq, M=None):
+    x = _f64(xyzq, 4)
+    out = np.zeros(P * (P + 1) // 2, np.complex128) if M is None else _c128(M).copy()
+    _kcheck(lib().exafmm_kernel_p2m(P, _p(_f64(X)), len(x), _p(x), _p(out)))
+    return out
+
+
+def m2m(P, Xp, Xc, Mc, Mp=None):
+    Xc = _f64(Xc).reshape(-1, 3)
+    Mc = _c128(Mc).reshape(len(Xc), -1)
+    out = np.zeros(P * (P + 1) // 2, np.complex128) if Mp is None else _c128(Mp).copy()
+    _kcheck(lib().exafmm_kernel_m2m(P, _p(_f64(Xp)), len(Xc), _p(Xc), _p(Mc), _p(out)))
+    return out
+
+
+def m2l(P, Xi, Xj, Mj, Li=None, Xper=None):
+    out = np.zeros(P * (P + 1) // 2, np.complex128) if Li is None else _c128(Li).copy()
+    xp = None if Xper is None else _f64(Xper)
+    _kcheck(lib().exafmm_kernel_m2l(P, _p(_f64(Xi)), _p(_f64(Xj)), _p(_c128(Mj)), _p(out), _p(xp)))
+    return out
+
+
+def l2l(P, Xc, Xp, Lp, Lc=None):
+    out = np.zeros(P * (P + 1) // 2, np.complex128) if Lc is None else _c128(Lc).copy()
+    _kcheck(lib().exafmm_kernel_l2l(P, _p(_f64(Xc)), _p(_f64(Xp)), _p(_c128(Lp)), _p(out)))
+    return out
+
+
+def l2p(P, X, L, xyzq, trg=None):
+    x = _f64(xyzq, 4)
+    out = np.zeros((len(x), 4)) if trg is None else _f64(trg).copy()
+    _kcheck(lib().exafmm_kernel_l2p(P, _p(_f64(X)), _p(_c128(L)), len(x), _p(x), _p(out)))
+    return out
+
+
+def p2p(xi, xj, Xper=None, trg=None):
+    a, b = _f64(xi, 4), _f64(xj, 4)
+    out = np.zeros((len(a), 4)) if trg is None else _f64(trg).copy()
+    xp = None if Xper is None else _f64(Xper)
+    _kcheck(lib().exafmm_kernel_p2p(len(a), _p(a), len(b), _p(b), _p(xp), _p(out)))
+    return out
+
+
+def drift(x: float, k: int, up: bool = False) -> float:
+    return lib().exafmm_drift(float(x), int(k), int(up))

@@ -1,0 +1,480 @@
+// extern "C" surface of the engine (include/exafmm_b200.h) and the solve driver.
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <vector>
+
+#include "../../include/exafmm_b200.h"
+#include "drift.cuh"
+#include "fmm.h"
+#include "harmonics.cuh"
+
+namespace exafmm_b200 {
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+void throw_cuda(cudaError_t e, const char *what, const char *file, int line) {
+  std::string m = std::string(cudaGetErrorString(e)) + " in " + what + " (" + file + ":" + std::to_string(line) + ")";
+  throw CudaError(m);
+}
+void throw_msg(const char *msg) { throw std::runtime_error(msg); }
+
+void direct_fp64(const double4 *tgt, long long nt, const double4 *src, long long ns, int prange, double cycle,
+                 double4 *trg, cudaStream_t st);
+
+namespace {
+
+struct Timing {
+  cudaEvent_t ev[8] = {};
+  bool live = false;
+  void init() {
+    if (live) return;
+    for (auto &e : ev) EXA_CUDA(cudaEventCreate(&e));
+    live = true;
+  }
+  ~Timing() {
+    if (live)
+      for (auto &e : ev) cudaEventDestroy(e);
+  }
+};
+
+}  // namespace
+
+struct Engine {
+  Context C;
+  ListBufs lists;
+  DBuf<double2> M, L;
+  DBuf<double4> trg, out;
+  Timing tm;
+  bool tree_ok = false, up_ok = false, lists_ok = false;
+
+  FmmArgs args() {
+    FmmArgs a;
+    a.P = C.prm.P;
+    a.ncrit = C.prm.ncrit;
+    a.ncells = C.tree.ncells;
+    a.cycle = C.prm.cycle;
+    a.stream = C.stream;
+    a.lvl = C.tree.lvl.p;
+    a.nd_cell = C.tree.nd_cell.p;
+    a.cell_b = C.tree.cell_b.p;
+    a.cell_pl = C.tree.cell_pl.p;
+    a.cell_x = C.tree.cell_x.p;
+    a.xt = C.tree.xyzq_tree.p;
+    a.m2l_off = lists.m2l_off.p;
+    a.m2l_src = lists.m2l_src.p;
+    a.p2p_off = lists.p2p_off.p;
+    a.p2p_src = lists.p2p_src.p;
+    a.M64 = M.p;
+    a.L64 = L.p;
+    a.trg64 = trg.p;
+    return a;
+  }
+
+  void check_err(const char *phase) {
+    EXA_CUDA(cudaMemcpyAsync(C.err_host, C.err.p, sizeof(int), cudaMemcpyDeviceToHost, C.stream));
+    EXA_CUDA(cudaStreamSynchronize(C.stream));
+    int e = *C.err_host;
+    if (e) {
+      EXA_CUDA(cudaMemsetAsync(C.err.p, 0, sizeof(int), C.stream));
+      std::string m = std::string(phase) + ": device error flags " + std::to_string(e);
+      if (e & kErrTreeTooDeep) m += " (tree deeper than 21 levels: more than ncrit coincident bodies?)";
+      throw std::runtime_error(m);
+    }
+  }
+
+  void set_bodies(const double *xyzq, long long n, cudaMemcpyKind kind) {
+    if (n < 0) throw std::runtime_error("negative body count");
+    if (n >= (1LL << 26)) throw std::runtime_error("more than 2^26 bodies per context is not supported");
+    C.tree.n = n;
+    C.tree.xyzq.ensure(n);
+    if (n) EXA_CUDA(cudaMemcpyAsync(C.tree.xyzq.p, xyzq, n * sizeof(double4), kind, C.stream));
+    tree_ok = up_ok = lists_ok = false;
+  }
+
+  void build(const double *bounds6) {
+    tm.init();
+    EXA_CUDA(cudaEventRecord(tm.ev[0], C.stream));
+    if (bounds6) set_bounds(C, bounds6);
+    else compute_bounds(C);
+    EXA_CUDA(cudaEventRecord(tm.ev[1], C.stream));
+    for (int attempt = 0;; attempt++) {
+      build_tree(C);
+      sync_tree(C);
+      int e = *C.err_host;
+      if ((e & kErrCellOverflow) && attempt < 8) {
+        EXA_CUDA(cudaMemsetAsync(C.err.p, 0, sizeof(int), C.stream));
+        build_tree_grow(2 * C.tree.node_cap);
+        continue;
+      }
+      break;
+    }
+    check_err("build_tree");
+    EXA_CUDA(cudaEventRecord(tm.ev[2], C.stream));
+    tree_ok = true;
+    up_ok = lists_ok = false;
+  }
+
+  void build_tree_grow(long long cap) {
+    TreeBufs &T = C.tree;
+    T.nd_begin.ensure(cap);
+    T.nd_count.ensure(cap);
+    T.nd_nchild.ensure(cap);
+    T.nd_childbeg.ensure(cap);
+    T.nd_nnode.ensure(cap);
+    T.nd_cell.ensure(cap);
+    T.nd_pcell.ensure(cap);
+    T.nd_ichild.ensure(cap);
+    T.nd_x.ensure(cap);
+    T.cell_b.ensure(cap);
+    T.cell_pl.ensure(cap);
+    T.cell_x.ensure(cap);
+    T.cell_node.ensure(cap);
+    T.node_cap = cap;
+    T.cell_cap = cap;
+  }
+
+  void upward() {
+    if (!tree_ok) throw std::runtime_error("upward pass before build_tree");
+    const long long nc = C.tree.ncells;
+    const int NT = tri(C.prm.P);
+    M.ensure(nc * NT);
+    L.ensure(nc * NT);
+    if (nc > 0) {
+      FmmArgs a = args();
+      p2m_fp64(a);
+      for (int l = C.tree.depth - 1; l >= 0; l--) m2m_fp64(a, l, C.tree.lvl_host[l]);
+    }
+    EXA_CUDA(cudaEventRecord(tm.ev[3], C.stream));
+    up_ok = true;
+  }
+
+  void traverse_and_evaluate() {
+    if (!up_ok) throw std::runtime_error("traverse before the upward pass");
+    const long long nc = C.tree.ncells;
+    const int NT = tri(C.prm.P);
+    trg.ensure(C.tree.n);
+    if (C.tree.n) EXA_CUDA(cudaMemsetAsync(trg.p, 0, C.tree.n * sizeof(double4), C.stream));
+    if (nc > 0) {
+      for (int attempt = 0; !traverse(C, lists); attempt++)
+        if (attempt > 8) throw std::runtime_error("traversal capacity growth did not converge");
+      check_err("traverse");
+      EXA_CUDA(cudaEventRecord(tm.ev[4], C.stream));
+      EXA_CUDA(cudaMemsetAsync(L.p, 0, nc * NT * sizeof(double2), C.stream));
+      FmmArgs a = args();
+      m2l_fp64(a);
+      p2p_fp64(a);
+    } else {
+      EXA_CUDA(cudaEventRecord(tm.ev[4], C.stream));
+    }
+    EXA_CUDA(cudaEventRecord(tm.ev[5], C.stream));
+    lists_ok = true;
+  }
+
+  void downward() {
+    if (!lists_ok) throw std::runtime_error("downward pass before traverse");
+    const long long nc = C.tree.ncells;
+    if (nc > 0) {
+      FmmArgs a = args();
+      for (int l = 1; l <= C.tree.depth; l++) l2l_fp64(a, l, C.tree.lvl_host[l]);
+      l2p_fp64(a);
+    }
+    EXA_CUDA(cudaEventRecord(tm.ev[6], C.stream));
+  }
+
+  void results(double *dst, cudaMemcpyKind kind);
+};
+
+namespace {
+__global__ void k_unsort(const double4 *trg, const int *perm, long long n, double4 *out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[perm[i]] = trg[i];
+}
+}  // namespace
+
+void Engine::results(double *dst, cudaMemcpyKind kind) {
+  if (!lists_ok) throw std::runtime_error("results before a solve");
+  const long long n = C.tree.n;
+  out.ensure(n);
+  if (n) {
+    k_unsort<<<kNumSMs * 4, 256, 0, C.stream>>>(trg.p, C.tree.perm.p, n, out.p);
+    EXA_CHECK_LAUNCH();
+    EXA_CUDA(cudaMemcpyAsync(dst, out.p, n * sizeof(double4), kind, C.stream));
+  }
+  EXA_CUDA(cudaStreamSynchronize(C.stream));
+}
+
+}  // namespace exafmm_b200
+
+using namespace exafmm_b200;
+
+struct exafmm_ctx {
+  Engine E;
+};
+
+namespace {
+thread_local std::string g_create_error;
+
+template <typename F>
+int guarded(exafmm_ctx *ctx, F &&f) {
+  if (!ctx) return 2;
+  try {
+    f();
+    return 0;
+  } catch (const std::exception &e) {
+    ctx->E.C.last_error = e.what();
+    return 1;
+  }
+}
+
+template <typename F>
+int guarded_free(F &&f, std::string &err) {
+  try {
+    f();
+    return 0;
+  } catch (const std::exception &e) {
+    err = e.what();
+    return 1;
+  }
+}
+thread_local std::string g_kernel_error;
+}  // namespace
+
+extern "C" {
+
+int exafmm_create(exafmm_ctx **out, int P, double theta, int ncrit, int nspawn, int images, double cycle,
+                  int precision, int device) {
+  if (!out) return 2;
+  *out = nullptr;
+  try {
+    if (P < 2 || P > kMaxP) throw std::runtime_error("P must be in [2, 20]");
+    if (ncrit < 1 || ncrit > 1024) throw std::runtime_error("ncrit must be in [1, 1024]");
+    if (!(theta > 0)) throw std::runtime_error("theta must be positive");
+    if (images < 0) throw std::runtime_error("images must be >= 0");
+    if (precision != EXAFMM_FP64 && precision != EXAFMM_MIXED) throw std::runtime_error("unknown precision");
+    int ndev = 0;
+    EXA_CUDA(cudaGetDeviceCount(&ndev));
+    if (ndev == 0) throw std::runtime_error("no CUDA device");
+    if (device >= 0) EXA_CUDA(cudaSetDevice(device));
+    std::unique_ptr<exafmm_ctx> c(new exafmm_ctx);
+    Context &C = c->E.C;
+    EXA_CUDA(cudaGetDevice(&C.device));
+    C.prm.P = P;
+    C.prm.theta = theta;
+    C.prm.ncrit = ncrit;
+    C.prm.nspawn = nspawn;
+    C.prm.images = images;
+    C.prm.cycle = cycle;
+    C.prm.precision = precision;
+    EXA_CUDA(cudaStreamCreateWithFlags(&C.stream, cudaStreamNonBlocking));
+    C.err.ensure(1);
+    EXA_CUDA(cudaMemsetAsync(C.err.p, 0, sizeof(int), C.stream));
+    EXA_CUDA(cudaMallocHost((void **)&C.err_host, sizeof(int)));
+    device_tables(P);
+    *out = c.release();
+    return 0;
+  } catch (const std::exception &e) {
+    g_create_error = e.what();
+    return 1;
+  }
+}
+
+int exafmm_destroy(exafmm_ctx *ctx) {
+  if (!ctx) return 0;
+  cudaSetDevice(ctx->E.C.device);
+  cudaStreamSynchronize(ctx->E.C.stream);
+  if (ctx->E.C.err_host) cudaFreeHost(ctx->E.C.err_host);
+  cudaStream_t st = ctx->E.C.stream;
+  delete ctx;
+  if (st) cudaStreamDestroy(st);
+  return 0;
+}
+
+const char *exafmm_last_error(const exafmm_ctx *ctx) { return ctx ? ctx->E.C.last_error.c_str() : "null context"; }
+const char *exafmm_create_error(void) { return g_create_error.c_str(); }
+
+int exafmm_set_bodies(exafmm_ctx *ctx, const double *xyzq, long long n) {
+  return guarded(ctx, [&] {
+    cudaSetDevice(ctx->E.C.device);
+    ctx->E.set_bodies(xyzq, n, cudaMemcpyHostToDevice);
+    EXA_CUDA(cudaStreamSynchronize(ctx->E.C.stream));
+  });
+}
+
+int exafmm_set_bodies_device(exafmm_ctx *ctx, const double *d_xyzq, long long n) {
+  return guarded(ctx, [&] {
+    cudaSetDevice(ctx->E.C.device);
+    ctx->E.set_bodies(d_xyzq, n, cudaMemcpyDeviceToDevice);
+  });
+}
+
+int exafmm_get_bounds(exafmm_ctx *ctx, double *b6) {
+  return guarded(ctx, [&] {
+    cudaSetDevice(ctx->E.C.device);
+    compute_bounds(ctx->E.C);
+    EXA_CUDA(cudaMemcpyAsync(b6, ctx->E.C.tree.bounds.p, 6 * sizeof(double), cudaMemcpyDeviceToHost,
+                             ctx->E.C.stream));
+    EXA_CUDA(cudaStreamSynchronize(ctx->E.C.stream));
+  });
+}
+
+int exafmm_build_tree(exafmm_ctx *ctx, const double *bounds6) {
+  return guarded(ctx, [&] {
+    cudaSetDevice(ctx->E.C.device);
+    ctx->E.build(bounds6);
+  });
+}
+
+int exafmm_upward(exafmm_ctx *ctx) {
+  return guarded(ctx, [&] {
+    cudaSetDevice(ctx->E.C.device);
+    ctx->E.upward();
+  });
+}
+
+int exafmm_traverse(exafmm_ctx *ctx) {
+  return guarded(ctx, [&] {
+    cudaSetDevice(ctx->E.C.device);
+    ctx->E.traverse_and_evaluate();
+  });
+}
+
+int exafmm_downward(exafmm_ctx *ctx) {
+  return guarded(ctx, [&] {
+    cudaSetDevice(ctx->E.C.device);
+    ctx->E.downward();
+    ctx->E.check_err("downward");
+  });
+}
+
+int exafmm_solve(exafmm_ctx *ctx) {
+  return guarded(ctx, [&] {
+    cudaSetDevice(ctx->E.C.device);
+    ctx->E.build(nullptr);
+    ctx->E.upward();
+    ctx->E.traverse_and_evaluate();
+    ctx->E.downward();
+  });
+}
+
+int exafmm_get_results(exafmm_ctx *ctx, double *trg) {
+  return guarded(ctx, [&] {
+    cudaSetDevice(ctx->E.C.device);
+    ctx->E.results(trg, cudaMemcpyDeviceToHost);
+  });
+}
+
+int exafmm_get_results_device(exafmm_ctx *ctx, double *d_trg) {
+  return guarded(ctx, [&] {
+    cudaSetDevice(ctx->E.C.device);
+    ctx->E.results(d_trg, cudaMemcpyDeviceToDevice);
+  });
+}
+
+int exafmm_tree_info(exafmm_ctx *ctx, long long *ncells, int *depth, long long *n_m2l, long long *n_p2p) {
+  return guarded(ctx, [&] {
+    if (ncells) *ncells = ctx->E.C.tree.ncells;
+    if (depth) *depth = ctx->E.C.tree.depth;
+    if (n_m2l) *n_m2l = ctx->E.lists_ok ? ctx->E.lists.n_m2l : -1;
+    if (n_p2p) *n_p2p = ctx->E.lists_ok ? ctx->E.lists.n_p2p : -1;
+  });
+}
+
+int exafmm_get_cells(exafmm_ctx *ctx, int *ints, double *reals) {
+  return guarded(ctx, [&] {
+    Engine &E = ctx->E;
+    if (!E.tree_ok) throw std::runtime_error("no tree");
+    cudaSetDevice(E.C.device);
+    const long long nc = E.C.tree.ncells;
+    std::vector<int4> b(nc);
+    std::vector<int2> pl(nc);
+    std::vector<double4> x(nc);
+    if (nc) {
+      EXA_CUDA(cudaMemcpy(b.data(), E.C.tree.cell_b.p, nc * sizeof(int4), cudaMemcpyDeviceToHost));
+      EXA_CUDA(cudaMemcpy(pl.data(), E.C.tree.cell_pl.p, nc * sizeof(int2), cudaMemcpyDeviceToHost));
+      EXA_CUDA(cudaMemcpy(x.data(), E.C.tree.cell_x.p, nc * sizeof(double4), cudaMemcpyDeviceToHost));
+    }
+    for (long long c = 0; c < nc; c++) {
+      if (ints) {
+        ints[5 * c + 0] = pl[c].x;
+        ints[5 * c + 1] = b[c].z;
+        ints[5 * c + 2] = b[c].w;
+        ints[5 * c + 3] = b[c].x;
+        ints[5 * c + 4] = b[c].y;
+      }
+      if (reals) {
+        reals[4 * c + 0] = x[c].x;
+        reals[4 * c + 1] = x[c].y;
+        reals[4 * c + 2] = x[c].z;
+        reals[4 * c + 3] = x[c].w;
+      }
+    }
+  });
+}
+
+int exafmm_get_perm(exafmm_ctx *ctx, int *perm) {
+  return guarded(ctx, [&] {
+    Engine &E = ctx->E;
+    if (!E.tree_ok) throw std::runtime_error("no tree");
+    cudaSetDevice(E.C.device);
+    if (E.C.tree.n)
+      EXA_CUDA(cudaMemcpy(perm, E.C.tree.perm.p, E.C.tree.n * sizeof(int), cudaMemcpyDeviceToHost));
+  });
+}
+
+int exafmm_get_lists(exafmm_ctx *ctx, int *m2l, int *p2p) {
+  return guarded(ctx, [&] {
+    Engine &E = ctx->E;
+    if (!E.lists_ok) throw std::runtime_error("no lists");
+    cudaSetDevice(E.C.device);
+    const long long nc = E.C.tree.ncells;
+    auto dump = [&](const DBuf<int> &off, const DBuf<int> &src, long long n, int *outp) {
+      if (!outp || n == 0) return;
+      std::vector<int> o(nc + 1), s(n);
+      EXA_CUDA(cudaMemcpy(o.data(), off.p, (nc + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+      EXA_CUDA(cudaMemcpy(s.data(), src.p, n * sizeof(int), cudaMemcpyDeviceToHost));
+      for (long long c = 0; c < nc; c++)
+        for (int q = o[c]; q < o[c + 1]; q++) {
+          outp[3 * q + 0] = (int)c;
+          outp[3 * q + 1] = s[q] & ((1 << 26) - 1);
+          outp[3 * q + 2] = s[q] >> 26;
+        }
+    };
+    dump(E.lists.m2l_off, E.lists.m2l_src, E.lists.n_m2l, m2l);
+    dump(E.lists.p2p_off, E.lists.p2p_src, E.lists.n_p2p, p2p);
+  });
+}
+
+int exafmm_get_expansions(exafmm_ctx *ctx, double *Mh, double *Lh) {
+  return guarded(ctx, [&] {
+    Engine &E = ctx->E;
+    cudaSetDevice(E.C.device);
+    const long long cnt = E.C.tree.ncells * (long long)tri(E.C.prm.P);
+    EXA_CUDA(cudaStreamSynchronize(E.C.stream));
+    if (Mh && E.up_ok && cnt) EXA_CUDA(cudaMemcpy(Mh, E.M.p, cnt * sizeof(double2), cudaMemcpyDeviceToHost));
+    if (Lh && E.lists_ok && cnt) EXA_CUDA(cudaMemcpy(Lh, E.L.p, cnt * sizeof(double2), cudaMemcpyDeviceToHost));
+  });
+}
+
+void *exafmm_stream(exafmm_ctx *ctx) { return ctx ? (void *)ctx->E.C.stream : nullptr; }
+
+int exafmm_phase_times(exafmm_ctx *ctx, double *ms7) {
+  return guarded(ctx, [&] {
+    Engine &E = ctx->E;
+    if (!E.tm.live) throw std::runtime_error("no timed solve");
+    EXA_CUDA(cudaStreamSynchronize(E.C.stream));
+    float t;
+    for (int k = 0; k < 6; k++) {
+      EXA_CUDA(cudaEventElapsedTime(&t, E.tm.ev[k], E.tm.ev[k + 1]));
+      ms7[k] = t;
+    }
+    EXA_CUDA(cudaEventElapsedTime(&t, E.tm.ev[0], E.tm.ev[6]));
+    ms7[6] = t;
+  });
+}
+
+double exafmm_drift(double x, long long k, int up) { return up ? drift_up(x, k) : drift_down(x, k); }
+
+}  // extern "C"

@@ -1,0 +1,64 @@
+// Solve context: every device buffer one FMM solve touches, owned per caller.
+#pragma once
+#include "engine.h"
+
+namespace exafmm_b200 {
+
+enum Precision : int { kFP64 = 0, kMixed = 1 };
+
+struct Params {
+  int P = 10;
+  double theta = 0.4;
+  int ncrit = 64;
+  int nspawn = 5000;
+  int images = 0;
+  double cycle = 6.283185307179586;
+  int precision = kFP64;
+};
+
+// Level-ordered octree nodes plus the reference-layout cell table.
+struct TreeBufs {
+  long long n = 0;
+  DBuf<double4> xyzq;        // bodies, caller order
+  DBuf<double4> xyzq_tree;   // bodies, tree order
+  DBuf<unsigned long long> keys, keys_alt;
+  DBuf<int> perm, perm_alt;  // perm[tree slot] = caller index
+  DBuf<double> bounds;       // Xmin[3], Xmax[3]
+  DBuf<double> box;          // X0[3], R0
+  DBuf<unsigned long long> bounds_enc;
+  // nodes (level order)
+  long long node_cap = 0;
+  DBuf<int> nd_begin, nd_count, nd_nchild, nd_childbeg, nd_nnode, nd_cell, nd_pcell, nd_ichild;
+  DBuf<double4> nd_x;
+  DBuf<long long> lvl;       // [0, L]: node count per level; [L+1, 2L+1]: level start
+  // cells (reference layout)
+  long long cell_cap = 0;
+  DBuf<int4> cell_b;         // ibody, nbody, ichild, nchild
+  DBuf<int2> cell_pl;        // iparent, level
+  DBuf<double4> cell_x;      // X, Y, Z, R
+  DBuf<int> cell_node;       // cell -> node
+  // host mirrors (valid after sync_tree)
+  int ncells = 0;
+  int depth = 0;
+  long long lvl_host[2 * (kMaxLevels + 1)];
+};
+
+struct Context {
+  Params prm;
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  DBuf<int> err;               // device error word
+  int *err_host = nullptr;     // pinned mirror
+  TreeBufs tree;
+  ScanWork scan;
+  SortWork sort;
+  std::string last_error;
+};
+
+// Tree construction (tree.cu).
+void compute_bounds(Context &C);
+void set_bounds(Context &C, const double *bounds6_host);
+void build_tree(Context &C);
+void sync_tree(Context &C);  // reads cell count, depth and the error word
+
+}  // namespace exafmm_b200

@@ -1,0 +1,75 @@
+// Internal host-side interfaces of the engine (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <stdexcept>
+#include <string>
+
+#include "common.cuh"
+#include "scan.cuh"
+
+namespace exafmm_b200 {
+
+// Grow-only device buffer.  Contents are not preserved across growth.
+template <typename T>
+struct DBuf {
+  T *p = nullptr;
+  size_t cap = 0;
+  void ensure(size_t n) {
+    if (n <= cap) return;
+    release();
+    size_t want = n < 16 ? 16 : n;
+    EXA_CUDA(cudaMalloc((void **)&p, want * sizeof(T)));
+    cap = want;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+  T *get() const { return p; }
+  ~DBuf() { release(); }
+  DBuf() = default;
+  DBuf(const DBuf &) = delete;
+  DBuf &operator=(const DBuf &) = delete;
+};
+
+// Reusable state for scan_kernel launches on one stream.
+struct ScanWork {
+  DBuf<unsigned> ctrl;       // [0] ticket, [1] done
+  DBuf<unsigned> flags;
+  DBuf<unsigned char> aggs, incl;
+  unsigned epoch = 0;
+  bool zeroed = false;
+  ScanScratch prepare(cudaStream_t st, int *err, long long tiles, size_t elem);
+};
+
+// Launch a scan over n items (n_dev may be null, then n_host is used).
+template <int BLOCK, int ITEMS, typename Producer>
+void launch_scan(const Producer &prod, const long long *n_dev, long long n_host, long long max_items,
+                 ScanWork &w, int *err, cudaStream_t st) {
+  constexpr int TILE = BLOCK * ITEMS;
+  long long tiles = (max_items + TILE - 1) / TILE + 1;
+  ScanScratch s = w.prepare(st, err, tiles, sizeof(typename Producer::T));
+  int grid = kNumSMs * 4;
+  if (!n_dev) {
+    long long need = (n_host + TILE - 1) / TILE;
+    if (need < grid) grid = need > 0 ? (int)need : 1;
+  }
+  scan_kernel<BLOCK, ITEMS, Producer><<<grid, BLOCK, 0, st>>>(prod, n_dev, n_host, s, w.epoch);
+  EXA_CHECK_LAUNCH();
+}
+
+// Stable LSD radix sort of (key, value) pairs over bits [begin_bit, end_bit).
+// Returns true when the sorted data ended up in the *_alt buffers.
+struct SortWork {
+  DBuf<unsigned> counts;
+  ScanWork scan;
+};
+bool radix_sort_u64(uint64_t *keys, int *vals, uint64_t *keys_alt, int *vals_alt, long long n,
+                    int begin_bit, int end_bit, SortWork &w, int *err, cudaStream_t st);
+bool radix_sort_u32(uint32_t *keys, int *vals, uint32_t *keys_alt, int *vals_alt, long long n,
+                    int begin_bit, int end_bit, SortWork &w, int *err, cudaStream_t st);
+
+}  // namespace exafmm_b200

@@ -1,0 +1,514 @@
+// FP64 expansion operators: P2M, M2M, M2L, L2L, L2P, P2P (kernels/laplace.h:150-388),
+// one warp per cell, in the conventions of harmonics.cuh.
+#include "fmm.h"
+#include "harmonics.cuh"
+
+namespace exafmm_b200 {
+namespace {
+
+constexpr int kWarpsPerBlock = 4;
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 acc) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(-a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(a.y, b.x, acc.y);
+  return acc;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ void image_shift(int img, double cycle, double &sx, double &sy, double &sz) {
+  sx = (double)(img / 9 - 1) * cycle;
+  sy = (double)((img / 3) % 3 - 1) * cycle;
+  sz = (double)(img % 3 - 1) * cycle;
+}
+
+// ---------------------------------------------------------------- P2M
+// M_n^m = sum_b q_b conj(Y_n^m(x_b - X_c)) (laplace.h:237-252); lanes take
+// bodies, every coefficient is reduced across the warp.
+__global__ void k_p2m(DevTables t, const int4 *cell_b, const double4 *cell_x, const double4 *xt, double2 *M,
+                      long long ncells) {
+  extern __shared__ double2 sh[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int P = t.P, NT = t.nterm;
+  double2 *acc = sh + warp * NT;
+  for (long long c = (long long)blockIdx.x * kWarpsPerBlock + warp; c < ncells;
+       c += (long long)gridDim.x * kWarpsPerBlock) {
+    const int4 cb = cell_b[c];
+    if (cb.w != 0) continue;
+    const double4 X = cell_x[c];
+    for (int o = lane; o < NT; o += 32) acc[o] = make_double2(0.0, 0.0);
+    __syncwarp();
+    for (int base = 0; base < cb.y; base += 32) {
+      const int i = base + lane;
+      double x = 0, y = 0, z = 0, q = 0;
+      if (i < cb.y) {
+        const double4 b = xt[cb.x + i];
+        x = b.x - X.x;
+        y = b.y - X.y;
+        z = b.z - X.z;
+        q = b.w;
+      }
+      const double r2 = x * x + y * y + z * z;
+      double2 w = make_double2(q, 0.0);  // q * diagonal, with e^{-i m beta}
+      for (int m = 0; m < P; m++) {
+        if (m > 0) {
+          const double f = -t.rd[m];
+          w = make_double2(f * (w.x * x + w.y * y), f * (w.y * x - w.x * y));
+        }
+        double2 prev = make_double2(0.0, 0.0), cur = w;
+        for (int n = m; n < P; n++) {
+          const double re = warp_sum(cur.x), im = warp_sum(cur.y);
+          if (lane == 0) {
+            acc[tri(n) + m].x += re;
+            acc[tri(n) + m].y += im;
+          }
+          if (n + 1 < P) {
+            const double a = t.ra[tri(n) + m], b = t.rb[tri(n) + m];
+            double2 nxt = make_double2(a * z * cur.x - b * r2 * prev.x, a * z * cur.y - b * r2 * prev.y);
+            prev = cur;
+            cur = nxt;
+          }
+        }
+      }
+    }
+    __syncwarp();
+    for (int o = lane; o < NT; o += 32) M[c * NT + o] = acc[o];
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------- M2M
+// Parent M from each child in child order (laplace.h:254-290), d = X_parent - X_child.
+template <int MAXO>
+__global__ void k_m2m(DevTables t, const long long *lvl, int level, const int *nd_cell, const int4 *cell_b,
+                      const double4 *cell_x, double2 *M) {
+  extern __shared__ double2 sh[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int P = t.P, NT = t.nterm;
+  double2 *Y = sh + warp * 2 * NT;
+  double2 *Mc = Y + NT;
+  const long long cnt = lvl[level], start = lvl[kMaxLevels + 1 + level];
+  int oj[MAXO], ok[MAXO];
+#pragma unroll
+  for (int u = 0; u < MAXO; u++) {
+    const int o = lane + 32 * u;
+    if (o < NT) tri_decode(o, oj[u], ok[u]);
+    else oj[u] = ok[u] = -1;
+  }
+  for (long long i = (long long)blockIdx.x * kWarpsPerBlock + warp; i < cnt; i += (long long)gridDim.x * kWarpsPerBlock) {
+    const int c = nd_cell[start + i];
+    const int4 cb = cell_b[c];
+    if (cb.w == 0) continue;
+    const double4 Xp = cell_x[c];
+    double2 acc[MAXO];
+#pragma unroll
+    for (int u = 0; u < MAXO; u++) acc[u] = make_double2(0.0, 0.0);
+    for (int ch = cb.z; ch < cb.z + cb.w; ch++) {
+      const double4 Xc = cell_x[ch];
+      const double dx = Xp.x - Xc.x, dy = Xp.y - Xc.y, dz = Xp.z - Xc.z;
+      if (lane < P) regular_column(t, lane, P, dx, dy, dz, true, Y);
+      for (int o = lane; o < NT; o += 32) Mc[o] = M[(long long)ch * NT + o];
+      __syncwarp();
+#pragma unroll
+      for (int u = 0; u < MAXO; u++) {
+        const int j = oj[u], k = ok[u];
+        if (j < 0) continue;
+        double2 a = acc[u];
+        const double ajk = t.anm[tri(j) + k];
+        for (int n = 0; n <= j; n++) {
+          for (int m = -n; m <= n; m++) {
+            const int km = k - m;
+            if (km > j - n || -km > j - n) continue;
+            const double w = t.anm[tri(n) + (m < 0 ? -m : m)] * t.anm[tri(j - n) + (km < 0 ? -km : km)] / ajk;
+            const double2 Z = m >= 0 ? Y[tri(n) + m] : cconj(Y[tri(n) - m]);
+            if (m < k) {
+              const double ph = (m < 0 && (m & 1)) ? -1.0 : 1.0;
+              const double2 src = Mc[tri(j - n) + km];
+              a = cfma(src, cscale(Z, ph * sgn_pow(n) * w), a);
+            } else {
+              const double2 src = cconj(Mc[tri(j - n) - km]);
+              a = cfma(src, cscale(Z, sgn_pow(k + n + m) * w), a);
+            }
+          }
+        }
+        acc[u] = a;
+      }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int u = 0; u < MAXO; u++) {
+      const int o = lane + 32 * u;
+      if (o < NT) M[(long long)c * NT + o] = acc[u];
+    }
+  }
+}
+
+// ---------------------------------------------------------------- M2L
+// L_j^k += (-1)^j A_j^k sum_{n,m} s(k,m) (A_n^m M_n^m) (Y2_{j+n}^{m-k} / A_{j+n}^{m-k})
+// which is the reference's Cnm product (laplace.h:137-147, 292-322) with the
+// sign s = +1 (m < 0), (-1)^m (0 <= m <= k), (-1)^k (m > k).
+template <int MAXO>
+__global__ void k_m2l(DevTables t, const int *off, const int *src, long long ncells, const double4 *cell_x,
+                      const double2 *M, double2 *L, double cycle) {
+  extern __shared__ double2 sh[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int P = t.P, NT = t.nterm, NS = tri(2 * P - 1);
+  double2 *Mp = sh + warp * (NT + NS);
+  double2 *S = Mp + NT;
+  int oj[MAXO], ok[MAXO];
+#pragma unroll
+  for (int u = 0; u < MAXO; u++) {
+    const int o = lane + 32 * u;
+    if (o < NT) tri_decode(o, oj[u], ok[u]);
+    else oj[u] = ok[u] = -1;
+  }
+  for (long long c = (long long)blockIdx.x * kWarpsPerBlock + warp; c < ncells; c += (long long)gridDim.x * kWarpsPerBlock) {
+    const int b = off[c], e = off[c + 1];
+    if (b == e) continue;
+    const double4 Xi = cell_x[c];
+    double2 acc[MAXO];
+#pragma unroll
+    for (int u = 0; u < MAXO; u++) acc[u] = make_double2(0.0, 0.0);
+    for (int q = b; q < e; q++) {
+      const int packed = src[q];
+      const int cj = packed & 0x3ffffff, img = packed >> 26;
+      double sx, sy, sz;
+      image_shift(img, cycle, sx, sy, sz);
+      const double4 Xj = cell_x[cj];
+      const double dx = Xi.x - Xj.x - sx, dy = Xi.y - Xj.y - sy, dz = Xi.z - Xj.z - sz;
+      for (int o = lane; o < NT; o += 32) Mp[o] = cscale(M[(long long)cj * NT + o], t.anm[o]);
+      if (lane < 2 * P - 1) singular_column(t, lane, 2 * P - 1, dx, dy, dz, t.ainv, S);
+      __syncwarp();
+#pragma unroll
+      for (int u = 0; u < MAXO; u++) {
+        const int j = oj[u], k = ok[u];
+        if (j < 0) continue;
+        double2 a = acc[u];
+        for (int n = 0; n < P; n++) {
+          const int p = j + n;
+          for (int m = -n; m <= n; m++) {
+            const double2 Mv = m >= 0 ? Mp[tri(n) + m] : cconj(Mp[tri(n) - m]);
+            const int qq = m - k;
+            const double2 Sv = qq >= 0 ? S[tri(p) + qq] : cconj(S[tri(p) - qq]);
+            const double s = (m < 0) ? 1.0 : (m <= k ? (double)sgn_pow(m) : (double)sgn_pow(k));
+            a = cfma(cscale(Mv, s), Sv, a);
+          }
+        }
+        acc[u] = a;
+      }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int u = 0; u < MAXO; u++) {
+      const int j = oj[u], k = ok[u];
+      if (j < 0) continue;
+      const int o = tri(j) + k;
+      const double w = sgn_pow(j) * t.anm[o];
+      double2 *dst = &L[(long long)c * NT + o];
+      *dst = cadd(*dst, cscale(acc[u], w));
+    }
+  }
+}
+
+// ---------------------------------------------------------------- L2L
+// Child L from its parent (laplace.h:324-357), d = X_child - X_parent.
+template <int MAXO>
+__global__ void k_l2l(DevTables t, const long long *lvl, int level, const int *nd_cell, const int2 *cell_pl,
+                      const double4 *cell_x, double2 *L) {
+  extern __shared__ double2 sh[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int P = t.P, NT = t.nterm;
+  double2 *Y = sh + warp * 2 * NT;
+  double2 *Lp = Y + NT;
+  const long long cnt = lvl[level], start = lvl[kMaxLevels + 1 + level];
+  int oj[MAXO], ok[MAXO];
+#pragma unroll
+  for (int u = 0; u < MAXO; u++) {
+    const int o = lane + 32 * u;
+    if (o < NT) tri_decode(o, oj[u], ok[u]);
+    else oj[u] = ok[u] = -1;
+  }
+  for (long long i = (long long)blockIdx.x * kWarpsPerBlock + warp; i < cnt; i += (long long)gridDim.x * kWarpsPerBlock) {
+    const int c = nd_cell[start + i];
+    const int p = cell_pl[c].x;
+    const double4 Xc = cell_x[c], Xp = cell_x[p];
+    const double dx = Xc.x - Xp.x, dy = Xc.y - Xp.y, dz = Xc.z - Xp.z;
+    if (lane < P) regular_column(t, lane, P, dx, dy, dz, false, Y);
+    for (int o = lane; o < NT; o += 32) Lp[o] = L[(long long)p * NT + o];
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < MAXO; u++) {
+      const int j = oj[u], k = ok[u];
+      if (j < 0) continue;
+      double2 a = make_double2(0.0, 0.0);
+      const double ajk = t.anm[tri(j) + k];
+      for (int n = j; n < P; n++) {
+        for (int m = -n; m <= n; m++) {
+          const int mk = m - k;
+          if (mk > n - j || -mk > n - j) continue;
+          const double w = t.anm[tri(n - j) + (mk < 0 ? -mk : mk)] * ajk / t.anm[tri(n) + (m < 0 ? -m : m)];
+          const double2 Yv = mk >= 0 ? Y[tri(n - j) + mk] : cconj(Y[tri(n - j) - mk]);
+          if (m < 0) {
+            a = cfma(cconj(Lp[tri(n) - m]), cscale(Yv, sgn_pow(k) * w), a);
+          } else {
+            const double ph = (mk < 0 && (mk & 1)) ? -1.0 : 1.0;
+            a = cfma(Lp[tri(n) + m], cscale(Yv, ph * w), a);
+          }
+        }
+      }
+      const int o = tri(j) + k;
+      double2 *dst = &L[(long long)c * NT + o];
+      *dst = cadd(*dst, a);
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------- L2P
+// Potential and gradient of the local expansion at each body (laplace.h:359-388),
+// evaluated as the j <= 1 terms of the expansion re-centered on the body:
+//   pot = sum w_m Re(L_n^m Y_n^m),  w_0 = 1, w_m = 2
+//   dz  = sum_{m<n} w_m sqrt(n^2-m^2) Re(L_n^m Y_{n-1}^m)
+//   L11 = sum_n [ sum_{m=1..n} L_n^m Y_{n-1}^{m-1} s(n,m) - L_n^0 conj(Y_{n-1}^1) s(n,0)
+//               - sum_{u=1..n-2} conj(L_n^u) conj(Y_{n-1}^{u+1}) s(n,-u) ],  s(n,m) = sqrt((n+m)(n+m-1)/2)
+//   dx  = -sqrt(2) Re L11,  dy = sqrt(2) Im L11
+// This has no 1/sin(theta) factor, so no offset of the body from the cell center is needed.
+__global__ void k_l2p(DevTables t, const int4 *cell_b, const double4 *cell_x, const double4 *xt, const double2 *L,
+                      double4 *trg, long long ncells) {
+  extern __shared__ double2 sh[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int P = t.P, NT = t.nterm;
+  double2 *Lc = sh + warp * NT;
+  for (long long c = (long long)blockIdx.x * kWarpsPerBlock + warp; c < ncells; c += (long long)gridDim.x * kWarpsPerBlock) {
+    const int4 cb = cell_b[c];
+    if (cb.w != 0) continue;
+    const double4 X = cell_x[c];
+    for (int o = lane; o < NT; o += 32) Lc[o] = L[c * NT + o];
+    __syncwarp();
+    for (int i = lane; i < cb.y; i += 32) {
+      const double4 b = xt[cb.x + i];
+      const double x = b.x - X.x, y = b.y - X.y, z = b.z - X.z;
+      const double r2 = x * x + y * y + z * z;
+      double pot = 0, gz = 0;
+      double2 l11 = make_double2(0.0, 0.0);
+      double2 diag = make_double2(1.0, 0.0);
+      for (int m = 0; m < P; m++) {
+        if (m > 0) {
+          const double f = -t.rd[m];
+          diag = make_double2(f * (diag.x * x - diag.y * y), f * (diag.x * y + diag.y * x));
+        }
+        const double wm = (m == 0) ? 1.0 : 2.0;
+        double2 prev = make_double2(0.0, 0.0), cur = diag;
+        for (int n = m; n < P; n++) {
+          // cur = Y_n^m
+          const double2 Lnm = Lc[tri(n) + m];
+          pot += wm * (Lnm.x * cur.x - Lnm.y * cur.y);
+          if (n + 1 < P) {
+            const double2 L1 = Lc[tri(n + 1) + m];
+            gz += wm * sqrt((double)((n + 1) * (n + 1) - m * m)) * (L1.x * cur.x - L1.y * cur.y);
+            if (m + 1 <= n + 1) {
+              const double2 L2 = Lc[tri(n + 1) + m + 1];
+              l11 = cfma(L2, cscale(cur, sqrt(0.5 * (double)((n + m + 2) * (n + m + 1)))), l11);
+            }
+            if (m == 1) {
+              const double2 L0 = Lc[tri(n + 1)];
+              l11 = cfma(L0, cscale(cconj(cur), -sqrt(0.5 * (double)((n + 1) * n))), l11);
+            } else if (m >= 2) {
+              const double2 Lu = cconj(Lc[tri(n + 1) + m - 1]);
+              l11 = cfma(Lu, cscale(cconj(cur), -sqrt(0.5 * (double)((n + 2 - m) * (n + 1 - m)))), l11);
+            }
+            const double a = t.ra[tri(n) + m], bb = t.rb[tri(n) + m];
+            double2 nxt = make_double2(a * z * cur.x - bb * r2 * prev.x, a * z * cur.y - bb * r2 * prev.y);
+            prev = cur;
+            cur = nxt;
+          }
+        }
+      }
+      double4 r = trg[cb.x + i];
+      r.x += pot;
+      r.y += -1.4142135623730951 * l11.x;
+      r.z += 1.4142135623730951 * l11.y;
+      r.w += gz;
+      trg[cb.x + i] = r;
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------- P2P
+// pot += q/r, grad += q (x_j - x_i)/r^3 with r = 0 pairs skipped (laplace.h:150-235).
+template <int TPL>
+__global__ void k_p2p(const int *off, const int *src, long long ncells, const int4 *cell_b, const double4 *xt,
+                      double4 *trg, double cycle) {
+  __shared__ double4 sbuf[kWarpsPerBlock][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (long long c = (long long)blockIdx.x * kWarpsPerBlock + warp; c < ncells; c += (long long)gridDim.x * kWarpsPerBlock) {
+    const int b = off[c], e = off[c + 1];
+    if (b == e) continue;
+    const int4 ci = cell_b[c];
+    for (int tb = 0; tb < ci.y; tb += 32 * TPL) {
+      double xi[TPL], yi[TPL], zi[TPL], pot[TPL], ax[TPL], ay[TPL], az[TPL];
+#pragma unroll
+      for (int u = 0; u < TPL; u++) {
+        const int i = tb + lane + 32 * u;
+        double4 v = make_double4(0, 0, 0, 0);
+        if (i < ci.y) v = xt[ci.x + i];
+        xi[u] = v.x;
+        yi[u] = v.y;
+        zi[u] = v.z;
+        pot[u] = ax[u] = ay[u] = az[u] = 0.0;
+      }
+      for (int q = b; q < e; q++) {
+        const int packed = src[q];
+        const int cj = packed & 0x3ffffff, img = packed >> 26;
+        double sx, sy, sz;
+        image_shift(img, cycle, sx, sy, sz);
+        const int4 cjb = cell_b[cj];
+        for (int sb = 0; sb < cjb.y; sb += 32) {
+          const int ns = min(32, cjb.y - sb);
+          if (lane < ns) {
+            double4 s = xt[cjb.x + sb + lane];
+            s.x += sx;
+            s.y += sy;
+            s.z += sz;
+            sbuf[warp][lane] = s;
+          }
+          __syncwarp();
+          for (int s = 0; s < ns; s++) {
+            const double4 sj = sbuf[warp][s];
+#pragma unroll
+            for (int u = 0; u < TPL; u++) {
+              const double dx = xi[u] - sj.x, dy = yi[u] - sj.y, dz = zi[u] - sj.z;
+              const double r2 = dx * dx + dy * dy + dz * dz;
+              if (r2 != 0.0) {
+                const double inv = rsqrt(r2);
+                const double qr = sj.w * inv;
+                const double qr3 = qr * inv * inv;
+                pot[u] += qr;
+                ax[u] = fma(dx, qr3, ax[u]);
+                ay[u] = fma(dy, qr3, ay[u]);
+                az[u] = fma(dz, qr3, az[u]);
+              }
+            }
+          }
+          __syncwarp();
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < TPL; u++) {
+        const int i = tb + lane + 32 * u;
+        if (i < ci.y) {
+          double4 r = trg[ci.x + i];
+          r.x += pot[u];
+          r.y -= ax[u];
+          r.z -= ay[u];
+          r.w -= az[u];
+          trg[ci.x + i] = r;
+        }
+      }
+    }
+  }
+}
+
+int maxo_for(int P) { return (tri(P) + 31) / 32; }
+
+template <template <int> class K>
+struct Dispatch;
+
+int blocks_for(long long items) {
+  long long g = (items + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  if (g > kNumSMs * 32) g = kNumSMs * 32;
+  return g < 1 ? 1 : (int)g;
+}
+
+template <typename F>
+void set_smem(F f, size_t bytes) {
+  if (bytes > 48 * 1024) EXA_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+}  // namespace
+
+#define EXA_MAXO_SWITCH(MAXO, ...)                    \
+  switch (MAXO) {                                      \
+    case 1: { constexpr int MO = 1; __VA_ARGS__; } break;     \
+    case 2: { constexpr int MO = 2; __VA_ARGS__; } break;     \
+    case 3: { constexpr int MO = 3; __VA_ARGS__; } break;     \
+    case 4: { constexpr int MO = 4; __VA_ARGS__; } break;     \
+    case 5: { constexpr int MO = 5; __VA_ARGS__; } break;     \
+    case 6: { constexpr int MO = 6; __VA_ARGS__; } break;     \
+    case 7: { constexpr int MO = 7; __VA_ARGS__; } break;     \
+    default: throw_msg("expansion order out of range"); \
+  }
+
+void p2m_fp64(const FmmArgs &a) {
+  const DevTables &t = device_tables(a.P);
+  size_t smem = kWarpsPerBlock * t.nterm * sizeof(double2);
+  set_smem(k_p2m, smem);
+  k_p2m<<<blocks_for(a.ncells), 32 * kWarpsPerBlock, smem, a.stream>>>(t, a.cell_b, a.cell_x, a.xt, a.M64, a.ncells);
+  EXA_CHECK_LAUNCH();
+}
+
+void m2m_fp64(const FmmArgs &a, int level, long long nodes_at_level) {
+  const DevTables &t = device_tables(a.P);
+  size_t smem = kWarpsPerBlock * 2 * t.nterm * sizeof(double2);
+  EXA_MAXO_SWITCH(maxo_for(a.P), {
+    set_smem(k_m2m<MO>, smem);
+    k_m2m<MO><<<blocks_for(nodes_at_level), 32 * kWarpsPerBlock, smem, a.stream>>>(t, a.lvl, level, a.nd_cell,
+                                                                                   a.cell_b, a.cell_x, a.M64);
+  });
+  EXA_CHECK_LAUNCH();
+}
+
+void m2l_fp64(const FmmArgs &a) {
+  const DevTables &t = device_tables(a.P);
+  size_t smem = kWarpsPerBlock * (t.nterm + tri(2 * a.P - 1)) * sizeof(double2);
+  EXA_MAXO_SWITCH(maxo_for(a.P), {
+    set_smem(k_m2l<MO>, smem);
+    k_m2l<MO><<<blocks_for(a.ncells), 32 * kWarpsPerBlock, smem, a.stream>>>(t, a.m2l_off, a.m2l_src, a.ncells,
+                                                                             a.cell_x, a.M64, a.L64, a.cycle);
+  });
+  EXA_CHECK_LAUNCH();
+}
+
+void l2l_fp64(const FmmArgs &a, int level, long long nodes_at_level) {
+  const DevTables &t = device_tables(a.P);
+  size_t smem = kWarpsPerBlock * 2 * t.nterm * sizeof(double2);
+  EXA_MAXO_SWITCH(maxo_for(a.P), {
+    set_smem(k_l2l<MO>, smem);
+    k_l2l<MO><<<blocks_for(nodes_at_level), 32 * kWarpsPerBlock, smem, a.stream>>>(t, a.lvl, level, a.nd_cell,
+                                                                                   a.cell_pl, a.cell_x, a.L64);
+  });
+  EXA_CHECK_LAUNCH();
+}
+
+void l2p_fp64(const FmmArgs &a) {
+  const DevTables &t = device_tables(a.P);
+  size_t smem = kWarpsPerBlock * t.nterm * sizeof(double2);
+  set_smem(k_l2p, smem);
+  k_l2p<<<blocks_for(a.ncells), 32 * kWarpsPerBlock, smem, a.stream>>>(t, a.cell_b, a.cell_x, a.xt, a.L64,
+                                                                       a.trg64, a.ncells);
+  EXA_CHECK_LAUNCH();
+}
+
+void p2p_fp64(const FmmArgs &a) {
+  const int tpl = (a.ncrit + 31) / 32;
+  if (tpl <= 1)
+    k_p2p<1><<<blocks_for(a.ncells), 32 * kWarpsPerBlock, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b,
+                                                                          a.xt, a.trg64, a.cycle);
+  else if (tpl <= 2)
+    k_p2p<2><<<blocks_for(a.ncells), 32 * kWarpsPerBlock, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b,
+                                                                          a.xt, a.trg64, a.cycle);
+  else
+    k_p2p<4><<<blocks_for(a.ncells), 32 * kWarpsPerBlock, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b,
+                                                                          a.xt, a.trg64, a.cycle);
+  EXA_CHECK_LAUNCH();
+}
+
+}  // namespace exafmm_b200

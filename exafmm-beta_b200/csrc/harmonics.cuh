@@ -1,0 +1,99 @@
+// Spherical-harmonic expansion math of kernels/laplace.h, in a trig-free
+// Cartesian form.
+//
+// The reference evaluates, for a vector d with spherical angles (alpha, beta),
+//   regular   Y_n^m  = rho^n      P_n^m(cos alpha) pref_n^m e^{i m beta}   (evalMultipole, laplace.h:48-80)
+//   singular  Y2_n^m = rho^{-n-1} P_n^m(cos alpha) pref_n^m e^{i m beta}   (evalLocal,     laplace.h:83-113)
+// with pref_n^m = sqrt((n-|m|)!/(n+|m|)!) and the Condon-Shortley phase in P.
+// Both are computed here straight from (x, y, z) with the normalized three-term
+// recurrences (no acos/atan2/exp):
+//   Y_m^m     = Y_{m-1}^{m-1} * (-(x + i y)) * sqrt((2m-1)/(2m))
+//   Y_{n+1}^m = a_n^m z Y_n^m - b_n^m rho^2 Y_{n-1}^m
+//   a_n^m = (2n+1)/sqrt((n+1)^2-m^2),  b_n^m = sqrt((n^2-m^2)/((n+1)^2-m^2))
+// and for the singular family the same recurrence divided by rho^2 with
+// Y2_0^0 = 1/rho.  Expansions are stored for m >= 0 at index n(n+1)/2+m;
+// negative orders are conjugates.
+#pragma once
+#include "common.cuh"
+
+namespace exafmm_b200 {
+
+// Device-side tables for one expansion order P (all FP64, n < 2P).
+struct DevTables {
+  int P;
+  int nterm;            // P(P+1)/2
+  const double *anm;    // A_n^m = (-1)^n / sqrt((n-m)!(n+m)!), index n*(n+1)/2+|m|
+  const double *ainv;   // 1 / A_n^m
+  const double *ra;     // a_n^m, index n*(n+1)/2+m
+  const double *rb;     // b_n^m
+  const double *rd;     // sqrt((2m-1)/(2m)), rd[0] = 1
+};
+
+// Host construction (tables.cu).
+struct HostTables;
+const DevTables &device_tables(int P);
+
+// Column m of the regular family for n = m .. nmax-1, written to Y[tri(n)+m].
+// conj_phase selects e^{-i m beta} (P2M, M2M) instead of e^{+i m beta}.
+__device__ __forceinline__ void regular_column(const DevTables &t, int m, int nmax, double x, double y, double z,
+                                               bool conj_phase, double2 *Y) {
+  const double r2 = x * x + y * y + z * z;
+  const double yy = conj_phase ? -y : y;
+  double2 w = make_double2(1.0, 0.0);
+  for (int k = 1; k <= m; k++) {
+    const double f = -t.rd[k];
+    w = make_double2(f * (w.x * x - w.y * yy), f * (w.x * yy + w.y * x));
+  }
+  if (m >= nmax) return;
+  Y[tri(m) + m] = w;
+  double2 prev = make_double2(0.0, 0.0), cur = w;
+  for (int n = m; n + 1 < nmax; n++) {
+    const double a = t.ra[tri(n) + m], b = t.rb[tri(n) + m];
+    double2 nxt = make_double2(a * z * cur.x - b * r2 * prev.x, a * z * cur.y - b * r2 * prev.y);
+    Y[tri(n + 1) + m] = nxt;
+    prev = cur;
+    cur = nxt;
+  }
+}
+
+// Column m of the singular family for n = m .. nmax-1, each scaled by scale[tri(n)+m]
+// when scale is non-null.
+__device__ __forceinline__ void singular_column(const DevTables &t, int m, int nmax, double x, double y, double z,
+                                                const double *scale, double2 *Y) {
+  const double r2 = x * x + y * y + z * z;
+  const double inv_r2 = 1.0 / r2;
+  double2 w = make_double2(rsqrt(r2), 0.0);
+  for (int k = 1; k <= m; k++) {
+    const double f = -t.rd[k] * inv_r2;
+    w = make_double2(f * (w.x * x - w.y * y), f * (w.x * y + w.y * x));
+  }
+  if (m >= nmax) return;
+  double s = scale ? scale[tri(m) + m] : 1.0;
+  Y[tri(m) + m] = make_double2(w.x * s, w.y * s);
+  double2 prev = make_double2(0.0, 0.0), cur = w;
+  for (int n = m; n + 1 < nmax; n++) {
+    const double a = t.ra[tri(n) + m] * inv_r2, b = t.rb[tri(n) + m] * inv_r2;
+    double2 nxt = make_double2(a * z * cur.x - b * prev.x, a * z * cur.y - b * prev.y);
+    s = scale ? scale[tri(n + 1) + m] : 1.0;
+    Y[tri(n + 1) + m] = make_double2(nxt.x * s, nxt.y * s);
+    prev = cur;
+    cur = nxt;
+  }
+}
+
+// Coefficient (n, m) for either sign of m from m >= 0 storage.
+__device__ __forceinline__ double2 coef_any(const double2 *E, int n, int m) {
+  return m >= 0 ? E[tri(n) + m] : cconj(E[tri(n) - m]);
+}
+
+__device__ __forceinline__ int sgn_pow(int e) { return (e & 1) ? -1 : 1; }
+
+// (n, m) of a storage index o = n(n+1)/2 + m.
+__device__ __forceinline__ void tri_decode(int o, int &n, int &m) {
+  n = (int)((sqrt(8.0 * o + 1.0) - 1.0) * 0.5);
+  while (tri(n + 1) <= o) n++;
+  while (tri(n) > o) n--;
+  m = o - tri(n);
+}
+
+}  // namespace exafmm_b200

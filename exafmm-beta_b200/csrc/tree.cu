@@ -1,0 +1,479 @@
+// Device octree, bit-exact with BuildTree (include/build_tree.h).
+//
+// The reference builds top-down: at every node it compares each body with the
+// node's FP64 center and stably partitions the node's bodies by octant, with
+// child centers X +- R0/2^(level+1) (build_tree.h:29-108).  Here each body
+// follows its own path through that same center recurrence (identical FP64
+// adds, so identical comparisons) and records one 3-bit octant digit per level
+// in a 63-bit key.  A stable radix sort of the keys groups every node's bodies
+// contiguously in the reference's octant order; the levels are then expanded
+// breadth first by binary search on the digit of each level, and the cell
+// table is laid out exactly as nodes2cells does (build_tree.h:123-165).  Inside
+// a leaf the reference keeps input order (its partitions are stable), so a final
+// per-leaf sort restores ascending input index there.
+#include "context.h"
+#include "drift.cuh"
+
+namespace exafmm_b200 {
+namespace {
+
+__device__ __forceinline__ unsigned long long order_enc(double d) {
+  unsigned long long u = (unsigned long long)__double_as_longlong(d);
+  return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+__host__ __device__ __forceinline__ double order_dec(unsigned long long u) {
+  unsigned long long v = (u >> 63) ? (u ^ 0x8000000000000000ull) : ~u;
+#ifdef __CUDA_ARCH__
+  return __longlong_as_double((long long)v);
+#else
+  double d;
+  memcpy(&d, &v, 8);
+  return d;
+#endif
+}
+
+__global__ void k_bounds_init(unsigned long long *enc) {
+  int t = threadIdx.x;
+  if (t < 3) enc[t] = ~0ull;      // running min
+  else if (t < 6) enc[t] = 0ull;  // running max
+}
+
+// Each body contributes g^(N-1-j)(X_j) to the min and the mirrored drift to the
+// max; body 0 also carries the initial value, which is drifted N times.
+__global__ void k_bounds(const double4 *x, long long n, unsigned long long *enc) {
+  unsigned long long lo[3] = {~0ull, ~0ull, ~0ull}, hi[3] = {0, 0, 0};
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
+    const double4 b = x[j];
+    const double v[3] = {b.x, b.y, b.z};
+    const long long k = (j == 0) ? n : n - 1 - j;
+    for (int d = 0; d < 3; d++) {
+      unsigned long long a = order_enc(drift_down(v[d], k));
+      unsigned long long c = order_enc(drift_up(v[d], k));
+      lo[d] = a < lo[d] ? a : lo[d];
+      hi[d] = c > hi[d] ? c : hi[d];
+    }
+  }
+  for (int d = 0; d < 3; d++) {
+    for (int o = 16; o > 0; o >>= 1) {
+      unsigned long long a = __shfl_xor_sync(0xffffffffu, lo[d], o);
+      unsigned long long c = __shfl_xor_sync(0xffffffffu, hi[d], o);
+      lo[d] = a < lo[d] ? a : lo[d];
+      hi[d] = c > hi[d] ? c : hi[d];
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+    for (int d = 0; d < 3; d++) {
+      atomicMin(&enc[d], lo[d]);
+      atomicMax(&enc[3 + d], hi[d]);
+    }
+  }
+}
+
+__global__ void k_bounds_final(const unsigned long long *enc, long long n, double *bounds) {
+  int t = threadIdx.x;
+  if (t < 6) bounds[t] = (n > 0) ? order_dec(enc[t]) : 0.0;
+}
+
+// bounds2box (build_tree.h:168-180): center, then half-width scaled by 1.00001.
+__global__ void k_box(const double *bounds, double *box) {
+  if (threadIdx.x != 0) return;
+  double R = 0;
+  double X[3];
+  for (int d = 0; d < 3; d++) X[d] = (bounds[3 + d] + bounds[d]) / 2;
+  for (int d = 0; d < 3; d++) {
+    double a = X[d] - bounds[d];
+    R = (R < a) ? a : R;
+    double b = bounds[3 + d] - X[d];
+    R = (R < b) ? b : R;
+  }
+  box[0] = X[0];
+  box[1] = X[1];
+  box[2] = X[2];
+  box[3] = __dmul_rn(R, 1.00001);
+}
+
+__device__ __forceinline__ double level_half(double R0, int level) {
+  // R0 / (1 << (level + 1)): an exact power-of-two scaling, as in build_tree.h:97.
+  return R0 / (double)(1 << (level + 1));
+}
+
+// One octant digit per level from the reference's center recurrence.
+__global__ void k_keys(const double4 *x, long long n, const double *box, unsigned long long *keys, int *vals) {
+  const double R0 = box[3];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double4 b = x[i];
+    double cx = box[0], cy = box[1], cz = box[2];
+    unsigned long long key = 0;
+#pragma unroll 1
+    for (int l = 0; l < kMaxLevels; l++) {
+      const int ox = b.x > cx, oy = b.y > cy, oz = b.z > cz;
+      key = (key << 3) | (unsigned long long)(ox | (oy << 1) | (oz << 2));
+      const double r = level_half(R0, l);
+      cx = __dadd_rn(cx, r * (ox ? 1.0 : -1.0));
+      cy = __dadd_rn(cy, r * (oy ? 1.0 : -1.0));
+      cz = __dadd_rn(cz, r * (oz ? 1.0 : -1.0));
+    }
+    keys[i] = key;
+    vals[i] = (int)i;
+  }
+}
+
+__global__ void k_tree_root(long long n, long long *lvl, int *nd_begin, int *nd_count, double4 *nd_x,
+                            const double *box, int *nd_cell, int *nd_pcell, int *nd_ichild) {
+  if (threadIdx.x != 0) return;
+  for (int l = 0; l <= kMaxLevels; l++) {
+    lvl[l] = 0;
+    lvl[kMaxLevels + 1 + l] = 0;
+  }
+  if (n > 0) {
+    lvl[0] = 1;
+    nd_begin[0] = 0;
+    nd_count[0] = (int)n;
+    nd_x[0] = make_double4(box[0], box[1], box[2], 0.0);
+    nd_cell[0] = 0;
+    nd_pcell[0] = 0;
+    nd_ichild[0] = 1;
+  }
+}
+
+__device__ __forceinline__ int digit_at(unsigned long long key, int level) {
+  return (int)((key >> (3 * (kMaxLevels - 1 - level))) & 7ull);
+}
+
+// First index in [b, e) whose level digit is >= o (digits are sorted inside a node).
+__device__ __forceinline__ int lower_digit(const unsigned long long *keys, int b, int e, int level, int o) {
+  int lo = b, hi = e;
+  while (lo < hi) {
+    int mid = lo + ((hi - lo) >> 1);
+    if (digit_at(keys[mid], level) < o) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+struct TreeArgs {
+  const unsigned long long *keys;
+  long long *lvl;
+  int *nd_begin, *nd_count, *nd_nchild, *nd_childbeg, *nd_nnode, *nd_cell, *nd_pcell, *nd_ichild;
+  double4 *nd_x;
+  int4 *cell_b;
+  int2 *cell_pl;
+  double4 *cell_x;
+  int *cell_node;
+  const double *box;
+  long long node_cap, cell_cap;
+  int ncrit;
+  int *err;
+};
+
+// Eight threads per node: thread o finds where octant o ends.
+__global__ void k_expand(TreeArgs a, int level) {
+  const long long cnt = a.lvl[level], start = a.lvl[kMaxLevels + 1 + level];
+  const long long total = cnt * 8;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ((total + 31) / 32) * 32;
+       t += (long long)gridDim.x * blockDim.x) {
+    const bool live = t < total;
+    const long long node = start + (live ? t / 8 : 0);
+    const int o = (int)(t & 7);
+    int nonempty = 0;
+    int b = 0, c = 0;
+    if (live) {
+      b = a.nd_begin[node];
+      c = a.nd_count[node];
+    }
+    // Keys hold digits for levels 0..kMaxLevels-1, so nodes down to that level split.
+    const bool split = live && c > a.ncrit && level < kMaxLevels;
+    if (live && c > a.ncrit && level == kMaxLevels && o == 0) atomicOr(a.err, kErrTreeTooDeep);
+    if (split) {
+      int s = lower_digit(a.keys, b, b + c, level, o);
+      int e = lower_digit(a.keys, b, b + c, level, o + 1);
+      nonempty = e > s;
+    }
+    unsigned m = __ballot_sync(0xffffffffu, nonempty);
+    const int lane = threadIdx.x & 31;
+    unsigned group = (m >> (lane & ~7)) & 0xffu;
+    if (live && o == 0) a.nd_nchild[node] = __popc(group);
+  }
+}
+
+// Exclusive scan of child counts over one level; its start is only known on the device.
+struct LevelScan {
+  using T = int;
+  TreeArgs a;
+  int level;
+  const long long *startp;
+  __device__ T value(long long i) const { return a.nd_nchild[*startp + i]; }
+  __device__ void emit(long long i, const T &, const T &excl) const { a.nd_childbeg[*startp + i] = excl; }
+  __device__ void total(const T &t) const {
+    a.lvl[level + 1] = t;
+    a.lvl[kMaxLevels + 1 + level + 1] = *startp + a.lvl[level];
+  }
+};
+
+__global__ void k_scan_prep(long long *lvl, int level, long long *n_out, long long *start_out) {
+  *n_out = lvl[level];
+  *start_out = lvl[kMaxLevels + 1 + level];
+}
+
+__global__ void k_emit(TreeArgs a, int level) {
+  const long long cnt = a.lvl[level], start = a.lvl[kMaxLevels + 1 + level];
+  const long long nstart = a.lvl[kMaxLevels + 1 + level + 1];
+  const long long total = cnt * 8;
+  const double R0 = a.box[3];
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ((total + 31) / 32) * 32;
+       t += (long long)gridDim.x * blockDim.x) {
+    const bool live = t < total;
+    const long long node = start + (live ? t / 8 : 0);
+    const int o = (int)(t & 7);
+    int b = 0, c = 0, s = 0, e = 0;
+    if (live) {
+      b = a.nd_begin[node];
+      c = a.nd_count[node];
+    }
+    const bool split = live && c > a.ncrit && level < kMaxLevels;
+    if (split) {
+      s = lower_digit(a.keys, b, b + c, level, o);
+      e = lower_digit(a.keys, b, b + c, level, o + 1);
+    }
+    const int nonempty = split && e > s;
+    unsigned m = __ballot_sync(0xffffffffu, nonempty);
+    const int lane = threadIdx.x & 31;
+    unsigned group = (m >> (lane & ~7)) & 0xffu;
+    if (nonempty) {
+      const int rank = __popc(group & ((1u << o) - 1u));
+      const long long child = nstart + a.nd_childbeg[node] + rank;
+      if (child >= a.node_cap) {
+        atomicOr(a.err, kErrCellOverflow);
+      } else {
+        const double4 X = a.nd_x[node];
+        const double r = level_half(R0, level);
+        a.nd_begin[child] = s;
+        a.nd_count[child] = e - s;
+        a.nd_x[child] = make_double4(__dadd_rn(X.x, r * ((o & 1) ? 1.0 : -1.0)),
+                                     __dadd_rn(X.y, r * ((o & 2) ? 1.0 : -1.0)),
+                                     __dadd_rn(X.z, r * ((o & 4) ? 1.0 : -1.0)), 0.0);
+        a.nd_nchild[child] = 0;
+      }
+    }
+  }
+}
+
+// Subtree sizes, deepest level first.
+__global__ void k_nnode(TreeArgs a, int level) {
+  const long long cnt = a.lvl[level], start = a.lvl[kMaxLevels + 1 + level];
+  const long long nstart = (level < kMaxLevels) ? a.lvl[kMaxLevels + 1 + level + 1] : 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cnt; i += (long long)gridDim.x * blockDim.x) {
+    const long long node = start + i;
+    if (node >= a.node_cap) continue;
+    int nn = 1;
+    const int nc = a.nd_nchild[node];
+    const long long cb = nstart + a.nd_childbeg[node];
+    for (int k = 0; k < nc; k++)
+      if (cb + k < a.node_cap) nn += a.nd_nnode[cb + k];
+    a.nd_nnode[node] = nn;
+  }
+}
+
+// Reference cell layout, root first.
+__global__ void k_cells(TreeArgs a, int level) {
+  const long long cnt = a.lvl[level], start = a.lvl[kMaxLevels + 1 + level];
+  const long long nstart = (level < kMaxLevels) ? a.lvl[kMaxLevels + 1 + level + 1] : 0;
+  const double R0 = a.box[3];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cnt; i += (long long)gridDim.x * blockDim.x) {
+    const long long node = start + i;
+    if (node >= a.node_cap) continue;
+    const int c = a.nd_cell[node];
+    if (c < 0 || c >= a.cell_cap) {
+      atomicOr(a.err, kErrCellOverflow);
+      continue;
+    }
+    const int nc = a.nd_nchild[node];
+    const int ichild = a.nd_ichild[node];
+    a.cell_b[c] = make_int4(a.nd_begin[node], a.nd_count[node], nc > 0 ? ichild : 0, nc);
+    a.cell_pl[c] = make_int2(a.nd_pcell[node], level);
+    const double4 X = a.nd_x[node];
+    a.cell_x[c] = make_double4(X.x, X.y, X.z, R0 / (double)(1 << level));
+    a.cell_node[c] = (int)node;
+    const long long cb = nstart + a.nd_childbeg[node];
+    int next = ichild + nc;
+    for (int k = 0; k < nc; k++) {
+      const long long ch = cb + k;
+      if (ch >= a.node_cap) break;
+      a.nd_cell[ch] = ichild + k;
+      a.nd_pcell[ch] = c;
+      a.nd_ichild[ch] = next;
+      next += a.nd_nnode[ch] - 1;
+    }
+  }
+}
+
+// Restore input order inside each leaf: rank each body by its caller index.
+__global__ void k_leaf_order(const int *nd_count, const int *nd_begin, const int *nd_nchild, const int *nd_nnode,
+                             int *perm, int ncrit, long long node_cap) {
+  extern __shared__ int sh[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int *buf = sh + warp * ncrit;
+  const long long total = nd_nnode[0] < node_cap ? nd_nnode[0] : node_cap;
+  const int wpb = blockDim.x >> 5;
+  for (long long node = (long long)blockIdx.x * wpb + warp; node < total; node += (long long)gridDim.x * wpb) {
+    if (nd_nchild[node] != 0) continue;
+    const int b = nd_begin[node], c = nd_count[node];
+    if (c > ncrit) continue;  // only a too-deep tree leaves such a node, already flagged
+    for (int k = lane; k < c; k += 32) buf[k] = perm[b + k];
+    __syncwarp();
+    for (int k = lane; k < c; k += 32) {
+      const int v = buf[k];
+      int r = 0;
+      for (int q = 0; q < c; q++) r += buf[q] < v;
+      perm[b + r] = v;
+    }
+    __syncwarp();
+  }
+}
+
+__global__ void k_gather(const double4 *x, const int *perm, long long n, double4 *out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = x[perm[i]];
+}
+
+int grid_for(long long n, int block) {
+  long long g = (n + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > kNumSMs * 16) g = kNumSMs * 16;
+  return (int)g;
+}
+
+}  // namespace
+
+void compute_bounds(Context &C) {
+  TreeBufs &T = C.tree;
+  T.bounds.ensure(6);
+  T.bounds_enc.ensure(6);
+  k_bounds_init<<<1, 32, 0, C.stream>>>(T.bounds_enc.p);
+  if (T.n > 0) k_bounds<<<grid_for(T.n, 256), 256, 0, C.stream>>>(T.xyzq.p, T.n, T.bounds_enc.p);
+  k_bounds_final<<<1, 32, 0, C.stream>>>(T.bounds_enc.p, T.n, T.bounds.p);
+  EXA_CHECK_LAUNCH();
+}
+
+void set_bounds(Context &C, const double *b6) {
+  C.tree.bounds.ensure(6);
+  EXA_CUDA(cudaMemcpyAsync(C.tree.bounds.p, b6, 6 * sizeof(double), cudaMemcpyHostToDevice, C.stream));
+}
+
+static void ensure_nodes(TreeBufs &T, long long cap) {
+  T.node_cap = cap;
+  T.nd_begin.ensure(cap);
+  T.nd_count.ensure(cap);
+  T.nd_nchild.ensure(cap);
+  T.nd_childbeg.ensure(cap);
+  T.nd_nnode.ensure(cap);
+  T.nd_cell.ensure(cap);
+  T.nd_pcell.ensure(cap);
+  T.nd_ichild.ensure(cap);
+  T.nd_x.ensure(cap);
+  T.cell_cap = cap;
+  T.cell_b.ensure(cap);
+  T.cell_pl.ensure(cap);
+  T.cell_x.ensure(cap);
+  T.cell_node.ensure(cap);
+}
+
+void build_tree(Context &C) {
+  TreeBufs &T = C.tree;
+  const long long n = T.n;
+  const int ncrit = C.prm.ncrit;
+  cudaStream_t st = C.stream;
+  T.box.ensure(4);
+  T.lvl.ensure(2 * (kMaxLevels + 1) + 4);
+  if (T.node_cap == 0) {
+    long long est = 1024 + 8 * 4 * (n / (ncrit + 1) + 1);
+    ensure_nodes(T, est);
+  }
+  T.keys.ensure(n);
+  T.keys_alt.ensure(n);
+  T.perm.ensure(n);
+  T.perm_alt.ensure(n);
+  T.xyzq_tree.ensure(n);
+  k_box<<<1, 32, 0, st>>>(T.bounds.p, T.box.p);
+  EXA_CHECK_LAUNCH();
+  if (n > 0) {
+    k_keys<<<grid_for(n, 256), 256, 0, st>>>(T.xyzq.p, n, T.box.p, T.keys.p, T.perm.p);
+    EXA_CHECK_LAUNCH();
+    bool alt = radix_sort_u64((uint64_t *)T.keys.p, T.perm.p, (uint64_t *)T.keys_alt.p, T.perm_alt.p, n, 0,
+                              3 * kMaxLevels, C.sort, C.err.p, st);
+    if (alt) {
+      std::swap(T.keys.p, T.keys_alt.p);
+      std::swap(T.perm.p, T.perm_alt.p);
+    }
+  }
+  TreeArgs a;
+  a.keys = T.keys.p;
+  a.lvl = T.lvl.p;
+  a.nd_begin = T.nd_begin.p;
+  a.nd_count = T.nd_count.p;
+  a.nd_nchild = T.nd_nchild.p;
+  a.nd_childbeg = T.nd_childbeg.p;
+  a.nd_nnode = T.nd_nnode.p;
+  a.nd_cell = T.nd_cell.p;
+  a.nd_pcell = T.nd_pcell.p;
+  a.nd_ichild = T.nd_ichild.p;
+  a.nd_x = T.nd_x.p;
+  a.cell_b = T.cell_b.p;
+  a.cell_pl = T.cell_pl.p;
+  a.cell_x = T.cell_x.p;
+  a.cell_node = T.cell_node.p;
+  a.box = T.box.p;
+  a.node_cap = T.node_cap;
+  a.cell_cap = T.cell_cap;
+  a.ncrit = ncrit;
+  a.err = C.err.p;
+  k_tree_root<<<1, 32, 0, st>>>(n, T.lvl.p, T.nd_begin.p, T.nd_count.p, T.nd_x.p, T.box.p, T.nd_cell.p,
+                                T.nd_pcell.p, T.nd_ichild.p);
+  EXA_CHECK_LAUNCH();
+  const int node_grid = kNumSMs * 4;
+  long long *lvl_n = T.lvl.p + 2 * (kMaxLevels + 1);
+  long long *lvl_s = lvl_n + 1;
+  for (int l = 0; l <= kMaxLevels; l++) {
+    k_expand<<<node_grid, 256, 0, st>>>(a, l);
+    EXA_CHECK_LAUNCH();
+    if (l == kMaxLevels) break;  // deepest level: only the too-deep check runs
+    k_scan_prep<<<1, 1, 0, st>>>(T.lvl.p, l, lvl_n, lvl_s);
+    EXA_CHECK_LAUNCH();
+    LevelScan ls{a, l, lvl_s};
+    launch_scan<256, 4>(ls, lvl_n, 0, T.node_cap, C.scan, C.err.p, st);
+    k_emit<<<node_grid, 256, 0, st>>>(a, l);
+    EXA_CHECK_LAUNCH();
+  }
+  for (int l = kMaxLevels; l >= 0; l--) {
+    k_nnode<<<node_grid, 256, 0, st>>>(a, l);
+    EXA_CHECK_LAUNCH();
+  }
+  for (int l = 0; l <= kMaxLevels; l++) {
+    k_cells<<<node_grid, 256, 0, st>>>(a, l);
+    EXA_CHECK_LAUNCH();
+  }
+  if (n > 0) {
+    const int wpb = 4;
+    k_leaf_order<<<kNumSMs * 8, 32 * wpb, wpb * ncrit * sizeof(int), st>>>(T.nd_count.p, T.nd_begin.p,
+                                                                           T.nd_nchild.p, T.nd_nnode.p, T.perm.p,
+                                                                           ncrit, T.node_cap);
+    EXA_CHECK_LAUNCH();
+    k_gather<<<grid_for(n, 256), 256, 0, st>>>(T.xyzq.p, T.perm.p, n, T.xyzq_tree.p);
+    EXA_CHECK_LAUNCH();
+  }
+}
+
+void sync_tree(Context &C) {
+  TreeBufs &T = C.tree;
+  EXA_CUDA(cudaMemcpyAsync(T.lvl_host, T.lvl.p, sizeof(T.lvl_host), cudaMemcpyDeviceToHost, C.stream));
+  int nn = 0;
+  if (T.n > 0) EXA_CUDA(cudaMemcpyAsync(&nn, T.nd_nnode.p, sizeof(int), cudaMemcpyDeviceToHost, C.stream));
+  EXA_CUDA(cudaMemcpyAsync(C.err_host, C.err.p, sizeof(int), cudaMemcpyDeviceToHost, C.stream));
+  EXA_CUDA(cudaStreamSynchronize(C.stream));
+  T.ncells = (T.n > 0) ? nn : 0;
+  T.depth = 0;
+  for (int l = 0; l <= kMaxLevels; l++)
+    if (T.lvl_host[l] > 0) T.depth = l;
+}
+
+}  // namespace exafmm_b200

@@ -1,0 +1,125 @@
+/* exafmm_b200.h -- C ABI of the B200 Laplace FMM engine.
+ *
+ * One opaque context per caller thread owns a CUDA stream and every device
+ * buffer of a solve.  Calls on one context are ordered; a context must not be
+ * used from two threads at once (the reference's Kernel/Traversal objects are
+ * not re-entrant either).  Every entry point returns 0 on success and a
+ * non-zero status otherwise, with the text available from
+ * exafmm_last_error().  No C++ exception crosses this boundary.  There is no
+ * CPU fallback: without a usable CUDA device, exafmm_create() fails.
+ *
+ * Data conventions
+ *   bodies   xyzq[4*i + {0,1,2,3}] = x, y, z, charge, caller order
+ *   results  trg[4*i + {0,1,2,3}]  = potential, d/dx, d/dy, d/dz (the gradient
+ *            of the potential, which is what the reference stores in
+ *            Body::TRG[1..3]), caller order
+ *   bounds   {Xmin[3], Xmax[3]}
+ *   cells    ints C x 5 = IPARENT, ICHILD, NCHILD, IBODY, NBODY;
+ *            reals C x 4 = X, Y, Z, R   (reference Cell layout, cell 0 = root)
+ *   expansions interleaved (re, im), C x NTERM, NTERM = P(P+1)/2,
+ *            coefficient (n, m >= 0) at n(n+1)/2 + m
+ *
+ * Each declaration names the reference interface it stands in for
+ * (paths inside the exafmm-beta tree).
+ */
+#ifndef EXAFMM_B200_H
+#define EXAFMM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct exafmm_ctx exafmm_ctx;
+
+enum {
+  EXAFMM_FP64 = 0,  /* plain method: every operator in FP64 */
+  EXAFMM_MIXED = 1  /* P2P and M2L in FP32 with compensated accumulation; FP64 at the root levels */
+};
+
+/* Kernel(P, eps2, wavek) + Traversal(kernel, theta, nspawn, images, path)
+ * + BuildTree(ncrit) (kernels/laplace.h:116, include/traversal.h:291,
+ * include/build_tree.h:183).  cycle is the periodic box edge (examples/fmm.cxx:14).
+ * device < 0 selects the current device. */
+int exafmm_create(exafmm_ctx **ctx, int P, double theta, int ncrit, int nspawn, int images, double cycle,
+                  int precision, int device);
+int exafmm_destroy(exafmm_ctx *ctx);
+const char *exafmm_last_error(const exafmm_ctx *ctx);
+/* Error text of the last failed exafmm_create on this thread. */
+const char *exafmm_create_error(void);
+
+/* Bodies in caller order (Dataset::initBodies / Bodies, include/types.h:72-86).
+ * The _device form takes a device pointer to n x 4 doubles on the context's device. */
+int exafmm_set_bodies(exafmm_ctx *ctx, const double *xyzq, long long n);
+int exafmm_set_bodies_device(exafmm_ctx *ctx, const double *d_xyzq, long long n);
+
+/* BoundBox::getBounds(Bodies&) (include/bound_box.h:11-25), including its
+ * sequential 1e-5 drift, evaluated on the device in closed form. */
+int exafmm_get_bounds(exafmm_ctx *ctx, double *bounds6);
+
+/* BuildTree::buildTree(bodies, buffer, bounds) (include/build_tree.h:186-209).
+ * bounds6 == NULL computes them as examples/fmm.cxx:163 does. */
+int exafmm_build_tree(exafmm_ctx *ctx, const double *bounds6);
+
+/* UpDownPass::upwardPass (include/up_down_pass.h:49-60). */
+int exafmm_upward(exafmm_ctx *ctx);
+
+/* Traversal::traverse(cells, cells, cycle, dual) (include/traversal.h:326-352):
+ * builds the M2L/P2P lists and evaluates them; clears the results first, as
+ * Dataset::initTarget does before a solve. */
+int exafmm_traverse(exafmm_ctx *ctx);
+
+/* UpDownPass::downwardPass (include/up_down_pass.h:63-75). */
+int exafmm_downward(exafmm_ctx *ctx);
+
+/* Bounds + build + upward + traverse + downward, the examples/fmm.cxx:163-179 loop body. */
+int exafmm_solve(exafmm_ctx *ctx);
+
+/* Results (Body::TRG scattered back by IBODY).  The _device form writes n x 4
+ * doubles to a device pointer. */
+int exafmm_get_results(exafmm_ctx *ctx, double *trg);
+int exafmm_get_results_device(exafmm_ctx *ctx, double *d_trg);
+
+/* Tree and list inspection for parity checks. */
+int exafmm_tree_info(exafmm_ctx *ctx, long long *ncells, int *depth, long long *n_m2l, long long *n_p2p);
+int exafmm_get_cells(exafmm_ctx *ctx, int *ints, double *reals);
+/* perm[i] = caller index of the body in tree slot i (Body::IBODY after buildTree). */
+int exafmm_get_perm(exafmm_ctx *ctx, int *perm);
+/* Pairs (target cell, source cell, periodic image 0..26, 13 = unshifted), grouped by target. */
+int exafmm_get_lists(exafmm_ctx *ctx, int *m2l, int *p2p);
+int exafmm_get_expansions(exafmm_ctx *ctx, double *M, double *L);
+
+/* The CUDA stream (cudaStream_t) the context runs on. */
+void *exafmm_stream(exafmm_ctx *ctx);
+/* Wall time (ms, CUDA events) of the phases of the last solve:
+ * bounds, tree, upward, traverse (lists), m2l+p2p, downward, total. */
+int exafmm_phase_times(exafmm_ctx *ctx, double *ms7);
+
+/* Traversal::direct (include/traversal.h:355-377): FP64 direct sum of all
+ * sources onto the targets over the periodic image range of images/theta.
+ * Host arrays; trg accumulates. */
+int exafmm_direct(const double *targets, long long nt, const double *sources, long long ns, int images,
+                  double theta, double cycle, double *trg);
+
+/* Error text of the last failed exafmm_direct / exafmm_kernel_* call on this thread. */
+const char *exafmm_kernel_error(void);
+
+/* Per-operator forms (the examples/kernel.cxx known-answer chain,
+ * kernels/laplace.h:150-388).  Host arrays; outputs accumulate. */
+int exafmm_kernel_p2m(int P, const double *X, long long n, const double *xyzq, double *M);
+int exafmm_kernel_m2m(int P, const double *Xp, int nchild, const double *Xc, const double *Mc, double *Mp);
+int exafmm_kernel_m2l(int P, const double *Xi, const double *Xj, const double *Mj, double *Li,
+                      const double *Xperiodic);
+int exafmm_kernel_l2l(int P, const double *Xc, const double *Xp, const double *Lp, double *Lc);
+int exafmm_kernel_l2p(int P, const double *X, const double *L, long long n, const double *xyzq, double *trg);
+int exafmm_kernel_p2p(long long ni, const double *xi, long long nj, const double *xj, const double *Xperiodic,
+                      double *trg);
+
+/* Host-side closed form of the bounds drift: fl(x -/+ 1e-5) applied k times
+ * (up != 0 adds).  Runs on the CPU; exposed so its exactness can be checked
+ * without a GPU. */
+double exafmm_drift(double x, long long k, int up);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
