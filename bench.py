@@ -1,0 +1,312 @@
+"""FMM throughput benchmark: bodies/s of full Laplace FMM solves on one B200 per rank.
+
+Workload (the single large adaptive solve): N = 4,194,304 bodies from a Plummer
+sphere (scale 1, truncated at r = 20), equal charges 1/N, P = 8, theta = 0.35,
+ncrit = 64, nspawn = 5000.  One step = one complete solve from bodies resident
+in device memory to results in device memory: getBounds (with the reference's
+drift), tree build, upward pass, dual tree traversal with M2L and P2P, downward
+pass, results scattered back to input order.
+
+  value : N * steps / device time of the steps (CUDA events on the solver's stream)
+  e2e   : the same through the public API from pinned host buffers: the host->device
+          copy of the bodies and the device->host copy of the results are timed
+  roofline : the dominant kernel (M2L) timed live with CUDA events
+  cpu_baseline : the reference's own CPU FMM (its headers compiled in place),
+          all host threads, on a bounded sample of the same workload
+
+Multi-GPU (torchrun): replicas only -- every rank solves its own instance, no
+data-path collective; the step time is the max over ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "exafmm-beta_b200")
+
+WORKLOAD = dict(name="plummer_4m_p8", n=4_194_304, P=8, theta=0.35, ncrit=64, nspawn=5000, seed=2)
+METRIC = "FMM bodies/s (full solve, Plummer N=4,194,304, P=8, theta=0.35)"
+CPU_SAMPLE_N = 262_144
+
+
+def _package():
+    if "exafmm_b200" in sys.modules:
+        return sys.modules["exafmm_b200"]
+    spec = importlib.util.spec_from_file_location("exafmm_b200", os.path.join(PKG_DIR, "__init__.py"),
+                                                  submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["exafmm_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), float(p["bf16_tflops"]), "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms while running."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9 and parts[1].isdigit():
+                    rows.append(parts)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [int(r[1]) for r in rows]
+        smax = int(rows[0][2])
+        power = [float(r[3]) if r[3].replace(".", "", 1).isdigit() else 0.0 for r in rows]
+        loaded = [s for s, p in zip(sm, power) if p > 0.35 * max(power)] or sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": int(statistics.median(loaded)), "sm_max_mhz": smax, "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(power)}
+
+
+def cpu_reference_baseline(n_sample: int, threads: int, steps: int = 1):
+    """The reference CPU FMM (oracle/_ref) or, if it was not built, the C restatement,
+    on a smaller Plummer system with the workload's parameters."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import bindings
+    pkg = _package()
+    from exafmm_b200 import datasets
+    x = datasets.plummer(n_sample, seed=WORKLOAD["seed"])
+    kw = dict(P=WORKLOAD["P"], theta=WORKLOAD["theta"], ncrit=WORKLOAD["ncrit"], nspawn=WORKLOAD["nspawn"])
+    if bindings.reference_available():
+        impl, kind = bindings.Reference(), "reference"
+        run = lambda: impl.solve(x, threads=threads, record_lists=False, **kw)
+    else:
+        impl, kind = bindings.Oracle(), "port"
+        run = lambda: impl.solve(x, **kw)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        run()
+        times.append(time.perf_counter() - t0)
+    return kind, times, x
+
+
+def run_reference_arm(args, rank: int):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    kind, _, _ = cpu_reference_baseline(8192, threads, steps=max(1, args.warmup))
+    kind, times, x = cpu_reference_baseline(CPU_SAMPLE_N, threads, steps=args.steps)
+    total = sum(times)
+    value = CPU_SAMPLE_N * len(times) / total
+    sample = (f"Plummer N={CPU_SAMPLE_N} (same generator and P/theta/ncrit/nspawn as the {WORKLOAD['n']}-body "
+              f"workload; each step one full CPU solve)")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "bodies/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD["name"], "n_bodies": WORKLOAD["n"], "P": WORKLOAD["P"],
+                   "theta": WORKLOAD["theta"], "ncrit": WORKLOAD["ncrit"], "sample_n": CPU_SAMPLE_N},
+        "cpu_baseline": {"value": value, "unit": "bodies/s", "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": "bodies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--n", type=int, default=WORKLOAD["n"], help=argparse.SUPPRESS)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    pkg = _package()
+    pkg.build()
+    from exafmm_b200 import datasets
+
+    n = args.n
+    wl = dict(WORKLOAD)
+    x = datasets.plummer(n, seed=wl["seed"] + rank)
+    prec = pkg.FP64 if args.precision == "fp64" else pkg.MIXED
+    fmm = pkg.Fmm(P=wl["P"], theta=wl["theta"], ncrit=wl["ncrit"], nspawn=wl["nspawn"], precision=prec,
+                  device=local_rank)
+    stream = torch.cuda.ExternalStream(fmm.stream())
+    dx = torch.from_numpy(x).cuda()
+    dout = torch.empty_like(dx)
+    hx = torch.from_numpy(x).pin_memory()
+    hout = torch.empty_like(hx).pin_memory()
+
+    def solve_device():
+        fmm.set_bodies_device(dx.data_ptr(), n)
+        fmm.solve()
+        fmm.results_device(dout.data_ptr())
+
+    for _ in range(args.warmup):
+        solve_device()
+    torch.cuda.synchronize()
+    info = fmm.info()
+
+    # ---- value: device-resident steps ----
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    phase_acc = {k: 0.0 for k in pkg.Fmm.PHASES}
+    launches0 = pkg.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            solve_device()
+            for k, v in fmm.phase_times().items():
+                phase_acc[k] += v
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    launches = pkg.launch_count() - launches0
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.summary()
+    t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    ms_max = float(t.item())
+    value = n * world * args.steps / (ms_max / 1e3)
+
+    # ---- e2e: public API from pinned host memory ----
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    hx_np, hout_np = hx.numpy(), hout.numpy()
+    e0.record(stream)
+    for _ in range(args.steps):
+        fmm.set_bodies(hx_np)
+        fmm.solve()
+        fmm.results(out=hout_np)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    te = torch.tensor([e0.elapsed_time(e1)], device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = n * world * args.steps / (float(te.item()) / 1e3)
+
+    # ---- roofline of the dominant kernel (M2L), from the timed steps ----
+    hbm_peak, bf16_peak, peak_kind = _peaks()
+    P = wl["P"]
+    nterm = P * (P + 1) // 2
+    m2l_ms = phase_acc["m2l"] / args.steps
+    n_m2l = info["n_m2l"]
+    cplx = 16 if prec == pkg.FP64 else 8
+    alg_bytes = n_m2l * (nterm * cplx + 8) + info["ncells"] * 2 * nterm * cplx
+    alg_flops = n_m2l * 8 * nterm * P * P
+    achieved = alg_bytes / (m2l_ms / 1e3) / 1e9
+    roofline = {
+        "kernel": "m2l", "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+        "frac": achieved / hbm_peak, "traffic": None, "peak_kind": peak_kind,
+        "ms_per_launch": m2l_ms, "algorithmic_bytes": alg_bytes, "algorithmic_flops": alg_flops,
+        "achieved_tflops": alg_flops / (m2l_ms / 1e3) / 1e12,
+        "note": "FP64 M2L on CUDA cores is compute-bound (~50 flop/B); the HBM fraction shows how far it is "
+                "from the memory roof, achieved_tflops the FP64 rate",
+    }
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "bodies/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if prec == pkg.FP64 else "f32+kahan", "data": "synthetic",
+        "config": {"workload": wl["name"], "n_bodies": n, "distribution": "plummer(scale=1, rmax=20), q=1/N",
+                   "P": P, "theta": wl["theta"], "ncrit": wl["ncrit"], "nspawn": wl["nspawn"],
+                   "precision": args.precision, "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (134 MB of bodies per solve)",
+                   "cells": info["ncells"], "depth": info["depth"], "m2l_pairs": n_m2l, "p2p_pairs": info["n_p2p"]},
+        "phases_ms": {k: v / args.steps for k, v in phase_acc.items()},
+        "roofline": roofline,
+        "e2e": {"value": e2e_value, "unit": "bodies/s", "h2d_bytes_per_step": int(n * 32),
+                "d2h_bytes_per_step": int(n * 32)},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        kind, times, _ = cpu_reference_baseline(CPU_SAMPLE_N, threads, steps=1)
+        cpu_v = CPU_SAMPLE_N / times[0]
+        line["cpu_baseline"] = {"value": cpu_v, "unit": "bodies/s", "cores": threads, "kind": kind,
+                                "sample": f"one solve of a Plummer N={CPU_SAMPLE_N} system with the same "
+                                          f"P/theta/ncrit/nspawn ({times[0]:.1f} s)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    fmm.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

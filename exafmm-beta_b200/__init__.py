@@ -31,9 +31,12 @@ _lib = None
 
 
 def build(force: bool = False) -> str:
-    """Compile libexafmm_b200.so for sm_100a (nvcc cross-compiles without a GPU)."""
-    if force or not os.path.exists(LIB_PATH):
-        subprocess.run(["make", "-s", "-j8", "-C", os.path.join(HERE, "csrc")], check=True)
+    """Compile libexafmm_b200.so for sm_100a (nvcc cross-compiles without a GPU).
+    make is incremental, so this is cheap when the library is current."""
+    args = ["make", "-s", "-j8", "-C", os.path.join(HERE, "csrc")]
+    if force:
+        subprocess.run(args + ["clean"], check=True)
+    subprocess.run(args, check=True)
     return LIB_PATH
 
 
@@ -84,6 +87,7 @@ def lib() -> ctypes.CDLL:
         "exafmm_kernel_l2p": (_c_int, [_c_int, _vp, _vp, _c_ll, _vp, _vp]),
         "exafmm_kernel_p2p": (_c_int, [_c_ll, _vp, _c_ll, _vp, _vp, _vp]),
         "exafmm_drift": (_c_double, [_c_double, _c_ll, _c_int]),
+        "exafmm_launch_count": (_c_ll, []),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -174,8 +178,12 @@ class Fmm:
     def solve(self):
         self._check(lib().exafmm_solve(self._h))
 
-    def results(self) -> np.ndarray:
-        out = np.zeros((self.n, 4))
+    def results(self, out: np.ndarray | None = None) -> np.ndarray:
+        """(n, 4) potential and gradient in input order; out may be a preallocated
+        (e.g. pinned) float64 array."""
+        if out is None:
+            out = np.zeros((self.n, 4))
+        assert out.dtype == np.float64 and out.shape == (self.n, 4) and out.flags.c_contiguous
         self._check(lib().exafmm_get_results(self._h, _p(out)))
         return out
 
@@ -219,10 +227,13 @@ class Fmm:
     def stream(self) -> int:
         return lib().exafmm_stream(self._h) or 0
 
+    PHASES = ("bounds", "tree", "upward", "lists", "m2l", "p2p", "downward", "total")
+
     def phase_times(self) -> dict:
-        t = np.zeros(7)
+        """Device milliseconds of each phase of the last solve (CUDA events on its stream)."""
+        t = np.zeros(8)
         self._check(lib().exafmm_phase_times(self._h, _p(t)))
-        return dict(zip(["bounds", "tree", "upward", "lists", "m2l_p2p", "downward", "total"], t.tolist()))
+        return dict(zip(self.PHASES, t.tolist()))
 
 
 # ---- free functions: direct sum and per-operator forms ----
@@ -283,3 +294,8 @@ def p2p(xi, xj, Xper=None, trg=None):
 
 def drift(x: float, k: int, up: bool = False) -> float:
     return lib().exafmm_drift(float(x), int(k), int(up))
+
+
+def launch_count() -> int:
+    """Kernels the engine has launched in this process."""
+    return int(lib().exafmm_launch_count())

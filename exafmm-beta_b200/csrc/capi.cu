@@ -1,4 +1,5 @@
 // extern "C" surface of the engine (include/exafmm_b200.h) and the solve driver.
+#include <atomic>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -20,6 +21,10 @@ void throw_cuda(cudaError_t e, const char *what, const char *file, int line) {
   throw CudaError(m);
 }
 void throw_msg(const char *msg) { throw std::runtime_error(msg); }
+
+static std::atomic<long long> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 void direct_fp64(const double4 *tgt, long long nt, const double4 *src, long long ns, int prange, double cycle,
                  double4 *trg, cudaStream_t st);
@@ -165,11 +170,13 @@ struct Engine {
       EXA_CUDA(cudaMemsetAsync(L.p, 0, nc * NT * sizeof(double2), C.stream));
       FmmArgs a = args();
       m2l_fp64(a);
+      EXA_CUDA(cudaEventRecord(tm.ev[5], C.stream));
       p2p_fp64(a);
     } else {
       EXA_CUDA(cudaEventRecord(tm.ev[4], C.stream));
+      EXA_CUDA(cudaEventRecord(tm.ev[5], C.stream));
     }
-    EXA_CUDA(cudaEventRecord(tm.ev[5], C.stream));
+    EXA_CUDA(cudaEventRecord(tm.ev[6], C.stream));
     lists_ok = true;
   }
 
@@ -181,7 +188,7 @@ struct Engine {
       for (int l = 1; l <= C.tree.depth; l++) l2l_fp64(a, l, C.tree.lvl_host[l]);
       l2p_fp64(a);
     }
-    EXA_CUDA(cudaEventRecord(tm.ev[6], C.stream));
+    EXA_CUDA(cudaEventRecord(tm.ev[7], C.stream));
   }
 
   void results(double *dst, cudaMemcpyKind kind);
@@ -460,20 +467,22 @@ int exafmm_get_expansions(exafmm_ctx *ctx, double *Mh, double *Lh) {
 
 void *exafmm_stream(exafmm_ctx *ctx) { return ctx ? (void *)ctx->E.C.stream : nullptr; }
 
-int exafmm_phase_times(exafmm_ctx *ctx, double *ms7) {
+int exafmm_phase_times(exafmm_ctx *ctx, double *ms8) {
   return guarded(ctx, [&] {
     Engine &E = ctx->E;
     if (!E.tm.live) throw std::runtime_error("no timed solve");
     EXA_CUDA(cudaStreamSynchronize(E.C.stream));
     float t;
-    for (int k = 0; k < 6; k++) {
+    for (int k = 0; k < 7; k++) {
       EXA_CUDA(cudaEventElapsedTime(&t, E.tm.ev[k], E.tm.ev[k + 1]));
-      ms7[k] = t;
+      ms8[k] = t;
     }
-    EXA_CUDA(cudaEventElapsedTime(&t, E.tm.ev[0], E.tm.ev[6]));
-    ms7[6] = t;
+    EXA_CUDA(cudaEventElapsedTime(&t, E.tm.ev[0], E.tm.ev[7]));
+    ms8[7] = t;
   });
 }
+
+long long exafmm_launch_count(void) { return launch_count(); }
 
 double exafmm_drift(double x, long long k, int up) { return up ? drift_up(x, k) : drift_down(x, k); }
 

@@ -29,7 +29,16 @@ void throw_msg(const char *msg);
     if (_e != cudaSuccess) ::exafmm_b200::throw_cuda(_e, #call, __FILE__, __LINE__); \
   } while (0)
 
-#define EXA_CHECK_LAUNCH() EXA_CUDA(cudaGetLastError())
+// Process-wide count of kernel launches issued by this library.
+void note_launch();
+long long launch_count();
+
+// Follows every kernel launch (exactly one per launch, so the count is exact).
+#define EXA_CHECK_LAUNCH()                \
+  do {                                    \
+    ::exafmm_b200::note_launch();         \
+    EXA_CUDA(cudaGetLastError());         \
+  } while (0)
 
 // ---- complex arithmetic on double2 / float2 (x = re, y = im) ----
 template <typename T> struct cplx_t;

@@ -166,10 +166,10 @@ void group_by_target(Context &C, const int2 *pairs, long long n, long long ncell
     int *v = alt ? lb.val_alt.p : lb.val.p;
     EXA_CUDA(cudaMemcpyAsync(src.p, v, n * sizeof(int), cudaMemcpyDeviceToDevice, st));
     k_csr<<<kNumSMs * 2, 256, 0, st>>>(k, n, ncells, off.p);
+    EXA_CHECK_LAUNCH();
   } else {
     EXA_CUDA(cudaMemsetAsync(off.p, 0, (ncells + 1) * sizeof(int), st));
   }
-  EXA_CHECK_LAUNCH();
 }
 
 }  // namespace

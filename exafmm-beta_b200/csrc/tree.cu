@@ -350,7 +350,11 @@ void compute_bounds(Context &C) {
   T.bounds.ensure(6);
   T.bounds_enc.ensure(6);
   k_bounds_init<<<1, 32, 0, C.stream>>>(T.bounds_enc.p);
-  if (T.n > 0) k_bounds<<<grid_for(T.n, 256), 256, 0, C.stream>>>(T.xyzq.p, T.n, T.bounds_enc.p);
+  EXA_CHECK_LAUNCH();
+  if (T.n > 0) {
+    k_bounds<<<grid_for(T.n, 256), 256, 0, C.stream>>>(T.xyzq.p, T.n, T.bounds_enc.p);
+    EXA_CHECK_LAUNCH();
+  }
   k_bounds_final<<<1, 32, 0, C.stream>>>(T.bounds_enc.p, T.n, T.bounds.p);
   EXA_CHECK_LAUNCH();
 }

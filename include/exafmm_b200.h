@@ -90,9 +90,11 @@ int exafmm_get_expansions(exafmm_ctx *ctx, double *M, double *L);
 
 /* The CUDA stream (cudaStream_t) the context runs on. */
 void *exafmm_stream(exafmm_ctx *ctx);
-/* Wall time (ms, CUDA events) of the phases of the last solve:
- * bounds, tree, upward, traverse (lists), m2l+p2p, downward, total. */
-int exafmm_phase_times(exafmm_ctx *ctx, double *ms7);
+/* Device time (ms, CUDA events on the context's stream) of the phases of the
+ * last solve: bounds, tree, upward, lists, m2l, p2p, downward, total. */
+int exafmm_phase_times(exafmm_ctx *ctx, double *ms8);
+/* Kernels this library has launched in this process (all contexts). */
+long long exafmm_launch_count(void);
 
 /* Traversal::direct (include/traversal.h:355-377): FP64 direct sum of all
  * sources onto the targets over the periodic image range of images/theta.

@@ -164,8 +164,7 @@ class Oracle(_Lib):
     prefix = "oracle_"
 
     def __init__(self, path: str = ORACLE_SO):
-        if not os.path.exists(path):
-            build(reference=False)
+        build(reference=False)  # incremental; keeps the .so in step with exafmm_oracle.c
         super().__init__(path)
 
     def _sig(self):
@@ -175,9 +174,13 @@ class Oracle(_Lib):
         self._f("build_tree", _vp, [_c_int, _vp, _c_int, _vp])
         self._f("get_cells", None, [_vp, _vp, _vp])
         self._f("depth", _c_int, [_vp])
+        self._f("drift_seq", _c_double, [_c_double, ctypes.c_longlong, _c_int])
 
     def _get_cells(self, h, ci, cr):
         self.lib.oracle_get_cells(h, _ptr(ci), _ptr(cr))
+
+    def drift_seq(self, x: float, k: int, up: bool = False) -> float:
+        return self.lib.oracle_drift_seq(float(x), int(k), int(up))
 
     def bounds(self, xyzq) -> np.ndarray:
         xyzq = _as_xyzq(xyzq)

@@ -331,6 +331,14 @@ void oracle_bounds(int n, const double *xyzq, double *b) {
   }
 }
 
+/* One coordinate of that recurrence with no body ever below the running value:
+ * x -/+ 1e-5 applied k times, one rounded step at a time. */
+double oracle_drift_seq(double x, long long k, int up) {
+  volatile double v = x;
+  for (long long i = 0; i < k; i++) v = up ? v + 1e-5 : v - 1e-5;
+  return v;
+}
+
 /* ------------------------------------------------------------------------ */
 /* Tree (include/build_tree.h).                                              */
 /* ------------------------------------------------------------------------ */

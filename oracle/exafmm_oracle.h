@@ -28,6 +28,8 @@ typedef struct oracle_run oracle_run;
 
 /* BoundBox::getBounds with its sequential drift (include/bound_box.h:11-25). */
 void oracle_bounds(int n, const double *xyzq, double *bounds6);
+/* One coordinate of the same recurrence: x -/+ 1e-5 applied k times, stepwise. */
+double oracle_drift_seq(double x, long long k, int up);
 
 /* Full solve (examples/fmm.cxx:163-179).  bounds6 may be NULL. */
 oracle_run *oracle_solve(int n, const double *xyzq, int P, double theta, int ncrit,
