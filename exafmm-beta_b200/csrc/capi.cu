@@ -51,6 +51,8 @@ struct Engine {
   Context C;
   ListBufs lists;
   DBuf<double2> M, L;
+  DBuf<unsigned char> Ms;  // scaled multipoles for the unrolled M2L (FP32 or FP64)
+  DBuf<float4> x32;        // bodies relative to their leaf center (mixed P2P)
   DBuf<double4> trg, out;
   Timing tm;
   bool tree_ok = false, up_ok = false, lists_ok = false;
@@ -169,9 +171,23 @@ struct Engine {
       EXA_CUDA(cudaEventRecord(tm.ev[4], C.stream));
       EXA_CUDA(cudaMemsetAsync(L.p, 0, nc * NT * sizeof(double2), C.stream));
       FmmArgs a = args();
-      m2l_fp64(a);
+      const bool mixed = C.prm.precision == kMixed;
+      if (m2l_fast_supported(C.prm.P, mixed)) {
+        Ms.ensure(nc * NT * (mixed ? sizeof(float2) : sizeof(double2)));
+        scale_multipoles(a, mixed, Ms.p);
+        m2l_fast(a, mixed, Ms.p);
+        if (mixed) m2l_fp64(a, kMixedMinLevel, kMixedMaxDl);  // root levels, large size ratios
+      } else {
+        m2l_fp64(a);
+      }
       EXA_CUDA(cudaEventRecord(tm.ev[5], C.stream));
-      p2p_fp64(a);
+      if (mixed) {
+        x32.ensure(C.tree.n);
+        rel_bodies32(a, x32.p);
+        p2p_mixed(a, x32.p);
+      } else {
+        p2p_fp64(a);
+      }
     } else {
       EXA_CUDA(cudaEventRecord(tm.ev[4], C.stream));
       EXA_CUDA(cudaEventRecord(tm.ev[5], C.stream));

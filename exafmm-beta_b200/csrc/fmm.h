@@ -24,10 +24,28 @@ struct FmmArgs {
 
 void p2m_fp64(const FmmArgs &a);
 void m2m_fp64(const FmmArgs &a, int level, long long nodes_at_level);
-void m2l_fp64(const FmmArgs &a);
+// Generic FP64 M2L.  With skip_min_level >= 0 it leaves out the pairs the
+// mixed-precision kernel takes (target level >= skip_min_level and
+// |level difference| <= skip_max_dl).
+void m2l_fp64(const FmmArgs &a, int skip_min_level = -1, int skip_max_dl = 0);
 void l2l_fp64(const FmmArgs &a, int level, long long nodes_at_level);
 void l2p_fp64(const FmmArgs &a);
 void p2p_fp64(const FmmArgs &a);
+
+// Mixed form: FP32 M2L for targets at level >= kMixedMinLevel and source/target
+// level differences of at most kMixedMaxDl; everything else in FP64.
+constexpr int kMixedMinLevel = 3;
+constexpr int kMixedMaxDl = 3;
+
+// Register-resident unrolled M2L (m2l.cu) for the orders it is built for.
+bool m2l_fast_supported(int P, bool mixed);
+// Ms = A_n^m M_n^m / R^n per cell, FP32 (mixed) or FP64.
+void scale_multipoles(const FmmArgs &a, bool mixed, void *Ms);
+bool m2l_fast(const FmmArgs &a, bool mixed, const void *Ms);
+
+// Mixed-precision P2P (p2p32.cu): bodies relative to their leaf center in FP32.
+void rel_bodies32(const FmmArgs &a, float4 *x32);
+void p2p_mixed(const FmmArgs &a, const float4 *x32);
 
 // Interaction lists of the dual tree traversal (traverse.cu).
 struct ListBufs {

@@ -156,7 +156,8 @@ __global__ void k_m2m(DevTables t, const long long *lvl, int level, const int *n
 // sign s = +1 (m < 0), (-1)^m (0 <= m <= k), (-1)^k (m > k).
 template <int MAXO>
 __global__ void k_m2l(DevTables t, const int *off, const int *src, long long ncells, const double4 *cell_x,
-                      const double2 *M, double2 *L, double cycle) {
+                      const double2 *M, double2 *L, double cycle, const int2 *cell_pl, int skip_min_level,
+                      int skip_max_dl) {
   extern __shared__ double2 sh[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int P = t.P, NT = t.nterm, NS = tri(2 * P - 1);
@@ -176,9 +177,15 @@ __global__ void k_m2l(DevTables t, const int *off, const int *src, long long nce
     double2 acc[MAXO];
 #pragma unroll
     for (int u = 0; u < MAXO; u++) acc[u] = make_double2(0.0, 0.0);
+    const int lt = cell_pl ? cell_pl[c].y : 0;
     for (int q = b; q < e; q++) {
       const int packed = src[q];
       const int cj = packed & 0x3ffffff, img = packed >> 26;
+      if (cell_pl) {
+        // pairs the mixed-precision kernel takes are skipped here
+        const int dl = lt - cell_pl[cj].y;
+        if (lt >= skip_min_level && dl <= skip_max_dl && dl >= -skip_max_dl) continue;
+      }
       double sx, sy, sz;
       image_shift(img, cycle, sx, sy, sz);
       const double4 Xj = cell_x[cj];
@@ -466,13 +473,14 @@ void m2m_fp64(const FmmArgs &a, int level, long long nodes_at_level) {
   EXA_CHECK_LAUNCH();
 }
 
-void m2l_fp64(const FmmArgs &a) {
+void m2l_fp64(const FmmArgs &a, int skip_min_level, int skip_max_dl) {
   const DevTables &t = device_tables(a.P);
   size_t smem = kWarpsPerBlock * (t.nterm + tri(2 * a.P - 1)) * sizeof(double2);
+  const int2 *pl = skip_min_level >= 0 ? a.cell_pl : nullptr;
   EXA_MAXO_SWITCH(maxo_for(a.P), {
     set_smem(k_m2l<MO>, smem);
-    k_m2l<MO><<<blocks_for(a.ncells), 32 * kWarpsPerBlock, smem, a.stream>>>(t, a.m2l_off, a.m2l_src, a.ncells,
-                                                                             a.cell_x, a.M64, a.L64, a.cycle);
+    k_m2l<MO><<<blocks_for(a.ncells), 32 * kWarpsPerBlock, smem, a.stream>>>(
+        t, a.m2l_off, a.m2l_src, a.ncells, a.cell_x, a.M64, a.L64, a.cycle, pl, skip_min_level, skip_max_dl);
   });
   EXA_CHECK_LAUNCH();
 }

@@ -1,0 +1,49 @@
+"""The mixed-precision form: FP32 M2L and P2P with compensated / FP64 accumulation,
+FP64 at the root levels.  Three errors are reported for every case:
+mixed vs FP64 direct, plain FP64 FMM vs FP64 direct (the truncation floor of
+the method at this P and theta) and mixed vs plain (the precision-only part,
+held to 1e-6)."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+PRECISION_TOL = 1e-6
+
+
+def _run(ex, x, precision, **kw):
+    f = ex.Fmm(precision=precision, **kw)
+    f.set_bodies(x)
+    f.solve()
+    out = f.results()
+    info = f.info()
+    f.close()
+    return out, info
+
+
+@pytest.mark.parametrize("dist,n,P,theta,ncrit", [
+    ("cube", 100000, 10, 0.4, 64),
+    ("plummer", 200000, 8, 0.35, 64),
+    ("sphere", 50000, 10, 0.4, 64),
+    ("plummer", 50000, 6, 0.4, 32),
+    ("cube", 30000, 4, 0.5, 32),
+])
+def test_mixed_precision_error_split(ex, datasets, dist, n, P, theta, ncrit):
+    x = getattr(datasets, dist)(n, seed=31)
+    plain, info64 = _run(ex, x, ex.FP64, P=P, theta=theta, ncrit=ncrit)
+    mixed, info32 = _run(ex, x, ex.MIXED, P=P, theta=theta, ncrit=ncrit)
+    assert info64 == info32  # same tree, same lists
+    idx = datasets.strided_sample(n, 512)
+    direct = ex.direct(x[idx], x)
+    e_mixed_direct = rel_l2(mixed[idx, 0], direct[:, 0])
+    e_plain_direct = rel_l2(plain[idx, 0], direct[:, 0])
+    e_precision = rel_l2(mixed[:, 0], plain[:, 0])
+    e_precision_acc = rel_l2(mixed[:, 1:], plain[:, 1:])
+    print(f"{dist} n={n} P={P}: mixed-direct {e_mixed_direct:.2e} plain-direct {e_plain_direct:.2e} "
+          f"mixed-plain pot {e_precision:.2e} acc {e_precision_acc:.2e}")
+    assert e_precision < PRECISION_TOL
+    assert e_precision_acc < 10 * PRECISION_TOL
+    # the mixed result is as close to the direct sum as the plain method, up to the precision part
+    assert e_mixed_direct < e_plain_direct + 2 * PRECISION_TOL
