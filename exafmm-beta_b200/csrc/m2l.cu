@@ -6,6 +6,7 @@
 // of the per-lane partial expansions; the root levels and the rare pairs of
 // very different sizes stay in FP64 (generic kernel in fmm64.cu).
 #include <mutex>
+#include <type_traits>
 
 #include "fmm.h"
 #include "harmonics.cuh"
@@ -120,26 +121,41 @@ k_m2l_part(M2LCtx g, DevTables t, double2 *L) {
   for (long long c = (long long)blockIdx.x * kM2LWarps + warp; c < g.ncells; c += (long long)gridDim.x * kM2LWarps) {
     const int b = g.off[c], e = g.off[c + 1];
     if (b == e) continue;
-    Cx<T> acc[NA];
+    constexpr bool kPacked = std::is_same<T, float>::value;  // FP32 runs on packed f32x2 pairs
+    using Acc = typename std::conditional<kPacked, f2p, Cx<T>>::type;
+    Acc acc[NA];
 #pragma unroll
-    for (int i = 0; i < NA; i++) acc[i] = Cx<T>{T(0), T(0)};
+    for (int i = 0; i < NA; i++) acc[i] = Acc{};
     const double4 Xt = g.cell_x[c];
     const int lt = g.cell_pl[c].y;
     const double inv_rt = 1.0 / Xt.w;
-    for (int q = b + lane; q < e; q += 32) {
-      const int packed = g.src[q];
-      const int cj = packed & 0x3ffffff, img = packed >> 26;
-      const int ls = g.cell_pl[cj].y;
-      if (g.mode == 1 && !mixed_regular(lt, ls)) continue;
-      const double4 Xs = g.cell_x[cj];
-      const double sx = (double)(img / 9 - 1) * g.cycle, sy = (double)((img / 3) % 3 - 1) * g.cycle,
-                   sz = (double)(img % 3 - 1) * g.cycle;
-      const T x = (T)((Xt.x - Xs.x - sx) * inv_rt), y = (T)((Xt.y - Xs.y - sy) * inv_rt),
-              z = (T)((Xt.z - Xs.z - sz) * inv_rt);
+    // Warp-uniform trip count: the pair code holds warp barriers, so every lane
+    // runs every iteration; a lane without a (kept) pair runs a dummy one with
+    // zero multipoles at a unit offset, which adds nothing.
+    for (int base = b; base < e; base += 32) {
+      const int q = base + lane;
+      bool live = q < e;
+      int cj = 0, img = 13, ls = lt;
+      if (live) {
+        const int packed = g.src[q];
+        cj = packed & 0x3ffffff;
+        img = packed >> 26;
+        ls = g.cell_pl[cj].y;
+        if (g.mode == 1 && !mixed_regular(lt, ls)) live = false;
+      }
+      T x = T(1), y = T(0), z = T(0);
+      if (live) {
+        const double4 Xs = g.cell_x[cj];
+        const double sx = (double)(img / 9 - 1) * g.cycle, sy = (double)((img / 3) % 3 - 1) * g.cycle,
+                     sz = (double)(img % 3 - 1) * g.cycle;
+        x = (T)((Xt.x - Xs.x - sx) * inv_rt);
+        y = (T)((Xt.y - Xs.y - sy) * inv_rt);
+        z = (T)((Xt.z - Xs.z - sz) * inv_rt);
+      }
       // M'' = Ms * (R_s / R_t)^n, an exact power of two: R_s / R_t = 2^(lt - ls).
       const T f1 = (T)ldexp(1.0, lt - ls);
       Cx<T> Mv[NM];
-      T fn = T(1);
+      T fn = live ? T(1) : T(0);
 #pragma unroll
       for (int n = 0; n < N1; n++) {
         if (n >= N0) {
@@ -151,12 +167,30 @@ k_m2l_part(M2LCtx g, DevTables t, double2 *L) {
         }
         fn *= f1;
       }
-      m2l_pair_unrolled<T, P, J0, J1, N0, N1>(tab<T>(), Mv, acc, x, y, z);
+      if constexpr (kPacked) {
+        f2p Mxx[NM], Myy[NM];
+#pragma unroll
+        for (int i = 0; i < NM; i++) {
+          Mxx[i] = pk2(Mv[i].x, Mv[i].x);
+          Myy[i] = pk2(Mv[i].y, Mv[i].y);
+        }
+        m2l_pair_f32x2<P, J0, J1, N0, N1>(tab<float>(), Mxx, Myy, acc, x, y, z);
+      } else {
+        m2l_pair_unrolled<T, P, J0, J1, N0, N1>(tab<T>(), Mv, acc, x, y, z);
+      }
     }
     const double rt = Xt.w;
 #pragma unroll
     for (int i = 0; i < NA; i++) {
-      double re = (double)acc[i].x, im = (double)acc[i].y;
+      double re, im;
+      if constexpr (kPacked) {
+        const float2 v = unpk2(acc[i]);
+        re = v.x;
+        im = v.y;
+      } else {
+        re = (double)acc[i].x;
+        im = (double)acc[i].y;
+      }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
         re += __shfl_xor_sync(0xffffffffu, re, o);
@@ -199,9 +233,12 @@ bool launch_for_P<float>(int P, const M2LCtx &g, const DevTables &t, double2 *L,
   switch (P) {
     case 4: launch_fast<float, 4, Part<0, 4, 0, 4>>(g, t, L, st); return true;
     case 6: launch_fast<float, 6, Part<0, 6, 0, 6>>(g, t, L, st); return true;
-    case 8: launch_fast<float, 8, Part<0, 8, 0, 6>, Part<0, 8, 6, 8>>(g, t, L, st); return true;
+    case 8:
+      launch_fast<float, 8, Part<0, 6, 0, 6>, Part<0, 6, 6, 8>, Part<6, 8, 0, 6>, Part<6, 8, 6, 8>>(g, t, L, st);
+      return true;
     case 10:
-      launch_fast<float, 10, Part<0, 10, 0, 7>, Part<0, 10, 7, 10>>(g, t, L, st);
+      launch_fast<float, 10, Part<0, 7, 0, 7>, Part<0, 7, 7, 10>, Part<7, 10, 0, 7>, Part<7, 10, 7, 10>>(g, t, L,
+                                                                                                     st);
       return true;
     default: return false;
   }

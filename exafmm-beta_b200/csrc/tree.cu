@@ -34,8 +34,8 @@ __host__ __device__ __forceinline__ double order_dec(unsigned long long u) {
 
 __global__ void k_bounds_init(unsigned long long *enc) {
   int t = threadIdx.x;
-  if (t < 3) enc[t] = ~0ull;      // running min
-  else if (t < 6) enc[t] = 0ull;  // running max
+  if (t < 3 || (t >= 6 && t < 9)) enc[t] = ~0ull;  // running minima (exact, estimate)
+  else if (t < 13) enc[t] = 0ull;                 // running maxima, max |x|
 }
 
 // Each body contributes g^(N-1-j)(X_j) to the min and the mirrored drift to the
@@ -65,6 +65,64 @@ __global__ void k_bounds(const double4 *x, long long n, unsigned long long *enc)
     for (int d = 0; d < 3; d++) {
       atomicMin(&enc[d], lo[d]);
       atomicMax(&enc[3 + d], hi[d]);
+    }
+  }
+}
+
+// Two-pass form of k_bounds.  The unrounded estimate x_j -/+ k_j * 1e-5 is
+// within k * ulp(max|x| + N * 1e-5) of the exact drifted value, so only bodies
+// whose estimate lies within twice that of the extreme estimate can hold the
+// exact extreme; only those evaluate the closed form.
+// enc[0..5]: exact result, enc[6..11]: estimates, enc[12]: max |x| over all coordinates.
+__global__ void k_bounds_estimate(const double4 *x, long long n, unsigned long long *enc) {
+  unsigned long long lo[3] = {~0ull, ~0ull, ~0ull}, hi[3] = {0, 0, 0}, amax = 0;
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
+    const double4 b = x[j];
+    const double v[3] = {b.x, b.y, b.z};
+    const double kc = (double)((j == 0) ? n : n - 1 - j) * 1e-5;
+    for (int d = 0; d < 3; d++) {
+      const unsigned long long a = order_enc(v[d] - kc), c = order_enc(v[d] + kc);
+      lo[d] = a < lo[d] ? a : lo[d];
+      hi[d] = c > hi[d] ? c : hi[d];
+      const unsigned long long ab = order_enc(fabs(v[d]));
+      amax = ab > amax ? ab : amax;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    for (int d = 0; d < 3; d++) {
+      const unsigned long long a = __shfl_xor_sync(0xffffffffu, lo[d], o);
+      const unsigned long long c = __shfl_xor_sync(0xffffffffu, hi[d], o);
+      lo[d] = a < lo[d] ? a : lo[d];
+      hi[d] = c > hi[d] ? c : hi[d];
+    }
+    const unsigned long long m = __shfl_xor_sync(0xffffffffu, amax, o);
+    amax = m > amax ? m : amax;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    for (int d = 0; d < 3; d++) {
+      atomicMin(&enc[6 + d], lo[d]);
+      atomicMax(&enc[9 + d], hi[d]);
+    }
+    atomicMax(&enc[12], amax);
+  }
+}
+
+__global__ void k_bounds_exact(const double4 *x, long long n, unsigned long long *enc) {
+  const double span = order_dec(enc[12]) + (double)n * 1e-5;
+  const double B = (double)n * ldexp(1.0, ilogb(span > 1e-300 ? span : 1e-300) - 52) + 1e-300;
+  double elo[3], ehi[3];
+  for (int d = 0; d < 3; d++) {
+    elo[d] = order_dec(enc[6 + d]) + 2.0 * B;
+    ehi[d] = order_dec(enc[9 + d]) - 2.0 * B;
+  }
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
+    const double4 b = x[j];
+    const double v[3] = {b.x, b.y, b.z};
+    const long long k = (j == 0) ? n : n - 1 - j;
+    const double kc = (double)k * 1e-5;
+    for (int d = 0; d < 3; d++) {
+      if (v[d] - kc <= elo[d]) atomicMin(&enc[d], order_enc(drift_down(v[d], k)));
+      if (v[d] + kc >= ehi[d]) atomicMax(&enc[3 + d], order_enc(drift_up(v[d], k)));
     }
   }
 }
@@ -348,11 +406,13 @@ int grid_for(long long n, int block) {
 void compute_bounds(Context &C) {
   TreeBufs &T = C.tree;
   T.bounds.ensure(6);
-  T.bounds_enc.ensure(6);
+  T.bounds_enc.ensure(16);
   k_bounds_init<<<1, 32, 0, C.stream>>>(T.bounds_enc.p);
   EXA_CHECK_LAUNCH();
   if (T.n > 0) {
-    k_bounds<<<grid_for(T.n, 256), 256, 0, C.stream>>>(T.xyzq.p, T.n, T.bounds_enc.p);
+    k_bounds_estimate<<<grid_for(T.n, 256), 256, 0, C.stream>>>(T.xyzq.p, T.n, T.bounds_enc.p);
+    EXA_CHECK_LAUNCH();
+    k_bounds_exact<<<grid_for(T.n, 256), 256, 0, C.stream>>>(T.xyzq.p, T.n, T.bounds_enc.p);
     EXA_CHECK_LAUNCH();
   }
   k_bounds_final<<<1, 32, 0, C.stream>>>(T.bounds_enc.p, T.n, T.bounds.p);
