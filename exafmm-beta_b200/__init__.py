@@ -88,6 +88,8 @@ def lib() -> ctypes.CDLL:
         "exafmm_kernel_p2p": (_c_int, [_c_ll, _vp, _c_ll, _vp, _vp, _vp]),
         "exafmm_drift": (_c_double, [_c_double, _c_ll, _c_int]),
         "exafmm_launch_count": (_c_ll, []),
+        "exafmm_set_params": (_c_int, [_vp, _c_int, _c_double, _c_int, _c_int, _c_int, _c_double]),
+        "exafmm_set_mixed_policy": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -146,6 +148,21 @@ class Fmm:
 
     def __exit__(self, *exc):
         self.close()
+
+    def set_params(self, P=None, theta=None, ncrit=None, nspawn=None, images=None, cycle=None):
+        """Change solve parameters between solves (unchanged ones keep their value)."""
+        P = self.P if P is None else P
+        theta = self.theta if theta is None else theta
+        ncrit = self.ncrit if ncrit is None else ncrit
+        nspawn = self.nspawn if nspawn is None else nspawn
+        images = self.images if images is None else images
+        cycle = self.cycle if cycle is None else cycle
+        self._check(lib().exafmm_set_params(self._h, P, theta, ncrit, nspawn, images, cycle))
+        self.P, self.theta, self.ncrit, self.nspawn, self.images, self.cycle = P, theta, ncrit, nspawn, images, cycle
+
+    def set_mixed_policy(self, m2l_fp32=True, p2p_fp32=True, min_level=4, max_dl=3):
+        """Mixed form: which operators run in FP32 and which M2L pairs may."""
+        self._check(lib().exafmm_set_mixed_policy(self._h, int(m2l_fp32), int(p2p_fp32), min_level, max_dl))
 
     # ---- solve steps (examples/fmm.cxx:163-179) ----
     def set_bodies(self, xyzq):

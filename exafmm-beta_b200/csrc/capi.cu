@@ -172,17 +172,22 @@ struct Engine {
       EXA_CUDA(cudaMemsetAsync(L.p, 0, nc * NT * sizeof(double2), C.stream));
       FmmArgs a = args();
       const bool mixed = C.prm.precision == kMixed;
-      if (m2l_fast_supported(C.prm.P, mixed)) {
-        Ms.ensure(nc * NT * (mixed ? sizeof(float2) : sizeof(double2)));
-        scale_multipoles(a, mixed, Ms.p);
-        m2l_fast(a, mixed, Ms.p);
-        if (mixed) m2l_fp64(a, kMixedMinLevel, kMixedMaxDl);  // root levels, large size ratios
+      const bool m2l32 = mixed && C.prm.mixed_m2l && m2l_fast_supported(C.prm.P, true);
+      if (m2l32) {
+        Ms.ensure(nc * NT * sizeof(float2));
+        scale_multipoles(a, true, Ms.p);
+        m2l_fast(a, true, Ms.p, C.prm.mixed_min_level, C.prm.mixed_max_dl);
+        m2l_fp64(a, C.prm.mixed_min_level, C.prm.mixed_max_dl);  // root levels, large size ratios
+      } else if (m2l_fast_supported(C.prm.P, false)) {
+        Ms.ensure(nc * NT * sizeof(double2));
+        scale_multipoles(a, false, Ms.p);
+        m2l_fast(a, false, Ms.p);
       } else {
         m2l_fp64(a);
       }
       EXA_CUDA(cudaEventRecord(tm.ev[5], C.stream));
-      if (mixed) {
-        x32.ensure(C.tree.n);
+      if (mixed && C.prm.mixed_p2p) {
+        x32.ensure(2 * C.tree.n);  // hi and lo float4 per body
         rel_bodies32(a, x32.p);
         p2p_mixed(a, x32.p);
       } else {
@@ -317,6 +322,42 @@ int exafmm_destroy(exafmm_ctx *ctx) {
 
 const char *exafmm_last_error(const exafmm_ctx *ctx) { return ctx ? ctx->E.C.last_error.c_str() : "null context"; }
 const char *exafmm_create_error(void) { return g_create_error.c_str(); }
+
+int exafmm_set_params(exafmm_ctx *ctx, int P, double theta, int ncrit, int nspawn, int images, double cycle) {
+  return guarded(ctx, [&] {
+    Engine &E = ctx->E;
+    Params &p = E.C.prm;
+    if (P < 2 || P > kMaxP) throw std::runtime_error("P must be in [2, 20]");
+    if (ncrit < 1 || ncrit > 1024) throw std::runtime_error("ncrit must be in [1, 1024]");
+    if (!(theta > 0)) throw std::runtime_error("theta must be positive");
+    if (images < 0) throw std::runtime_error("images must be >= 0");
+    cudaSetDevice(E.C.device);
+    device_tables(P);
+    if (ncrit != p.ncrit) E.tree_ok = false;
+    if (ncrit != p.ncrit || P != p.P) E.up_ok = false;
+    if (ncrit != p.ncrit || P != p.P || theta != p.theta || nspawn != p.nspawn || images != p.images ||
+        cycle != p.cycle)
+      E.lists_ok = false;
+    p.P = P;
+    p.theta = theta;
+    p.ncrit = ncrit;
+    p.nspawn = nspawn;
+    p.images = images;
+    p.cycle = cycle;
+  });
+}
+
+int exafmm_set_mixed_policy(exafmm_ctx *ctx, int m2l_fp32, int p2p_fp32, int min_level, int max_dl) {
+  return guarded(ctx, [&] {
+    Params &p = ctx->E.C.prm;
+    if (min_level < 0 || max_dl < 0) throw std::runtime_error("min_level and max_dl must be >= 0");
+    p.mixed_m2l = m2l_fp32 != 0;
+    p.mixed_p2p = p2p_fp32 != 0;
+    p.mixed_min_level = min_level;
+    p.mixed_max_dl = max_dl;
+    ctx->E.lists_ok = false;
+  });
+}
 
 int exafmm_set_bodies(exafmm_ctx *ctx, const double *xyzq, long long n) {
   return guarded(ctx, [&] {

@@ -14,6 +14,12 @@ struct Params {
   int images = 0;
   double cycle = 6.283185307179586;
   int precision = kFP64;
+  // Mixed form: which operators run in FP32, and which M2L pairs (target level
+  // and source/target level difference) may; the rest stays FP64.
+  int mixed_m2l = 1;
+  int mixed_p2p = 1;
+  int mixed_min_level = 4;
+  int mixed_max_dl = 3;
 };
 
 // Level-ordered octree nodes plus the reference-layout cell table.

@@ -41,7 +41,9 @@ constexpr int kMixedMaxDl = 3;
 bool m2l_fast_supported(int P, bool mixed);
 // Ms = A_n^m M_n^m / R^n per cell, FP32 (mixed) or FP64.
 void scale_multipoles(const FmmArgs &a, bool mixed, void *Ms);
-bool m2l_fast(const FmmArgs &a, bool mixed, const void *Ms);
+// In mixed mode only pairs with target level >= min_level and |level difference|
+// <= max_dl are taken (the generic FP64 kernel handles the rest).
+bool m2l_fast(const FmmArgs &a, bool mixed, const void *Ms, int min_level = 0, int max_dl = 0);
 
 // Mixed-precision P2P (p2p32.cu): bodies relative to their leaf center in FP32.
 void rel_bodies32(const FmmArgs &a, float4 *x32);

@@ -96,11 +96,12 @@ struct M2LCtx {
   const void *Ms;
   double cycle;
   int mode;  // 0: every pair; 1: mixed-regular pairs only
+  int min_level, max_dl;
 };
 
-__device__ __forceinline__ bool mixed_regular(int lt, int ls) {
+__device__ __forceinline__ bool mixed_regular(const M2LCtx &g, int lt, int ls) {
   const int dl = lt - ls;
-  return lt >= kMixedMinLevel && dl <= kMixedMaxDl && dl >= -kMixedMaxDl;
+  return lt >= g.min_level && dl <= g.max_dl && dl >= -g.max_dl;
 }
 
 // One (J, N) part of the contraction for every target: warp per target cell,
@@ -141,7 +142,7 @@ k_m2l_part(M2LCtx g, DevTables t, double2 *L) {
         cj = packed & 0x3ffffff;
         img = packed >> 26;
         ls = g.cell_pl[cj].y;
-        if (g.mode == 1 && !mixed_regular(lt, ls)) live = false;
+        if (g.mode == 1 && !mixed_regular(g, lt, ls)) live = false;
       }
       T x = T(1), y = T(0), z = T(0);
       if (live) {
@@ -237,8 +238,9 @@ bool launch_for_P<float>(int P, const M2LCtx &g, const DevTables &t, double2 *L,
       launch_fast<float, 8, Part<0, 6, 0, 6>, Part<0, 6, 6, 8>, Part<6, 8, 0, 6>, Part<6, 8, 6, 8>>(g, t, L, st);
       return true;
     case 10:
-      launch_fast<float, 10, Part<0, 7, 0, 7>, Part<0, 7, 7, 10>, Part<7, 10, 0, 7>, Part<7, 10, 7, 10>>(g, t, L,
-                                                                                                     st);
+      launch_fast<float, 10, Part<0, 6, 0, 5>, Part<0, 6, 5, 8>, Part<0, 6, 8, 10>, Part<6, 8, 0, 5>,
+                  Part<6, 8, 5, 8>, Part<6, 8, 8, 10>, Part<8, 10, 0, 5>, Part<8, 10, 5, 8>, Part<8, 10, 8, 10>>(
+          g, t, L, st);
       return true;
     default: return false;
   }
@@ -278,7 +280,7 @@ void scale_multipoles(const FmmArgs &a, bool mixed, void *Ms) {
   EXA_CHECK_LAUNCH();
 }
 
-bool m2l_fast(const FmmArgs &a, bool mixed, const void *Ms) {
+bool m2l_fast(const FmmArgs &a, bool mixed, const void *Ms, int min_level, int max_dl) {
   if (!m2l_fast_supported(a.P, mixed)) return false;
   init_tables();
   const DevTables &t = device_tables(a.P);
@@ -291,6 +293,8 @@ bool m2l_fast(const FmmArgs &a, bool mixed, const void *Ms) {
   g.Ms = Ms;
   g.cycle = a.cycle;
   g.mode = mixed ? 1 : 0;
+  g.min_level = min_level;
+  g.max_dl = max_dl;
   return mixed ? launch_for_P<float>(a.P, g, t, a.L64, a.stream) : launch_for_P<double>(a.P, g, t, a.L64, a.stream);
 }
 

@@ -1,12 +1,15 @@
 // Mixed-precision P2P (kernels/laplace.h:150-235) in FP32.
 //
-// Bodies are stored relative to the center of their own leaf (FP32), and each
-// source leaf's offset from the target leaf is formed in FP64 and rounded once,
-// so a separation is rounded relative to the cell size, not to the absolute
-// coordinates.  Each target accumulates one source leaf at a time in FP32 and
-// adds that partial into its running sums with Kahan compensation
-// (include/kahan.h:34-48 semantics), so the error does not grow with the
-// number of neighbour leaves.  Results are added to the FP64 outputs.
+// Each body is stored relative to the center of its own leaf as a two-float
+// pair (hi + lo, about 48 significant bits), and each target is re-expressed
+// relative to the source leaf in FP64 once per source leaf.  The separation of
+// a pair is then (t_hi - s_hi) + (t_lo - s_lo): the hi difference is exact for
+// close bodies, so close pairs keep their relative accuracy, and the rest of
+// the interaction (r^2, rsqrt, the sums) is plain FP32.  Each target
+// accumulates one source leaf at a time in FP32 and adds that partial into its
+// running sums with Kahan compensation (include/kahan.h:34-48 semantics), so
+// the error does not grow with the number of neighbour leaves.  Results are
+// added to the FP64 outputs.
 #include "fmm.h"
 
 namespace exafmm_b200 {
@@ -14,6 +17,7 @@ namespace {
 
 constexpr int kWarps = 4;
 
+// x32[2i] = (hi of x - X_leaf, q), x32[2i+1] = (lo parts, 0).
 __global__ void k_rel32(const int4 *cell_b, const double4 *cell_x, long long ncells, const double4 *xt, float4 *x32) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (long long c = (long long)blockIdx.x * kWarps + warp; c < ncells; c += (long long)gridDim.x * kWarps) {
@@ -22,7 +26,11 @@ __global__ void k_rel32(const int4 *cell_b, const double4 *cell_x, long long nce
     const double4 X = cell_x[c];
     for (int i = lane; i < cb.y; i += 32) {
       const double4 b = xt[cb.x + i];
-      x32[cb.x + i] = make_float4((float)(b.x - X.x), (float)(b.y - X.y), (float)(b.z - X.z), (float)b.w);
+      const double dx = b.x - X.x, dy = b.y - X.y, dz = b.z - X.z;
+      const float hx = (float)dx, hy = (float)dy, hz = (float)dz;
+      x32[2 * (long long)(cb.x + i)] = make_float4(hx, hy, hz, (float)b.w);
+      x32[2 * (long long)(cb.x + i) + 1] =
+          make_float4((float)(dx - (double)hx), (float)(dy - (double)hy), (float)(dz - (double)hz), 0.f);
     }
   }
 }
@@ -43,7 +51,7 @@ template <int TPL>
 __global__ void __launch_bounds__(32 * kWarps)
 k_p2p32(const int *off, const int *src, long long ncells, const int4 *cell_b, const double4 *cell_x,
         const float4 *x32, double4 *trg, double cycle) {
-  __shared__ float4 sbuf[kWarps][32];
+  __shared__ float4 shi[kWarps][32], slo[kWarps][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (long long c = (long long)blockIdx.x * kWarps + warp; c < ncells; c += (long long)gridDim.x * kWarps) {
     const int b = off[c], e = off[c + 1];
@@ -51,45 +59,59 @@ k_p2p32(const int *off, const int *src, long long ncells, const int4 *cell_b, co
     const int4 ci = cell_b[c];
     const double4 Xc = cell_x[c];
     for (int tb = 0; tb < ci.y; tb += 32 * TPL) {
-      float xi[TPL], yi[TPL], zi[TPL];
+      double xi[TPL], yi[TPL], zi[TPL];  // target offset from its own leaf center
       Kahan pot[TPL], ax[TPL], ay[TPL], az[TPL];
 #pragma unroll
       for (int u = 0; u < TPL; u++) {
         const int i = tb + lane + 32 * u;
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (i < ci.y) v = x32[ci.x + i];
-        xi[u] = v.x;
-        yi[u] = v.y;
-        zi[u] = v.z;
+        float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h;
+        if (i < ci.y) {
+          h = x32[2 * (long long)(ci.x + i)];
+          l = x32[2 * (long long)(ci.x + i) + 1];
+        }
+        xi[u] = (double)h.x + (double)l.x;
+        yi[u] = (double)h.y + (double)l.y;
+        zi[u] = (double)h.z + (double)l.z;
       }
       for (int q = b; q < e; q++) {
         const int packed = src[q];
         const int cj = packed & 0x3ffffff, img = packed >> 26;
         const double4 Xj = cell_x[cj];
-        const float Dx = (float)(Xj.x + (double)(img / 9 - 1) * cycle - Xc.x);
-        const float Dy = (float)(Xj.y + (double)((img / 3) % 3 - 1) * cycle - Xc.y);
-        const float Dz = (float)(Xj.z + (double)(img % 3 - 1) * cycle - Xc.z);
+        const double Dx = Xj.x + (double)(img / 9 - 1) * cycle - Xc.x;
+        const double Dy = Xj.y + (double)((img / 3) % 3 - 1) * cycle - Xc.y;
+        const double Dz = Xj.z + (double)(img % 3 - 1) * cycle - Xc.z;
         const int4 cjb = cell_b[cj];
-        float tx[TPL], ty[TPL], tz[TPL], pp[TPL], px[TPL], py[TPL], pz[TPL];
+        // target relative to the source leaf center, as hi + lo floats
+        float thx[TPL], thy[TPL], thz[TPL], tlx[TPL], tly[TPL], tlz[TPL];
+        float pp[TPL], px[TPL], py[TPL], pz[TPL];
 #pragma unroll
         for (int u = 0; u < TPL; u++) {
-          tx[u] = xi[u] - Dx;
-          ty[u] = yi[u] - Dy;
-          tz[u] = zi[u] - Dz;
+          const double tx = xi[u] - Dx, ty = yi[u] - Dy, tz = zi[u] - Dz;
+          thx[u] = (float)tx;
+          thy[u] = (float)ty;
+          thz[u] = (float)tz;
+          tlx[u] = (float)(tx - (double)thx[u]);
+          tly[u] = (float)(ty - (double)thy[u]);
+          tlz[u] = (float)(tz - (double)thz[u]);
           pp[u] = px[u] = py[u] = pz[u] = 0.f;
         }
         for (int sb = 0; sb < cjb.y; sb += 32) {
           const int ns = min(32, cjb.y - sb);
-          if (lane < ns) sbuf[warp][lane] = x32[cjb.x + sb + lane];
+          if (lane < ns) {
+            shi[warp][lane] = x32[2 * (long long)(cjb.x + sb + lane)];
+            slo[warp][lane] = x32[2 * (long long)(cjb.x + sb + lane) + 1];
+          }
           __syncwarp();
           for (int s = 0; s < ns; s++) {
-            const float4 sj = sbuf[warp][s];
+            const float4 sh = shi[warp][s], sl = slo[warp][s];
 #pragma unroll
             for (int u = 0; u < TPL; u++) {
-              const float dx = tx[u] - sj.x, dy = ty[u] - sj.y, dz = tz[u] - sj.z;
+              const float dx = (thx[u] - sh.x) + (tlx[u] - sl.x);
+              const float dy = (thy[u] - sh.y) + (tly[u] - sl.y);
+              const float dz = (thz[u] - sh.z) + (tlz[u] - sl.z);
               const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
               const float inv = (r2 > 0.f) ? rsqrtf(r2) : 0.f;
-              const float qr = sj.w * inv;
+              const float qr = sh.w * inv;
               const float qr3 = qr * inv * inv;
               pp[u] += qr;
               px[u] = fmaf(dx, qr3, px[u]);

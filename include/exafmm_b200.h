@@ -47,6 +47,18 @@ const char *exafmm_last_error(const exafmm_ctx *ctx);
 /* Error text of the last failed exafmm_create on this thread. */
 const char *exafmm_create_error(void);
 
+/* Change the solve parameters of an existing context (the arguments of
+ * Kernel/Traversal/BuildTree, as in exafmm_create).  Takes effect at the next
+ * build/upward/traverse call; results of earlier steps that depend on a
+ * changed parameter must be recomputed. */
+int exafmm_set_params(exafmm_ctx *ctx, int P, double theta, int ncrit, int nspawn, int images, double cycle);
+
+/* Mixed form only: which operators run in FP32 (m2l_fp32, p2p_fp32) and which
+ * M2L pairs may (target level >= min_level, |level difference| <= max_dl); the
+ * rest runs in FP64.  Defaults: 1, 1, 4, 3.  No counterpart in the reference
+ * (its precision is a compile-time switch, EXAFMM_SINGLE). */
+int exafmm_set_mixed_policy(exafmm_ctx *ctx, int m2l_fp32, int p2p_fp32, int min_level, int max_dl);
+
 /* Bodies in caller order (Dataset::initBodies / Bodies, include/types.h:72-86).
  * The _device form takes a device pointer to n x 4 doubles on the context's device. */
 int exafmm_set_bodies(exafmm_ctx *ctx, const double *xyzq, long long n);
