@@ -128,6 +128,20 @@ int exafmm_kernel_l2p(int P, const double *X, const double *L, long long n, cons
 int exafmm_kernel_p2p(long long ni, const double *xi, long long nj, const double *xj, const double *Xperiodic,
                       double *trg);
 
+/* Allocation-free form of exafmm_get_bounds, for callers that may not allocate
+ * device memory (a host framework that owns all device memory through its own
+ * pool, or a latency-bound loop that cannot pay for cudaMalloc/cudaFree).  No
+ * counterpart in the reference.  d_xyzq: n x 4 doubles on the current device;
+ * d_bounds6: 6 doubles on the current device, written on `stream` (a
+ * cudaStream_t; NULL is the legacy default stream).  Needs no context and
+ * allocates nothing: its only scratch is a 128-byte array built into the
+ * library, held by every GPU that loads it until the process exits.  The first
+ * call on a device looks up that array's address, so make it before any stream
+ * capture.  All calls share the array, so calls that overlap on the GPU race.
+ * Returns 0, or 2 when n is outside [0, 2^31 - 1], 3 for a null pointer,
+ * 4 for a CUDA error. */
+int exafmm_get_bounds_noalloc(const double *d_xyzq, long long n, double *d_bounds6, void *stream);
+
 /* Host-side closed form of the bounds drift: fl(x -/+ 1e-5) applied k times
  * (up != 0 adds).  Runs on the CPU; exposed so its exactness can be checked
  * without a GPU. */
