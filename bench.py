@@ -2,7 +2,8 @@
 
 Workload (the single large adaptive solve): N = 4,194,304 bodies from a Plummer
 sphere (scale 1, truncated at r = 20), equal charges 1/N, P = 8, theta = 0.35,
-ncrit = 64, nspawn = 5000.  One step = one complete solve from bodies resident
+ncrit tuned in {32, 64, 128}, nspawn = 5000, mixed precision (FP32 M2L/P2P with
+compensated accumulation, FP64 root levels).  One step = one complete solve from bodies resident
 in device memory to results in device memory: getBounds (with the reference's
 drift), tree build, upward pass, dual tree traversal with M2L and P2P, downward
 pass, results scattered back to input order.
@@ -37,7 +38,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG_DIR = os.path.join(ROOT, "exafmm-beta_b200")
 
 WORKLOAD = dict(name="plummer_4m_p8", n=4_194_304, P=8, theta=0.35, ncrit=64, nspawn=5000, seed=2)
-METRIC = "FMM bodies/s (full solve, Plummer N=4,194,304, P=8, theta=0.35)"
+METRIC = "FMM bodies/s (full mixed-precision solve, Plummer N=4,194,304, P=8, theta=0.35)"
 CPU_SAMPLE_N = 262_144
 
 
@@ -81,6 +82,15 @@ class ClockSampler:
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+        # nvidia-smi start-up is CPU-heavy: let it reach its first sample before timing
+        t0 = time.time()
+        while self.proc and time.time() - t0 < 5.0:
+            try:
+                if os.path.getsize(self.path) > 0:
+                    break
+            except OSError:
+                pass
+            time.sleep(0.05)
         time.sleep(0.3)
         return self
 
@@ -170,8 +180,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--n", type=int, default=WORKLOAD["n"], help=argparse.SUPPRESS)
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--ncrit", type=int, default=0, help="0: pick the fastest of 32, 64, 128 during warm-up")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain-method comparison run")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -198,21 +210,42 @@ def main():
     wl = dict(WORKLOAD)
     x = datasets.plummer(n, seed=wl["seed"] + rank)
     prec = pkg.FP64 if args.precision == "fp64" else pkg.MIXED
-    fmm = pkg.Fmm(P=wl["P"], theta=wl["theta"], ncrit=wl["ncrit"], nspawn=wl["nspawn"], precision=prec,
-                  device=local_rank)
-    stream = torch.cuda.ExternalStream(fmm.stream())
     dx = torch.from_numpy(x).cuda()
     dout = torch.empty_like(dx)
     hx = torch.from_numpy(x).pin_memory()
     hout = torch.empty_like(hx).pin_memory()
 
-    def solve_device():
-        fmm.set_bodies_device(dx.data_ptr(), n)
-        fmm.solve()
-        fmm.results_device(dout.data_ptr())
+    def make(precision, ncrit):
+        return pkg.Fmm(P=wl["P"], theta=wl["theta"], ncrit=ncrit, nspawn=wl["nspawn"], precision=precision,
+                       device=local_rank)
 
+    def solve_device(f, out):
+        f.set_bodies_device(dx.data_ptr(), n)
+        f.solve()
+        f.results_device(out.data_ptr())
+
+    # ncrit autotuning (warm-up, untimed): one solve per candidate, keep the fastest.
+    tuned = {}
+    if args.ncrit:
+        ncrit = args.ncrit
+    else:
+        for cand in (32, 64, 128):
+            f = make(prec, cand)
+            solve_device(f, dout)
+            solve_device(f, dout)
+            tuned[cand] = f.phase_times()["total"]
+            f.close()
+        best = [min(tuned, key=tuned.get)]
+        if world > 1:  # every rank must use the same ncrit
+            tb = torch.tensor(best, device="cuda")
+            dist.broadcast(tb, 0)
+            best = [int(tb.item())]
+        ncrit = best[0]
+
+    fmm = make(prec, ncrit)
+    stream = torch.cuda.ExternalStream(fmm.stream())
     for _ in range(args.warmup):
-        solve_device()
+        solve_device(fmm, dout)
     torch.cuda.synchronize()
     info = fmm.info()
 
@@ -226,7 +259,7 @@ def main():
     with ClockSampler(local_rank) as clocks:
         ev0.record(stream)
         for _ in range(args.steps):
-            solve_device()
+            solve_device(fmm, dout)
             for k, v in fmm.phase_times().items():
                 phase_acc[k] += v
         ev1.record(stream)
@@ -259,6 +292,38 @@ def main():
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = n * world * args.steps / (float(te.item()) / 1e3)
 
+    # ---- plain FP64 run of the same input, and the three-way error split ----
+    plain = None
+    if not args.no_plain and prec == pkg.MIXED:
+        f64 = make(pkg.FP64, ncrit)
+        dref = torch.empty_like(dx)
+        solve_device(f64, dref)
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s64 = torch.cuda.ExternalStream(f64.stream())
+        p0.record(s64)
+        for _ in range(args.steps):
+            solve_device(f64, dref)
+        p1.record(s64)
+        torch.cuda.synchronize()
+        tp = torch.tensor([p0.elapsed_time(p1)], device="cuda")
+        if world > 1:
+            dist.all_reduce(tp, op=dist.ReduceOp.MAX)
+        plain_ms = float(tp.item()) / args.steps
+        mixed_out, plain_out = dout.cpu().numpy(), dref.cpu().numpy()
+        idx = datasets.strided_sample(n, 4096)
+        direct = pkg.direct(x[idx], x)
+        plain = {"value": n * world / (plain_ms / 1e3), "unit": "bodies/s", "ms_per_step": plain_ms,
+                 "speedup_of_mixed": (n * world / (ms_max / args.steps / 1e3)) / (n * world / (plain_ms / 1e3)),
+                 "rel_l2": {"mixed_vs_direct_pot": datasets.rel_l2(mixed_out[idx, 0], direct[:, 0]),
+                            "plain_vs_direct_pot": datasets.rel_l2(plain_out[idx, 0], direct[:, 0]),
+                            "mixed_vs_plain_pot": datasets.rel_l2(mixed_out[:, 0], plain_out[:, 0]),
+                            "mixed_vs_direct_acc": datasets.rel_l2(mixed_out[idx, 1:], direct[:, 1:]),
+                            "plain_vs_direct_acc": datasets.rel_l2(plain_out[idx, 1:], direct[:, 1:]),
+                            "mixed_vs_plain_acc": datasets.rel_l2(mixed_out[:, 1:], plain_out[:, 1:]),
+                            "direct_sample": 4096}}
+        f64.close()
+
     # ---- roofline of the dominant kernel (M2L), from the timed steps ----
     hbm_peak, bf16_peak, peak_kind = _peaks()
     P = wl["P"]
@@ -274,8 +339,8 @@ def main():
         "frac": achieved / hbm_peak, "traffic": None, "peak_kind": peak_kind,
         "ms_per_launch": m2l_ms, "algorithmic_bytes": alg_bytes, "algorithmic_flops": alg_flops,
         "achieved_tflops": alg_flops / (m2l_ms / 1e3) / 1e12,
-        "note": "FP64 M2L on CUDA cores is compute-bound (~50 flop/B); the HBM fraction shows how far it is "
-                "from the memory roof, achieved_tflops the FP64 rate",
+        "note": "M2L runs on the CUDA-core FP32 (mixed) / FP64 pipes and is compute-bound (~50 flop/B): "
+                "frac is its distance from the memory roof; achieved_tflops is its arithmetic rate",
     }
 
     line = {
@@ -283,7 +348,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if prec == pkg.FP64 else "f32+kahan", "data": "synthetic",
         "config": {"workload": wl["name"], "n_bodies": n, "distribution": "plummer(scale=1, rmax=20), q=1/N",
-                   "P": P, "theta": wl["theta"], "ncrit": wl["ncrit"], "nspawn": wl["nspawn"],
+                   "P": P, "theta": wl["theta"], "ncrit": ncrit, "ncrit_tuning_ms": tuned, "nspawn": wl["nspawn"],
                    "precision": args.precision, "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (134 MB of bodies per solve)",
                    "cells": info["ncells"], "depth": info["depth"], "m2l_pairs": n_m2l, "p2p_pairs": info["n_p2p"]},
@@ -294,6 +359,8 @@ def main():
         "gpu_launches": int(launches),
         "clocks": clk,
     }
+    if plain is not None:
+        line["plain_fp64"] = plain
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         kind, times, _ = cpu_reference_baseline(CPU_SAMPLE_N, threads, steps=1)

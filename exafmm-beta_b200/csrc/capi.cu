@@ -52,7 +52,7 @@ struct Engine {
   ListBufs lists;
   DBuf<double2> M, L;
   DBuf<unsigned char> Ms;  // scaled multipoles for the unrolled M2L (FP32 or FP64)
-  DBuf<float4> x32;        // bodies relative to their leaf center (mixed P2P)
+  DBuf<float4> x32;        // bodies as two-float pairs relative to the root center (mixed P2P)
   DBuf<double4> trg, out;
   Timing tm;
   bool tree_ok = false, up_ok = false, lists_ok = false;
@@ -62,6 +62,7 @@ struct Engine {
     a.P = C.prm.P;
     a.ncrit = C.prm.ncrit;
     a.ncells = C.tree.ncells;
+    a.n = C.tree.n;
     a.cycle = C.prm.cycle;
     a.stream = C.stream;
     a.lvl = C.tree.lvl.p;
@@ -189,7 +190,7 @@ struct Engine {
       if (mixed && C.prm.mixed_p2p) {
         x32.ensure(2 * C.tree.n);  // hi and lo float4 per body
         rel_bodies32(a, x32.p);
-        p2p_mixed(a, x32.p);
+        p2p_mixed(a, x32.p, C.prm.images > 0);
       } else {
         p2p_fp64(a);
       }

@@ -8,6 +8,7 @@ struct FmmArgs {
   int P = 10;
   int ncrit = 64;
   long long ncells = 0;
+  long long n = 0;                     // bodies
   double cycle = 0;
   cudaStream_t stream = nullptr;
   const long long *lvl = nullptr;
@@ -45,9 +46,10 @@ void scale_multipoles(const FmmArgs &a, bool mixed, void *Ms);
 // <= max_dl are taken (the generic FP64 kernel handles the rest).
 bool m2l_fast(const FmmArgs &a, bool mixed, const void *Ms, int min_level = 0, int max_dl = 0);
 
-// Mixed-precision P2P (p2p32.cu): bodies relative to their leaf center in FP32.
+// Mixed-precision P2P (p2p32.cu): bodies as two-float pairs relative to the
+// root center; periodic selects the form that tests every pair for r = 0.
 void rel_bodies32(const FmmArgs &a, float4 *x32);
-void p2p_mixed(const FmmArgs &a, const float4 *x32);
+void p2p_mixed(const FmmArgs &a, const float4 *x32, bool periodic);
 
 // Interaction lists of the dual tree traversal (traverse.cu).
 struct ListBufs {

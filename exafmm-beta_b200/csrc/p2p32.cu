@@ -1,38 +1,83 @@
 // Mixed-precision P2P (kernels/laplace.h:150-235) in FP32.
 //
-// Each body is stored relative to the center of its own leaf as a two-float
-// pair (hi + lo, about 48 significant bits), and each target is re-expressed
-// relative to the source leaf in FP64 once per source leaf.  The separation of
-// a pair is then (t_hi - s_hi) + (t_lo - s_lo): the hi difference is exact for
-// close bodies, so close pairs keep their relative accuracy, and the rest of
-// the interaction (r^2, rsqrt, the sums) is plain FP32.  Each target
-// accumulates one source leaf at a time in FP32 and adds that partial into its
-// running sums with Kahan compensation (include/kahan.h:34-48 semantics), so
-// the error does not grow with the number of neighbour leaves.  Results are
-// added to the FP64 outputs.
+// Coordinates.  Every body is stored once per solve as a two-float pair
+// (hi + lo, about 48 significant bits) relative to the root cell's center.
+// The separation of a pair is (t_hi - s_hi) + (t_lo - s_lo): for close bodies
+// the hi difference is exact, so close pairs keep their relative accuracy,
+// and the rest of the interaction (r^2, rsqrt, the sums) is plain FP32.
+// A periodic image shift is added to the source's two-float pair when it is
+// staged (TwoSum of the hi parts, the rounding error carried into lo).
+//
+// Work mapping.  One warp evaluates one target leaf at a time.  The leaf's
+// source bodies (the bodies of every leaf in its P2P list, one after another)
+// form a stream that the warp stages into shared memory in chunks.  The 32
+// lanes are split into G = 32 / S groups of S lanes; each lane holds two
+// targets, so a group covers 2S targets, and the G groups take interleaved
+// pairs of the chunk's sources.  S is chosen from the leaf's size so that
+// small leaves still fill the warp (<= 8 bodies: 8 groups of 4 lanes; <= 16:
+// 4 x 8; <= 32: 2 x 16; larger: 1 x 32, in passes of 64 targets).  Two
+// consecutive sources go through one packed f32x2 operation, so the
+// arithmetic of two interactions is one instruction stream.
+//
+// Accumulation.  Each lane sums a chunk (at most 32 sources per group) in
+// FP32 and then adds that partial into Kahan-compensated running sums
+// (include/kahan.h:34-48 semantics), so the error does not grow with the
+// number of chunks; the groups' sums are combined in FP64 and added to the
+// FP64 outputs.
+//
+// r = 0.  A pair at zero distance contributes nothing, as in the reference
+// (kernels/laplace.h:171: invR2 = 0 when R2 = 0).  The test is applied to
+// every pair: it runs on the integer/select pipe, beside the FP32 pipe that
+// bounds this kernel.  The rsqrt flushes subnormal inputs, so a pair closer
+// than about 1e-19 (an r^2 below the FP32 normal range) also contributes
+// nothing; such inputs need the FP64 plain method.
+#include <stdexcept>
+
 #include "fmm.h"
 
 namespace exafmm_b200 {
 namespace {
 
-constexpr int kWarps = 4;
+constexpr int kMaxGroups = 8;                 // groups of 4 lanes
+constexpr int kStagePairs = 16 * kMaxGroups;  // chunk = 32 * G sources = 16 * G pairs
+constexpr unsigned kFull = 0xffffffffu;
 
-// x32[2i] = (hi of x - X_leaf, q), x32[2i+1] = (lo parts, 0).
-__global__ void k_rel32(const int4 *cell_b, const double4 *cell_x, long long ncells, const double4 *xt, float4 *x32) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (long long c = (long long)blockIdx.x * kWarps + warp; c < ncells; c += (long long)gridDim.x * kWarps) {
-    const int4 cb = cell_b[c];
-    if (cb.w != 0) continue;
-    const double4 X = cell_x[c];
-    for (int i = lane; i < cb.y; i += 32) {
-      const double4 b = xt[cb.x + i];
-      const double dx = b.x - X.x, dy = b.y - X.y, dz = b.z - X.z;
-      const float hx = (float)dx, hy = (float)dy, hz = (float)dz;
-      x32[2 * (long long)(cb.x + i)] = make_float4(hx, hy, hz, (float)b.w);
-      x32[2 * (long long)(cb.x + i) + 1] =
-          make_float4((float)(dx - (double)hx), (float)(dy - (double)hy), (float)(dz - (double)hz), 0.f);
-    }
-  }
+typedef unsigned long long f2p;  // two floats in one 64-bit register
+
+__device__ __forceinline__ f2p pk2(float a, float b) {
+  f2p r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ float2 unpk2(f2p v) {
+  float a, b;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+  return make_float2(a, b);
+}
+__device__ __forceinline__ f2p add2(f2p a, f2p b) {
+  f2p d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2p sub2(f2p a, f2p b) {
+  f2p d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2p mul2(f2p a, f2p b) {
+  f2p d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2p fma2(f2p a, f2p b, f2p c) {
+  f2p d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
 }
 
 // Compensated running sum: c holds the rounding error of the last addition,
@@ -47,128 +92,261 @@ struct Kahan {
   }
 };
 
-template <int TPL>
-__global__ void __launch_bounds__(32 * kWarps)
-k_p2p32(const int *off, const int *src, long long ncells, const int4 *cell_b, const double4 *cell_x,
-        const float4 *x32, double4 *trg, double cycle) {
-  __shared__ float4 shi[kWarps][32], slo[kWarps][32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (long long c = (long long)blockIdx.x * kWarps + warp; c < ncells; c += (long long)gridDim.x * kWarps) {
-    const int b = off[c], e = off[c + 1];
-    if (b == e) continue;
-    const int4 ci = cell_b[c];
-    const double4 Xc = cell_x[c];
-    for (int tb = 0; tb < ci.y; tb += 32 * TPL) {
-      double xi[TPL], yi[TPL], zi[TPL];  // target offset from its own leaf center
-      Kahan pot[TPL], ax[TPL], ay[TPL], az[TPL];
+// One warp's chunk of staged sources, as pairs of consecutive sources:
+//   A = (hx0, hx1, hy0, hy1), B = (hz0, hz1, q0, q1),
+//   C = (lx0, lx1, ly0, ly1), D = (lz0, lz1, -, -)
+// Four arrays rather than one array of 64-byte records, so that the G groups,
+// which read G consecutive pairs at once, hit distinct banks.
+struct Stage {
+  float4 A[kStagePairs], B[kStagePairs], C[kStagePairs], D[kStagePairs];
+};
+
+// x32[2i] = (hi of x - X_root, q), x32[2i+1] = (lo parts, 0), bodies in tree order.
+__global__ void k_abs32(const double4 *xt, long long n, const double4 *cell_x, float4 *x32) {
+  const double4 X0 = cell_x[0];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double4 b = xt[i];
+    const double dx = b.x - X0.x, dy = b.y - X0.y, dz = b.z - X0.z;
+    const float hx = (float)dx, hy = (float)dy, hz = (float)dz;
+    x32[2 * i] = make_float4(hx, hy, hz, (float)b.w);
+    x32[2 * i + 1] = make_float4((float)(dx - (double)hx), (float)(dy - (double)hy), (float)(dz - (double)hz), 0.f);
+  }
+}
+
+// (hi, lo) += s, with s split into two floats and the hi sum made exact by TwoSum.
+__device__ __forceinline__ void add_shift(float &hi, float &lo, double s) {
+  const float sh = (float)s, sl = (float)(s - (double)sh);
+  const float t = hi + sh;
+  const float bb = t - hi;
+  const float err = (hi - (t - bb)) + (sh - bb);
+  hi = t;
+  lo = (lo + err) + sl;
+}
+
+template <bool PERIODIC>
+__device__ __forceinline__ void stage_body(Stage &sm, int k, const float4 *x32, long long body, int img, double cycle) {
+  float4 h = x32[2 * body], l = x32[2 * body + 1];
+  if (PERIODIC && img != 13) {
+    add_shift(h.x, l.x, (double)(img / 9 - 1) * cycle);
+    add_shift(h.y, l.y, (double)((img / 3) % 3 - 1) * cycle);
+    add_shift(h.z, l.z, (double)(img % 3 - 1) * cycle);
+  }
+  const int p = k >> 1, o = k & 1;
+  float *A = reinterpret_cast<float *>(&sm.A[p]);
+  float *B = reinterpret_cast<float *>(&sm.B[p]);
+  float *C = reinterpret_cast<float *>(&sm.C[p]);
+  float *D = reinterpret_cast<float *>(&sm.D[p]);
+  A[o] = h.x;
+  A[2 + o] = h.y;
+  B[o] = h.z;
+  B[2 + o] = h.w;
+  C[o] = l.x;
+  C[2 + o] = l.y;
+  D[o] = l.z;
+}
+
+// Padding source: far away with zero charge, so it adds exactly zero.
+__device__ __forceinline__ void stage_dummy(Stage &sm, int k) {
+  const int p = k >> 1, o = k & 1;
+  float *A = reinterpret_cast<float *>(&sm.A[p]);
+  float *B = reinterpret_cast<float *>(&sm.B[p]);
+  float *C = reinterpret_cast<float *>(&sm.C[p]);
+  float *D = reinterpret_cast<float *>(&sm.D[p]);
+  A[o] = 1e18f;
+  A[2 + o] = 1e18f;
+  B[o] = 1e18f;
+  B[2 + o] = 0.f;
+  C[o] = 0.f;
+  C[2 + o] = 0.f;
+  D[o] = 0.f;
+}
+
+constexpr int kTPL = 2;  // targets per lane
+
+// Targets of one lane: t[u] = packed (hx, hy, hz, lx, ly, lz), each value in both halves.
+struct Targets {
+  f2p t[kTPL][6];
+};
+
+struct Sums {
+  Kahan k[kTPL][4];  // potential, gradient x, y, z
+};
+
+// One pair step: two staged sources (pair p) against the lane's targets.
+__device__ __forceinline__ void pair_step(const Stage &sm, int p, const Targets &T, f2p (&pp)[kTPL],
+                                          f2p (&px)[kTPL], f2p (&py)[kTPL], f2p (&pz)[kTPL]) {
+  const float4 A = sm.A[p], B = sm.B[p], C = sm.C[p], D = sm.D[p];
+  const f2p shx = pk2(A.x, A.y), shy = pk2(A.z, A.w), shz = pk2(B.x, B.y), w = pk2(B.z, B.w);
+  const f2p slx = pk2(C.x, C.y), sly = pk2(C.z, C.w), slz = pk2(D.x, D.y);
 #pragma unroll
-      for (int u = 0; u < TPL; u++) {
-        const int i = tb + lane + 32 * u;
-        float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h;
-        if (i < ci.y) {
-          h = x32[2 * (long long)(ci.x + i)];
-          l = x32[2 * (long long)(ci.x + i) + 1];
+  for (int u = 0; u < kTPL; u++) {
+    const f2p dx = add2(sub2(T.t[u][0], shx), sub2(T.t[u][3], slx));
+    const f2p dy = add2(sub2(T.t[u][1], shy), sub2(T.t[u][4], sly));
+    const f2p dz = add2(sub2(T.t[u][2], shz), sub2(T.t[u][5], slz));
+    const f2p r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
+    const float2 rr = unpk2(r2);
+    const float i0 = rr.x >= 1.17549435e-38f ? rsqrt_ftz(rr.x) : 0.f;
+    const float i1 = rr.y >= 1.17549435e-38f ? rsqrt_ftz(rr.y) : 0.f;
+    const f2p inv = pk2(i0, i1);
+    const f2p qr = mul2(w, inv);
+    const f2p qr3 = mul2(mul2(qr, inv), inv);
+    pp[u] = add2(pp[u], qr);
+    px[u] = fma2(dx, qr3, px[u]);
+    py[u] = fma2(dy, qr3, py[u]);
+    pz[u] = fma2(dz, qr3, pz[u]);
+  }
+}
+
+// Streams the bodies of the P2P list entries [qb, qe) through the warp and
+// accumulates their action on the lane's targets into `acc`.
+template <int S, bool PERIODIC>
+__device__ __forceinline__ void p2p_stream(Stage &sm, const int *src, const int4 *cell_b, const float4 *x32,
+                                           double cycle, int qb, int qe, const Targets &T, Sums &acc) {
+  constexpr int G = 32 / S, CH = 32 * G;
+  const int lane = threadIdx.x & 31, g = lane / S;
+  int q = qb, o = 0, qw = qb - 64;
+  int w_start = 0, w_size = 0, w_img = 13;
+  for (;;) {
+    // ---- fill one chunk (warp-uniform walk over the segments) ----
+    int filled = 0;
+    while (filled < CH && q < qe) {
+      if (q - qw >= 32) {  // next window of 32 segment descriptors, one per lane
+        qw = q;
+        const int qq = qw + lane;
+        w_start = 0;
+        w_size = 0;
+        w_img = 13;
+        if (qq < qe) {
+          const int packed = src[qq];
+          const int4 cb = cell_b[packed & 0x3ffffff];
+          w_start = cb.x;
+          w_size = cb.y;
+          w_img = packed >> 26;
         }
-        xi[u] = (double)h.x + (double)l.x;
-        yi[u] = (double)h.y + (double)l.y;
-        zi[u] = (double)h.z + (double)l.z;
       }
-      for (int q = b; q < e; q++) {
-        const int packed = src[q];
-        const int cj = packed & 0x3ffffff, img = packed >> 26;
-        const double4 Xj = cell_x[cj];
-        const double Dx = Xj.x + (double)(img / 9 - 1) * cycle - Xc.x;
-        const double Dy = Xj.y + (double)((img / 3) % 3 - 1) * cycle - Xc.y;
-        const double Dz = Xj.z + (double)(img % 3 - 1) * cycle - Xc.z;
-        const int4 cjb = cell_b[cj];
-        // target relative to the source leaf center, as hi + lo floats
-        float thx[TPL], thy[TPL], thz[TPL], tlx[TPL], tly[TPL], tlz[TPL];
-        float pp[TPL], px[TPL], py[TPL], pz[TPL];
-#pragma unroll
-        for (int u = 0; u < TPL; u++) {
-          const double tx = xi[u] - Dx, ty = yi[u] - Dy, tz = zi[u] - Dz;
-          thx[u] = (float)tx;
-          thy[u] = (float)ty;
-          thz[u] = (float)tz;
-          tlx[u] = (float)(tx - (double)thx[u]);
-          tly[u] = (float)(ty - (double)thy[u]);
-          tlz[u] = (float)(tz - (double)thz[u]);
-          pp[u] = px[u] = py[u] = pz[u] = 0.f;
-        }
-        for (int sb = 0; sb < cjb.y; sb += 32) {
-          const int ns = min(32, cjb.y - sb);
-          if (lane < ns) {
-            shi[warp][lane] = x32[2 * (long long)(cjb.x + sb + lane)];
-            slo[warp][lane] = x32[2 * (long long)(cjb.x + sb + lane) + 1];
-          }
-          __syncwarp();
-          for (int s = 0; s < ns; s++) {
-            const float4 sh = shi[warp][s], sl = slo[warp][s];
-#pragma unroll
-            for (int u = 0; u < TPL; u++) {
-              const float dx = (thx[u] - sh.x) + (tlx[u] - sl.x);
-              const float dy = (thy[u] - sh.y) + (tly[u] - sl.y);
-              const float dz = (thz[u] - sh.z) + (tlz[u] - sl.z);
-              const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-              const float inv = (r2 > 0.f) ? rsqrtf(r2) : 0.f;
-              const float qr = sh.w * inv;
-              const float qr3 = qr * inv * inv;
-              pp[u] += qr;
-              px[u] = fmaf(dx, qr3, px[u]);
-              py[u] = fmaf(dy, qr3, py[u]);
-              pz[u] = fmaf(dz, qr3, pz[u]);
-            }
-          }
-          __syncwarp();
-        }
-#pragma unroll
-        for (int u = 0; u < TPL; u++) {
-          pot[u].add(pp[u]);
-          ax[u].add(px[u]);
-          ay[u].add(py[u]);
-          az[u].add(pz[u]);
-        }
+      const int l = q - qw;
+      const int start = __shfl_sync(kFull, w_start, l);
+      const int size = __shfl_sync(kFull, w_size, l);
+      const int img = PERIODIC ? __shfl_sync(kFull, w_img, l) : 13;
+      const int m = min(CH - filled, size - o);
+      for (int k = lane; k < m; k += 32) stage_body<PERIODIC>(sm, filled + k, x32, (long long)start + o + k, img, cycle);
+      filled += m;
+      o += m;
+      if (o == size) {
+        q++;
+        o = 0;
       }
+    }
+    if (filled == 0) break;
+    const int steps = (filled + 2 * G - 1) / (2 * G);  // pair steps per group
+    const int padded = 2 * G * (steps + (steps & 1));   // even step count for the unrolled loop
+    for (int k = filled + lane; k < padded; k += 32) stage_dummy(sm, k);
+    __syncwarp();
+
+    // ---- evaluate: group g takes pairs g, g + G, g + 2G, ... ----
+    f2p pp[kTPL], px[kTPL], py[kTPL], pz[kTPL];
 #pragma unroll
-      for (int u = 0; u < TPL; u++) {
-        const int i = tb + lane + 32 * u;
-        if (i < ci.y) {
-          double4 r = trg[ci.x + i];
-          r.x += (double)pot[u].s - (double)pot[u].c;
-          r.y -= (double)ax[u].s - (double)ax[u].c;
-          r.z -= (double)ay[u].s - (double)ay[u].c;
-          r.w -= (double)az[u].s - (double)az[u].c;
-          trg[ci.x + i] = r;
-        }
+    for (int u = 0; u < kTPL; u++) pp[u] = px[u] = py[u] = pz[u] = 0ull;
+    for (int s = 0; s < steps; s += 2) {
+      pair_step(sm, g + G * s, T, pp, px, py, pz);
+      pair_step(sm, g + G * (s + 1), T, pp, px, py, pz);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < kTPL; u++) {
+      const float2 a = unpk2(pp[u]), bx = unpk2(px[u]), by = unpk2(py[u]), bz = unpk2(pz[u]);
+      acc.k[u][0].add(a.x + a.y);
+      acc.k[u][1].add(bx.x + bx.y);
+      acc.k[u][2].add(by.x + by.y);
+      acc.k[u][3].add(bz.x + bz.y);
+    }
+  }
+}
+
+template <int S, bool PERIODIC>
+__device__ __forceinline__ void p2p_leaf(Stage &sm, int4 cb, int b, int e, const int *src, const int4 *cell_b,
+                                         const float4 *x32, double4 *trg, double cycle) {
+  const int lane = threadIdx.x & 31, g = lane / S, j = lane % S;
+  for (int tb = 0; tb < cb.y; tb += S * kTPL) {
+    Targets T;
+#pragma unroll
+    for (int u = 0; u < kTPL; u++) {
+      const int i = tb + j + S * u;
+      float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h;
+      if (i < cb.y) {
+        h = x32[2 * ((long long)cb.x + i)];
+        l = x32[2 * ((long long)cb.x + i) + 1];
+      }
+      T.t[u][0] = pk2(h.x, h.x);
+      T.t[u][1] = pk2(h.y, h.y);
+      T.t[u][2] = pk2(h.z, h.z);
+      T.t[u][3] = pk2(l.x, l.x);
+      T.t[u][4] = pk2(l.y, l.y);
+      T.t[u][5] = pk2(l.z, l.z);
+    }
+    Sums acc;
+    p2p_stream<S, PERIODIC>(sm, src, cell_b, x32, cycle, b, e, T, acc);
+    // combine the groups (lanes j, j + S, j + 2S, ... hold the same targets) in FP64
+#pragma unroll
+    for (int u = 0; u < kTPL; u++) {
+      double v[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) v[k] = (double)acc.k[u][k].s - (double)acc.k[u][k].c;
+#pragma unroll
+      for (int off = S; off < 32; off <<= 1)
+#pragma unroll
+        for (int k = 0; k < 4; k++) v[k] += __shfl_xor_sync(kFull, v[k], off);
+      const int i = tb + j + S * u;
+      if (g == 0 && i < cb.y) {
+        double4 r = trg[cb.x + i];
+        r.x += v[0];
+        r.y -= v[1];
+        r.z -= v[2];
+        r.w -= v[3];
+        trg[cb.x + i] = r;
       }
     }
   }
 }
 
-int blocks_for(long long items) {
-  long long g = (items + kWarps - 1) / kWarps;
-  if (g > kNumSMs * 32) g = kNumSMs * 32;
-  return g < 1 ? 1 : (int)g;
+// One block of one warp per target cell: the hardware block scheduler hands
+// out cells as warps finish, which balances leaves of very different cost.
+template <bool PERIODIC>
+__global__ void __launch_bounds__(32, 16)
+k_p2p32(const int *off, const int *src, const int4 *cell_b, const float4 *x32, double4 *trg, double cycle) {
+  __shared__ Stage sm;
+  const long long c = blockIdx.x;
+  const int b = off[c], e = off[c + 1];
+  if (b == e) return;
+  const int4 cb = cell_b[c];
+  if (cb.y <= 8)
+    p2p_leaf<4, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
+  else if (cb.y <= 16)
+    p2p_leaf<8, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
+  else if (cb.y <= 32)
+    p2p_leaf<16, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
+  else
+    p2p_leaf<32, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
 }
 
 }  // namespace
 
 void rel_bodies32(const FmmArgs &a, float4 *x32) {
-  k_rel32<<<blocks_for(a.ncells), 32 * kWarps, 0, a.stream>>>(a.cell_b, a.cell_x, a.ncells, a.xt, x32);
+  if (a.n <= 0) return;
+  long long g = (a.n + 255) / 256;
+  if (g > kNumSMs * 16) g = kNumSMs * 16;
+  k_abs32<<<(int)g, 256, 0, a.stream>>>(a.xt, a.n, a.cell_x, x32);
   EXA_CHECK_LAUNCH();
 }
 
-void p2p_mixed(const FmmArgs &a, const float4 *x32) {
-  const int tpl = (a.ncrit + 31) / 32;
-  if (tpl <= 1)
-    k_p2p32<1><<<blocks_for(a.ncells), 32 * kWarps, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b,
-                                                                   a.cell_x, x32, a.trg64, a.cycle);
-  else if (tpl <= 2)
-    k_p2p32<2><<<blocks_for(a.ncells), 32 * kWarps, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b,
-                                                                   a.cell_x, x32, a.trg64, a.cycle);
+void p2p_mixed(const FmmArgs &a, const float4 *x32, bool periodic) {
+  if (a.ncells <= 0) return;
+  if (a.ncells > 0x7fffffffLL) throw std::runtime_error("p2p_mixed: too many cells for one launch");
+  const unsigned grid = (unsigned)a.ncells;
+  if (periodic)
+    k_p2p32<true><<<grid, 32, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.cell_b, x32, a.trg64, a.cycle);
   else
-    k_p2p32<4><<<blocks_for(a.ncells), 32 * kWarps, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b,
-                                                                   a.cell_x, x32, a.trg64, a.cycle);
+    k_p2p32<false><<<grid, 32, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.cell_b, x32, a.trg64, a.cycle);
   EXA_CHECK_LAUNCH();
 }
 
