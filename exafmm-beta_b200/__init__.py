@@ -90,6 +90,8 @@ def lib() -> ctypes.CDLL:
         "exafmm_launch_count": (_c_ll, []),
         "exafmm_set_params": (_c_int, [_vp, _c_int, _c_double, _c_int, _c_int, _c_int, _c_double]),
         "exafmm_set_mixed_policy": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int]),
+        "exafmm_get_dipole": (_c_int, [_vp, _vp, _vp]),
+        "exafmm_dipole_correction": (_c_int, [_vp, _vp, _c_ll]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -206,6 +208,20 @@ class Fmm:
 
     def results_device(self, ptr: int):
         self._check(lib().exafmm_get_results_device(self._h, _vp(ptr)))
+
+    # ---- periodic systems (include/up_down_pass.h:78-99) ----
+    def get_dipole(self, X0=None) -> np.ndarray:
+        """UpDownPass::getDipole: sum of (x_i - X0) q_i (X0 defaults to the origin)."""
+        d = np.zeros(3)
+        x0 = None if X0 is None else np.ascontiguousarray(X0, dtype=np.float64)
+        self._check(lib().exafmm_get_dipole(self._h, None if x0 is None else _p(x0), _p(d)))
+        return d
+
+    def dipole_correction(self, dipole, num_bodies=None):
+        """UpDownPass::dipoleCorrection on the results of the last solve."""
+        d = np.ascontiguousarray(dipole, dtype=np.float64)
+        nb = self.n if num_bodies is None else int(num_bodies)
+        self._check(lib().exafmm_dipole_correction(self._h, _p(d), nb))
 
     # ---- inspection ----
     def info(self) -> dict:

@@ -53,6 +53,8 @@ struct Engine {
   DBuf<double2> M, L;
   DBuf<unsigned char> Ms;  // scaled multipoles for the unrolled M2L (FP32 or FP64)
   DBuf<float4> x32;        // bodies as two-float pairs relative to the root center (mixed P2P)
+  DBuf<double2> lat;        // periodic lattice: supercell multipoles and warp partials
+  DBuf<double> dip;         // dipole reduction scratch and result
   DBuf<double4> trg, out;
   Timing tm;
   bool tree_ok = false, up_ok = false, lists_ok = false;
@@ -186,6 +188,10 @@ struct Engine {
       } else {
         m2l_fp64(a);
       }
+      if (C.prm.images > 1) {  // Traversal::traversePeriodic
+        lat.ensure(lattice_scratch_terms(C.prm.P));
+        lattice_fp64(a, C.prm.images, C.prm.theta, lat.p);
+      }
       EXA_CUDA(cudaEventRecord(tm.ev[5], C.stream));
       if (mixed && C.prm.mixed_p2p) {
         x32.ensure(2 * C.tree.n);  // hi and lo float4 per body
@@ -214,6 +220,21 @@ struct Engine {
   }
 
   void results(double *dst, cudaMemcpyKind kind);
+
+  void get_dipole(const double *X0, double *dipole3) {
+    const double zero[3] = {0.0, 0.0, 0.0};
+    dip.ensure(3 * 256 + 3);
+    dipole_fp64(C.tree.xyzq.p, C.tree.n, X0 ? X0 : zero, dip.p, dip.p + 3 * 256, C.stream);
+    EXA_CUDA(cudaMemcpyAsync(dipole3, dip.p + 3 * 256, 3 * sizeof(double), cudaMemcpyDeviceToHost, C.stream));
+    EXA_CUDA(cudaStreamSynchronize(C.stream));
+  }
+
+  void dipole_correction(const double *dipole3, long long num_bodies) {
+    if (!lists_ok) throw std::runtime_error("dipole correction before a solve");
+    if (num_bodies <= 0) throw std::runtime_error("dipole correction needs num_bodies > 0");
+    dipole_correction_fp64(C.tree.xyzq_tree.p, trg.p, C.tree.n, C.prm.cycle, dipole3, (double)num_bodies,
+                           C.stream);
+  }
 };
 
 namespace {
@@ -541,6 +562,20 @@ int exafmm_phase_times(exafmm_ctx *ctx, double *ms8) {
 }
 
 long long exafmm_launch_count(void) { return launch_count(); }
+
+int exafmm_get_dipole(exafmm_ctx *ctx, const double *X0, double *dipole3) {
+  return guarded(ctx, [&] {
+    if (!dipole3) throw std::runtime_error("null dipole output");
+    ctx->E.get_dipole(X0, dipole3);
+  });
+}
+
+int exafmm_dipole_correction(exafmm_ctx *ctx, const double *dipole3, long long num_bodies) {
+  return guarded(ctx, [&] {
+    if (!dipole3) throw std::runtime_error("null dipole");
+    ctx->E.dipole_correction(dipole3, num_bodies);
+  });
+}
 
 double exafmm_drift(double x, long long k, int up) { return up ? drift_up(x, k) : drift_down(x, k); }
 

@@ -46,6 +46,16 @@ void scale_multipoles(const FmmArgs &a, bool mixed, void *Ms);
 // <= max_dl are taken (the generic FP64 kernel handles the rest).
 bool m2l_fast(const FmmArgs &a, bool mixed, const void *Ms, int min_level = 0, int max_dl = 0);
 
+// Periodic lattice of root images (traversePeriodic), FP64, into L of the root.
+// scratch holds lattice_scratch_terms(P) complex values.
+long long lattice_scratch_terms(int P);
+void lattice_fp64(const FmmArgs &a, int images, double theta, double2 *scratch);
+// getDipole about X0 into out3 (device), scratch: 3 * 256 doubles.
+void dipole_fp64(const double4 *x, long long n, const double X0[3], double *scratch, double *out3, cudaStream_t st);
+// dipoleCorrection on results in tree order (xt: bodies in the same order).
+void dipole_correction_fp64(const double4 *xt, double4 *trg, long long n, double cycle, const double dip[3],
+                            double nbodies, cudaStream_t st);
+
 // Mixed-precision P2P (p2p32.cu): bodies as two-float pairs relative to the
 // root center; periodic selects the form that tests every pair for r = 0.
 void rel_bodies32(const FmmArgs &a, float4 *x32);

@@ -1,5 +1,7 @@
 // FP64 expansion operators: P2M, M2M, M2L, L2L, L2P, P2P (kernels/laplace.h:150-388),
 // one warp per cell, in the conventions of harmonics.cuh.
+#include <algorithm>
+
 #include "fmm.h"
 #include "harmonics.cuh"
 
@@ -85,6 +87,37 @@ __global__ void k_p2m(DevTables t, const int4 *cell_b, const double4 *cell_x, co
 }
 
 // ---------------------------------------------------------------- M2M
+// One child's contribution to the lane's parent coefficients (laplace.h:254-290):
+// Y = regular harmonics of X_parent - X_child, Mc = the child's multipole.
+template <int MAXO>
+__device__ __forceinline__ void m2m_accumulate(const DevTables &t, const int (&oj)[MAXO], const int (&ok)[MAXO],
+                                               const double2 *Y, const double2 *Mc, double2 (&acc)[MAXO]) {
+#pragma unroll
+  for (int u = 0; u < MAXO; u++) {
+    const int j = oj[u], k = ok[u];
+    if (j < 0) continue;
+    double2 a = acc[u];
+    const double ajk = t.anm[tri(j) + k];
+    for (int n = 0; n <= j; n++) {
+      for (int m = -n; m <= n; m++) {
+        const int km = k - m;
+        if (km > j - n || -km > j - n) continue;
+        const double w = t.anm[tri(n) + (m < 0 ? -m : m)] * t.anm[tri(j - n) + (km < 0 ? -km : km)] / ajk;
+        const double2 Z = m >= 0 ? Y[tri(n) + m] : cconj(Y[tri(n) - m]);
+        if (m < k) {
+          const double ph = (m < 0 && (m & 1)) ? -1.0 : 1.0;
+          const double2 src = Mc[tri(j - n) + km];
+          a = cfma(src, cscale(Z, ph * sgn_pow(n) * w), a);
+        } else {
+          const double2 src = cconj(Mc[tri(j - n) - km]);
+          a = cfma(src, cscale(Z, sgn_pow(k + n + m) * w), a);
+        }
+      }
+    }
+    acc[u] = a;
+  }
+}
+
 // Parent M from each child in child order (laplace.h:254-290), d = X_parent - X_child.
 template <int MAXO>
 __global__ void k_m2m(DevTables t, const long long *lvl, int level, const int *nd_cell, const int4 *cell_b,
@@ -116,30 +149,7 @@ __global__ void k_m2m(DevTables t, const long long *lvl, int level, const int *n
       if (lane < P) regular_column(t, lane, P, dx, dy, dz, true, Y);
       for (int o = lane; o < NT; o += 32) Mc[o] = M[(long long)ch * NT + o];
       __syncwarp();
-#pragma unroll
-      for (int u = 0; u < MAXO; u++) {
-        const int j = oj[u], k = ok[u];
-        if (j < 0) continue;
-        double2 a = acc[u];
-        const double ajk = t.anm[tri(j) + k];
-        for (int n = 0; n <= j; n++) {
-          for (int m = -n; m <= n; m++) {
-            const int km = k - m;
-            if (km > j - n || -km > j - n) continue;
-            const double w = t.anm[tri(n) + (m < 0 ? -m : m)] * t.anm[tri(j - n) + (km < 0 ? -km : km)] / ajk;
-            const double2 Z = m >= 0 ? Y[tri(n) + m] : cconj(Y[tri(n) - m]);
-            if (m < k) {
-              const double ph = (m < 0 && (m & 1)) ? -1.0 : 1.0;
-              const double2 src = Mc[tri(j - n) + km];
-              a = cfma(src, cscale(Z, ph * sgn_pow(n) * w), a);
-            } else {
-              const double2 src = cconj(Mc[tri(j - n) - km]);
-              a = cfma(src, cscale(Z, sgn_pow(k + n + m) * w), a);
-            }
-          }
-        }
-        acc[u] = a;
-      }
+      m2m_accumulate<MAXO>(t, oj, ok, Y, Mc, acc);
       __syncwarp();
     }
 #pragma unroll
@@ -151,6 +161,31 @@ __global__ void k_m2m(DevTables t, const long long *lvl, int level, const int *n
 }
 
 // ---------------------------------------------------------------- M2L
+// One source's contribution to the lane's target coefficients: Mp = A M of the
+// source, S = singular harmonics of d over A (singular_column with t.ainv).
+template <int MAXO>
+__device__ __forceinline__ void m2l_accumulate(const DevTables &t, const int (&oj)[MAXO], const int (&ok)[MAXO],
+                                               const double2 *Mp, const double2 *S, double2 (&acc)[MAXO]) {
+  const int P = t.P;
+#pragma unroll
+  for (int u = 0; u < MAXO; u++) {
+    const int j = oj[u], k = ok[u];
+    if (j < 0) continue;
+    double2 a = acc[u];
+    for (int n = 0; n < P; n++) {
+      const int p = j + n;
+      for (int m = -n; m <= n; m++) {
+        const double2 Mv = m >= 0 ? Mp[tri(n) + m] : cconj(Mp[tri(n) - m]);
+        const int qq = m - k;
+        const double2 Sv = qq >= 0 ? S[tri(p) + qq] : cconj(S[tri(p) - qq]);
+        const double s = (m < 0) ? 1.0 : (m <= k ? (double)sgn_pow(m) : (double)sgn_pow(k));
+        a = cfma(cscale(Mv, s), Sv, a);
+      }
+    }
+    acc[u] = a;
+  }
+}
+
 // L_j^k += (-1)^j A_j^k sum_{n,m} s(k,m) (A_n^m M_n^m) (Y2_{j+n}^{m-k} / A_{j+n}^{m-k})
 // which is the reference's Cnm product (laplace.h:137-147, 292-322) with the
 // sign s = +1 (m < 0), (-1)^m (0 <= m <= k), (-1)^k (m > k).
@@ -193,23 +228,7 @@ __global__ void k_m2l(DevTables t, const int *off, const int *src, long long nce
       for (int o = lane; o < NT; o += 32) Mp[o] = cscale(M[(long long)cj * NT + o], t.anm[o]);
       if (lane < 2 * P - 1) singular_column(t, lane, 2 * P - 1, dx, dy, dz, t.ainv, S);
       __syncwarp();
-#pragma unroll
-      for (int u = 0; u < MAXO; u++) {
-        const int j = oj[u], k = ok[u];
-        if (j < 0) continue;
-        double2 a = acc[u];
-        for (int n = 0; n < P; n++) {
-          const int p = j + n;
-          for (int m = -n; m <= n; m++) {
-            const double2 Mv = m >= 0 ? Mp[tri(n) + m] : cconj(Mp[tri(n) - m]);
-            const int qq = m - k;
-            const double2 Sv = qq >= 0 ? S[tri(p) + qq] : cconj(S[tri(p) - qq]);
-            const double s = (m < 0) ? 1.0 : (m <= k ? (double)sgn_pow(m) : (double)sgn_pow(k));
-            a = cfma(cscale(Mv, s), Sv, a);
-          }
-        }
-        acc[u] = a;
-      }
+      m2l_accumulate<MAXO>(t, oj, ok, Mp, S, acc);
       __syncwarp();
     }
 #pragma unroll
@@ -424,6 +443,162 @@ __global__ void k_p2p(const int *off, const int *src, long long ncells, const in
   }
 }
 
+// ---------------------------------------------------------------- periodic lattice
+// Traversal::traversePeriodic (traversal.h:233-287).  The root multipole is
+// replicated over a supercell of nb^3 copies (nb = 2 prange + 1).  Each lattice
+// level adds, into the root's local expansion, the M2L from every copy in the
+// nb^3 - 1 neighboring supercells; then the supercell's multipole is formed by
+// M2M of its nb^3 - 1 shifted copies onto the center, and the lattice spacing
+// grows by nb.  Root-level work: FP64 in every precision mode.  The warps write
+// partial sums that k_part_sum adds in a fixed order.
+
+__device__ __forceinline__ void lattice_index(int idx, int nb, int prange, int &x, int &y, int &z) {
+  x = idx / (nb * nb) - prange;
+  y = (idx / nb) % nb - prange;
+  z = idx % nb - prange;
+}
+
+template <int MAXO>
+__global__ void k_lattice_m2l(DevTables t, const double2 *Msup, double cycle, int prange, double2 *part) {
+  extern __shared__ double2 sh[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int P = t.P, NT = t.nterm, NS = tri(2 * P - 1);
+  double2 *Mp = sh + warp * (NT + NS);
+  double2 *S = Mp + NT;
+  const int nb = 2 * prange + 1, n3 = nb * nb * nb;
+  const long long nshift = (long long)(n3 - 1) * n3;
+  const long long gw = (long long)blockIdx.x * kWarpsPerBlock + warp, nw = (long long)gridDim.x * kWarpsPerBlock;
+  int oj[MAXO], ok[MAXO];
+  double2 acc[MAXO];
+#pragma unroll
+  for (int u = 0; u < MAXO; u++) {
+    const int o = lane + 32 * u;
+    if (o < NT) tri_decode(o, oj[u], ok[u]);
+    else oj[u] = ok[u] = -1;
+    acc[u] = make_double2(0.0, 0.0);
+  }
+  for (int o = lane; o < NT; o += 32) Mp[o] = cscale(Msup[o], t.anm[o]);
+  __syncwarp();
+  for (long long s = gw; s < nshift; s += nw) {
+    int im = (int)(s / n3);
+    const int cl = (int)(s - (long long)im * n3);
+    if (im >= (n3 - 1) / 2) im++;  // the central supercell is not an image
+    int ix, iy, iz, cx, cy, cz;
+    lattice_index(im, nb, prange, ix, iy, iz);
+    lattice_index(cl, nb, prange, cx, cy, cz);
+    // d = X_root - X_root - Xperiodic
+    const double dx = -(double)(ix * nb + cx) * cycle, dy = -(double)(iy * nb + cy) * cycle,
+                 dz = -(double)(iz * nb + cz) * cycle;
+    if (lane < 2 * P - 1) singular_column(t, lane, 2 * P - 1, dx, dy, dz, t.ainv, S);
+    __syncwarp();
+    m2l_accumulate<MAXO>(t, oj, ok, Mp, S, acc);
+    __syncwarp();
+  }
+#pragma unroll
+  for (int u = 0; u < MAXO; u++) {
+    const int j = oj[u], k = ok[u];
+    if (j < 0) continue;
+    const int o = tri(j) + k;
+    part[gw * NT + o] = cscale(acc[u], sgn_pow(j) * t.anm[o]);
+  }
+}
+
+template <int MAXO>
+__global__ void k_lattice_m2m(DevTables t, const double2 *Msup, double cycle, int prange, double2 *part) {
+  extern __shared__ double2 sh[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int P = t.P, NT = t.nterm;
+  double2 *Y = sh + warp * 2 * NT;
+  double2 *Mc = Y + NT;
+  const int nb = 2 * prange + 1, n3 = nb * nb * nb;
+  const long long gw = (long long)blockIdx.x * kWarpsPerBlock + warp, nw = (long long)gridDim.x * kWarpsPerBlock;
+  int oj[MAXO], ok[MAXO];
+  double2 acc[MAXO];
+#pragma unroll
+  for (int u = 0; u < MAXO; u++) {
+    const int o = lane + 32 * u;
+    if (o < NT) tri_decode(o, oj[u], ok[u]);
+    else oj[u] = ok[u] = -1;
+    acc[u] = make_double2(0.0, 0.0);
+  }
+  for (int o = lane; o < NT; o += 32) Mc[o] = Msup[o];
+  __syncwarp();
+  for (long long s = gw; s < n3 - 1; s += nw) {
+    int im = (int)s;
+    if (im >= (n3 - 1) / 2) im++;
+    int ix, iy, iz;
+    lattice_index(im, nb, prange, ix, iy, iz);
+    // d = X_parent - X_child = -(i * cycle)
+    if (lane < P)
+      regular_column(t, lane, P, -(double)ix * cycle, -(double)iy * cycle, -(double)iz * cycle, true, Y);
+    __syncwarp();
+    m2m_accumulate<MAXO>(t, oj, ok, Y, Mc, acc);
+    __syncwarp();
+  }
+#pragma unroll
+  for (int u = 0; u < MAXO; u++) {
+    const int o = lane + 32 * u;
+    if (o < NT) part[gw * NT + o] = acc[u];
+  }
+}
+
+// out[o] = (base ? base[o] : out[o]) + sum_w part[w][o], w in order.
+__global__ void k_part_sum(const double2 *part, int nparts, int NT, const double2 *base, double2 *out) {
+  for (int o = threadIdx.x; o < NT; o += blockDim.x) {
+    double2 v = base ? base[o] : out[o];
+    for (int w = 0; w < nparts; w++) v = cadd(v, part[(long long)w * NT + o]);
+    out[o] = v;
+  }
+}
+
+// ---------------------------------------------------------------- dipole
+// UpDownPass::getDipole (up_down_pass.h:78-86): sum_i (x_i - X0) q_i in FP64.
+constexpr int kDipoleBlocks = 256;
+
+__global__ void k_dipole_part(const double4 *x, long long n, double X0x, double X0y, double X0z, double *part) {
+  __shared__ double sh[3][256 / 32];
+  double a[3] = {0.0, 0.0, 0.0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double4 b = x[i];
+    a[0] += (b.x - X0x) * b.w;
+    a[1] += (b.y - X0y) * b.w;
+    a[2] += (b.z - X0z) * b.w;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int d = 0; d < 3; d++) {
+    const double v = warp_sum(a[d]);
+    if (lane == 0) sh[d][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x / 32); w++) v += sh[threadIdx.x][w];
+    part[blockIdx.x * 3 + threadIdx.x] = v;
+  }
+}
+
+__global__ void k_dipole_final(const double *part, int nparts, double *out) {
+  if (threadIdx.x < 3) {
+    double v = 0.0;
+    for (int b = 0; b < nparts; b++) v += part[b * 3 + threadIdx.x];
+    out[threadIdx.x] = v;
+  }
+}
+
+// UpDownPass::dipoleCorrection (up_down_pass.h:89-99), on results in tree order.
+__global__ void k_dipole_apply(const double4 *xt, double4 *trg, long long n, double coef, double dx, double dy,
+                               double dz, double nbodies) {
+  const double nd = dx * dx + dy * dy + dz * dz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    double4 r = trg[i];
+    r.x -= coef * nd / nbodies / xt[i].w;
+    r.y -= coef * dx;
+    r.z -= coef * dy;
+    r.w -= coef * dz;
+    trg[i] = r;
+  }
+}
+
 int maxo_for(int P) { return (tri(P) + 31) / 32; }
 
 template <template <int> class K>
@@ -516,6 +691,61 @@ void p2p_fp64(const FmmArgs &a) {
   else
     k_p2p<4><<<blocks_for(a.ncells), 32 * kWarpsPerBlock, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b,
                                                                           a.xt, a.trg64, a.cycle);
+  EXA_CHECK_LAUNCH();
+}
+
+long long lattice_scratch_terms(int P) {
+  return (long long)kNumSMs * 4 * kWarpsPerBlock * tri(P) + 2LL * tri(P);
+}
+
+void lattice_fp64(const FmmArgs &a, int images, double theta, double2 *scratch) {
+  if (images <= 1 || a.ncells <= 0) return;
+  const DevTables &t = device_tables(a.P);
+  const int NT = t.nterm;
+  const int prange = (int)(0.5 / theta + 1);
+  const int nb = 2 * prange + 1;
+  double2 *msup[2] = {scratch, scratch + NT};
+  double2 *part = scratch + 2 * NT;
+  EXA_CUDA(cudaMemcpyAsync(msup[0], a.M64, NT * sizeof(double2), cudaMemcpyDeviceToDevice, a.stream));
+  const int grid_l = kNumSMs * 4;
+  const int grid_m = std::min((nb * nb * nb - 1 + kWarpsPerBlock - 1) / kWarpsPerBlock, grid_l);
+  double cycle = a.cycle;
+  for (int level = 0; level < images - 1; level++) {
+    double2 *cur = msup[level & 1], *nxt = msup[(level + 1) & 1];
+    EXA_MAXO_SWITCH(maxo_for(a.P), {
+      const size_t smem = kWarpsPerBlock * (NT + tri(2 * a.P - 1)) * sizeof(double2);
+      set_smem(k_lattice_m2l<MO>, smem);
+      k_lattice_m2l<MO><<<grid_l, 32 * kWarpsPerBlock, smem, a.stream>>>(t, cur, cycle, prange, part);
+    });
+    EXA_CHECK_LAUNCH();
+    k_part_sum<<<1, 64, 0, a.stream>>>(part, grid_l * kWarpsPerBlock, NT, nullptr, a.L64);
+    EXA_CHECK_LAUNCH();
+    EXA_MAXO_SWITCH(maxo_for(a.P), {
+      const size_t smem = kWarpsPerBlock * 2 * NT * sizeof(double2);
+      set_smem(k_lattice_m2m<MO>, smem);
+      k_lattice_m2m<MO><<<grid_m, 32 * kWarpsPerBlock, smem, a.stream>>>(t, cur, cycle, prange, part);
+    });
+    EXA_CHECK_LAUNCH();
+    k_part_sum<<<1, 64, 0, a.stream>>>(part, grid_m * kWarpsPerBlock, NT, cur, nxt);
+    EXA_CHECK_LAUNCH();
+    cycle *= nb;
+  }
+}
+
+void dipole_fp64(const double4 *x, long long n, const double X0[3], double *scratch, double *out3, cudaStream_t st) {
+  k_dipole_part<<<kDipoleBlocks, 256, 0, st>>>(x, n, X0[0], X0[1], X0[2], scratch);
+  EXA_CHECK_LAUNCH();
+  k_dipole_final<<<1, 32, 0, st>>>(scratch, kDipoleBlocks, out3);
+  EXA_CHECK_LAUNCH();
+}
+
+void dipole_correction_fp64(const double4 *xt, double4 *trg, long long n, double cycle, const double dip[3],
+                            double nbodies, cudaStream_t st) {
+  if (n <= 0) return;
+  const double coef = 4 * M_PI / (3 * cycle * cycle * cycle);
+  long long g = (n + 255) / 256;
+  if (g > kNumSMs * 16) g = kNumSMs * 16;
+  k_dipole_apply<<<(int)g, 256, 0, st>>>(xt, trg, n, coef, dip[0], dip[1], dip[2], nbodies);
   EXA_CHECK_LAUNCH();
 }
 

@@ -77,7 +77,9 @@ int exafmm_upward(exafmm_ctx *ctx);
 
 /* Traversal::traverse(cells, cells, cycle, dual) (include/traversal.h:326-352):
  * builds the M2L/P2P lists and evaluates them; clears the results first, as
- * Dataset::initTarget does before a solve. */
+ * Dataset::initTarget does before a solve.  With images > 0 the lists cover the
+ * 27 nearest images of the root, and images > 1 adds the lattice of
+ * Traversal::traversePeriodic (include/traversal.h:233-287) in FP64. */
 int exafmm_traverse(exafmm_ctx *ctx);
 
 /* UpDownPass::downwardPass (include/up_down_pass.h:63-75). */
@@ -85,6 +87,16 @@ int exafmm_downward(exafmm_ctx *ctx);
 
 /* Bounds + build + upward + traverse + downward, the examples/fmm.cxx:163-179 loop body. */
 int exafmm_solve(exafmm_ctx *ctx);
+
+/* UpDownPass::getDipole(bodies, X0) (include/up_down_pass.h:78-86): sum of
+ * (x_i - X0) q_i over the context's bodies, FP64 on the device.  X0 == NULL is
+ * the origin. */
+int exafmm_get_dipole(exafmm_ctx *ctx, const double *X0, double *dipole3);
+/* UpDownPass::dipoleCorrection(bodies, dipole, numBodies, cycle)
+ * (include/up_down_pass.h:89-99) applied to the results of the last solve:
+ * pot -= 4 pi / (3 cycle^3) |dipole|^2 / numBodies / q_i, grad -= 4 pi / (3 cycle^3) dipole.
+ * As in the reference, a zero charge makes its potential non-finite. */
+int exafmm_dipole_correction(exafmm_ctx *ctx, const double *dipole3, long long num_bodies);
 
 /* Results (Body::TRG scattered back by IBODY).  The _device form writes n x 4
  * doubles to a device pointer. */

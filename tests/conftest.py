@@ -57,7 +57,13 @@ def reference():
 
 
 def golden_cases():
-    return sorted(p for p in glob.glob(os.path.join(GOLDEN, "*.npz")) if not p.endswith("kernel_kat.npz"))
+    """Free-space solve fixtures (periodic ones and the operator chain are separate)."""
+    return sorted(p for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
+                  if not p.endswith("kernel_kat.npz") and not os.path.basename(p).startswith("periodic_"))
+
+
+def periodic_golden_cases():
+    return sorted(glob.glob(os.path.join(GOLDEN, "periodic_*.npz")))
 
 
 def load_golden(path):

@@ -79,11 +79,39 @@ def make_kat(ref: Reference):
     print("kernel_kat: P in (4, 8, 10, 14)")
 
 
+# Periodic systems (Traversal::traverse with images, traversePeriodic and
+# UpDownPass::dipoleCorrection): bodies in the reference's box [-pi, pi]^3,
+# cycle 2 pi.  (name, generator, n, seed, P, theta, ncrit, nspawn, images)
+PERIODIC_CASES = [
+    ("periodic_cube_n600_p6_images2", "cube", 600, 21, 6, 0.4, 16, 5000, 2),
+    ("periodic_cube_n800_p8_images3", "cube", 800, 22, 8, 0.4, 32, 5000, 3),
+]
+
+
+def make_periodic_case(ref: Reference, name, gen, n, seed, P, theta, ncrit, nspawn, images):
+    x = getattr(datasets, gen)(n, seed)
+    x[:, :3] *= np.pi
+    cycle = 2 * np.pi
+    run = ref.solve(x, P=P, theta=theta, ncrit=ncrit, nspawn=nspawn, images=images, cycle=cycle, threads=1,
+                    record_lists=True, dipole_correction=True)
+    nc = len(run.cells_int)
+    # the log also holds traversePeriodic's M2Ls from temporary cells outside the tree
+    lattice = (run.m2l[:, 1] >= nc) | (run.m2l[:, 1] < 0)
+    data = dict(xyzq=x, params=np.array([P, theta, ncrit, nspawn, images, cycle], dtype=np.float64),
+                bounds=run.bounds, perm=run.perm, cells_int=run.cells_int, cells_real=run.cells_real,
+                m2l=sorted_pairs(run.m2l[~lattice]), p2p=sorted_pairs(run.p2p), trg=run.trg,
+                n_lattice=np.array([lattice.sum()]))
+    np.savez_compressed(os.path.join(OUT, name + ".npz"), **data)
+    print(f"{name}: cells={nc} m2l={len(data['m2l'])} (+{lattice.sum()} lattice) p2p={len(run.p2p)}")
+
+
 def main():
     build(reference=True)
     ref = Reference()
     for c in CASES:
         make_case(ref, *c)
+    for c in PERIODIC_CASES:
+        make_periodic_case(ref, *c)
     make_kat(ref)
 
 

@@ -6,7 +6,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import golden_cases, load_golden, pair_set, rel_l2, GOLDEN
+from conftest import golden_cases, load_golden, pair_set, periodic_golden_cases, rel_l2, GOLDEN
 
 
 def _sorted(p):
@@ -107,3 +107,18 @@ def test_oracle_drift_is_stepwise(oracle, x, k, up):
         assert oracle.drift_seq(x, k, up) == v
     else:
         assert abs(oracle.drift_seq(x, k, up) - (x + (k * step if up else -k * step))) < 1e-6
+
+
+@pytest.mark.parametrize("path", periodic_golden_cases(), ids=lambda p: os.path.basename(p)[:-4])
+def test_oracle_periodic_matches_golden(oracle, path):
+    """The C restatement against the reference's periodic fixtures (near images,
+    lattice and dipole correction)."""
+    g = load_golden(path)
+    P, theta, ncrit, nspawn, images, cycle = g["params"]
+    r = oracle.solve(g["xyzq"], P=int(P), theta=float(theta), ncrit=int(ncrit), nspawn=int(nspawn),
+                     images=int(images), cycle=float(cycle), dipole_correction=True)
+    assert np.array_equal(r.bounds, g["bounds"])
+    assert np.array_equal(r.cells_int, g["cells_int"])
+    assert np.array_equal(_sorted(r.m2l), g["m2l"])
+    assert np.array_equal(_sorted(r.p2p), g["p2p"])
+    assert rel_l2(r.trg, g["trg"]) < 1e-11
