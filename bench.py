@@ -184,7 +184,13 @@ def main():
     ap.add_argument("--ncrit", type=int, default=0, help="0: pick the fastest of 32, 64, 128 during warm-up")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain-method comparison run")
+    ap.add_argument("--workload", default="solve", choices=["solve", "batch", "serve"],
+                    help="solve: the single large solve (default); batch: 512 independent systems per step; "
+                         "serve: Poisson request trace through the request server")
+    ap.add_argument("--workers", type=int, default=16, help="contexts (streams) of the batch / serve runtime")
     args = ap.parse_args()
+    if args.workload != "solve":
+        return run_runtime_workload(args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -373,6 +379,201 @@ def main():
     fmm.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------- batched and served workloads
+BATCH = dict(name="batch_512_p10", count=512, lo=2000, hi=200_000, P=10, theta=0.4, ncrit=64, nspawn=5000)
+SERVE = dict(name="serve_poisson_p6_8_10", count=60, lo=1000, hi=1_000_000, theta=0.4, ncrit=64, nspawn=5000,
+             budget=150e9, repeat_frac=0.2, repeat_steps=50, loads=(0.5, 0.8))
+
+
+def _three_way(ex, datasets, xs, mixed, plain, sample=256, take=8):
+    """rel-L2 (pot, acc) of mixed vs direct, plain vs direct, mixed vs plain on `take`
+    systems spread over the sizes, each on `sample` strided targets."""
+    order = np.argsort([len(x) for x in xs])
+    pick = order[np.linspace(0, len(xs) - 1, min(take, len(xs))).astype(int)]
+    acc = {k: [] for k in ("mixed_vs_direct", "plain_vs_direct", "mixed_vs_plain")}
+    for i in pick:
+        x = xs[i]
+        idx = datasets.strided_sample(len(x), sample)
+        d = ex.direct(x[idx], x)
+        for key, a, b in (("mixed_vs_direct", mixed[i][idx], d), ("plain_vs_direct", plain[i][idx], d),
+                          ("mixed_vs_plain", mixed[i], plain[i])):
+            acc[key].append((datasets.rel_l2(a[:, 0], b[:, 0]), datasets.rel_l2(a[:, 1:], b[:, 1:])))
+    return {k: {"pot_max": max(v[0] for v in vals), "acc_max": max(v[1] for v in vals)} for k, vals in acc.items()}
+
+
+def _batch_cpu_baseline(xs, threads):
+    """The reference CPU FMM on a bounded sample of the systems (about 10 s)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import bindings
+    if not bindings.reference_available():
+        return None
+    ref = bindings.Reference()
+    kw = dict(P=BATCH["P"], theta=BATCH["theta"], ncrit=BATCH["ncrit"], nspawn=BATCH["nspawn"])
+    order = np.argsort([len(x) for x in xs])
+    pick = order[np.linspace(0, len(xs) - 1, 6).astype(int)]
+    t0 = time.perf_counter()
+    bodies = 0
+    for i in pick:
+        ref.solve(xs[i], threads=threads, record_lists=False, **kw)
+        bodies += len(xs[i])
+    dt = time.perf_counter() - t0
+    return {"value": bodies / dt, "unit": "bodies/s", "cores": threads, "kind": "reference",
+            "sample": f"{len(pick)} of the systems ({bodies} bodies, smallest to largest), one after another, "
+                      f"each with all host threads ({dt:.1f} s)"}
+
+
+def run_runtime_workload(args):
+    import torch
+    pkg = _package()
+    pkg.build()
+    from exafmm_b200 import datasets, workloads
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    prec = pkg.FP64 if args.precision == "fp64" else pkg.MIXED
+    if args.workload == "batch":
+        line = _run_batch(args, pkg, datasets, workloads, prec, rank, world, local_rank)
+    else:
+        line = _run_serve(args, pkg, datasets, workloads, prec, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        if args.workload == "batch":  # whole-job bodies/s over the slowest rank's time
+            t = torch.tensor([line["_time"]], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            line["value"] = line["_units"] * world / float(t.item())
+        else:  # latency: the worst rank's p99
+            t = torch.tensor([line["value"]], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            line["value"] = float(t.item())
+        dist.barrier()
+        dist.destroy_process_group()
+    line.pop("_time")
+    line.pop("_units")
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def _run_batch(args, pkg, datasets, workloads, prec, rank, world, local_rank):
+    import torch
+    cfg = BATCH
+    xs = workloads.batch_systems(cfg["count"], cfg["lo"], cfg["hi"], seed0=1000 + 100000 * rank)
+    nbodies = sum(len(x) for x in xs)
+    outs = [np.zeros((len(x), 4)) for x in xs]
+    b = pkg.Batch(P=cfg["P"], theta=cfg["theta"], ncrit=cfg["ncrit"], nspawn=cfg["nspawn"], precision=prec,
+                  device=local_rank, workers=args.workers)
+    b.autotune(True)   # the first warm-up step tunes ncrit per size class, then the table is frozen
+    for w in range(max(1, args.warmup)):
+        b.solve(xs, outs)
+        if w == 0:
+            b.autotune(False)
+    torch.cuda.synchronize()
+    launches0 = pkg.launch_count()
+    with ClockSampler(local_rank) as clocks:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            b.solve(xs, outs)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+    clk = clocks.summary()
+    launches = pkg.launch_count() - launches0
+    dev_ms = float(b.times(len(xs)).sum())
+    line = {
+        "metric": "batched FMM bodies/s (512 systems per step, N log-uniform [2e3, 2e5], P=10, theta=0.4)",
+        "value": nbodies * args.steps / dt, "unit": "bodies/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if prec == pkg.FP64 else "f32+kahan", "data": "synthetic",
+        "config": {"workload": cfg["name"], "systems": cfg["count"], "bodies_per_step": nbodies,
+                   "distribution": "even systems uniform in [-1,1]^3, odd on the unit sphere; q U[-1,1]",
+                   "P": cfg["P"], "theta": cfg["theta"], "ncrit_table": b.ncrit_table(), "workers": args.workers,
+                   "precision": args.precision, "parallelism": f"replicas{world}",
+                   "timing": "host wall clock around each batch call, device synchronized on both sides "
+                             "(host buffers in and out, so value is end to end)",
+                   "l2": "each step streams 0.7 GB of bodies in and results out (larger than L2)"},
+        "e2e": {"value": nbodies * args.steps / dt, "unit": "bodies/s", "h2d_bytes_per_step": nbodies * 32,
+                "d2h_bytes_per_step": nbodies * 32},
+        "device_ms_per_step": dev_ms, "concurrency": dev_ms / (1e3 * dt / args.steps),
+        "gpu_launches": int(launches), "clocks": clk, "roofline": None,
+        "_time": dt, "_units": nbodies * args.steps,
+    }
+    if not args.no_plain and prec == pkg.MIXED:
+        bp = pkg.Batch(P=cfg["P"], theta=cfg["theta"], ncrit=cfg["ncrit"], nspawn=cfg["nspawn"],
+                       precision=pkg.FP64, device=local_rank, workers=args.workers)
+        bp.autotune(True)
+        plain = [np.zeros((len(x), 4)) for x in xs]
+        bp.solve(xs, plain)
+        bp.autotune(False)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        bp.solve(xs, plain)
+        torch.cuda.synchronize()
+        tp = time.perf_counter() - t0
+        line["plain_fp64"] = {"value": nbodies / tp, "unit": "bodies/s", "ms_per_step": 1e3 * tp,
+                              "speedup_of_mixed": (nbodies * args.steps / dt) / (nbodies / tp),
+                              "rel_l2": _three_way(pkg, datasets, xs, outs, plain)}
+        bp.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = _batch_cpu_baseline(xs, os.cpu_count() or 1)
+        if cb:
+            line["cpu_baseline"] = cb
+    b.close()
+    return line
+
+
+def _run_serve(args, pkg, datasets, workloads, prec, rank, world, local_rank):
+    import torch
+    cfg = SERVE
+    srv = pkg.Server(device=local_rank, workers=args.workers, hbm_budget_bytes=cfg["budget"])
+    # warm-up: one request per order, then a saturated replay measures the service rate
+    for P in (6, 8, 10):
+        srv.wait(srv.submit(datasets.cube(20000, seed=P), P=P, theta=cfg["theta"], ncrit=cfg["ncrit"],
+                            precision=prec))
+    sat = workloads.make_trace(cfg["count"], rate=1e6, lo=cfg["lo"], hi=cfg["hi"], repeat_frac=cfg["repeat_frac"],
+                               repeat_steps=cfg["repeat_steps"], seed=4000 + 1000 * rank, theta=cfg["theta"])
+    launches0 = pkg.launch_count()
+    with ClockSampler(local_rank) as clocks:
+        done, wall = workloads.replay(srv, sat, precision=prec, ncrit=cfg["ncrit"], nspawn=cfg["nspawn"],
+                                      deadline_s=240.0)
+        capacity = len(sat.jobs) / wall  # jobs per second with everything queued at once
+        saturated = workloads.latency_summary(done, wall)
+        rates = {}
+        for load in cfg["loads"]:
+            tr = workloads.make_trace(cfg["count"], rate=load * capacity, lo=cfg["lo"], hi=cfg["hi"],
+                                      repeat_frac=cfg["repeat_frac"], repeat_steps=cfg["repeat_steps"],
+                                      seed=5000 + int(100 * load) + 1000 * rank, theta=cfg["theta"])
+            d, w = workloads.replay(srv, tr, precision=prec, ncrit=cfg["ncrit"], nspawn=cfg["nspawn"],
+                                    deadline_s=240.0)
+            rates[f"{load:.2f}"] = dict(workloads.latency_summary(d, w), rate_jobs_per_s=load * capacity)
+        torch.cuda.synchronize()
+    clk = clocks.summary()
+    launches = pkg.launch_count() - launches0
+    st = srv.stats()
+    srv.close()
+    top = rates[f"{max(cfg['loads']):.2f}"]
+    return {
+        "metric": "served p99 latency (Poisson arrivals at 0.8 of capacity; N log-uniform [1e3, 1e6], "
+                  "P in {6, 8, 10}, theta=0.4)",
+        "value": top["p99_ms"], "unit": "ms", "n_gpus": world, "steps": 1, "warmup": 1,
+        "ms_per_step": top["mean_ms"], "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if prec == pkg.FP64 else "f32+kahan", "data": "synthetic",
+        "config": {"workload": cfg["name"], "jobs_per_trace": cfg["count"], "repeat_fraction": cfg["repeat_frac"],
+                   "repeat_steps": cfg["repeat_steps"], "hbm_budget_bytes": cfg["budget"],
+                   "workers": args.workers, "precision": args.precision, "parallelism": f"replicas{world}",
+                   "timing": "host wall clock: scheduled arrival (or the previous chain step's return) to "
+                             "results in host memory",
+                   "l2": "requests stream their bodies in and results out"},
+        "saturated": saturated, "capacity_jobs_per_s": capacity, "loads": rates,
+        "server_stats": st,
+        "e2e": {"value": top["p99_ms"], "unit": "ms", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
+        "gpu_launches": int(launches), "clocks": clk, "roofline": None,
+        "_time": top["wall_s"], "_units": top["requests"],
+    }
 
 
 if __name__ == "__main__":

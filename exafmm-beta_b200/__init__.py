@@ -91,6 +91,23 @@ def lib() -> ctypes.CDLL:
         "exafmm_set_params": (_c_int, [_vp, _c_int, _c_double, _c_int, _c_int, _c_int, _c_double]),
         "exafmm_set_mixed_policy": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int]),
         "exafmm_get_dipole": (_c_int, [_vp, _vp, _vp]),
+        "exafmm_device_bytes": (_c_int, [_vp, ctypes.POINTER(_c_ll)]),
+        "exafmm_batch_create": (_c_int, [ctypes.POINTER(_vp), _c_int, _c_double, _c_int, _c_int, _c_int, _c_int,
+                                         _c_int]),
+        "exafmm_batch_destroy": (_c_int, [_vp]),
+        "exafmm_batch_error": (ctypes.c_char_p, [_vp]),
+        "exafmm_batch_solve": (_c_int, [_vp, _c_int, _vp, _vp, _vp]),
+        "exafmm_batch_times": (_c_int, [_vp, _vp]),
+        "exafmm_batch_autotune": (_c_int, [_vp, _c_int]),
+        "exafmm_batch_ncrit_table": (_c_int, [_vp, _vp, _c_int]),
+        "exafmm_server_create": (_c_int, [ctypes.POINTER(_vp), _c_int, _c_int, _c_double]),
+        "exafmm_server_destroy": (_c_int, [_vp]),
+        "exafmm_server_submit": (_c_int, [_vp, _vp, _c_ll, _vp, _c_int, _c_double, _c_int, _c_int, _c_int,
+                                          ctypes.POINTER(_c_ll)]),
+        "exafmm_server_poll": (_c_int, [_vp, _c_ll, ctypes.POINTER(_c_int)]),
+        "exafmm_server_wait": (_c_int, [_vp, _c_ll, _vp]),
+        "exafmm_server_stats": (_c_int, [_vp, _vp]),
+        "exafmm_server_error": (ctypes.c_char_p, []),
         "exafmm_dipole_correction": (_c_int, [_vp, _vp, _c_ll]),
     }
     for name, (res, args) in sig.items():
@@ -208,6 +225,11 @@ class Fmm:
 
     def results_device(self, ptr: int):
         self._check(lib().exafmm_get_results_device(self._h, _vp(ptr)))
+
+    def device_bytes(self) -> int:
+        v = _c_ll()
+        self._check(lib().exafmm_device_bytes(self._h, ctypes.byref(v)))
+        return int(v.value)
 
     # ---- periodic systems (include/up_down_pass.h:78-99) ----
     def get_dipole(self, X0=None) -> np.ndarray:
@@ -332,3 +354,102 @@ def drift(x: float, k: int, up: bool = False) -> float:
 def launch_count() -> int:
     """Kernels the engine has launched in this process."""
     return int(lib().exafmm_launch_count())
+
+
+class Batch:
+    """Many independent systems per call, on a pool of solve contexts (one host
+    thread and CUDA stream each)."""
+
+    def __init__(self, P=10, theta=0.4, ncrit=64, nspawn=5000, precision=FP64, device=-1, workers=8):
+        h = _vp()
+        rc = lib().exafmm_batch_create(ctypes.byref(h), P, theta, ncrit, nspawn, precision, device, workers)
+        if rc != 0:
+            raise FmmError(f"exafmm_batch_create failed ({rc})")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().exafmm_batch_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def autotune(self, enable: bool):
+        lib().exafmm_batch_autotune(self._h, int(enable))
+
+    def ncrit_table(self) -> dict:
+        buf = (_c_int * 128)()
+        k = lib().exafmm_batch_ncrit_table(self._h, buf, 64)
+        return {buf[2 * i]: buf[2 * i + 1] for i in range(k)}
+
+    def solve(self, systems, outs=None):
+        """systems: list of (n_i, 4) float64 arrays; returns the list of (n_i, 4) results."""
+        xs = [_f64(x, 4) for x in systems]
+        if outs is None:
+            outs = [np.zeros((len(x), 4)) for x in xs]
+        for o, x in zip(outs, xs):
+            assert o.dtype == np.float64 and o.shape == (len(x), 4) and o.flags.c_contiguous
+        k = len(xs)
+        n = (_c_ll * k)(*[len(x) for x in xs])
+        px = (_vp * k)(*[x.ctypes.data for x in xs])
+        po = (_vp * k)(*[o.ctypes.data for o in outs])
+        if lib().exafmm_batch_solve(self._h, k, n, px, po) != 0:
+            raise FmmError(lib().exafmm_batch_error(self._h).decode())
+        return outs
+
+    def times(self, count: int) -> np.ndarray:
+        t = np.zeros(count)
+        lib().exafmm_batch_times(self._h, _p(t))
+        return t
+
+
+class Server:
+    """Asynchronous request server with HBM-budget admission."""
+
+    def __init__(self, device=-1, workers=8, hbm_budget_bytes=150e9):
+        h = _vp()
+        rc = lib().exafmm_server_create(ctypes.byref(h), device, workers, float(hbm_budget_bytes))
+        if rc != 0:
+            raise FmmError(f"exafmm_server_create failed ({rc})")
+        self._h = h
+        self._live = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().exafmm_server_destroy(self._h)
+            self._h = None
+            self._live.clear()
+
+    __del__ = close
+
+    def submit(self, xyzq, P=10, theta=0.4, ncrit=64, nspawn=5000, precision=FP64, out=None) -> int:
+        x = _f64(xyzq, 4)
+        o = np.zeros((len(x), 4)) if out is None else out
+        assert o.dtype == np.float64 and o.shape == (len(x), 4) and o.flags.c_contiguous
+        t = _c_ll()
+        rc = lib().exafmm_server_submit(self._h, _p(x), len(x), _p(o), P, theta, ncrit, nspawn, precision,
+                                        ctypes.byref(t))
+        if rc != 0:
+            raise FmmError(f"exafmm_server_submit failed ({rc})")
+        self._live[t.value] = (x, o)   # both must outlive the request
+        return t.value
+
+    def done(self, ticket: int) -> bool:
+        d = _c_int()
+        lib().exafmm_server_poll(self._h, ticket, ctypes.byref(d))
+        return bool(d.value)
+
+    def wait(self, ticket: int):
+        """(results, times) with times = (queue ms, start-to-results ms, submit-to-results ms, device ms)."""
+        t = np.zeros(4)
+        rc = lib().exafmm_server_wait(self._h, ticket, _p(t))
+        x, o = self._live.pop(ticket)
+        if rc != 0:
+            raise FmmError(lib().exafmm_server_error().decode())
+        return o, t
+
+    def stats(self) -> dict:
+        v = np.zeros(6)
+        lib().exafmm_server_stats(self._h, _p(v))
+        return dict(in_flight=v[0], held=v[1], peak_admitted=v[2], completed=int(v[3]), queued=int(v[4]),
+                    budget=v[5])

@@ -264,12 +264,24 @@ struct exafmm_ctx {
   Engine E;
 };
 
+namespace exafmm_b200 {
+thread_local long long *g_dbuf_account = nullptr;
+}
+
 namespace {
 thread_local std::string g_create_error;
+
+// Charges the buffers a call allocates to one context's byte counter.
+struct AccountScope {
+  long long *prev;
+  explicit AccountScope(long long *a) : prev(g_dbuf_account) { g_dbuf_account = a; }
+  ~AccountScope() { g_dbuf_account = prev; }
+};
 
 template <typename F>
 int guarded(exafmm_ctx *ctx, F &&f) {
   if (!ctx) return 2;
+  AccountScope scope(&ctx->E.C.dev_bytes);
   try {
     f();
     return 0;
@@ -310,6 +322,7 @@ int exafmm_create(exafmm_ctx **out, int P, double theta, int ncrit, int nspawn, 
     if (device >= 0) EXA_CUDA(cudaSetDevice(device));
     std::unique_ptr<exafmm_ctx> c(new exafmm_ctx);
     Context &C = c->E.C;
+    AccountScope scope(&C.dev_bytes);
     EXA_CUDA(cudaGetDevice(&C.device));
     C.prm.P = P;
     C.prm.theta = theta;
@@ -575,6 +588,12 @@ int exafmm_dipole_correction(exafmm_ctx *ctx, const double *dipole3, long long n
     if (!dipole3) throw std::runtime_error("null dipole");
     ctx->E.dipole_correction(dipole3, num_bodies);
   });
+}
+
+int exafmm_device_bytes(exafmm_ctx *ctx, long long *bytes) {
+  if (!ctx || !bytes) return 2;
+  *bytes = ctx->E.C.dev_bytes;
+  return 0;
 }
 
 double exafmm_drift(double x, long long k, int up) { return up ? drift_up(x, k) : drift_down(x, k); }

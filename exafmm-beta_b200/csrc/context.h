@@ -50,6 +50,7 @@ struct TreeBufs {
 };
 
 struct Context {
+  long long dev_bytes = 0;     // device bytes held by this context's buffers (declared first: outlives them)
   Params prm;
   cudaStream_t stream = nullptr;
   int device = 0;

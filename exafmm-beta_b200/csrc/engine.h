@@ -12,21 +12,32 @@
 namespace exafmm_b200 {
 
 // Grow-only device buffer.  Contents are not preserved across growth.
+// Device bytes held by the context whose entry point is running on this
+// thread (null outside such a call): grow-only buffers charge it.
+extern thread_local long long *g_dbuf_account;
+
 template <typename T>
 struct DBuf {
   T *p = nullptr;
   size_t cap = 0;
+  long long *acct = nullptr;  // byte counter of the owning context, set at allocation
   void ensure(size_t n) {
     if (n <= cap) return;
     release();
     size_t want = n < 16 ? 16 : n;
     EXA_CUDA(cudaMalloc((void **)&p, want * sizeof(T)));
     cap = want;
+    acct = g_dbuf_account;
+    if (acct) *acct += (long long)(want * sizeof(T));
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      cudaFree(p);
+      if (acct) *acct -= (long long)(cap * sizeof(T));
+    }
     p = nullptr;
     cap = 0;
+    acct = nullptr;
   }
   T *get() const { return p; }
   ~DBuf() { release(); }

@@ -1,0 +1,484 @@
+// Host runtime over the solve contexts: a batch solver for many independent
+// systems and a request server with HBM-budget admission.
+//
+// Both keep a pool of workers; each worker is a host thread that owns one
+// solve context (its own CUDA stream and buffers), so independent systems run
+// concurrently on the GPU while each one's launches stay ordered.  A system's
+// result depends only on its own bodies and parameters: every kernel of a
+// solve reduces in a fixed order, so a system gives the same bits alone, in a
+// batch, or beside other requests.
+//
+// The reference has no counterpart: it solves one system per process
+// (examples/fmm.cxx:163-179) and leaves concurrency to the caller.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/exafmm_b200.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+  return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+// ---------------------------------------------------------------- ncrit autotuner
+// Per size class (floor(log2 n)) the candidates are tried in turn on the first
+// systems of that class; the one with the lowest device time per body is kept.
+class NcritTuner {
+ public:
+  explicit NcritTuner(std::vector<int> cand) : cand_(std::move(cand)) {}
+
+  int pick(long long n, int fallback) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (!enabled_) {
+      auto it = best_.find(size_class(n));
+      return it == best_.end() ? fallback : it->second;
+    }
+    Class &c = cls_[size_class(n)];
+    if (c.trials.size() < cand_.size()) return cand_[c.trials.size()];
+    return best_of(c);
+  }
+
+  void report(long long n, int ncrit, double ms) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (!enabled_ || n <= 0) return;
+    Class &c = cls_[size_class(n)];
+    if (c.trials.size() < cand_.size() && ncrit == cand_[c.trials.size()]) c.trials.push_back(ms / (double)n);
+    if (c.trials.size() == cand_.size()) best_[size_class(n)] = best_of(c);
+  }
+
+  void enable(bool on) {
+    std::lock_guard<std::mutex> lk(mu_);
+    enabled_ = on;
+  }
+
+  // class -> chosen ncrit, as pairs
+  std::vector<int> table() {
+    std::lock_guard<std::mutex> lk(mu_);
+    std::vector<int> out;
+    for (auto &kv : best_) {
+      out.push_back(kv.first);
+      out.push_back(kv.second);
+    }
+    return out;
+  }
+
+ private:
+  struct Class {
+    std::vector<double> trials;  // ms per body, in candidate order
+  };
+  static int size_class(long long n) { return n <= 1 ? 0 : (int)std::floor(std::log2((double)n)); }
+  int best_of(const Class &c) const {
+    size_t b = 0;
+    for (size_t i = 1; i < c.trials.size(); i++)
+      if (c.trials[i] < c.trials[b]) b = i;
+    return cand_[b];
+  }
+  std::vector<int> cand_;
+  std::mutex mu_;
+  bool enabled_ = false;
+  std::map<int, Class> cls_;
+  std::map<int, int> best_;
+};
+
+struct SolveParams {
+  int P = 10;
+  double theta = 0.4;
+  int ncrit = 64;
+  int nspawn = 5000;
+  int images = 0;
+  double cycle = 6.283185307179586;
+  int precision = EXAFMM_FP64;
+};
+
+// One worker's context, created on first use and re-parameterized per system.
+struct Slot {
+  exafmm_ctx *ctx = nullptr;
+  SolveParams cur;
+  ~Slot() { release(); }
+  void release() {
+    if (ctx) exafmm_destroy(ctx);
+    ctx = nullptr;
+  }
+  long long bytes() const {
+    long long b = 0;
+    if (ctx) exafmm_device_bytes(ctx, &b);
+    return b;
+  }
+  // Solve one system; returns the device time of the solve (ms).
+  double solve(int device, const SolveParams &p, const double *xyzq, long long n, double *trg) {
+    if (!ctx || p.precision != cur.precision) {
+      release();
+      if (exafmm_create(&ctx, p.P, p.theta, p.ncrit, p.nspawn, p.images, p.cycle, p.precision, device) != 0) {
+        ctx = nullptr;
+        throw std::runtime_error(exafmm_create_error());
+      }
+      cur = p;
+    } else if (p.P != cur.P || p.theta != cur.theta || p.ncrit != cur.ncrit || p.nspawn != cur.nspawn ||
+               p.images != cur.images || p.cycle != cur.cycle) {
+      check(exafmm_set_params(ctx, p.P, p.theta, p.ncrit, p.nspawn, p.images, p.cycle));
+      cur = p;
+    }
+    check(exafmm_set_bodies(ctx, xyzq, n));
+    check(exafmm_solve(ctx));
+    check(exafmm_get_results(ctx, trg));
+    double ms[8];
+    check(exafmm_phase_times(ctx, ms));
+    return ms[7];
+  }
+  void check(int rc) {
+    if (rc != 0) throw std::runtime_error(exafmm_last_error(ctx));
+  }
+};
+
+}  // namespace
+
+// ================================================================ batch
+struct exafmm_batch {
+  int device = 0;
+  int workers = 1;
+  SolveParams prm;
+  std::vector<Slot> slots;
+  NcritTuner tuner{{32, 64, 128}};
+  std::vector<double> last_ms;  // per system of the last call, device ms
+  std::string error;
+};
+
+// ================================================================ server
+namespace {
+
+struct Request {
+  long long id = 0;
+  SolveParams prm;
+  const double *xyzq = nullptr;
+  long long n = 0;
+  double *trg = nullptr;
+  long long est_bytes = 0;   // estimate at submission, then the bytes charged while in flight
+  Clock::time_point t_submit, t_start, t_end;
+  double device_ms = 0;
+  bool done = false;
+  int status = 0;
+  std::string err;
+};
+
+thread_local std::string g_server_error;
+
+}  // namespace
+
+struct exafmm_server {
+  int device = 0;
+  int workers = 1;
+  double budget = 0;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<Request *> queue;
+  std::unordered_map<long long, std::unique_ptr<Request>> reqs;
+  std::vector<Slot> slots;
+  std::vector<long long> held;     // device bytes held by each worker's idle context
+  long long in_flight = 0;         // bytes charged to the requests being solved
+  int running = 0;                 // requests being solved
+  long long peak_admitted = 0;
+  long long next_id = 1, completed = 0;
+  bool stop = false;
+  std::vector<std::thread> threads;
+
+  // Upper estimate of a solve's device bytes: per body the bodies, keys,
+  // permutation, results and two-float copies, the cells' expansions and the
+  // interaction lists at their initial capacities; plus a fixed part.  A
+  // worker's context keeps its buffers, so a request is charged the larger of
+  // this and what that context already holds.
+  static long long estimate(long long n, int P) {
+    const long long nt = (long long)P * (P + 1) / 2;
+    return n * (1400 + 24 * nt) + (64LL << 20);
+  }
+
+  long long held_total(int except) const {
+    long long s = 0;
+    for (int w = 0; w < (int)held.size(); w++)
+      if (w != except) s += held[w];
+    return s;
+  }
+
+  // Head-of-line admission: the request fits beside what the other workers
+  // hold and what is in flight; with nothing in flight it is always admitted,
+  // so a request larger than the budget still runs (alone).
+  bool admissible(const Request *r, int w) const {
+    if (running == 0) return true;
+    return (double)(held_total(w) + in_flight + std::max(r->est_bytes, held[w])) <= budget;
+  }
+
+  void worker(int w) {
+    cudaSetDevice(device);
+    for (;;) {
+      Request *r = nullptr;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_work.wait(lk, [&] { return (stop && queue.empty()) || (!queue.empty() && admissible(queue.front(), w)); });
+        if (queue.empty()) return;
+        r = queue.front();
+        queue.pop_front();
+        const long long charge = std::max(r->est_bytes, held[w]);
+        in_flight += charge;
+        running++;
+        held[w] = 0;
+        peak_admitted = std::max(peak_admitted, in_flight + held_total(w));
+        r->est_bytes = charge;
+        r->t_start = Clock::now();
+      }
+      int status = 0;
+      std::string err;
+      double dev_ms = 0;
+      try {
+        dev_ms = slots[w].solve(device, r->prm, r->xyzq, r->n, r->trg);
+      } catch (const std::exception &e) {
+        status = 1;
+        err = e.what();
+        slots[w].release();
+      }
+      const long long now_held = slots[w].bytes();
+      bool release = false;
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        in_flight -= r->est_bytes;
+        running--;
+        // keep the context for reuse unless idle contexts crowd the budget
+        release = (double)(held_total(w) + now_held) > 0.5 * budget;
+        held[w] = release ? 0 : now_held;
+      }
+      if (release) slots[w].release();
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        r->t_end = Clock::now();
+        r->device_ms = dev_ms;
+        r->status = status;
+        r->err = err;
+        r->done = true;
+        completed++;
+      }
+      cv_done.notify_all();
+      cv_work.notify_all();
+    }
+  }
+};
+
+extern "C" {
+
+// ---------------------------------------------------------------- batch entry points
+int exafmm_batch_create(exafmm_batch **out, int P, double theta, int ncrit, int nspawn, int precision, int device,
+                        int workers) {
+  if (!out) return 2;
+  *out = nullptr;
+  if (workers < 1 || workers > 256 || P < 2 || ncrit < 1 || !(theta > 0)) return 2;
+  if (precision != EXAFMM_FP64 && precision != EXAFMM_MIXED) return 2;
+  int dev = device;
+  if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) return 1;
+  auto *b = new exafmm_batch;
+  b->device = dev;
+  b->workers = workers;
+  b->prm.P = P;
+  b->prm.theta = theta;
+  b->prm.ncrit = ncrit;
+  b->prm.nspawn = nspawn;
+  b->prm.precision = precision;
+  b->slots.resize(workers);
+  *out = b;
+  return 0;
+}
+
+int exafmm_batch_destroy(exafmm_batch *b) {
+  delete b;
+  return 0;
+}
+
+const char *exafmm_batch_error(const exafmm_batch *b) { return b ? b->error.c_str() : "null batch"; }
+
+int exafmm_batch_autotune(exafmm_batch *b, int enable) {
+  if (!b) return 2;
+  b->tuner.enable(enable != 0);
+  return 0;
+}
+
+int exafmm_batch_ncrit_table(exafmm_batch *b, int *pairs, int cap) {
+  if (!b) return -1;
+  std::vector<int> t = b->tuner.table();
+  const int k = (int)t.size() / 2;
+  for (int i = 0; i < k && i < cap; i++) {
+    pairs[2 * i] = t[2 * i];
+    pairs[2 * i + 1] = t[2 * i + 1];
+  }
+  return k;
+}
+
+int exafmm_batch_solve(exafmm_batch *b, int count, const long long *n, const double *const *xyzq, double *const *trg) {
+  if (!b) return 2;
+  if (count < 0 || (count > 0 && (!n || !xyzq || !trg))) return 2;
+  b->error.clear();
+  b->last_ms.assign(count, 0.0);
+  std::vector<int> order(count);
+  for (int i = 0; i < count; i++) order[i] = i;
+  // largest first: the long solves start early and the short ones fill in
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return n[x] > n[y]; });
+  std::atomic<int> next{0};
+  std::atomic<bool> failed{false};
+  std::mutex emu;
+  auto run = [&](int w) {
+    cudaSetDevice(b->device);
+    for (;;) {
+      const int i = next.fetch_add(1);
+      if (i >= count || failed.load()) return;
+      const int k = order[i];
+      SolveParams p = b->prm;
+      p.ncrit = b->tuner.pick(n[k], b->prm.ncrit);
+      try {
+        const double ms = b->slots[w].solve(b->device, p, xyzq[k], n[k], trg[k]);
+        b->last_ms[k] = ms;
+        b->tuner.report(n[k], p.ncrit, ms);
+      } catch (const std::exception &e) {
+        std::lock_guard<std::mutex> lk(emu);
+        if (!failed.exchange(true)) b->error = std::string("system ") + std::to_string(k) + ": " + e.what();
+        b->slots[w].release();
+        return;
+      }
+    }
+  };
+  const int nw = std::min(b->workers, std::max(count, 1));
+  std::vector<std::thread> th;
+  for (int w = 1; w < nw; w++) th.emplace_back(run, w);
+  run(0);
+  for (auto &t : th) t.join();
+  return failed.load() ? 1 : 0;
+}
+
+int exafmm_batch_times(exafmm_batch *b, double *ms) {
+  if (!b || !ms) return 2;
+  std::copy(b->last_ms.begin(), b->last_ms.end(), ms);
+  return 0;
+}
+
+// ---------------------------------------------------------------- server entry points
+int exafmm_server_create(exafmm_server **out, int device, int workers, double hbm_budget_bytes) {
+  if (!out) return 2;
+  *out = nullptr;
+  if (workers < 1 || workers > 256 || !(hbm_budget_bytes > 0)) return 2;
+  int dev = device;
+  if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) return 1;
+  auto *s = new exafmm_server;
+  s->device = dev;
+  s->workers = workers;
+  s->budget = hbm_budget_bytes;
+  s->slots.resize(workers);
+  s->held.assign(workers, 0);
+  for (int w = 0; w < workers; w++) s->threads.emplace_back(&exafmm_server::worker, s, w);
+  *out = s;
+  return 0;
+}
+
+int exafmm_server_destroy(exafmm_server *s) {
+  if (!s) return 0;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  for (auto &t : s->threads) t.join();
+  delete s;
+  return 0;
+}
+
+int exafmm_server_submit(exafmm_server *s, const double *xyzq, long long n, double *trg, int P, double theta,
+                         int ncrit, int nspawn, int precision, long long *ticket) {
+  if (!s || !ticket || n < 0 || (n > 0 && (!xyzq || !trg))) return 2;
+  if (P < 2 || P > 20 || ncrit < 1 || !(theta > 0)) return 2;
+  if (precision != EXAFMM_FP64 && precision != EXAFMM_MIXED) return 2;
+  auto r = std::make_unique<Request>();
+  r->prm.P = P;
+  r->prm.theta = theta;
+  r->prm.ncrit = ncrit;
+  r->prm.nspawn = nspawn;
+  r->prm.precision = precision;
+  r->xyzq = xyzq;
+  r->n = n;
+  r->trg = trg;
+  r->t_submit = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) return 1;
+    r->id = s->next_id++;
+    r->est_bytes = s->estimate(n, P);
+    *ticket = r->id;
+    s->queue.push_back(r.get());
+    s->reqs.emplace(r->id, std::move(r));
+  }
+  s->cv_work.notify_all();
+  return 0;
+}
+
+int exafmm_server_poll(exafmm_server *s, long long ticket, int *done) {
+  if (!s || !done) return 2;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(ticket);
+  if (it == s->reqs.end()) return 2;
+  *done = it->second->done ? 1 : 0;
+  return 0;
+}
+
+// times4: queue wait, host time from start to results, total from submit (ms), device solve time (ms).
+int exafmm_server_wait(exafmm_server *s, long long ticket, double *times4) {
+  if (!s) return 2;
+  std::unique_ptr<Request> r;
+  {
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(ticket);
+    if (it == s->reqs.end()) {
+      g_server_error = "unknown ticket";
+      return 2;
+    }
+    Request *q = it->second.get();
+    s->cv_done.wait(lk, [&] { return q->done; });
+    r = std::move(it->second);
+    s->reqs.erase(it);
+  }
+  if (times4) {
+    times4[0] = ms_between(r->t_submit, r->t_start);
+    times4[1] = ms_between(r->t_start, r->t_end);
+    times4[2] = ms_between(r->t_submit, r->t_end);
+    times4[3] = r->device_ms;
+  }
+  if (r->status != 0) g_server_error = r->err;
+  return r->status;
+}
+
+// stats6: bytes in flight, bytes held by idle contexts, peak admitted bytes,
+// completed requests, queued requests, budget.
+int exafmm_server_stats(exafmm_server *s, double *stats6) {
+  if (!s || !stats6) return 2;
+  std::lock_guard<std::mutex> lk(s->mu);
+  stats6[0] = (double)s->in_flight;
+  stats6[1] = (double)s->held_total(-1);
+  stats6[2] = (double)s->peak_admitted;
+  stats6[3] = (double)s->completed;
+  stats6[4] = (double)s->queue.size();
+  stats6[5] = s->budget;
+  return 0;
+}
+
+const char *exafmm_server_error(void) { return g_server_error.c_str(); }
+
+}  // extern "C"

@@ -11,6 +11,8 @@
 // writes children, M2L and P2P pairs at their scanned offsets -- deterministic
 // output, no atomics.  The lists are then grouped by target cell with a stable
 // radix sort, which keeps traversal order among a target's sources.
+#include <algorithm>
+
 #include "fmm.h"
 
 namespace exafmm_b200 {
@@ -61,8 +63,11 @@ struct PairScan {
   int sweep;
   long long q_cap, m2l_cap, p2p_cap;
   int *err;
+  // After an overflow the queue holds slots that were never written: every
+  // later sweep of this attempt does nothing, and the host reruns it larger.
+  __device__ bool stopped() const { return (*(volatile int *)err & (kErrQueueOverflow | kErrListOverflow)) != 0; }
   __device__ T value(long long i) const {
-    if (i >= q_cap) return T{0, 0};  // only after an overflow, which forces a rerun
+    if (i >= q_cap || stopped()) return T{0, 0};
     int4 bi, bj;
     const int mode = decide(c, qin[i], bi, bj);
     T v{0, 0};
@@ -74,7 +79,7 @@ struct PairScan {
     return v;
   }
   __device__ void emit(long long i, const T &, const T &excl) const {
-    if (i >= q_cap) return;
+    if (i >= q_cap || stopped()) return;
     const int2 pr = qin[i];
     int4 bi, bj;
     const int mode = decide(c, pr, bi, bj);
@@ -177,11 +182,10 @@ void group_by_target(Context &C, const int2 *pairs, long long n, long long ncell
 bool traverse(Context &C, ListBufs &lb) {
   const long long ncells = C.tree.ncells;
   cudaStream_t st = C.stream;
-  if (lb.q_cap == 0) {
-    lb.m2l_cap = 256 * ncells + 1024;
-    lb.p2p_cap = 64 * ncells + 1024;
-    lb.q_cap = lb.m2l_cap + lb.p2p_cap;
-  }
+  // capacities for this tree (a reused context may hold a larger one now)
+  lb.m2l_cap = std::max(lb.m2l_cap, 256 * ncells + 1024);
+  lb.p2p_cap = std::max(lb.p2p_cap, 64 * ncells + 1024);
+  lb.q_cap = std::max(lb.q_cap, lb.m2l_cap + lb.p2p_cap);
   lb.q0.ensure(lb.q_cap);
   lb.q1.ensure(lb.q_cap);
   lb.m2l.ensure(lb.m2l_cap);

@@ -262,9 +262,19 @@ struct LevelScan {
   const long long *startp;
   __device__ T value(long long i) const { return a.nd_nchild[*startp + i]; }
   __device__ void emit(long long i, const T &, const T &excl) const { a.nd_childbeg[*startp + i] = excl; }
+  // Children beyond the node capacity are not created (k_emit skips them and
+  // flags the overflow, which makes the host grow the buffers and rebuild), so
+  // the next level's count is clamped to what fits: no kernel of this build
+  // then touches a node slot past the capacity.
   __device__ void total(const T &t) const {
-    a.lvl[level + 1] = t;
-    a.lvl[kMaxLevels + 1 + level + 1] = *startp + a.lvl[level];
+    const long long nstart = *startp + a.lvl[level];
+    long long cnt = t;
+    if (nstart + cnt > a.node_cap) {
+      atomicOr(a.err, kErrCellOverflow);
+      cnt = a.node_cap > nstart ? a.node_cap - nstart : 0;
+    }
+    a.lvl[level + 1] = cnt;
+    a.lvl[kMaxLevels + 1 + level + 1] = nstart;
   }
 };
 
@@ -449,10 +459,10 @@ void build_tree(Context &C) {
   cudaStream_t st = C.stream;
   T.box.ensure(4);
   T.lvl.ensure(2 * (kMaxLevels + 1) + 4);
-  if (T.node_cap == 0) {
-    long long est = 1024 + 8 * 4 * (n / (ncrit + 1) + 1);
-    ensure_nodes(T, est);
-  }
+  // Node capacity for this system (a reused context may receive a larger one);
+  // deeper trees than this estimate overflow, are flagged and rebuilt larger.
+  const long long est = 1024 + 8 * 4 * (n / (ncrit + 1) + 1);
+  if (est > T.node_cap) ensure_nodes(T, est);
   T.keys.ensure(n);
   T.keys_alt.ensure(n);
   T.perm.ensure(n);

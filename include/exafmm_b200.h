@@ -117,6 +117,9 @@ void *exafmm_stream(exafmm_ctx *ctx);
 /* Device time (ms, CUDA events on the context's stream) of the phases of the
  * last solve: bounds, tree, upward, lists, m2l, p2p, downward, total. */
 int exafmm_phase_times(exafmm_ctx *ctx, double *ms8);
+/* Device memory held by the context's grow-only buffers, in bytes (no
+ * counterpart in the reference; used by the request server's admission). */
+int exafmm_device_bytes(exafmm_ctx *ctx, long long *bytes);
 /* Kernels this library has launched in this process (all contexts). */
 long long exafmm_launch_count(void);
 
@@ -139,6 +142,55 @@ int exafmm_kernel_l2l(int P, const double *Xc, const double *Xp, const double *L
 int exafmm_kernel_l2p(int P, const double *X, const double *L, long long n, const double *xyzq, double *trg);
 int exafmm_kernel_p2p(long long ni, const double *xi, long long nj, const double *xj, const double *Xperiodic,
                       double *trg);
+
+/* ---- Batched and served solves (no counterpart in the reference, which
+ * solves one system per process, examples/fmm.cxx:163-179) ----
+ *
+ * Both run a pool of `workers` solve contexts, each on its own host thread and
+ * CUDA stream, so independent systems overlap on the GPU.  A system's results
+ * do not depend on what else runs: every reduction of a solve has a fixed
+ * order, so its bits are the same alone, in a batch or beside other requests. */
+typedef struct exafmm_batch exafmm_batch;
+int exafmm_batch_create(exafmm_batch **b, int P, double theta, int ncrit, int nspawn, int precision, int device,
+                        int workers);
+int exafmm_batch_destroy(exafmm_batch *b);
+const char *exafmm_batch_error(const exafmm_batch *b);
+/* Solves count systems (n[i] bodies at xyzq[i], results to trg[i], caller
+ * order, host memory); blocks until all are done.  Largest systems first. */
+int exafmm_batch_solve(exafmm_batch *b, int count, const long long *n, const double *const *xyzq,
+                       double *const *trg);
+/* Device time (ms) of each system of the last exafmm_batch_solve. */
+int exafmm_batch_times(exafmm_batch *b, double *ms);
+/* enable != 0: the following solves try ncrit 32, 64 and 128 on the first
+ * systems of each size class (floor(log2 n)) and keep the fastest per body;
+ * enable == 0 freezes the table found so far (systems of classes without an
+ * entry use the batch's ncrit). */
+int exafmm_batch_autotune(exafmm_batch *b, int enable);
+/* The tuned table as (size class, ncrit) pairs; returns the number of pairs. */
+int exafmm_batch_ncrit_table(exafmm_batch *b, int *pairs, int cap);
+
+typedef struct exafmm_server exafmm_server;
+/* Request server: submitted systems wait in a FIFO queue and start when their
+ * estimated device memory fits beside the requests in flight and the idle
+ * contexts' buffers within hbm_budget_bytes (a request is always admitted
+ * when nothing else is in flight). */
+int exafmm_server_create(exafmm_server **s, int device, int workers, double hbm_budget_bytes);
+/* Drains the queue, then stops the workers. */
+int exafmm_server_destroy(exafmm_server *s);
+/* Queues one system; xyzq and trg (host, n x 4 doubles) must stay valid until
+ * the request completes.  *ticket identifies it for poll / wait. */
+int exafmm_server_submit(exafmm_server *s, const double *xyzq, long long n, double *trg, int P, double theta,
+                         int ncrit, int nspawn, int precision, long long *ticket);
+int exafmm_server_poll(exafmm_server *s, long long ticket, int *done);
+/* Blocks until the request is done and releases its ticket.  times4: queue
+ * wait, start to results on the host, submit to results on the host (ms), and
+ * the solve's device time (ms).  Returns the request's status. */
+int exafmm_server_wait(exafmm_server *s, long long ticket, double *times4);
+/* stats6: bytes in flight, bytes held by idle contexts, peak admitted bytes,
+ * completed requests, queued requests, budget. */
+int exafmm_server_stats(exafmm_server *s, double *stats6);
+/* Error text of the last failed exafmm_server_wait on this thread. */
+const char *exafmm_server_error(void);
 
 /* Allocation-free form of exafmm_get_bounds, for callers that may not allocate
  * device memory (a host framework that owns all device memory through its own

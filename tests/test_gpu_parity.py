@@ -220,3 +220,21 @@ def test_gpu_results_follow_input_order(ex, datasets):
         f.downward()
         outs.append(f.results())
     assert rel_l2(outs[1], outs[0][p]) < 1e-12
+
+
+def test_gpu_context_reuse_with_growing_systems(ex, datasets):
+    """One context solving ever larger systems (its buffers grow between solves)
+    gives the same bits as fresh contexts, in both precision modes."""
+    for prec in (ex.FP64, ex.MIXED):
+        f = ex.Fmm(P=6, theta=0.4, ncrit=32, precision=prec)
+        for n, gen in ((700, "cube"), (40000, "plummer"), (3000, "sphere"), (250000, "plummer")):
+            x = getattr(datasets, gen)(n, seed=n)
+            f.set_bodies(x)
+            f.solve()
+            reused = f.results()
+            g = ex.Fmm(P=6, theta=0.4, ncrit=32, precision=prec)
+            g.set_bodies(x)
+            g.solve()
+            assert np.array_equal(reused, g.results())
+            g.close()
+        f.close()

@@ -1,0 +1,95 @@
+"""The batch solver and the request server (host runtime over pools of solve
+contexts).  A system's result must not depend on what runs beside it: the
+same bits alone, in a batch, or among other requests."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _systems(datasets, k, lo, hi, seed):
+    sizes = datasets.log_uniform_sizes(k, lo, hi, seed)
+    return [datasets.cube(int(n), seed=seed + i) if i % 2 == 0 else datasets.sphere(int(n), seed=seed + i)
+            for i, n in enumerate(sizes)]
+
+
+def _alone(ex, x, **kw):
+    f = ex.Fmm(**kw)
+    f.set_bodies(x)
+    f.solve()
+    r = f.results()
+    f.close()
+    return r
+
+
+def test_batch_matches_single_solves(ex, datasets):
+    xs = _systems(datasets, 12, 500, 40000, 100)
+    b = ex.Batch(P=6, theta=0.4, ncrit=32, workers=4)
+    outs = b.solve(xs)
+    for x, o in zip(xs, outs):
+        assert np.array_equal(o, _alone(ex, x, P=6, theta=0.4, ncrit=32))
+    again = b.solve(xs)
+    assert all(np.array_equal(a, c) for a, c in zip(outs, again))
+    assert (b.times(len(xs)) > 0).all()
+    b.close()
+
+
+def test_batch_mixed_precision_and_empty(ex, datasets):
+    xs = _systems(datasets, 6, 1000, 20000, 300) + [np.zeros((0, 4)), datasets.cube(1, seed=9)]
+    b = ex.Batch(P=8, theta=0.4, ncrit=64, precision=ex.MIXED, workers=3)
+    outs = b.solve(xs)
+    for x, o in zip(xs, outs):
+        assert np.array_equal(o, _alone(ex, x, P=8, theta=0.4, ncrit=64, precision=ex.MIXED))
+    b.close()
+
+
+def test_batch_autotune_then_frozen(ex, datasets):
+    xs = _systems(datasets, 12, 3000, 5000, 200)
+    b = ex.Batch(P=4, theta=0.4, ncrit=64, workers=3)
+    b.autotune(True)
+    b.solve(xs)
+    b.autotune(False)
+    table = b.ncrit_table()
+    assert table and all(v in (32, 64, 128) for v in table.values())
+    o1 = b.solve(xs)
+    o2 = b.solve(xs)
+    assert all(np.array_equal(a, c) for a, c in zip(o1, o2))
+    for x, o in zip(xs, o1):  # each system ran with its class's tuned ncrit
+        nc = table.get(int(np.floor(np.log2(len(x)))), 64)
+        assert np.array_equal(o, _alone(ex, x, P=4, theta=0.4, ncrit=nc))
+    b.close()
+
+
+def test_server_result_same_alone_and_in_mix(ex, datasets):
+    s = ex.Server(workers=4, hbm_budget_bytes=40e9)
+    x = datasets.plummer(30000, seed=5)
+    kw = dict(P=8, theta=0.4, ncrit=64, precision=ex.MIXED)
+    alone, t_alone = s.wait(s.submit(x, **kw))
+    mix = []
+    for i, n in enumerate([50000, 2000, 120000, 8000]):
+        mix.append(s.submit(datasets.cube(n, seed=40 + i), P=(6, 8, 10)[i % 3], theta=0.4, ncrit=64,
+                            precision=(ex.FP64, ex.MIXED)[i % 2]))
+    tk = s.submit(x, **kw)
+    for i, n in enumerate([30000, 70000, 1000]):
+        mix.append(s.submit(datasets.sphere(n, seed=60 + i), P=10, theta=0.4, ncrit=32))
+    in_mix, times = s.wait(tk)
+    for t in mix:
+        s.wait(t)
+    assert np.array_equal(alone, in_mix)
+    assert np.array_equal(alone, _alone(ex, x, **kw))
+    assert times[2] >= times[1] >= 0 and times[3] > 0
+    st = s.stats()
+    assert st["completed"] == 2 + len(mix) and st["queued"] == 0
+    s.close()
+
+
+def test_server_admission_serializes_under_tiny_budget(ex, datasets):
+    s = ex.Server(workers=4, hbm_budget_bytes=1.0)  # no two requests fit together
+    xs = _systems(datasets, 6, 2000, 30000, 500)
+    tickets = [s.submit(x, P=6, theta=0.4, ncrit=32) for x in xs]
+    outs = [s.wait(t)[0] for t in tickets]
+    for x, o in zip(xs, outs):
+        assert np.array_equal(o, _alone(ex, x, P=6, theta=0.4, ncrit=32))
+    st = s.stats()
+    assert st["completed"] == len(xs) and st["held"] == 0 and st["in_flight"] == 0
+    s.close()
