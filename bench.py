@@ -40,6 +40,7 @@ PKG_DIR = os.path.join(ROOT, "exafmm-beta_b200")
 WORKLOAD = dict(name="plummer_4m_p8", n=4_194_304, P=8, theta=0.35, ncrit=64, nspawn=5000, seed=2)
 METRIC = "FMM bodies/s (full mixed-precision solve, Plummer N=4,194,304, P=8, theta=0.35)"
 CPU_SAMPLE_N = 262_144
+M2L_DRAM_BYTES_PER_PAIR = 27.5
 
 
 def _package():
@@ -340,9 +341,12 @@ def main():
     alg_bytes = n_m2l * (nterm * cplx + 8) + info["ncells"] * 2 * nterm * cplx
     alg_flops = n_m2l * 8 * nterm * P * P
     achieved = alg_bytes / (m2l_ms / 1e3) / 1e9
+    # DRAM bytes per M2L pair of the four FP32 part launches, from the ncu capture of the same
+    # kernels on the 1M-body case (profiles/m2l_p2p_plummer_1m_p8_mixed_ncrit128.txt), scaled by pairs
+    traffic = M2L_DRAM_BYTES_PER_PAIR * n_m2l if prec == pkg.MIXED and P == 8 else None
     roofline = {
         "kernel": "m2l", "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-        "frac": achieved / hbm_peak, "traffic": None, "peak_kind": peak_kind,
+        "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
         "ms_per_launch": m2l_ms, "algorithmic_bytes": alg_bytes, "algorithmic_flops": alg_flops,
         "achieved_tflops": alg_flops / (m2l_ms / 1e3) / 1e12,
         "note": "M2L runs on the CUDA-core FP32 (mixed) / FP64 pipes and is compute-bound (~50 flop/B): "
@@ -505,10 +509,9 @@ def _run_batch(args, pkg, datasets, workloads, prec, rank, world, local_rank):
     if not args.no_plain and prec == pkg.MIXED:
         bp = pkg.Batch(P=cfg["P"], theta=cfg["theta"], ncrit=cfg["ncrit"], nspawn=cfg["nspawn"],
                        precision=pkg.FP64, device=local_rank, workers=args.workers)
-        bp.autotune(True)
+        bp.set_ncrit_table(b.ncrit_table())  # the same trees, so mixed vs plain is precision only
         plain = [np.zeros((len(x), 4)) for x in xs]
         bp.solve(xs, plain)
-        bp.autotune(False)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         bp.solve(xs, plain)

@@ -100,6 +100,7 @@ def lib() -> ctypes.CDLL:
         "exafmm_batch_times": (_c_int, [_vp, _vp]),
         "exafmm_batch_autotune": (_c_int, [_vp, _c_int]),
         "exafmm_batch_ncrit_table": (_c_int, [_vp, _vp, _c_int]),
+        "exafmm_batch_set_ncrit_table": (_c_int, [_vp, _vp, _c_int]),
         "exafmm_server_create": (_c_int, [ctypes.POINTER(_vp), _c_int, _c_int, _c_double]),
         "exafmm_server_destroy": (_c_int, [_vp]),
         "exafmm_server_submit": (_c_int, [_vp, _vp, _c_ll, _vp, _c_int, _c_double, _c_int, _c_int, _c_int,
@@ -381,6 +382,11 @@ class Batch:
         buf = (_c_int * 128)()
         k = lib().exafmm_batch_ncrit_table(self._h, buf, 64)
         return {buf[2 * i]: buf[2 * i + 1] for i in range(k)}
+
+    def set_ncrit_table(self, table: dict):
+        pairs = (_c_int * (2 * max(1, len(table))))(*[v for kv in sorted(table.items()) for v in kv])
+        if lib().exafmm_batch_set_ncrit_table(self._h, pairs, len(table)) != 0:
+            raise FmmError("invalid ncrit table")
 
     def solve(self, systems, outs=None):
         """systems: list of (n_i, 4) float64 arrays; returns the list of (n_i, 4) results."""

@@ -69,6 +69,13 @@ class NcritTuner {
     enabled_ = on;
   }
 
+  void load(const int *pairs, int k) {
+    std::lock_guard<std::mutex> lk(mu_);
+    enabled_ = false;
+    best_.clear();
+    for (int i = 0; i < k; i++) best_[pairs[2 * i]] = pairs[2 * i + 1];
+  }
+
   // class -> chosen ncrit, as pairs
   std::vector<int> table() {
     std::lock_guard<std::mutex> lk(mu_);
@@ -324,6 +331,14 @@ int exafmm_batch_ncrit_table(exafmm_batch *b, int *pairs, int cap) {
     pairs[2 * i + 1] = t[2 * i + 1];
   }
   return k;
+}
+
+int exafmm_batch_set_ncrit_table(exafmm_batch *b, const int *pairs, int k) {
+  if (!b || k < 0 || (k > 0 && !pairs)) return 2;
+  for (int i = 0; i < k; i++)
+    if (pairs[2 * i + 1] < 1 || pairs[2 * i + 1] > 1024) return 2;
+  b->tuner.load(pairs, k);
+  return 0;
 }
 
 int exafmm_batch_solve(exafmm_batch *b, int count, const long long *n, const double *const *xyzq, double *const *trg) {

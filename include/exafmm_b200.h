@@ -168,6 +168,9 @@ int exafmm_batch_times(exafmm_batch *b, double *ms);
 int exafmm_batch_autotune(exafmm_batch *b, int enable);
 /* The tuned table as (size class, ncrit) pairs; returns the number of pairs. */
 int exafmm_batch_ncrit_table(exafmm_batch *b, int *pairs, int cap);
+/* Replaces the table with k (size class, ncrit) pairs and freezes it (so two
+ * batches can solve on the same trees). */
+int exafmm_batch_set_ncrit_table(exafmm_batch *b, const int *pairs, int k);
 
 typedef struct exafmm_server exafmm_server;
 /* Request server: submitted systems wait in a FIFO queue and start when their

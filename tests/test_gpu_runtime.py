@@ -57,6 +57,11 @@ def test_batch_autotune_then_frozen(ex, datasets):
     for x, o in zip(xs, o1):  # each system ran with its class's tuned ncrit
         nc = table.get(int(np.floor(np.log2(len(x)))), 64)
         assert np.array_equal(o, _alone(ex, x, P=4, theta=0.4, ncrit=nc))
+    b2 = ex.Batch(P=4, theta=0.4, ncrit=64, workers=2)  # a loaded table reproduces the same trees
+    b2.set_ncrit_table(table)
+    assert b2.ncrit_table() == table
+    assert all(np.array_equal(a, c) for a, c in zip(o1, b2.solve(xs)))
+    b2.close()
     b.close()
 
 
