@@ -185,9 +185,10 @@ def main():
     ap.add_argument("--ncrit", type=int, default=0, help="0: pick the fastest of 32, 64, 128 during warm-up")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain-method comparison run")
-    ap.add_argument("--workload", default="solve", choices=["solve", "batch", "serve"],
+    ap.add_argument("--workload", default="solve", choices=["solve", "batch", "serve", "periodic"],
                     help="solve: the single large solve (default); batch: 512 independent systems per step; "
-                         "serve: Poisson request trace through the request server")
+                         "serve: Poisson request trace through the request server; periodic: water box "
+                         "with images=3 against Ewald")
     ap.add_argument("--workers", type=int, default=16, help="contexts (streams) of the batch / serve runtime")
     args = ap.parse_args()
     if args.workload != "solve":
@@ -444,11 +445,13 @@ def run_runtime_workload(args):
     prec = pkg.FP64 if args.precision == "fp64" else pkg.MIXED
     if args.workload == "batch":
         line = _run_batch(args, pkg, datasets, workloads, prec, rank, world, local_rank)
+    elif args.workload == "periodic":
+        line = _run_periodic(args, pkg, datasets, prec, rank, world, local_rank)
     else:
         line = _run_serve(args, pkg, datasets, workloads, prec, rank, world, local_rank)
     if world > 1:
         import torch.distributed as dist
-        if args.workload == "batch":  # whole-job bodies/s over the slowest rank's time
+        if args.workload in ("batch", "periodic"):  # whole-job bodies/s over the slowest rank's time
             t = torch.tensor([line["_time"]], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             line["value"] = line["_units"] * world / float(t.item())
@@ -577,6 +580,109 @@ def _run_serve(args, pkg, datasets, workloads, prec, rank, world, local_rank):
         "gpu_launches": int(launches), "clocks": clk, "roofline": None,
         "_time": top["wall_s"], "_units": top["requests"],
     }
+
+
+PERIODIC = dict(name="water_1m_images3_p10", waters=333_333, P=10, theta=0.4, ncrit=64, nspawn=5000, images=3,
+                cutoff=30.0, alpha_cutoff=3.8, cpu_waters=20_000)
+
+
+def _run_periodic(args, pkg, datasets, prec, rank, world, local_rank):
+    """Periodic water box (config 5): FMM with the lattice (images=3) and the dipole
+    correction, against Ewald summation on the GPU (FP64)."""
+    import torch
+    cfg = PERIODIC
+    x, L = datasets.water_box(cfg["waters"], seed=5 + rank)
+    n = len(x)
+    kw = dict(P=cfg["P"], theta=cfg["theta"], ncrit=cfg["ncrit"], nspawn=cfg["nspawn"], images=cfg["images"],
+              cycle=L, device=local_rank)
+    dx = torch.from_numpy(x).cuda()
+    dout = torch.empty_like(dx)
+
+    def solve(f, out):
+        f.set_bodies_device(dx.data_ptr(), n)
+        f.solve()
+        f.dipole_correction(f.get_dipole())
+        f.results_device(out.data_ptr())
+
+    fmm = pkg.Fmm(precision=prec, **kw)
+    for _ in range(max(3, args.warmup)):
+        solve(fmm, dout)
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(fmm.stream())
+    launches0 = pkg.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            solve(fmm, dout)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.summary()
+    launches = pkg.launch_count() - launches0
+    phases = fmm.phase_times()
+    info = fmm.info()
+    mixed = dout.cpu().numpy()
+    fmm.close()
+    # Ewald: real part to erfc(alpha rc), wave part to exp(-K^2 / 4 alpha^2) at |k| = ksize, both ~1e-7
+    alpha = cfg["alpha_cutoff"] / cfg["cutoff"]
+    ksize = int(np.ceil(2 * alpha * np.sqrt(np.log(1e7)) * L / (2 * np.pi)))
+    t0 = time.perf_counter()
+    ew = pkg.ewald(x, ksize=ksize, alpha=alpha, sigma=0.25 / np.pi, cutoff=cfg["cutoff"], cycle=L)
+    ewald_s = time.perf_counter() - t0
+    q = x[:, 3]
+
+    def vs(a, b):
+        ea, eb = float(q @ a[:, 0]), float(q @ b[:, 0])
+        return {"energy_rel": abs(ea - eb) / abs(eb), "grad_rel_l2": datasets.rel_l2(a[:, 1:], b[:, 1:])}
+
+    line = {
+        "metric": "periodic FMM bodies/s (water box, 1.0M charges, images=3, P=10, theta=0.4, dipole correction)",
+        "value": n * args.steps / (ms / 1e3), "unit": "bodies/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if prec == pkg.FP64 else "f32+kahan", "data": "synthetic",
+        "config": {"workload": cfg["name"], "charges": n, "box_edge_A": L, "P": cfg["P"], "theta": cfg["theta"],
+                   "ncrit": cfg["ncrit"], "images": cfg["images"], "precision": args.precision,
+                   "parallelism": f"replicas{world}", "cells": info["ncells"], "m2l_pairs": info["n_m2l"],
+                   "p2p_pairs": info["n_p2p"],
+                   "ewald": {"alpha": alpha, "cutoff_A": cfg["cutoff"], "ksize": ksize, "sigma": 0.25 / np.pi,
+                             "seconds": ewald_s},
+                   "l2": "inputs larger than L2 (32 MB of bodies plus 0.5 GB of lists per solve)"},
+        "phases_ms": phases, "vs_ewald": vs(mixed, ew), "gpu_launches": int(launches), "clocks": clk,
+        "roofline": None, "_time": ms / 1e3, "_units": n * args.steps,
+    }
+    if not args.no_plain and prec == pkg.MIXED:
+        f64 = pkg.Fmm(precision=pkg.FP64, **kw)
+        plain = torch.empty_like(dx)
+        solve(f64, plain)
+        torch.cuda.synchronize()
+        s64 = torch.cuda.ExternalStream(f64.stream())
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(s64)
+        solve(f64, plain)
+        p1.record(s64)
+        torch.cuda.synchronize()
+        pl = plain.cpu().numpy()
+        line["plain_fp64"] = {"value": n / (p0.elapsed_time(p1) / 1e3), "unit": "bodies/s",
+                              "ms_per_step": p0.elapsed_time(p1), "vs_ewald": vs(pl, ew),
+                              "mixed_vs_plain": {"pot": datasets.rel_l2(mixed[:, 0], pl[:, 0]),
+                                                 "grad": datasets.rel_l2(mixed[:, 1:], pl[:, 1:])}}
+        f64.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import bindings
+        if bindings.reference_available():
+            xs, Ls = datasets.water_box(cfg["cpu_waters"], seed=6)
+            threads = os.cpu_count() or 1
+            t0 = time.perf_counter()
+            bindings.Reference().solve(xs, P=cfg["P"], theta=cfg["theta"], ncrit=cfg["ncrit"], nspawn=cfg["nspawn"],
+                                       images=cfg["images"], cycle=Ls, threads=threads, record_lists=False,
+                                       dipole_correction=True)
+            dt = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": len(xs) / dt, "unit": "bodies/s", "cores": threads, "kind": "reference",
+                                    "sample": f"one periodic solve of a {len(xs)}-charge water box at the same "
+                                              f"density, P, theta and images ({dt:.1f} s)"}
+    return line
 
 
 if __name__ == "__main__":

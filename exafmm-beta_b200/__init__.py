@@ -109,6 +109,8 @@ def lib() -> ctypes.CDLL:
         "exafmm_server_wait": (_c_int, [_vp, _c_ll, _vp]),
         "exafmm_server_stats": (_c_int, [_vp, _vp]),
         "exafmm_server_error": (ctypes.c_char_p, []),
+        "exafmm_ewald": (_c_int, [_vp, _c_ll, _c_int, _c_double, _c_double, _c_double, _c_double, _vp]),
+        "exafmm_ewald_error": (ctypes.c_char_p, []),
         "exafmm_dipole_correction": (_c_int, [_vp, _vp, _c_ll]),
     }
     for name, (res, args) in sig.items():
@@ -296,6 +298,16 @@ class Fmm:
 def _kcheck(rc):
     if rc != 0:
         raise FmmError(lib().exafmm_kernel_error().decode())
+
+
+def ewald(xyzq, ksize, alpha, sigma, cutoff, cycle, trg=None) -> np.ndarray:
+    """Ewald summation (include/ewald.h) on the GPU in FP64; (n, 4) potential and
+    gradient in input order (accumulated into trg when given)."""
+    x = _f64(xyzq, 4)
+    out = np.zeros((len(x), 4)) if trg is None else trg
+    if lib().exafmm_ewald(_p(x), len(x), ksize, alpha, sigma, cutoff, cycle, _p(out)) != 0:
+        raise FmmError(lib().exafmm_ewald_error().decode())
+    return out
 
 
 def direct(targets, sources, images=0, theta=0.4, cycle=2 * np.pi, trg=None) -> np.ndarray:

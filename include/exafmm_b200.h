@@ -129,6 +129,16 @@ long long exafmm_launch_count(void);
 int exafmm_direct(const double *targets, long long nt, const double *sources, long long ns, int images,
                   double theta, double cycle, double *trg);
 
+/* Ewald summation (include/ewald.h:7-197, as examples/ewald.cxx drives it), FP64
+ * on the device: wave part over the integer waves |k| <= ksize of
+ * Ewald::initWaves, real part (erfc) over pairs closer than cutoff at their
+ * nearest periodic image, self term.  alpha and sigma as in Ewald's
+ * constructor; cycle = box edge, bodies taken modulo the box.  Host arrays;
+ * trg accumulates (potential, gradient) in caller order. */
+int exafmm_ewald(const double *xyzq, long long n, int ksize, double alpha, double sigma, double cutoff, double cycle,
+                 double *trg);
+const char *exafmm_ewald_error(void);
+
 /* Error text of the last failed exafmm_direct / exafmm_kernel_* call on this thread. */
 const char *exafmm_kernel_error(void);
 

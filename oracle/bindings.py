@@ -90,6 +90,10 @@ class _Lib:
         p("l2p", None, [_c_int, _vp, _vp, _c_int, _vp, _vp])
         p("p2p", None, [_c_int, _vp, _c_int, _vp, _vp, _vp])
         p("direct", None, [_c_int, _vp, _c_int, _vp, _c_int, _c_double, _c_double, _vp])
+        if self.prefix == "oracle_":
+            p("ewald", None, [_c_int, _vp, _c_int, _c_double, _c_double, _c_double, _c_double, _vp])
+        else:
+            p("ewald", None, [_c_int, _vp, _c_int, _c_double, _c_double, _c_double, _c_double, _c_int, _vp])
 
     def _collect(self, h, n, P, lists=True, trg=True, expansions=False) -> TreeRun:
         g = lambda name: getattr(self.lib, self.prefix + name)
@@ -151,6 +155,16 @@ class _Lib:
         out = np.zeros((len(xi), 4)) if trg is None else np.array(trg, np.float64)
         xp = None if Xper is None else np.asarray(Xper, np.float64)
         getattr(self.lib, self.prefix + "p2p")(len(xi), _ptr(xi), len(xj), _ptr(xj), _ptr(xp), _ptr(out))
+        return out
+
+    def ewald(self, xyzq, ksize, alpha, sigma, cutoff, cycle, ncrit=64):
+        """Ewald summation (include/ewald.h): (n, 4) potential and gradient, caller order."""
+        x = _as_xyzq(xyzq)
+        out = np.zeros((len(x), 4))
+        if self.prefix == "oracle_":
+            self.lib.oracle_ewald(len(x), _ptr(x), ksize, alpha, sigma, cutoff, cycle, _ptr(out))
+        else:
+            self.lib.ref_ewald(len(x), _ptr(x), ksize, alpha, sigma, cutoff, cycle, ncrit, _ptr(out))
         return out
 
     def direct(self, xi, xj, images=0, theta=0.4, cycle=2 * np.pi):

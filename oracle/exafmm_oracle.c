@@ -825,3 +825,78 @@ void oracle_direct(int ni, const double *xi, int nj, const double *xj, int image
         }
   }
 }
+
+/* Ewald summation (ewald.h:7-197) for small systems: wave part over the waves of
+ * Ewald::initWaves (ewald.h:69-95) with dft/idft (ewald.h:27-66) and the wave
+ * factor of wavePart (ewald.h:160-176); real part (ewald.h:98-120) over all
+ * pairs at their nearest periodic image; self term (ewald.h:150-155).  trg
+ * accumulates. */
+void oracle_ewald(int n, const double *xyzq, int ksize, double alpha, double sigma, double cutoff, double cycle,
+                  double *trg) {
+  const double scale = 2 * M_PI / cycle;
+  const double coef = 2 / sigma / (cycle * cycle * cycle), coef2 = 1 / (4 * alpha * alpha);
+  int nw = 0;
+  for (int l = 0; l <= ksize; l++)
+    for (int m = (l == 0 ? 0 : -ksize); m <= ksize; m++)
+      for (int k = (l == 0 && m == 0 ? 1 : -ksize); k <= ksize; k++)
+        if (l * l + m * m + k * k <= ksize * ksize) nw++;
+  int *K = (int *)malloc(sizeof(int) * 3 * (nw > 0 ? nw : 1));
+  double *S = (double *)calloc(2 * (nw > 0 ? nw : 1), sizeof(double));
+  int w = 0;
+  for (int l = 0; l <= ksize; l++)
+    for (int m = (l == 0 ? 0 : -ksize); m <= ksize; m++)
+      for (int k = (l == 0 && m == 0 ? 1 : -ksize); k <= ksize; k++)
+        if (l * l + m * m + k * k <= ksize * ksize) {
+          K[3 * w] = l;
+          K[3 * w + 1] = m;
+          K[3 * w + 2] = k;
+          w++;
+        }
+#pragma omp parallel for schedule(static)
+  for (int v = 0; v < nw; v++) {
+    double re = 0, im = 0;
+    for (int j = 0; j < n; j++) {
+      double th = 0;
+      for (int d = 0; d < 3; d++) th += K[3 * v + d] * xyzq[4 * j + d] * scale;
+      re += xyzq[4 * j + 3] * cos(th);
+      im += xyzq[4 * j + 3] * sin(th);
+    }
+    double k2 = 0;
+    for (int d = 0; d < 3; d++) k2 += (K[3 * v + d] * scale) * (K[3 * v + d] * scale);
+    const double f = coef * exp(-k2 * coef2) / k2;
+    S[2 * v] = re * f;
+    S[2 * v + 1] = im * f;
+  }
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; i++) {
+    double t[4] = {0, 0, 0, 0};
+    for (int v = 0; v < nw; v++) {
+      double th = 0;
+      for (int d = 0; d < 3; d++) th += K[3 * v + d] * xyzq[4 * i + d] * scale;
+      const double dtmp = S[2 * v] * sin(th) - S[2 * v + 1] * cos(th);
+      t[0] += S[2 * v] * cos(th) + S[2 * v + 1] * sin(th);
+      for (int d = 0; d < 3; d++) t[d + 1] -= dtmp * K[3 * v + d];
+    }
+    trg[4 * i] += t[0];
+    for (int d = 0; d < 3; d++) trg[4 * i + 1 + d] += t[d + 1] * scale;
+    /* real part at the nearest image, then the self term */
+    for (int j = 0; j < n; j++) {
+      double dX[3];
+      for (int d = 0; d < 3; d++) {
+        dX[d] = xyzq[4 * i + d] - xyzq[4 * j + d];
+        dX[d] -= cycle * rint(dX[d] / cycle);
+      }
+      const double r2 = dX[0] * dX[0] + dX[1] * dX[1] + dX[2] * dX[2];
+      if (0 < r2 && r2 < cutoff * cutoff) {
+        const double r2s = r2 * alpha * alpha, rs = sqrt(r2s), inv = 1 / rs, inv2 = inv * inv;
+        const double q = xyzq[4 * j + 3];
+        const double dtmp = q * (M_2_SQRTPI * exp(-r2s) * inv2 + erfc(rs) * inv2 * inv) * alpha * alpha * alpha;
+        trg[4 * i] += q * erfc(rs) * inv * alpha;
+        for (int d = 0; d < 3; d++) trg[4 * i + 1 + d] -= dX[d] * dtmp;
+      }
+    }
+    trg[4 * i] -= M_2_SQRTPI * xyzq[4 * i + 3] * alpha;
+  }
+  free(K);
+  free(S);
+}

@@ -60,6 +60,9 @@ void oracle_l2p(int P, const double *X, const double *L, int n, const double *xy
 void oracle_p2p(int ni, const double *xi, int nj, const double *xj, const double *Xperiodic,
                 double *trg);
 /* Traversal::direct (include/traversal.h:355-377), multithreaded over targets. */
+/* Ewald summation (ewald.h): wave part, real part at the nearest image, self term; trg accumulates. */
+void oracle_ewald(int n, const double *xyzq, int ksize, double alpha, double sigma, double cutoff, double cycle,
+                  double *trg);
 void oracle_direct(int ni, const double *xi, int nj, const double *xj, int images, double theta,
                    double cycle, double *trg);
 

@@ -61,6 +61,7 @@ namespace exafmm_laplace {
 #include "build_tree.h"
 #include "up_down_pass.h"
 #include "traversal.h"
+#include "ewald.h"
 
 using namespace exafmm_laplace;
 
@@ -332,6 +333,26 @@ void ref_p2p(int ni, const double * xi, int nj, const double * xj, const double 
   kernel.RefKernelBase::P2P(Ci, Cj);
   kernel.Xperiodic = saved;
   for (int i = 0; i < ni; i++) for (int k = 0; k < 4; k++) trg_i[4 * i + k] = bi[i].TRG[k];
+}
+
+// Ewald summation (include/ewald.h) driven as examples/ewald.cxx:122-136 does for one
+// rank: a tree of the bodies, wavePart(bodies, bodies), realPart(cells, cells),
+// selfTerm(bodies).  Results (potential, gradient) overwrite trg in caller order.
+void ref_ewald(int n, const double * xyzq, int ksize, double alpha, double sigma, double cutoff,
+               double cycle, int ncrit, double * trg) {
+  Bodies bodies, buffer;
+  loadBodies(bodies, n, xyzq);
+  buffer.reserve(n);
+  BoundBox boundBox;
+  BuildTree buildTree(ncrit);
+  Bounds bounds = boundBox.getBounds(bodies);
+  Cells cells = buildTree.buildTree(bodies, buffer, bounds);
+  Ewald ewald(ksize, alpha, sigma, cutoff, vec3(cycle));
+  ewald.wavePart(bodies, bodies);
+  ewald.realPart(cells, cells);
+  ewald.selfTerm(bodies);
+  for (int i = 0; i < n; i++)
+    for (int k = 0; k < 4; k++) trg[4 * bodies[i].IBODY + k] = bodies[i].TRG[k];
 }
 
 // Traversal::direct (include/traversal.h:355-377): targets accumulate over all sources
