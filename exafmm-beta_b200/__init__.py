@@ -182,8 +182,9 @@ class Fmm:
         self._check(lib().exafmm_set_params(self._h, P, theta, ncrit, nspawn, images, cycle))
         self.P, self.theta, self.ncrit, self.nspawn, self.images, self.cycle = P, theta, ncrit, nspawn, images, cycle
 
-    def set_mixed_policy(self, m2l_fp32=True, p2p_fp32=True, min_level=4, max_dl=3):
-        """Mixed form: which operators run in FP32 and which M2L pairs may."""
+    def set_mixed_policy(self, m2l_fp32=1, p2p_fp32=True, min_level=4, max_dl=3):
+        """Mixed form: which operators run in FP32 and which M2L pairs may.
+        m2l_fp32: 0 FP64, 1 FP32 with class-grouped tiles, 2 FP32 pair by pair."""
         self._check(lib().exafmm_set_mixed_policy(self._h, int(m2l_fp32), int(p2p_fp32), min_level, max_dl))
 
     # ---- solve steps (examples/fmm.cxx:163-179) ----

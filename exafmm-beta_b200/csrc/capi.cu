@@ -53,6 +53,7 @@ struct Engine {
   DBuf<double2> M, L;
   DBuf<unsigned char> Ms;  // scaled multipoles for the unrolled M2L (FP32 or FP64)
   DBuf<float4> x32;        // bodies as two-float pairs relative to the root center (mixed P2P)
+  M2LGemmBufs gemm;         // class-grouped tile M2L (mixed form)
   DBuf<double2> lat;        // periodic lattice: supercell multipoles and warp partials
   DBuf<double> dip;         // dipole reduction scratch and result
   DBuf<double4> trg, out;
@@ -177,9 +178,14 @@ struct Engine {
       const bool mixed = C.prm.precision == kMixed;
       const bool m2l32 = mixed && C.prm.mixed_m2l && m2l_fast_supported(C.prm.P, true);
       if (m2l32) {
+        FmmArgs left = a;  // the pairs the pair-by-pair FP32 kernel takes
+        if (C.prm.mixed_gemm && m2l_gemm(C, a, gemm, lists.n_m2l, C.prm.mixed_min_level, C.prm.mixed_max_dl)) {
+          left.m2l_off = gemm.left_off.p;
+          left.m2l_src = gemm.left_src.p;
+        }
         Ms.ensure(nc * NT * sizeof(float2));
         scale_multipoles(a, true, Ms.p);
-        m2l_fast(a, true, Ms.p, C.prm.mixed_min_level, C.prm.mixed_max_dl);
+        m2l_fast(left, true, Ms.p, C.prm.mixed_min_level, C.prm.mixed_max_dl);
         m2l_fp64(a, C.prm.mixed_min_level, C.prm.mixed_max_dl);  // root levels, large size ratios
       } else if (m2l_fast_supported(C.prm.P, false)) {
         Ms.ensure(nc * NT * sizeof(double2));
@@ -386,7 +392,9 @@ int exafmm_set_mixed_policy(exafmm_ctx *ctx, int m2l_fp32, int p2p_fp32, int min
   return guarded(ctx, [&] {
     Params &p = ctx->E.C.prm;
     if (min_level < 0 || max_dl < 0) throw std::runtime_error("min_level and max_dl must be >= 0");
+    if (m2l_fp32 < 0 || m2l_fp32 > 2) throw std::runtime_error("m2l_fp32 must be 0, 1 or 2");
     p.mixed_m2l = m2l_fp32 != 0;
+    p.mixed_gemm = m2l_fp32 == 1;
     p.mixed_p2p = p2p_fp32 != 0;
     p.mixed_min_level = min_level;
     p.mixed_max_dl = max_dl;

@@ -20,6 +20,7 @@ struct Params {
   int mixed_p2p = 1;
   int mixed_min_level = 4;
   int mixed_max_dl = 3;
+  int mixed_gemm = 1;  // class-grouped tile M2L for frequent offset classes
 };
 
 // Level-ordered octree nodes plus the reference-layout cell table.

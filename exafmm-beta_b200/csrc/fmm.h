@@ -44,7 +44,33 @@ bool m2l_fast_supported(int P, bool mixed);
 void scale_multipoles(const FmmArgs &a, bool mixed, void *Ms);
 // In mixed mode only pairs with target level >= min_level and |level difference|
 // <= max_dl are taken (the generic FP64 kernel handles the rest).
-bool m2l_fast(const FmmArgs &a, bool mixed, const void *Ms, int min_level = 0, int max_dl = 0);
+// taken: pairs another kernel evaluates (skipped here), or null.
+bool m2l_fast(const FmmArgs &a, bool mixed, const void *Ms, int min_level = 0, int max_dl = 0,
+              const unsigned char *taken = nullptr);
+
+// Class-grouped tile M2L (m2l_gemm.cu): the mixed-regular pairs whose offset
+// class is frequent, FP32 products with FP64 accumulation, added to L.  When it
+// returns true, left_off / left_src hold the other mixed-regular pairs, grouped
+// by target, for the pair-by-pair FP32 kernel.
+struct M2LGemmBufs {
+  DBuf<unsigned long long> hk;        // class hash table: keys
+  DBuf<unsigned> hc;                  // pairs per slot
+  DBuf<int> hid;                      // slot -> class id (or -1)
+  DBuf<int> pair_slot;                // per list entry: hash slot (or -1)
+  DBuf<unsigned long long> ck, ck_alt;
+  DBuf<int> cs, cs_alt;
+  DBuf<float> K;                      // per class operator, FP32, k-major
+  DBuf<float> Msr;                    // scaled multipoles over real degrees of freedom
+  DBuf<unsigned char> taken;
+  DBuf<unsigned> grp, grp_alt;
+  DBuf<int> cidx, cidx_alt, gstart, tbase, tile_of, tile_cell;
+  DBuf<unsigned long long> pkey, pkey_alt;
+  DBuf<int> pval, pval_alt;
+  DBuf<int> cnt;
+  DBuf<int> left_cnt, left_off, left_src;
+};
+bool m2l_gemm_supported(int P);
+bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int min_level, int max_dl);
 
 // Periodic lattice of root images (traversePeriodic), FP64, into L of the root.
 // scratch holds lattice_scratch_terms(P) complex values.

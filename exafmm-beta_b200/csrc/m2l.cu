@@ -97,6 +97,7 @@ struct M2LCtx {
   double cycle;
   int mode;  // 0: every pair; 1: mixed-regular pairs only
   int min_level, max_dl;
+  const unsigned char *taken;  // pairs the tile kernel (m2l_gemm.cu) evaluates, or null
 };
 
 __device__ __forceinline__ bool mixed_regular(const M2LCtx &g, int lt, int ls) {
@@ -143,6 +144,7 @@ k_m2l_part(M2LCtx g, DevTables t, double2 *L) {
         img = packed >> 26;
         ls = g.cell_pl[cj].y;
         if (g.mode == 1 && !mixed_regular(g, lt, ls)) live = false;
+        if (g.taken && g.taken[q]) live = false;
       }
       T x = T(1), y = T(0), z = T(0);
       if (live) {
@@ -280,7 +282,7 @@ void scale_multipoles(const FmmArgs &a, bool mixed, void *Ms) {
   EXA_CHECK_LAUNCH();
 }
 
-bool m2l_fast(const FmmArgs &a, bool mixed, const void *Ms, int min_level, int max_dl) {
+bool m2l_fast(const FmmArgs &a, bool mixed, const void *Ms, int min_level, int max_dl, const unsigned char *taken) {
   if (!m2l_fast_supported(a.P, mixed)) return false;
   init_tables();
   const DevTables &t = device_tables(a.P);
@@ -295,6 +297,7 @@ bool m2l_fast(const FmmArgs &a, bool mixed, const void *Ms, int min_level, int m
   g.mode = mixed ? 1 : 0;
   g.min_level = min_level;
   g.max_dl = max_dl;
+  g.taken = taken;
   return mixed ? launch_for_P<float>(a.P, g, t, a.L64, a.stream) : launch_for_P<double>(a.P, g, t, a.L64, a.stream);
 }
 

@@ -53,10 +53,12 @@ const char *exafmm_create_error(void);
  * changed parameter must be recomputed. */
 int exafmm_set_params(exafmm_ctx *ctx, int P, double theta, int ncrit, int nspawn, int images, double cycle);
 
-/* Mixed form only: which operators run in FP32 (m2l_fp32, p2p_fp32) and which
- * M2L pairs may (target level >= min_level, |level difference| <= max_dl); the
- * rest runs in FP64.  Defaults: 1, 1, 4, 3.  No counterpart in the reference
- * (its precision is a compile-time switch, EXAFMM_SINGLE). */
+/* Mixed form only: which operators run in FP32 and which M2L pairs may
+ * (target level >= min_level, |level difference| <= max_dl); the rest runs in
+ * FP64.  m2l_fp32: 0 = FP64, 1 = FP32 with frequent offset classes evaluated
+ * as class-grouped tiles, 2 = FP32 pair by pair only.  p2p_fp32: 0 or 1.
+ * Defaults: 1, 1, 4, 3.  No counterpart in the reference (its precision is a
+ * compile-time switch, EXAFMM_SINGLE). */
 int exafmm_set_mixed_policy(exafmm_ctx *ctx, int m2l_fp32, int p2p_fp32, int min_level, int max_dl);
 
 /* Bodies in caller order (Dataset::initBodies / Bodies, include/types.h:72-86).

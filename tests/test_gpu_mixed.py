@@ -47,3 +47,25 @@ def test_mixed_precision_error_split(ex, datasets, dist, n, P, theta, ncrit):
     assert e_precision_acc < 10 * PRECISION_TOL
     # the mixed result is as close to the direct sum as the plain method, up to the precision part
     assert e_mixed_direct < e_plain_direct + 2 * PRECISION_TOL
+
+
+@pytest.mark.parametrize("P", [4, 6, 8, 10])
+def test_tile_m2l_matches_pair_by_pair(ex, datasets, P):
+    """The class-grouped tile M2L and the pair-by-pair FP32 M2L evaluate the same
+    operator: both within the precision bar of the FP64 plain method on the same
+    tree, and of each other (a wrong operator would be off by O(1))."""
+    for gen, n in (("plummer", 60000), ("cube", 40000), ("sphere", 30000)):
+        x = getattr(datasets, gen)(n, seed=P)
+        res = []
+        for prec, pol in ((ex.FP64, None), (ex.MIXED, 1), (ex.MIXED, 2)):
+            f = ex.Fmm(P=P, theta=0.4, ncrit=32, precision=prec)
+            if pol is not None:
+                f.set_mixed_policy(m2l_fp32=pol)
+            f.set_bodies(x)
+            f.solve()
+            res.append(f.results())
+            f.close()
+        plain, tile, pair = res
+        for a, b in ((tile, plain), (pair, plain), (tile, pair)):
+            assert rel_l2(a[:, 0], b[:, 0]) < PRECISION_TOL
+            assert rel_l2(a[:, 1:], b[:, 1:]) < PRECISION_TOL
