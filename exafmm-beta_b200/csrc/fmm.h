@@ -62,10 +62,10 @@ struct M2LGemmBufs {
   DBuf<float> K;                      // per class operator, FP32, k-major
   DBuf<float> Msr;                    // scaled multipoles over real degrees of freedom
   DBuf<unsigned char> taken;
-  DBuf<unsigned> grp, grp_alt;
-  DBuf<int> cidx, cidx_alt, gstart, tbase, tile_of, tile_cell;
-  DBuf<unsigned long long> pkey, pkey_alt;
-  DBuf<int> pval, pval_alt;
+  DBuf<unsigned> skey, skey_alt;      // pairs sorted by class
+  DBuf<int> pval, pval_alt;           // their list positions
+  DBuf<int> cstart, cbase;            // class ranges, chunk offsets per class
+  DBuf<float> Y;                      // per list entry: the pair's contribution (real dofs)
   DBuf<int> cnt;
   DBuf<int> left_cnt, left_off, left_src;
 };

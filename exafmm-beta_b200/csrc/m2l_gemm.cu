@@ -1,5 +1,5 @@
-// M2L as dense tiles: pairs grouped by offset class, each class one real
-// operator matrix (the mixed form's FP32 M2L for regular pairs).
+// M2L as dense products per offset class (the mixed form's FP32 M2L for regular
+// pairs).
 //
 // Between scaled expansions the M2L (kernels/laplace.h:292-322; the scaled form
 // of m2l_fast.cuh) is a linear map that depends only on the offset of the two
@@ -10,16 +10,15 @@
 // d / min(R_s, R_t) is an integer vector: (level difference, that vector) is a
 // class key.  Written over real degrees of freedom (Re of every coefficient,
 // Im of those with m > 0: 2 NTERM - P of them, 64 at P = 8), a class's map is
-// one ND x ND real matrix K.
+// one ND x ND real matrix K (built once per solve from FP64 harmonics).
 //
-// Targets are grouped by (level, octant within the parent) -- cells in the
-// same position relative to their parents have alike interaction lists -- and
-// cut into tiles of 32 in cell order.  The pairs are sorted by (tile, class):
-// a run of equal keys pairs at most one source with each target of the tile,
-// so a tile's local expansions accumulate, column per target, as
-//   D[:, targets] += K_class x B,   B[:, t] = Ms of t's source of that class (or 0),
-// over the tile's runs, with no scatter and in a fixed order.  FP32 products,
-// FP32 sums over at most eight runs, flushed into FP64 accumulators.
+// The pairs of each frequent class are sorted together; one block takes up to
+// 128 of them and forms Y = K x [Ms of their sources] as a dense product in
+// FP32 (the operator loaded once per block, 8 x 8 outputs per thread), writing
+// each pair's column of Y at the pair's position in the target-grouped list.
+// A second pass sums, per target, its pairs' columns in list order in FP64 and
+// adds them to L: deterministic, no atomics.  The 4,096 multiply-adds per pair
+// (at P = 8) replace the 9,216 of the pair-by-pair complex contraction.
 //
 // Classes used by fewer than kMinClassPairs pairs and pairs through periodic
 // images stay with the pair-by-pair FP32 kernel, which then runs on a compacted
@@ -37,7 +36,6 @@ namespace {
 
 constexpr unsigned long long kEmpty = ~0ull;
 constexpr int kMinClassPairs = 16;
-constexpr int kTile = 32;         // targets per tile
 constexpr int kClsBits = 20;      // class id field of the pair key
 constexpr int kProbe = 64;        // hash probe limit (a pair that finds no slot stays per-pair)
 
@@ -205,113 +203,32 @@ __global__ void k_scale_M_real(DevTables t, const double2 *M, const double4 *cel
   }
 }
 
-// 4. Per target: take its pairs of frequent classes; group key (level, octant) or 255.
+// 4. Per target: flag the pairs of frequent classes (taken) and count the
+// leftover pairs of the mixed policy (for the pair-by-pair kernel).
 __device__ __forceinline__ bool policy_pair(int lt, int ls, int min_level, int max_dl) {
   const int dl = lt - ls;
   return lt >= min_level && dl <= max_dl && dl >= -max_dl;
 }
 
 __global__ void k_gemm_flags(const int *off, const int *src, long long ncells, const int *pair_slot, const int *hid,
-                             const double4 *cell_x, const int2 *cell_pl, int min_level, int max_dl,
-                             unsigned char *taken, unsigned *grp, int *cellidx, int *left_cnt) {
+                             const int2 *cell_pl, int min_level, int max_dl, unsigned char *taken, int *left_cnt,
+                             unsigned *pkey, int *pval) {
   const int lane = threadIdx.x & 31;
   const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
   for (long long c = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < ncells; c += warps) {
     const int b = off[c], e = off[c + 1];
     const int lt = cell_pl[c].y;
-    bool any = false;
     int left = 0;
     for (int q = b + lane; q < e; q += 32) {
       const int s = pair_slot[q];
-      const bool tk = s >= 0 && hid[s] >= 0;
-      taken[q] = tk ? 1 : 0;
-      any |= tk;
-      if (!tk && policy_pair(lt, cell_pl[src[q] & 0x3ffffff].y, min_level, max_dl)) left++;
+      const int cls = s >= 0 ? hid[s] : -1;
+      taken[q] = cls >= 0 ? 1 : 0;
+      pkey[q] = cls >= 0 ? (unsigned)cls : 0xffffffffu;  // sort key: class, the rest last
+      pval[q] = q;
+      if (cls < 0 && policy_pair(lt, cell_pl[src[q] & 0x3ffffff].y, min_level, max_dl)) left++;
     }
-    any = __any_sync(0xffffffffu, any);
     for (int o = 16; o > 0; o >>= 1) left += __shfl_xor_sync(0xffffffffu, left, o);
     if (lane == 0) left_cnt[c] = left;
-    if (lane == 0) {
-      unsigned g = 255u;
-      if (any) {
-        const int2 pl = cell_pl[c];
-        int oct = 0;
-        if (pl.x >= 0 && pl.y > 0) {
-          const double4 X = cell_x[c], Xp = cell_x[pl.x];
-          oct = (X.x > Xp.x ? 1 : 0) | (X.y > Xp.y ? 2 : 0) | (X.z > Xp.z ? 4 : 0);
-        }
-        g = (unsigned)(pl.y * 8 + oct);
-        if (g > 254u) g = 254u;  // levels beyond 31 (not reachable: depth <= 21)
-      }
-      grp[c] = g;
-      cellidx[c] = (int)c;
-    }
-  }
-}
-
-// 5. Group starts in the cells sorted by group, tiles per group, tile bases.
-__global__ void k_tile_bases(const unsigned *gsorted, long long ncells, int *gstart, int *tbase, int *ntiles) {
-  const int g = threadIdx.x;  // 256 threads
-  long long lo = 0, hi = ncells;
-  while (lo < hi) {
-    const long long mid = (lo + hi) >> 1;
-    if (gsorted[mid] < (unsigned)g) lo = mid + 1;
-    else hi = mid;
-  }
-  long long lo2 = lo, hi2 = ncells;
-  while (lo2 < hi2) {
-    const long long mid = (lo2 + hi2) >> 1;
-    if (gsorted[mid] <= (unsigned)g) lo2 = mid + 1;
-    else hi2 = mid;
-  }
-  __shared__ int cnt[256];
-  gstart[g] = (int)lo;
-  cnt[g] = (g == 255) ? 0 : (int)((lo2 - lo + kTile - 1) / kTile);
-  __syncthreads();
-  if (g == 0) {
-    int acc = 0;
-    for (int i = 0; i < 256; i++) {
-      tbase[i] = acc;
-      acc += cnt[i];
-    }
-    *ntiles = acc;
-  }
-}
-
-__global__ void k_tile_assign(const unsigned *gsorted, const int *csorted, long long ncells, const int *gstart,
-                              const int *tbase, int *tile_of, int *tile_cell) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ncells; i += (long long)gridDim.x * blockDim.x) {
-    const unsigned g = gsorted[i];
-    const int c = csorted[i];
-    if (g == 255u) {
-      tile_of[c] = -1;
-      continue;
-    }
-    const int rank = (int)(i - gstart[g]);
-    const int tile = tbase[g] + rank / kTile, slot = rank % kTile;
-    tile_of[c] = tile * kTile + slot;
-    tile_cell[tile * kTile + slot] = c;
-  }
-}
-
-// 6. Sort keys: (tile, class) for taken pairs, all ones for the rest.
-__global__ void k_pair_keys(const int *off, const int *src, long long ncells, const int *pair_slot, const int *hid,
-                            const unsigned char *taken, const int *tile_of, unsigned long long *pkey, int *pval) {
-  const int lane = threadIdx.x & 31;
-  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
-  for (long long c = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < ncells; c += warps) {
-    const int b = off[c], e = off[c + 1];
-    const int ts = tile_of[c];
-    for (int q = b + lane; q < e; q += 32) {
-      if (taken[q] && ts >= 0) {
-        const int tile = ts / kTile, slot = ts % kTile;
-        pkey[q] = ((unsigned long long)tile << kClsBits) | (unsigned long long)hid[pair_slot[q]];
-        pval[q] = (slot << 26) | (src[q] & 0x3ffffff);
-      } else {
-        pkey[q] = kEmpty;
-        pval[q] = 0;
-      }
-    }
   }
 }
 
@@ -326,7 +243,7 @@ struct LeftScan {
   __device__ void total(const T &t) const { off2[n] = t; }
 };
 
-// The leftover pairs (not taken by the tiles, inside the mixed policy) in list order.
+// The leftover pairs (not taken, inside the mixed policy) in list order.
 __global__ void k_left_fill(const int *off, const int *src, long long ncells, const unsigned char *taken,
                             const int2 *cell_pl, int min_level, int max_dl, const int *off2, int *src2) {
   const int lane = threadIdx.x & 31;
@@ -350,106 +267,150 @@ __global__ void k_left_fill(const int *off, const int *src, long long ncells, co
   }
 }
 
-__device__ __forceinline__ long long lower_bound_u64(const unsigned long long *a, long long n, unsigned long long v) {
-  long long lo = 0, hi = n;
-  while (lo < hi) {
-    const long long mid = (lo + hi) >> 1;
-    if (a[mid] < v) lo = mid + 1;
-    else hi = mid;
+// 5. Class ranges in the class-sorted pairs, and chunks of kChunk pairs.
+constexpr int kChunk = 128;
+
+__global__ void k_class_ranges(const unsigned *skey, long long n, int ncls, int *cstart) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c <= ncls; c += gridDim.x * blockDim.x) {
+    long long lo = 0, hi = n;
+    while (lo < hi) {
+      const long long mid = (lo + hi) >> 1;
+      if (skey[mid] < (unsigned)c) lo = mid + 1;
+      else hi = mid;
+    }
+    cstart[c] = (int)lo;
   }
-  return lo;
 }
 
-// 7. One block per tile: D (NDP x 32, FP32, 4 x 4 per thread) += K x B per run.
+struct ChunkScan {
+  using T = int;
+  const int *cstart;
+  int *cbase;
+  int n;
+  __device__ T value(long long i) const { return (cstart[i + 1] - cstart[i] + kChunk - 1) / kChunk; }
+  __device__ void emit(long long i, const T &, const T &excl) const { cbase[i] = excl; }
+  __device__ void total(const T &t) const { cbase[n] = t; }
+};
+
+__device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// 6. One block per chunk (one class, up to kChunk pairs): Y[pair] = K_class x Ms[source].
+// The operator and the gathered source columns sit in shared memory; 128
+// threads hold 8 x 8 outputs each (NDP / 8 row groups x 16 column groups).
+// Y is written per pair at its position in the target-grouped list.
 template <int NDP>
-__global__ void __launch_bounds__(NDP / 4 * (kTile / 4))
-k_m2l_gemm(const unsigned long long *pkey, const int *pval, long long npairs, const int *ntiles, const float *Kt,
-           const float *Msr, const int *tile_cell, const double4 *cell_x, DevTables t, int P, double2 *L) {
-  constexpr int THREADS = NDP / 4 * (kTile / 4);
-  extern __shared__ float sm[];
-  float *sK = sm;                  // [NDP input][NDP output]
-  float *sB = sm + NDP * NDP;      // [NDP input][kTile]
-  __shared__ int s_len;
-  const int tile = blockIdx.x;
-  if (tile >= *ntiles) return;
-  const long long lo = lower_bound_u64(pkey, npairs, (unsigned long long)tile << kClsBits);
-  const long long hi = lower_bound_u64(pkey, npairs, (unsigned long long)(tile + 1) << kClsBits);
-  const int tx = threadIdx.x % (kTile / 4), ty = threadIdx.x / (kTile / 4);
-  float acc[4][4];
-  double accd[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; a++)
-#pragma unroll
-    for (int b = 0; b < 4; b++) {
-      acc[a][b] = 0.f;
-      accd[a][b] = 0.0;
-    }
-  int nrun = 0;
-  for (long long p = lo; p < hi;) {
-    __syncthreads();  // the previous run's products are done with sK and sB
-    if (threadIdx.x < 32) {
-      const unsigned long long k0 = pkey[p];
-      const long long q = p + threadIdx.x;
-      const bool same = q < hi && pkey[q] == k0;
-      const unsigned m = __ballot_sync(0xffffffffu, same);
-      if (threadIdx.x == 0) s_len = (m == 0xffffffffu) ? 32 : __ffs(~m) - 1;
-    }
-    const int cls = (int)(pkey[p] & ((1ull << kClsBits) - 1));
-    const float4 *Kg = (const float4 *)(Kt + (long long)cls * NDP * NDP);
-    for (int i = threadIdx.x; i < NDP * NDP / 4; i += THREADS) ((float4 *)sK)[i] = Kg[i];
-    for (int i = threadIdx.x; i < NDP * kTile / 4; i += THREADS) ((float4 *)sB)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    __syncthreads();
-    const int len = s_len;
-    // gather: consecutive threads take different pairs (different columns, no bank conflicts)
-    for (int i = threadIdx.x; i < len * (NDP / 4); i += THREADS) {
-      const int pr = i % len, q4 = i / len;
-      const int v = pval[p + pr];
-      const int slot = v >> 26, srcc = v & 0x3ffffff;
-      const float4 m = ((const float4 *)(Msr + (long long)srcc * NDP))[q4];
-      sB[(4 * q4 + 0) * kTile + slot] = m.x;
-      sB[(4 * q4 + 1) * kTile + slot] = m.y;
-      sB[(4 * q4 + 2) * kTile + slot] = m.z;
-      sB[(4 * q4 + 3) * kTile + slot] = m.w;
-    }
-    __syncthreads();
-#pragma unroll 4
-    for (int kk = 0; kk < NDP; kk++) {
-      const float4 a = ((const float4 *)(sK + kk * NDP))[ty];
-      const float4 b = ((const float4 *)(sB + kk * kTile))[tx];
-      const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
-#pragma unroll
-      for (int r = 0; r < 4; r++)
-#pragma unroll
-        for (int c = 0; c < 4; c++) acc[r][c] = fmaf(av[r], bv[c], acc[r][c]);
-    }
-    if (++nrun == 8) {
-      nrun = 0;
-#pragma unroll
-      for (int r = 0; r < 4; r++)
-#pragma unroll
-        for (int c = 0; c < 4; c++) {
-          accd[r][c] += (double)acc[r][c];
-          acc[r][c] = 0.f;
-        }
-    }
-    p += len;
+__global__ void __launch_bounds__(128)
+k_m2l_class_gemm(const unsigned *skey, const int *sval, const int *cstart, const int *cbase, int ncls,
+                 const int *src, const float *Kt, const float *Msr, float *Y) {
+  constexpr int RG = NDP / 8;                    // row groups of 8
+  constexpr int CG = 128 / RG;                   // column groups of 8 (16 at NDP = 64)
+  constexpr int NC = CG * 8;                     // columns per pass (128 at NDP = 64)
+  constexpr int BROW = kChunk + 4;               // padded column-block row (floats)
+  extern __shared__ float4 smem4[];
+  float *sK = reinterpret_cast<float *>(smem4);  // [NDP input][NDP output]
+  float *sB = sK + NDP * NDP;                    // [NDP input][BROW]: column = pair of the chunk
+  __shared__ int s_q[kChunk];
+  const int chunk = blockIdx.x;
+  if (chunk >= cbase[ncls]) return;
+  int lo = 0, hi = ncls;  // class of this chunk: last c with cbase[c] <= chunk
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (cbase[mid] <= chunk) lo = mid;
+    else hi = mid;
   }
+  const int cls = lo;
+  const int p0 = cstart[cls] + (chunk - cbase[cls]) * kChunk;
+  const int cnt = min(kChunk, cstart[cls + 1] - p0);
+  const float *Kg = Kt + (long long)cls * NDP * NDP;
+  for (int i = threadIdx.x; i < NDP * NDP / 4; i += 128) cp_async16(sK + 4 * i, Kg + 4 * i);
+  cp_async_commit();
+  if (threadIdx.x < kChunk) s_q[threadIdx.x] = threadIdx.x < cnt ? sval[p0 + threadIdx.x] : -1;
+  __syncthreads();
+  // gather: thread (pair i, quarter) copies 16 of the source's NDP values, transposed
+  for (int w = threadIdx.x; w < kChunk * (NDP / 4); w += 128) {
+    const int i = w % kChunk, q4 = w / kChunk;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (i < cnt) v = reinterpret_cast<const float4 *>(Msr + (long long)(src[s_q[i]] & 0x3ffffff) * NDP)[q4];
+    sB[(4 * q4 + 0) * BROW + i] = v.x;
+    sB[(4 * q4 + 1) * BROW + i] = v.y;
+    sB[(4 * q4 + 2) * BROW + i] = v.z;
+    sB[(4 * q4 + 3) * BROW + i] = v.w;
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  const int ty = threadIdx.x % RG, tx = threadIdx.x / RG;
+  if (tx >= CG) return;  // 128 threads need not split evenly into row groups (no barrier follows)
+  for (int c0 = 0; c0 < cnt; c0 += NC) {
+    if (c0 + 8 * tx >= cnt) continue;
+    float acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+      for (int j = 0; j < 8; j++) acc[i][j] = 0.f;
+#pragma unroll 2
+    for (int kk = 0; kk < NDP; kk++) {
+      const float4 a0 = reinterpret_cast<const float4 *>(sK + kk * NDP)[2 * ty];
+      const float4 a1 = reinterpret_cast<const float4 *>(sK + kk * NDP)[2 * ty + 1];
+      const float4 b0 = *reinterpret_cast<const float4 *>(sB + kk * BROW + c0 + 8 * tx);
+      const float4 b1 = *reinterpret_cast<const float4 *>(sB + kk * BROW + c0 + 8 * tx + 4);
+      const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+      const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+    }
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const int i = c0 + 8 * tx + j;
+      if (i < cnt) {
+        float4 *dst = reinterpret_cast<float4 *>(Y + (long long)s_q[i] * NDP + 8 * ty);
+        dst[0] = make_float4(acc[0][j], acc[1][j], acc[2][j], acc[3][j]);
+        dst[1] = make_float4(acc[4][j], acc[5][j], acc[6][j], acc[7][j]);
+      }
+    }
+  }
+}
+
+// 7. Per target: its taken pairs' contributions summed in list order in FP64,
+// scaled by (-1)^j A_j^k R_t^{-(j+1)}, added to L.
+template <int NDP>
+__global__ void k_m2l_class_reduce(const int *off, long long ncells, const unsigned char *taken, const float *Y,
+                                   const double4 *cell_x, DevTables t, int P, double2 *L) {
+  constexpr int PER = (NDP + 31) / 32;
+  const int lane = threadIdx.x & 31;
   const int NT = t.nterm, ND = nd_of(P);
+  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long c = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < ncells; c += warps) {
+    const int b = off[c], e = off[c + 1];
+    double acc[PER];
+    bool any = false;
 #pragma unroll
-  for (int c = 0; c < 4; c++) {
-    const int cell = tile_cell[tile * kTile + 4 * tx + c];
-    if (cell < 0) continue;
-    const double rt = cell_x[cell].w;
+    for (int u = 0; u < PER; u++) acc[u] = 0.0;
+    for (int q = b; q < e; q++) {
+      if (!taken[q]) continue;
+      any = true;
+      const float *y = Y + (long long)q * NDP;
 #pragma unroll
-    for (int r = 0; r < 4; r++) {
-      const int d = 4 * ty + r;
+      for (int u = 0; u < PER; u++)
+        if (lane + 32 * u < NDP) acc[u] += (double)y[lane + 32 * u];
+    }
+    if (!any) continue;
+    const double rt = cell_x[c].w;
+#pragma unroll
+    for (int u = 0; u < PER; u++) {
+      const int d = lane + 32 * u;
       if (d >= ND) continue;
       int j, k, part;
       dof_decode(d, NT, j, k, part);
       const int o = tri(j) + k;
-      const double w = sgn_pow(j) * t.anm[o] * pow(rt, -(double)(j + 1));
-      const double v = (accd[r][c] + (double)acc[r][c]) * w;
-      double2 *dst = &L[(long long)cell * NT + o];
+      const double v = acc[u] * sgn_pow(j) * t.anm[o] * pow(rt, -(double)(j + 1));
+      double2 *dst = &L[c * NT + o];
       if (part == 0) dst->x += v;
       else dst->y += v;
     }
@@ -520,59 +481,47 @@ bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int
   g.Msr.ensure(nc * NDP);
   k_scale_M_real<<<kNumSMs * 8, 256, 0, st>>>(t, a.M64, a.cell_x, nc, P, g.Msr.p);
   EXA_CHECK_LAUNCH();
-  // ---- tiles
+  // ---- pairs of frequent classes, sorted by class
   g.taken.ensure(n_m2l);
-  g.grp.ensure(nc);
-  g.grp_alt.ensure(nc);
-  g.cidx.ensure(nc);
-  g.cidx_alt.ensure(nc);
   g.left_cnt.ensure(nc);
   g.left_off.ensure(nc + 1);
   g.left_src.ensure(n_m2l);
-  k_gemm_flags<<<kNumSMs * 8, 256, 0, st>>>(a.m2l_off, a.m2l_src, nc, g.pair_slot.p, g.hid.p, a.cell_x, a.cell_pl,
-                                            min_level, max_dl, g.taken.p, g.grp.p, g.cidx.p, g.left_cnt.p);
+  g.skey.ensure(n_m2l);
+  g.skey_alt.ensure(n_m2l);
+  g.pval.ensure(n_m2l);
+  g.pval_alt.ensure(n_m2l);
+  k_gemm_flags<<<kNumSMs * 8, 256, 0, st>>>(a.m2l_off, a.m2l_src, nc, g.pair_slot.p, g.hid.p, a.cell_pl, min_level,
+                                            max_dl, g.taken.p, g.left_cnt.p, g.skey.p, g.pval.p);
   EXA_CHECK_LAUNCH();
   LeftScan ls{g.left_cnt.p, g.left_off.p, nc};
   launch_scan<256, 8>(ls, nullptr, nc, nc, C.scan, C.err.p, st);
   k_left_fill<<<kNumSMs * 8, 256, 0, st>>>(a.m2l_off, a.m2l_src, nc, g.taken.p, a.cell_pl, min_level, max_dl,
                                            g.left_off.p, g.left_src.p);
   EXA_CHECK_LAUNCH();
-  alt = radix_sort_u32(g.grp.p, g.cidx.p, g.grp_alt.p, g.cidx_alt.p, nc, 0, 8, C.sort, C.err.p, st);
-  unsigned *gs = alt ? g.grp_alt.p : g.grp.p;
-  int *csort = alt ? g.cidx_alt.p : g.cidx.p;
-  g.gstart.ensure(256);
-  g.tbase.ensure(256);
-  k_tile_bases<<<1, 256, 0, st>>>(gs, nc, g.gstart.p, g.tbase.p, g.cnt.p + 1);
+  const int end_bit = std::min(32, (bits_for(ncls + 1) + 7) / 8 * 8);
+  alt = radix_sort_u32(g.skey.p, g.pval.p, g.skey_alt.p, g.pval_alt.p, n_m2l, 0, end_bit, C.sort, C.err.p, st);
+  const unsigned *sk = alt ? g.skey_alt.p : g.skey.p;
+  const int *sv = alt ? g.pval_alt.p : g.pval.p;
+  g.cstart.ensure(ncls + 1);
+  g.cbase.ensure(ncls + 1);
+  k_class_ranges<<<(ncls + 256) / 256, 256, 0, st>>>(sk, n_m2l, ncls, g.cstart.p);
   EXA_CHECK_LAUNCH();
-  const long long tiles_max = nc / kTile + 257;
-  g.tile_of.ensure(nc);
-  g.tile_cell.ensure(tiles_max * kTile);
-  EXA_CUDA(cudaMemsetAsync(g.tile_cell.p, 0xff, tiles_max * kTile * sizeof(int), st));
-  k_tile_assign<<<kNumSMs * 4, 256, 0, st>>>(gs, csort, nc, g.gstart.p, g.tbase.p, g.tile_of.p, g.tile_cell.p);
-  EXA_CHECK_LAUNCH();
-  // ---- pairs by (tile, class)
-  g.pkey.ensure(n_m2l);
-  g.pkey_alt.ensure(n_m2l);
-  g.pval.ensure(n_m2l);
-  g.pval_alt.ensure(n_m2l);
-  k_pair_keys<<<kNumSMs * 8, 256, 0, st>>>(a.m2l_off, a.m2l_src, nc, g.pair_slot.p, g.hid.p, g.taken.p, g.tile_of.p,
-                                           g.pkey.p, g.pval.p);
-  EXA_CHECK_LAUNCH();
-  const int end_bit = std::min(64, ((kClsBits + bits_for(tiles_max + 1)) + 7) / 8 * 8);
-  alt = radix_sort_u64((uint64_t *)g.pkey.p, g.pval.p, (uint64_t *)g.pkey_alt.p, g.pval_alt.p, n_m2l, 0, end_bit,
-                       C.sort, C.err.p, st);
-  const unsigned long long *pk = alt ? g.pkey_alt.p : g.pkey.p;
-  const int *pv = alt ? g.pval_alt.p : g.pval.p;
-  // ---- tile products
+  ChunkScan cs2{g.cstart.p, g.cbase.p, ncls};
+  launch_scan<256, 8>(cs2, nullptr, ncls, ncls, C.scan, C.err.p, st);
+  // ---- products per class chunk, then per-target sums
+  g.Y.ensure(n_m2l * NDP);
+  const long long chunks_max = n_m2l / kChunk + ncls + 1;
   switch (NDP) {
-#define EXA_GEMM_CASE(N)                                                                                        \
-  case N: {                                                                                                     \
-    const size_t smem = (size_t)(N * N + N * kTile) * sizeof(float);                                            \
-    set_smem(k_m2l_gemm<N>, smem);                                                                              \
-    k_m2l_gemm<N><<<(unsigned)tiles_max, N / 4 * (kTile / 4), smem, st>>>(pk, pv, n_m2l, g.cnt.p + 1, g.K.p,    \
-                                                                         g.Msr.p, g.tile_cell.p, a.cell_x, t, P, \
-                                                                         a.L64);                                 \
-    break;                                                                                                      \
+#define EXA_GEMM_CASE(N)                                                                                      \
+  case N: {                                                                                                   \
+    const size_t smem = (size_t)(N * N + N * (kChunk + 4)) * sizeof(float);                                   \
+    set_smem(k_m2l_class_gemm<N>, smem);                                                                      \
+    k_m2l_class_gemm<N><<<(unsigned)chunks_max, 128, smem, st>>>(sk, sv, g.cstart.p, g.cbase.p, ncls,        \
+                                                                 a.m2l_src, g.K.p, g.Msr.p, g.Y.p);           \
+    EXA_CHECK_LAUNCH();                                                                                       \
+    k_m2l_class_reduce<N><<<kNumSMs * 8, 256, 0, st>>>(a.m2l_off, nc, g.taken.p, g.Y.p, a.cell_x, t, P, a.L64); \
+    EXA_CHECK_LAUNCH();                                                                                       \
+    break;                                                                                                    \
   }
     EXA_GEMM_CASE(16)
     EXA_GEMM_CASE(48)
@@ -581,7 +530,6 @@ bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int
 #undef EXA_GEMM_CASE
     default: return false;
   }
-  EXA_CHECK_LAUNCH();
   return true;
 }
 
