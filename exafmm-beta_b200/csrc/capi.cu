@@ -56,6 +56,7 @@ struct Engine {
   M2LGemmBufs gemm;         // class-grouped tile M2L (mixed form)
   DBuf<double2> lat;        // periodic lattice: supercell multipoles and warp partials
   DBuf<double> dip;         // dipole reduction scratch and result
+  DBuf<unsigned long long> work;  // work counter of persistent kernels
   DBuf<double4> trg, out;
   Timing tm;
   bool tree_ok = false, up_ok = false, lists_ok = false;
@@ -202,7 +203,8 @@ struct Engine {
       if (mixed && C.prm.mixed_p2p) {
         x32.ensure(2 * C.tree.n);  // hi and lo float4 per body
         rel_bodies32(a, x32.p);
-        p2p_mixed(a, x32.p, C.prm.images > 0);
+        work.ensure(1);
+        p2p_mixed(a, x32.p, C.prm.images > 0, work.p);
       } else {
         p2p_fp64(a);
       }

@@ -85,7 +85,8 @@ void dipole_correction_fp64(const double4 *xt, double4 *trg, long long n, double
 // Mixed-precision P2P (p2p32.cu): bodies as two-float pairs relative to the
 // root center; periodic selects the form that tests every pair for r = 0.
 void rel_bodies32(const FmmArgs &a, float4 *x32);
-void p2p_mixed(const FmmArgs &a, const float4 *x32, bool periodic);
+// counter: one device word of scratch (the kernel's work counter).
+void p2p_mixed(const FmmArgs &a, const float4 *x32, bool periodic, unsigned long long *counter);
 
 // Interaction lists of the dual tree traversal (traverse.cu).
 struct ListBufs {

@@ -31,6 +31,7 @@
 // bounds this kernel.  The rsqrt flushes subnormal inputs, so a pair closer
 // than about 1e-19 (an r^2 below the FP32 normal range) also contributes
 // nothing; such inputs need the FP64 plain method.
+#include <algorithm>
 #include <stdexcept>
 
 #include "fmm.h"
@@ -309,24 +310,32 @@ __device__ __forceinline__ void p2p_leaf(Stage &sm, int4 cb, int b, int e, const
   }
 }
 
-// One block of one warp per target cell: the hardware block scheduler hands
-// out cells as warps finish, which balances leaves of very different cost.
+// Persistent one-warp blocks, as many as fit on the GPU; each takes target
+// cells in order from a counter until none is left, so leaves of very
+// different cost balance out without the launch of one block per cell.
 template <bool PERIODIC>
 __global__ void __launch_bounds__(32, 16)
-k_p2p32(const int *off, const int *src, const int4 *cell_b, const float4 *x32, double4 *trg, double cycle) {
+k_p2p32(const int *off, const int *src, long long ncells, const int4 *cell_b, const float4 *x32, double4 *trg,
+        double cycle, unsigned long long *next) {
   __shared__ Stage sm;
-  const long long c = blockIdx.x;
-  const int b = off[c], e = off[c + 1];
-  if (b == e) return;
-  const int4 cb = cell_b[c];
-  if (cb.y <= 8)
-    p2p_leaf<4, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
-  else if (cb.y <= 16)
-    p2p_leaf<8, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
-  else if (cb.y <= 32)
-    p2p_leaf<16, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
-  else
-    p2p_leaf<32, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
+  for (;;) {
+    unsigned long long c = 0;
+    if (threadIdx.x == 0) c = atomicAdd(next, 1ull);
+    c = __shfl_sync(kFull, c, 0);
+    if ((long long)c >= ncells) return;
+    const int b = off[c], e = off[c + 1];
+    if (b == e) continue;
+    const int4 cb = cell_b[c];
+    if (cb.y <= 8)
+      p2p_leaf<4, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
+    else if (cb.y <= 16)
+      p2p_leaf<8, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
+    else if (cb.y <= 32)
+      p2p_leaf<16, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
+    else
+      p2p_leaf<32, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
+    __syncwarp();  // the stage buffer is free before the next cell's first fill
+  }
 }
 
 }  // namespace
@@ -339,14 +348,15 @@ void rel_bodies32(const FmmArgs &a, float4 *x32) {
   EXA_CHECK_LAUNCH();
 }
 
-void p2p_mixed(const FmmArgs &a, const float4 *x32, bool periodic) {
+void p2p_mixed(const FmmArgs &a, const float4 *x32, bool periodic, unsigned long long *counter) {
   if (a.ncells <= 0) return;
-  if (a.ncells > 0x7fffffffLL) throw std::runtime_error("p2p_mixed: too many cells for one launch");
-  const unsigned grid = (unsigned)a.ncells;
+  EXA_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), a.stream));
+  const unsigned grid = (unsigned)std::min<long long>(a.ncells, (long long)kNumSMs * 16);
   if (periodic)
-    k_p2p32<true><<<grid, 32, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.cell_b, x32, a.trg64, a.cycle);
+    k_p2p32<true><<<grid, 32, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b, x32, a.trg64, a.cycle, counter);
   else
-    k_p2p32<false><<<grid, 32, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.cell_b, x32, a.trg64, a.cycle);
+    k_p2p32<false><<<grid, 32, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b, x32, a.trg64, a.cycle,
+                                              counter);
   EXA_CHECK_LAUNCH();
 }
 
