@@ -300,21 +300,25 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // 6. One block per chunk (one class, up to kChunk pairs): Y[pair] = K_class x Ms[source].
-// The operator and the gathered source columns sit in shared memory; 128
-// threads hold 8 x 8 outputs each (NDP / 8 row groups x 16 column groups).
-// Y is written per pair at its position in the target-grouped list.
+// The operator ([input][output]) and the sources' columns ([pair][input], row
+// stride BSTR) are copied into shared memory with cp.async.  Thread (tx, ty)
+// holds rows 4ty..4ty+3 and H+4ty..H+4ty+3 (H = NDP / 2) of columns tx + 4j,
+// j < 8: both operand reads are conflict-free (rows: consecutive threads take
+// consecutive 16-byte groups; columns: the four tx read four distinct banks),
+// and every 16-byte column read feeds 32 multiply-adds over four inputs.
 template <int NDP>
 __global__ void __launch_bounds__(128)
 k_m2l_class_gemm(const unsigned *skey, const int *sval, const int *cstart, const int *cbase, int ncls,
                  const int *src, const float *Kt, const float *Msr, float *Y) {
-  constexpr int RG = NDP / 8;                    // row groups of 8
-  constexpr int CG = 128 / RG;                   // column groups of 8 (16 at NDP = 64)
-  constexpr int NC = CG * 8;                     // columns per pass (128 at NDP = 64)
-  constexpr int BROW = kChunk + 4;               // padded column-block row (floats)
+  constexpr int H = NDP / 2;
+  constexpr int RG = H / 4;                      // row groups: 8 at NDP = 64
+  constexpr int CG = 128 / RG;                   // column groups: 16 at NDP = 64
+  constexpr int NC = CG * 8;                     // columns per pass
+  constexpr int BSTR = NDP + 4;                  // floats per staged column
   extern __shared__ float4 smem4[];
   float *sK = reinterpret_cast<float *>(smem4);  // [NDP input][NDP output]
-  float *sB = sK + NDP * NDP;                    // [NDP input][BROW]: column = pair of the chunk
-  __shared__ int s_q[kChunk];
+  float *sB = sK + NDP * NDP;                    // [kChunk pair][BSTR]
+  __shared__ int s_q[kChunk], s_src[kChunk];
   const int chunk = blockIdx.x;
   if (chunk >= cbase[ncls]) return;
   int lo = 0, hi = ncls;  // class of this chunk: last c with cbase[c] <= chunk
@@ -328,50 +332,55 @@ k_m2l_class_gemm(const unsigned *skey, const int *sval, const int *cstart, const
   const int cnt = min(kChunk, cstart[cls + 1] - p0);
   const float *Kg = Kt + (long long)cls * NDP * NDP;
   for (int i = threadIdx.x; i < NDP * NDP / 4; i += 128) cp_async16(sK + 4 * i, Kg + 4 * i);
-  cp_async_commit();
-  if (threadIdx.x < kChunk) s_q[threadIdx.x] = threadIdx.x < cnt ? sval[p0 + threadIdx.x] : -1;
-  __syncthreads();
-  // gather: thread (pair i, quarter) copies 16 of the source's NDP values, transposed
-  for (int w = threadIdx.x; w < kChunk * (NDP / 4); w += 128) {
-    const int i = w % kChunk, q4 = w / kChunk;
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (i < cnt) v = reinterpret_cast<const float4 *>(Msr + (long long)(src[s_q[i]] & 0x3ffffff) * NDP)[q4];
-    sB[(4 * q4 + 0) * BROW + i] = v.x;
-    sB[(4 * q4 + 1) * BROW + i] = v.y;
-    sB[(4 * q4 + 2) * BROW + i] = v.z;
-    sB[(4 * q4 + 3) * BROW + i] = v.w;
+  if (threadIdx.x < kChunk) {
+    const int q = threadIdx.x < cnt ? sval[p0 + threadIdx.x] : -1;
+    s_q[threadIdx.x] = q;
+    s_src[threadIdx.x] = q >= 0 ? (src[q] & 0x3ffffff) : -1;
   }
+  __syncthreads();
+  for (int w = threadIdx.x; w < kChunk * (NDP / 4); w += 128) {
+    const int i = w / (NDP / 4), q4 = w % (NDP / 4);
+    float *dst = sB + i * BSTR + 4 * q4;
+    if (i < cnt) cp_async16(dst, Msr + (long long)s_src[i] * NDP + 4 * q4);
+    else *reinterpret_cast<float4 *>(dst) = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  cp_async_commit();
   cp_async_wait_all();
   __syncthreads();
   const int ty = threadIdx.x % RG, tx = threadIdx.x / RG;
-  if (tx >= CG) return;  // 128 threads need not split evenly into row groups (no barrier follows)
+  if (tx >= CG) return;  // 128 threads need not split evenly (no barrier follows)
   for (int c0 = 0; c0 < cnt; c0 += NC) {
-    if (c0 + 8 * tx >= cnt) continue;
+    if (c0 + tx >= cnt) continue;
     float acc[8][8];
 #pragma unroll
     for (int i = 0; i < 8; i++)
 #pragma unroll
       for (int j = 0; j < 8; j++) acc[i][j] = 0.f;
-#pragma unroll 2
-    for (int kk = 0; kk < NDP; kk++) {
-      const float4 a0 = reinterpret_cast<const float4 *>(sK + kk * NDP)[2 * ty];
-      const float4 a1 = reinterpret_cast<const float4 *>(sK + kk * NDP)[2 * ty + 1];
-      const float4 b0 = *reinterpret_cast<const float4 *>(sB + kk * BROW + c0 + 8 * tx);
-      const float4 b1 = *reinterpret_cast<const float4 *>(sB + kk * BROW + c0 + 8 * tx + 4);
-      const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-      const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+    for (int k4 = 0; k4 < NDP; k4 += 4) {
+      float4 b[8];
 #pragma unroll
-      for (int i = 0; i < 8; i++)
+      for (int j = 0; j < 8; j++)  // columns past the chunk (discarded below) read its last column
+        b[j] = *reinterpret_cast<const float4 *>(sB + min(c0 + tx + CG * j, kChunk - 1) * BSTR + k4);
 #pragma unroll
-        for (int j = 0; j < 8; j++) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+      for (int kq = 0; kq < 4; kq++) {
+        const float4 a0 = *reinterpret_cast<const float4 *>(sK + (k4 + kq) * NDP + 4 * ty);
+        const float4 a1 = *reinterpret_cast<const float4 *>(sK + (k4 + kq) * NDP + H + 4 * ty);
+        const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          const float bv = kq == 0 ? b[j].x : kq == 1 ? b[j].y : kq == 2 ? b[j].z : b[j].w;
+#pragma unroll
+          for (int i = 0; i < 8; i++) acc[i][j] = fmaf(av[i], bv, acc[i][j]);
+        }
+      }
     }
 #pragma unroll
     for (int j = 0; j < 8; j++) {
-      const int i = c0 + 8 * tx + j;
+      const int i = c0 + tx + CG * j;
       if (i < cnt) {
-        float4 *dst = reinterpret_cast<float4 *>(Y + (long long)s_q[i] * NDP + 8 * ty);
-        dst[0] = make_float4(acc[0][j], acc[1][j], acc[2][j], acc[3][j]);
-        dst[1] = make_float4(acc[4][j], acc[5][j], acc[6][j], acc[7][j]);
+        float *y = Y + (long long)s_q[i] * NDP;
+        *reinterpret_cast<float4 *>(y + 4 * ty) = make_float4(acc[0][j], acc[1][j], acc[2][j], acc[3][j]);
+        *reinterpret_cast<float4 *>(y + H + 4 * ty) = make_float4(acc[4][j], acc[5][j], acc[6][j], acc[7][j]);
       }
     }
   }
@@ -514,7 +523,7 @@ bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int
   switch (NDP) {
 #define EXA_GEMM_CASE(N)                                                                                      \
   case N: {                                                                                                   \
-    const size_t smem = (size_t)(N * N + N * (kChunk + 4)) * sizeof(float);                                   \
+    const size_t smem = (size_t)(N * N + kChunk * (N + 4)) * sizeof(float);                                   \
     set_smem(k_m2l_class_gemm<N>, smem);                                                                      \
     k_m2l_class_gemm<N><<<(unsigned)chunks_max, 128, smem, st>>>(sk, sv, g.cstart.p, g.cbase.p, ncls,        \
                                                                  a.m2l_src, g.K.p, g.Msr.p, g.Y.p);           \
