@@ -180,6 +180,7 @@ struct Engine {
       const bool m2l32 = mixed && C.prm.mixed_m2l && m2l_fast_supported(C.prm.P, true);
       if (m2l32) {
         FmmArgs left = a;  // the pairs the pair-by-pair FP32 kernel takes
+        gemm.force = C.prm.mixed_gemm == 2;
         if (C.prm.mixed_gemm && m2l_gemm(C, a, gemm, lists.n_m2l, C.prm.mixed_min_level, C.prm.mixed_max_dl)) {
           left.m2l_off = gemm.left_off.p;
           left.m2l_src = gemm.left_src.p;
@@ -274,22 +275,31 @@ struct exafmm_ctx {
 
 namespace exafmm_b200 {
 thread_local long long *g_dbuf_account = nullptr;
+thread_local cudaStream_t g_dbuf_stream = nullptr;
 }
 
 namespace {
 thread_local std::string g_create_error;
 
-// Charges the buffers a call allocates to one context's byte counter.
+// Charges the buffers a call allocates to one context's byte counter and
+// orders their allocation on its stream.
 struct AccountScope {
   long long *prev;
-  explicit AccountScope(long long *a) : prev(g_dbuf_account) { g_dbuf_account = a; }
-  ~AccountScope() { g_dbuf_account = prev; }
+  cudaStream_t prev_st;
+  AccountScope(long long *a, cudaStream_t s) : prev(g_dbuf_account), prev_st(g_dbuf_stream) {
+    g_dbuf_account = a;
+    g_dbuf_stream = s;
+  }
+  ~AccountScope() {
+    g_dbuf_account = prev;
+    g_dbuf_stream = prev_st;
+  }
 };
 
 template <typename F>
 int guarded(exafmm_ctx *ctx, F &&f) {
   if (!ctx) return 2;
-  AccountScope scope(&ctx->E.C.dev_bytes);
+  AccountScope scope(&ctx->E.C.dev_bytes, ctx->E.C.stream);
   try {
     f();
     return 0;
@@ -330,7 +340,7 @@ int exafmm_create(exafmm_ctx **out, int P, double theta, int ncrit, int nspawn, 
     if (device >= 0) EXA_CUDA(cudaSetDevice(device));
     std::unique_ptr<exafmm_ctx> c(new exafmm_ctx);
     Context &C = c->E.C;
-    AccountScope scope(&C.dev_bytes);
+    AccountScope scope(&C.dev_bytes, nullptr);  // the stream is made below
     EXA_CUDA(cudaGetDevice(&C.device));
     C.prm.P = P;
     C.prm.theta = theta;
@@ -340,6 +350,16 @@ int exafmm_create(exafmm_ctx **out, int P, double theta, int ncrit, int nspawn, 
     C.prm.cycle = cycle;
     C.prm.precision = precision;
     EXA_CUDA(cudaStreamCreateWithFlags(&C.stream, cudaStreamNonBlocking));
+    {
+      // Buffers come from the device's stream-ordered pool; keep what contexts
+      // free in the pool for reuse instead of handing it back to the driver at
+      // every synchronization.
+      cudaMemPool_t pool;
+      EXA_CUDA(cudaDeviceGetDefaultMemPool(&pool, C.device));
+      unsigned long long keep = ~0ull;
+      EXA_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
+    g_dbuf_stream = C.stream;
     C.err.ensure(1);
     EXA_CUDA(cudaMemsetAsync(C.err.p, 0, sizeof(int), C.stream));
     EXA_CUDA(cudaMallocHost((void **)&C.err_host, sizeof(int)));
@@ -394,9 +414,9 @@ int exafmm_set_mixed_policy(exafmm_ctx *ctx, int m2l_fp32, int p2p_fp32, int min
   return guarded(ctx, [&] {
     Params &p = ctx->E.C.prm;
     if (min_level < 0 || max_dl < 0) throw std::runtime_error("min_level and max_dl must be >= 0");
-    if (m2l_fp32 < 0 || m2l_fp32 > 2) throw std::runtime_error("m2l_fp32 must be 0, 1 or 2");
+    if (m2l_fp32 < 0 || m2l_fp32 > 3) throw std::runtime_error("m2l_fp32 must be 0, 1, 2 or 3");
     p.mixed_m2l = m2l_fp32 != 0;
-    p.mixed_gemm = m2l_fp32 == 1;
+    p.mixed_gemm = m2l_fp32 == 1 ? 1 : (m2l_fp32 == 3 ? 2 : 0);
     p.mixed_p2p = p2p_fp32 != 0;
     p.mixed_min_level = min_level;
     p.mixed_max_dl = max_dl;

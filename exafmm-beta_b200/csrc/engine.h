@@ -15,29 +15,38 @@ namespace exafmm_b200 {
 // Device bytes held by the context whose entry point is running on this
 // thread (null outside such a call): grow-only buffers charge it.
 extern thread_local long long *g_dbuf_account;
+// That context's stream: buffers are allocated and freed in its order
+// (cudaMallocAsync / cudaFreeAsync), so a context that grows does not stall
+// the device for the others, as cudaFree would.
+extern thread_local cudaStream_t g_dbuf_stream;
 
 template <typename T>
 struct DBuf {
   T *p = nullptr;
   size_t cap = 0;
   long long *acct = nullptr;  // byte counter of the owning context, set at allocation
+  cudaStream_t st = nullptr;  // stream of a stream-ordered allocation (else plain cudaMalloc)
   void ensure(size_t n) {
     if (n <= cap) return;
     release();
     size_t want = n < 16 ? 16 : n;
-    EXA_CUDA(cudaMalloc((void **)&p, want * sizeof(T)));
+    st = g_dbuf_stream;
+    if (st) EXA_CUDA(cudaMallocAsync((void **)&p, want * sizeof(T), st));
+    else EXA_CUDA(cudaMalloc((void **)&p, want * sizeof(T)));
     cap = want;
     acct = g_dbuf_account;
     if (acct) *acct += (long long)(want * sizeof(T));
   }
   void release() {
     if (p) {
-      cudaFree(p);
+      if (st) cudaFreeAsync(p, st);
+      else cudaFree(p);
       if (acct) *acct -= (long long)(cap * sizeof(T));
     }
     p = nullptr;
     cap = 0;
     acct = nullptr;
+    st = nullptr;
   }
   T *get() const { return p; }
   ~DBuf() { release(); }
@@ -63,11 +72,12 @@ void launch_scan(const Producer &prod, const long long *n_dev, long long n_host,
   constexpr int TILE = BLOCK * ITEMS;
   long long tiles = (max_items + TILE - 1) / TILE + 1;
   ScanScratch s = w.prepare(st, err, tiles, sizeof(typename Producer::T));
+  // enough tiles for the most items the scan can see (the count on the device
+  // is at most max_items), so small scans do not occupy the whole GPU
   int grid = kNumSMs * 4;
-  if (!n_dev) {
-    long long need = (n_host + TILE - 1) / TILE;
-    if (need < grid) grid = need > 0 ? (int)need : 1;
-  }
+  const long long bound = n_dev ? max_items : n_host;
+  const long long need = (bound + TILE - 1) / TILE;
+  if (need < grid) grid = need > 0 ? (int)need : 1;
   scan_kernel<BLOCK, ITEMS, Producer><<<grid, BLOCK, 0, st>>>(prod, n_dev, n_host, s, w.epoch);
   EXA_CHECK_LAUNCH();
 }

@@ -68,6 +68,7 @@ struct M2LGemmBufs {
   DBuf<float> Y;                      // per list entry: the pair's contribution (real dofs)
   DBuf<int> cnt;
   DBuf<int> left_cnt, left_off, left_src;
+  bool force = false;  // use the class products whatever the size (parity tests)
 };
 bool m2l_gemm_supported(int P);
 bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int min_level, int max_dl);

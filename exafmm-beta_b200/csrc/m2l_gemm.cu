@@ -441,16 +441,29 @@ void set_smem(F f, size_t bytes) {
 
 bool m2l_gemm_supported(int P) { return P == 4 || P == 6 || P == 8 || P == 10; }
 
+// Where the class products beat the pair-by-pair kernel for one solve on a
+// B200: from about 1M pairs at P = 8 and 0.4M pairs at P = 10; at P <= 6 the
+// pair-by-pair code is small and fast enough that they never do.
+bool m2l_gemm_worthwhile(int P, long long n_m2l) {
+  if (P == 8) return n_m2l >= 1000000;
+  if (P == 10) return n_m2l >= 400000;
+  return false;
+}
+
 bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int min_level, int max_dl) {
   const int P = a.P;
   if (!m2l_gemm_supported(P) || a.ncells <= 0 || n_m2l <= 0) return false;
+  if (!g.force && !m2l_gemm_worthwhile(P, n_m2l)) return false;
   cudaStream_t st = a.stream;
   const DevTables &t = device_tables(P);
   const long long nc = a.ncells;
   const int NDP = ndp_of(P);
   // ---- classes
-  long long hcap = 1 << 16;
-  while (hcap < 4 * std::min<long long>(n_m2l, 1LL << 22)) hcap <<= 1;
+  // classes are far fewer than pairs (thousands to ~1e5): a table of about a
+  // sixteenth of the pairs, within [2^14, 2^20] slots; a pair that finds no
+  // slot stays with the pair-by-pair kernel
+  long long hcap = 1 << 14;
+  while (hcap < n_m2l / 16 && hcap < (1LL << 20)) hcap <<= 1;
   g.hk.ensure(hcap);
   g.hc.ensure(hcap);
   g.hid.ensure(hcap);

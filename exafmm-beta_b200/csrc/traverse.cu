@@ -206,24 +206,28 @@ bool traverse(Context &C, ListBufs &lb) {
   ps.m2l_cap = lb.m2l_cap;
   ps.p2p_cap = lb.p2p_cap;
   ps.err = C.err.p;
-  for (int s = 0; s < kMaxSweeps; s++) {
+  // Every split takes one side of a pair a level deeper and leaf pairs are
+  // decided where they are met, so a tree of depth d needs at most 2d + 1
+  // sweeps; two more are launched, and the queue after the last must be empty.
+  const int nsw = std::min(kMaxSweeps, 2 * (C.tree.depth + 1) + 2);
+  for (int s = 0; s < nsw; s++) {
     ps.sweep = s;
     ps.qin = (s & 1) ? lb.q1.p : lb.q0.p;
     ps.qout = (s & 1) ? lb.q0.p : lb.q1.p;
     launch_scan<128, 4>(ps, lb.cnt.p + 3 * s, 0, lb.q_cap, C.scan, C.err.p, st);
   }
   long long cnt[3 * (kMaxSweeps + 1)];
-  EXA_CUDA(cudaMemcpyAsync(cnt, lb.cnt.p, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+  EXA_CUDA(cudaMemcpyAsync(cnt, lb.cnt.p, 3 * (nsw + 1) * sizeof(long long), cudaMemcpyDeviceToHost, st));
   EXA_CUDA(cudaMemcpyAsync(C.err_host, C.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   EXA_CUDA(cudaStreamSynchronize(st));
   long long qmax = 0;
   lb.sweeps = 0;
-  for (int s = 0; s <= kMaxSweeps; s++) {
+  for (int s = 0; s <= nsw; s++) {
     qmax = cnt[3 * s] > qmax ? cnt[3 * s] : qmax;
     if (cnt[3 * s] > 0) lb.sweeps = s + 1;
   }
-  lb.n_m2l = cnt[3 * kMaxSweeps + 1];
-  lb.n_p2p = cnt[3 * kMaxSweeps + 2];
+  lb.n_m2l = cnt[3 * nsw + 1];
+  lb.n_p2p = cnt[3 * nsw + 2];
   const int e = *C.err_host;
   if (e & (kErrQueueOverflow | kErrListOverflow)) {
     lb.q_cap = (qmax > lb.q_cap ? qmax : 2 * lb.q_cap) * 5 / 4 + 1024;
@@ -232,7 +236,7 @@ bool traverse(Context &C, ListBufs &lb) {
     EXA_CUDA(cudaMemsetAsync(C.err.p, 0, sizeof(int), st));
     return false;
   }
-  if (lb.sweeps >= kMaxSweeps) throw_msg("traversal did not terminate within the sweep limit");
+  if (lb.sweeps > nsw) throw_msg("traversal did not terminate within the sweep limit");
   group_by_target(C, lb.m2l.p, lb.n_m2l, ncells, lb, lb.m2l_off, lb.m2l_src);
   group_by_target(C, lb.p2p.p, lb.n_p2p, ncells, lb, lb.p2p_off, lb.p2p_src);
   return true;

@@ -11,6 +11,8 @@
 // table is laid out exactly as nodes2cells does (build_tree.h:123-165).  Inside
 // a leaf the reference keeps input order (its partitions are stable), so a final
 // per-leaf sort restores ascending input index there.
+#include <algorithm>
+
 #include "context.h"
 #include "drift.cuh"
 
@@ -504,7 +506,8 @@ void build_tree(Context &C) {
   k_tree_root<<<1, 32, 0, st>>>(n, T.lvl.p, T.nd_begin.p, T.nd_count.p, T.nd_x.p, T.box.p, T.nd_cell.p,
                                 T.nd_pcell.p, T.nd_ichild.p);
   EXA_CHECK_LAUNCH();
-  const int node_grid = kNumSMs * 4;
+  // per-level kernels: eight threads per node at most node_cap nodes
+  const int node_grid = (int)std::max<long long>(1, std::min<long long>(kNumSMs * 4, (8 * T.node_cap + 255) / 256));
   long long *lvl_n = T.lvl.p + 2 * (kMaxLevels + 1);
   long long *lvl_s = lvl_n + 1;
   for (int l = 0; l <= kMaxLevels; l++) {

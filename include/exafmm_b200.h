@@ -55,8 +55,10 @@ int exafmm_set_params(exafmm_ctx *ctx, int P, double theta, int ncrit, int nspaw
 
 /* Mixed form only: which operators run in FP32 and which M2L pairs may
  * (target level >= min_level, |level difference| <= max_dl); the rest runs in
- * FP64.  m2l_fp32: 0 = FP64, 1 = FP32 with frequent offset classes evaluated
- * as class-grouped tiles, 2 = FP32 pair by pair only.  p2p_fp32: 0 or 1.
+ * FP64.  m2l_fp32: 0 = FP64; 1 = FP32, with the pairs of frequent offset
+ * classes evaluated as dense per-class products when the system is large
+ * enough for that to pay (P = 8 or 10); 2 = FP32 pair by pair only; 3 = FP32
+ * with the per-class products at any size.  p2p_fp32: 0 or 1.
  * Defaults: 1, 1, 4, 3.  No counterpart in the reference (its precision is a
  * compile-time switch, EXAFMM_SINGLE). */
 int exafmm_set_mixed_policy(exafmm_ctx *ctx, int m2l_fp32, int p2p_fp32, int min_level, int max_dl);

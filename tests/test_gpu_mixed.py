@@ -57,7 +57,7 @@ def test_tile_m2l_matches_pair_by_pair(ex, datasets, P):
     for gen, n in (("plummer", 60000), ("cube", 40000), ("sphere", 30000)):
         x = getattr(datasets, gen)(n, seed=P)
         res = []
-        for prec, pol in ((ex.FP64, None), (ex.MIXED, 1), (ex.MIXED, 2)):
+        for prec, pol in ((ex.FP64, None), (ex.MIXED, 3), (ex.MIXED, 2)):
             f = ex.Fmm(P=P, theta=0.4, ncrit=32, precision=prec)
             if pol is not None:
                 f.set_mixed_policy(m2l_fp32=pol)
