@@ -40,7 +40,10 @@ PKG_DIR = os.path.join(ROOT, "exafmm-beta_b200")
 WORKLOAD = dict(name="plummer_4m_p8", n=4_194_304, P=8, theta=0.35, ncrit=64, nspawn=5000, seed=2)
 METRIC = "FMM bodies/s (full mixed-precision solve, Plummer N=4,194,304, P=8, theta=0.35)"
 CPU_SAMPLE_N = 262_144
-M2L_DRAM_BYTES_PER_PAIR = 27.5
+# DRAM bytes per M2L pair of the mixed M2L phase at P = 8: the per-class products write each
+# pair's contribution (256 B) and the per-target pass reads it back; measured (DRAM throughput
+# x duration of those two kernels) in the ncu capture of the 1M-body case, scaled by pairs
+M2L_DRAM_BYTES_PER_PAIR = 440.0
 
 
 def _package():
@@ -342,16 +345,17 @@ def main():
     alg_bytes = n_m2l * (nterm * cplx + 8) + info["ncells"] * 2 * nterm * cplx
     alg_flops = n_m2l * 8 * nterm * P * P
     achieved = alg_bytes / (m2l_ms / 1e3) / 1e9
-    # DRAM bytes per M2L pair of the four FP32 part launches, from the ncu capture of the same
-    # kernels on the 1M-body case (profiles/m2l_p2p_plummer_1m_p8_mixed_ncrit128.txt), scaled by pairs
     traffic = M2L_DRAM_BYTES_PER_PAIR * n_m2l if prec == pkg.MIXED and P == 8 else None
     roofline = {
         "kernel": "m2l", "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
         "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
         "ms_per_launch": m2l_ms, "algorithmic_bytes": alg_bytes, "algorithmic_flops": alg_flops,
         "achieved_tflops": alg_flops / (m2l_ms / 1e3) / 1e12,
-        "note": "M2L runs on the CUDA-core FP32 (mixed) / FP64 pipes and is compute-bound (~50 flop/B): "
-                "frac is its distance from the memory roof; achieved_tflops is its arithmetic rate",
+        "note": "the M2L phase: per-offset-class dense products on the CUDA-core FP32 pipes (4,096 "
+                "multiply-adds per pair at P=8) plus a per-target FP64 pass over their contributions; "
+                "compute-bound, so frac is its distance from the memory roof, achieved_tflops its rate "
+                "by the reference's per-pair count (8 NTERM P^2), and traffic above the algorithmic "
+                "bytes is the contributions' round trip through HBM",
     }
 
     line = {
