@@ -41,9 +41,10 @@ WORKLOAD = dict(name="plummer_4m_p8", n=4_194_304, P=8, theta=0.35, ncrit=64, ns
 METRIC = "FMM bodies/s (full mixed-precision solve, Plummer N=4,194,304, P=8, theta=0.35)"
 CPU_SAMPLE_N = 262_144
 # DRAM bytes per M2L pair of the mixed M2L phase at P = 8: the per-class products write each
-# pair's contribution (256 B) and the per-target pass reads it back; measured (DRAM throughput
-# x duration of those two kernels) in the ncu capture of the 1M-body case, scaled by pairs
-M2L_DRAM_BYTES_PER_PAIR = 440.0
+# pair's contribution (256 B) and the per-target pass reads it back; dram__bytes_read.sum +
+# dram__bytes_write.sum of those two kernels in the ncu capture of the 1M-body case (4.41 GB
+# for 8,233,680 pairs), scaled by pairs
+M2L_DRAM_BYTES_PER_PAIR = 535.0
 
 
 def _package():
@@ -187,6 +188,7 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--ncrit", type=int, default=0, help="0: pick the fastest of 32, 64, 128 during warm-up")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--m2l-policy", type=int, default=1, help=argparse.SUPPRESS)  # Fmm.set_mixed_policy m2l_fp32
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain-method comparison run")
     ap.add_argument("--workload", default="solve", choices=["solve", "batch", "serve", "periodic"],
                     help="solve: the single large solve (default); batch: 512 independent systems per step; "
@@ -227,8 +229,11 @@ def main():
     hout = torch.empty_like(hx).pin_memory()
 
     def make(precision, ncrit):
-        return pkg.Fmm(P=wl["P"], theta=wl["theta"], ncrit=ncrit, nspawn=wl["nspawn"], precision=precision,
-                       device=local_rank)
+        f = pkg.Fmm(P=wl["P"], theta=wl["theta"], ncrit=ncrit, nspawn=wl["nspawn"], precision=precision,
+                    device=local_rank)
+        if precision == pkg.MIXED and args.m2l_policy != 1:
+            f.set_mixed_policy(m2l_fp32=args.m2l_policy)
+        return f
 
     def solve_device(f, out):
         f.set_bodies_device(dx.data_ptr(), n)
@@ -351,11 +356,12 @@ def main():
         "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
         "ms_per_launch": m2l_ms, "algorithmic_bytes": alg_bytes, "algorithmic_flops": alg_flops,
         "achieved_tflops": alg_flops / (m2l_ms / 1e3) / 1e12,
-        "note": "the M2L phase: per-offset-class dense products on the CUDA-core FP32 pipes (4,096 "
-                "multiply-adds per pair at P=8) plus a per-target FP64 pass over their contributions; "
-                "compute-bound, so frac is its distance from the memory roof, achieved_tflops its rate "
-                "by the reference's per-pair count (8 NTERM P^2), and traffic above the algorithmic "
-                "bytes is the contributions' round trip through HBM",
+        "note": "the M2L phase: per-offset-class dense products on the tensor cores (tcgen05, bf16x3 "
+                "pieces, 6 x 4,096 multiply-adds per pair at P=8, FP32 accumulation in TMEM) plus a "
+                "per-target FP64 pass over their contributions, the class hashing and sorting, and the "
+                "FP64 pairs of the root levels; frac is its distance from the memory roof, "
+                "achieved_tflops its rate by the reference's per-pair count (8 NTERM P^2), and traffic "
+                "above the algorithmic bytes is the contributions' round trip through HBM",
     }
 
     line = {

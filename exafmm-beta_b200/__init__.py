@@ -184,8 +184,10 @@ class Fmm:
 
     def set_mixed_policy(self, m2l_fp32=1, p2p_fp32=True, min_level=4, max_dl=3):
         """Mixed form: which operators run in FP32 and which M2L pairs may.
-        m2l_fp32: 0 FP64; 1 FP32 with per-class products where they pay; 2 FP32 pair by
-        pair; 3 FP32 with per-class products at any size."""
+        m2l_fp32: 0 FP64; 1 FP32 with per-class products on the tensor cores (bf16x3
+        pieces, FP32 accumulation) where they pay; 2 FP32 pair by pair; 3 as 1 with the
+        per-class products at any size; 4 and 5 as 1 and 3 with the per-class products in
+        FP32 on the CUDA cores."""
         self._check(lib().exafmm_set_mixed_policy(self._h, int(m2l_fp32), int(p2p_fp32), min_level, max_dl))
 
     # ---- solve steps (examples/fmm.cxx:163-179) ----

@@ -181,6 +181,7 @@ struct Engine {
       if (m2l32) {
         FmmArgs left = a;  // the pairs the pair-by-pair FP32 kernel takes
         gemm.force = C.prm.mixed_gemm == 2;
+        gemm.tensor_cores = C.prm.mixed_gemm_tc != 0;
         if (C.prm.mixed_gemm && m2l_gemm(C, a, gemm, lists.n_m2l, C.prm.mixed_min_level, C.prm.mixed_max_dl)) {
           left.m2l_off = gemm.left_off.p;
           left.m2l_src = gemm.left_src.p;
@@ -414,9 +415,10 @@ int exafmm_set_mixed_policy(exafmm_ctx *ctx, int m2l_fp32, int p2p_fp32, int min
   return guarded(ctx, [&] {
     Params &p = ctx->E.C.prm;
     if (min_level < 0 || max_dl < 0) throw std::runtime_error("min_level and max_dl must be >= 0");
-    if (m2l_fp32 < 0 || m2l_fp32 > 3) throw std::runtime_error("m2l_fp32 must be 0, 1, 2 or 3");
+    if (m2l_fp32 < 0 || m2l_fp32 > 5) throw std::runtime_error("m2l_fp32 must be in 0..5");
     p.mixed_m2l = m2l_fp32 != 0;
-    p.mixed_gemm = m2l_fp32 == 1 ? 1 : (m2l_fp32 == 3 ? 2 : 0);
+    p.mixed_gemm = (m2l_fp32 == 1 || m2l_fp32 == 4) ? 1 : ((m2l_fp32 == 3 || m2l_fp32 == 5) ? 2 : 0);
+    p.mixed_gemm_tc = m2l_fp32 <= 3;
     p.mixed_p2p = p2p_fp32 != 0;
     p.mixed_min_level = min_level;
     p.mixed_max_dl = max_dl;

@@ -63,6 +63,7 @@ enum DeviceError : int {
   kErrQueueOverflow = 2,     // traversal pair queue exceeded its capacity
   kErrListOverflow = 4,      // an interaction list exceeded its capacity
   kErrCellOverflow = 8,      // more cells than the cell buffers hold
+  kErrMmaTimeout = 16,       // a tensor-core product did not signal completion in time
 };
 
 inline int div_up(long long a, long long b) { return int((a + b - 1) / b); }

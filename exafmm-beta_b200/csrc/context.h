@@ -20,7 +20,8 @@ struct Params {
   int mixed_p2p = 1;
   int mixed_min_level = 4;
   int mixed_max_dl = 3;
-  int mixed_gemm = 1;  // class-grouped tile M2L for frequent offset classes
+  int mixed_gemm = 1;     // per-class products for frequent offset classes: 0 off, 1 where they pay, 2 always
+  int mixed_gemm_tc = 1;  // ... on the tensor cores (bf16x3), else FP32 on the CUDA cores
 };
 
 // Level-ordered octree nodes plus the reference-layout cell table.

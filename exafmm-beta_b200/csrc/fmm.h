@@ -59,8 +59,12 @@ struct M2LGemmBufs {
   DBuf<int> pair_slot;                // per list entry: hash slot (or -1)
   DBuf<unsigned long long> ck, ck_alt;
   DBuf<int> cs, cs_alt;
-  DBuf<float> K;                      // per class operator, FP32, k-major
-  DBuf<float> Msr;                    // scaled multipoles over real degrees of freedom
+  DBuf<float> K;                      // per class operator, FP32, k-major (CUDA-core engine)
+  DBuf<float> Msr;                    // scaled multipoles over real degrees of freedom (CUDA-core engine)
+  DBuf<unsigned short> Kb;            // per class operator, three bf16 pieces (tensor-core engine)
+  DBuf<unsigned short> Msb;           // scaled multipoles, three bf16 pieces (tensor-core engine)
+  DBuf<int4> chunks;                  // per chunk: class, first sorted position, pairs (tensor-core engine)
+  DBuf<int> ssrc;                     // per sorted taken pair: its source cell (tensor-core engine)
   DBuf<unsigned char> taken;
   DBuf<unsigned> skey, skey_alt;      // pairs sorted by class
   DBuf<int> pval, pval_alt;           // their list positions
@@ -68,7 +72,8 @@ struct M2LGemmBufs {
   DBuf<float> Y;                      // per list entry: the pair's contribution (real dofs)
   DBuf<int> cnt;
   DBuf<int> left_cnt, left_off, left_src;
-  bool force = false;  // use the class products whatever the size (parity tests)
+  bool force = false;         // use the class products whatever the size (parity tests)
+  bool tensor_cores = true;   // tcgen05 bf16x3 products, else FP32 on the CUDA cores
 };
 bool m2l_gemm_supported(int P);
 bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int min_level, int max_dl);

@@ -24,6 +24,16 @@
 // images stay with the pair-by-pair FP32 kernel, which then runs on a compacted
 // list of just those pairs (left_off / left_src); pairs outside the mixed
 // policy stay with the FP64 kernel as before.
+//
+// Two engines form the products.  The tensor-core one (k_m2l_class_mma) splits
+// every operand entry into three bf16 pieces, x = hi + mid + lo (24 significant
+// bits, the FP32 mantissa), and accumulates the six products of pieces whose
+// weights reach 2^-16 (hi.hi, hi.mid, mid.hi, hi.lo, lo.hi, mid.mid) with
+// tcgen05.mma into an FP32 accumulator in tensor memory: the terms left out
+// weigh about 2^-24, FP32 rounding.  The CUDA-core one (k_m2l_class_gemm) is a
+// plain FP32 product.
+#include <cuda_bf16.h>
+
 #include <algorithm>
 #include <stdexcept>
 
@@ -68,6 +78,26 @@ __device__ __forceinline__ void dof_decode(int d, int NT, int &n, int &m, int &p
     m = e + 1;
     part = 1;
   }
+}
+
+// Three bf16 pieces of x (hi, mid, lo; each the rounding of what the previous
+// ones leave), as raw bits.
+__device__ __forceinline__ void split_bf16x3(double x, unsigned short out[3]) {
+#pragma unroll
+  for (int p = 0; p < 3; p++) {
+    const __nv_bfloat16 h = __double2bfloat16(x);
+    out[p] = __bfloat16_as_ushort(h);
+    x -= (double)__bfloat162float(h);
+  }
+}
+
+// Offset, in bf16 elements, of entry (row, k) of a K-major tensor-core operand
+// with NDP entries per row, in the canonical layout without swizzle: core
+// matrices of 8 rows x 16 bytes (8 entries) stored as 128 contiguous bytes, the
+// NDP / 8 core matrices of an 8-row group side by side along k (leading byte
+// offset 128), row groups NDP / 8 x 128 bytes apart (stride byte offset).
+__host__ __device__ __forceinline__ int core_off(int row, int k, int NDP) {
+  return ((row >> 3) * (NDP >> 3) + (k >> 3)) * 64 + (row & 7) * 8 + (k & 7);
 }
 
 __device__ __forceinline__ unsigned long long class_key(int dl, long long dx, long long dy, long long dz) {
@@ -133,8 +163,10 @@ __global__ void k_class_ids(const int *cs_sorted, int ncls, int *hid) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncls; i += gridDim.x * blockDim.x) hid[cs_sorted[i]] = i;
 }
 
-// 3. Operator of each class, k-major: Kt[class][input dof][output dof], FP32.
-__global__ void k_build_K(DevTables t, const unsigned long long *ck, int P, float *Kt) {
+// 3. Operator of each class: FP32 k-major, Kt[class][input dof][output dof]
+// (CUDA-core engine), or three bf16 pieces of it per class, each an operand
+// image of NDP output rows x NDP inputs in the core_off layout (tensor cores).
+__global__ void k_build_K(DevTables t, const unsigned long long *ck, int P, float *Kt, unsigned short *Kb) {
   extern __shared__ double2 S[];  // S'_p^q, q >= 0, at d / R_t
   const int NT = t.nterm, ND = nd_of(P), NDP = ndp_of(P);
   const unsigned long long key = ck[blockIdx.x];
@@ -146,9 +178,16 @@ __global__ void k_build_K(DevTables t, const unsigned long long *ck, int P, floa
   if ((int)threadIdx.x < 2 * P - 1)
     singular_column(t, threadIdx.x, 2 * P - 1, ux * to_rt, uy * to_rt, uz * to_rt, t.ainv, S);
   __syncthreads();
-  float *K = Kt + (long long)blockIdx.x * NDP * NDP;
   for (int e = threadIdx.x; e < NDP * NDP; e += blockDim.x) {
-    const int c = e / NDP, r = e - c * NDP;
+    int c, r;  // input and output dof; with Kb, e walks the core_off layout so the stores are contiguous
+    if (Kb) {
+      const int ci = e >> 6, w = e & 63;
+      r = (ci / (NDP >> 3)) * 8 + (w >> 3);
+      c = (ci % (NDP >> 3)) * 8 + (w & 7);
+    } else {
+      c = e / NDP;
+      r = e - c * NDP;
+    }
     double val = 0.0;
     if (r < ND && c < ND) {
       int j, k, rp, n, mp, cp;
@@ -178,28 +217,42 @@ __global__ void k_build_K(DevTables t, const unsigned long long *ck, int P, floa
       }
       val = fn * (rp == 0 ? sr : si);
     }
-    K[e] = (float)val;
+    if (Kt) Kt[(long long)blockIdx.x * NDP * NDP + c * NDP + r] = (float)val;
+    if (Kb) {
+      unsigned short h[3];
+      split_bf16x3(val, h);
+      unsigned short *dst = Kb + (long long)blockIdx.x * 3 * NDP * NDP + e;  // e == core_off(r, c, NDP)
+#pragma unroll
+      for (int p = 0; p < 3; p++) dst[p * NDP * NDP] = h[p];
+    }
   }
 }
 
-// Scaled multipoles over real degrees of freedom, FP32, padded to NDP.
+// Scaled multipoles over real degrees of freedom, padded to NDP: FP32 rows
+// (Msr[cell][dof]), or three bf16 pieces per cell (Msb[cell][piece][dof]).
 __global__ void k_scale_M_real(DevTables t, const double2 *M, const double4 *cell_x, long long ncells, int P,
-                               float *Msr) {
+                               float *Msr, unsigned short *Msb) {
   const int NT = t.nterm, ND = nd_of(P), NDP = ndp_of(P);
   const long long total = ncells * NDP;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
     const long long c = i / NDP;
     const int d = (int)(i - c * NDP);
-    float v = 0.f;
+    double v = 0.0;
     if (d < ND) {
       int n, m, part;
       dof_decode(d, NT, n, m, part);
       const int o = tri(n) + m;
       const double s = t.anm[o] * pow(cell_x[c].w, -(double)n);
       const double2 mv = M[c * NT + o];
-      v = (float)((part == 0 ? mv.x : mv.y) * s);
+      v = (part == 0 ? mv.x : mv.y) * s;
     }
-    Msr[i] = v;
+    if (Msr) Msr[i] = (float)v;
+    if (Msb) {
+      unsigned short h[3];
+      split_bf16x3(v, h);
+#pragma unroll
+      for (int p = 0; p < 3; p++) Msb[(c * 3 + p) * NDP + d] = h[p];
+    }
   }
 }
 
@@ -292,6 +345,22 @@ struct ChunkScan {
   __device__ void total(const T &t) const { cbase[n] = t; }
 };
 
+// Per chunk: (class, first sorted position, pairs); and per sorted position of
+// a taken pair, its source cell (so a product block starts from two
+// independent loads rather than a search and a chain of dependent ones).
+__global__ void k_chunk_table(const int *cstart, const int *cbase, int ncls, int4 *chunks) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncls; c += gridDim.x * blockDim.x) {
+    const int b = cstart[c], e = cstart[c + 1];
+    for (int j = cbase[c], p = b; p < e; j++, p += kChunk) chunks[j] = make_int4(c, p, min(kChunk, e - p), 0);
+  }
+}
+
+__global__ void k_sorted_sources(const int *sval, const int *src, const int *ntaken, int *ssrc) {
+  const int n = *ntaken;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    ssrc[i] = src[sval[i]] & 0x3ffffff;
+}
+
 __device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gsrc) : "memory");
@@ -383,6 +452,252 @@ k_m2l_class_gemm(const unsigned *skey, const int *sval, const int *cstart, const
         *reinterpret_cast<float4 *>(y + H + 4 * ty) = make_float4(acc[4][j], acc[5][j], acc[6][j], acc[7][j]);
       }
     }
+  }
+}
+
+// ---- tensor-core engine (tcgen05, sm_100a)
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor of a K-major operand without swizzle:
+// start address, leading byte offset (between the two core matrices along k
+// that one instruction reads) and stride byte offset (between 8-row groups),
+// all in 16-byte units; descriptor version 1 at bit 46; layout 0 = no swizzle.
+__device__ __forceinline__ unsigned long long umma_desc(unsigned addr, unsigned lbo, unsigned sbo) {
+  return (unsigned long long)((addr >> 4) & 0x3fffu) | ((unsigned long long)((lbo >> 4) & 0x3fffu) << 16) |
+         ((unsigned long long)((sbo >> 4) & 0x3fffu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void umma_bf16(unsigned tmem_d, unsigned long long da, unsigned long long db, unsigned idesc,
+                                          unsigned accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Waits for phase `parity` of the mbarrier at bar for at most about 2^31 clocks
+// (about a second); false if it did not complete.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity) {
+  const long long t0 = clock64();
+  while (true) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (clock64() - t0 > (1ll << 31)) return false;
+  }
+}
+
+// TMEM columns: two accumulators of NDP FP32 columns each (hi.hi, and the
+// five smaller products), at column 0 and NCOLS / 2; a power of two >= 32.
+__host__ __device__ constexpr int mma_cols(int NDP) {
+  return 2 * NDP <= 32 ? 32 : 2 * NDP <= 64 ? 64 : 2 * NDP <= 128 ? 128 : 256;
+}
+
+// Dynamic shared memory of k_m2l_class_mma<NDP>: the three pieces of the
+// gathered source tile and of the operator, raised where needed to at least
+// 456 bytes per TMEM column claimed.  An SM has 233,472 bytes of shared memory
+// and 512 TMEM columns, so the CTAs that fit on one SM by shared memory never
+// ask for more columns than it has and tcgen05.alloc never waits.
+__host__ __device__ constexpr size_t mma_smem_bytes(int NDP) {
+  return (size_t)3 * (kChunk * NDP + NDP * NDP) * 2 > (size_t)mma_cols(NDP) * 456
+             ? (size_t)3 * (kChunk * NDP + NDP * NDP) * 2
+             : (size_t)mma_cols(NDP) * 456;
+}
+
+// CTAs of k_m2l_class_mma<NDP> that fit on one SM (by shared memory).
+__host__ __device__ constexpr int mma_ctas_per_sm(int NDP) {
+  return (int)(233472 / (mma_smem_bytes(NDP) + 1152 + 1024));
+}
+
+// 6'. The per-class products on the tensor cores.  Persistent: each CTA takes a
+// contiguous range of chunks (one class, up to kChunk pairs each; consecutive
+// chunks mostly share a class, whose operator then stays in shared memory).
+// Per chunk: D[pair][output] = sum_k Ms[source][k] K[k][output] with M = 128
+// pairs, N = NDP outputs, K = NDP inputs, both operands K-major bf16 in shared
+// memory (core_off layout), the accumulators (128 lanes x NDP FP32 columns) in
+// tensor memory.  The tensor cores' FP32 sums are not round-to-nearest, so the
+// hi.hi product gets its own accumulator and the five smaller products
+// (2^-8 and 2^-16 of it) another: the large one sees NDP / 16 additions, and
+// the epilogue adds the two in FP32.
+// Per chunk j: thread 0 issues the 6 x NDP / 16 MMAs and commits them to an
+// mbarrier; every thread loads chunk j+1's indices meanwhile; once the
+// products are done, all threads start the cp.async gather of chunk j+1's
+// source pieces (lane pairs fetch whole 32-byte sectors) and, while it is in
+// flight, read chunk j's accumulators (warp w: TMEM lanes 32w..32w+31) and
+// write each pair's column of Y with 32-byte stores.
+template <int NDP>
+__device__ __forceinline__ void mma_gather(unsigned short *sA, unsigned short *sB, const int *s_src, int cnt,
+                                           int cls, int &cur_cls, const unsigned short *Kb,
+                                           const unsigned short *Msb) {
+  constexpr int NG = NDP / 8, A_ELEMS = kChunk * NDP, B_ELEMS = NDP * NDP;
+  if (cls != cur_cls) {  // a new class: its operator pieces
+    const unsigned short *Kg = Kb + (long long)cls * 3 * B_ELEMS;
+    for (int i = threadIdx.x; i < 3 * B_ELEMS / 8; i += 128) cp_async16(sB + 8 * i, Kg + 8 * i);
+    cur_cls = cls;
+  }
+  // unit u: bit 0 = group parity, bits 1-4 = row within 16, then (row block of
+  // 16, group pair, piece): a warp fetches 16 rows x 32 bytes (16 whole
+  // sectors) and writes four whole core matrices (conflict-free)
+  for (int u = threadIdx.x; u < kChunk * 3 * NG; u += 128) {
+    const int i = ((u >> 5) & 7) * 16 + ((u >> 1) & 15);
+    const int r2 = u >> 8;  // (group pair, piece)
+    const int gp = r2 % (NG / 2), p = r2 / (NG / 2);
+    const int g = 2 * gp + (u & 1);
+    unsigned short *dst = sA + p * A_ELEMS + core_off(i, 8 * g, NDP);
+    if (i < cnt) cp_async16(dst, Msb + ((long long)s_src[i] * 3 + p) * NDP + 8 * g);
+    else *reinterpret_cast<uint4 *>(dst) = make_uint4(0u, 0u, 0u, 0u);
+  }
+  cp_async_commit();
+}
+
+// The gathered tiles complete and visible to the tensor cores; the previous
+// TMEM reads ordered before the next MMAs.
+__device__ __forceinline__ void mma_tiles_ready() {
+  cp_async_wait_all();
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+}
+
+__device__ __forceinline__ void tmem_ld16(unsigned taddr, unsigned (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+      "%14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+
+__device__ __forceinline__ void st_global_v8(float *p, const float (&v)[8]) {
+  asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(v[0]), "f"(v[1]), "f"(v[2]),
+               "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
+               : "memory");
+}
+
+template <int NDP>
+__global__ void __launch_bounds__(128)
+k_m2l_class_mma(const int4 *chunks, const int *nchunks, const int *sval, const int *ssrc,
+                const unsigned short *Kb, const unsigned short *Msb, float *Y, int *err) {
+  constexpr int NG = NDP / 8;                // 16-byte groups per operand row
+  constexpr int A_ELEMS = kChunk * NDP;      // one piece of the source tile
+  constexpr int B_ELEMS = NDP * NDP;         // one piece of the operator
+  constexpr int NCOLS = mma_cols(NDP);
+  constexpr unsigned D1 = NCOLS / 2;         // column of the small products' accumulator
+  constexpr unsigned SBO = NG * 128;         // bytes between 8-row groups
+  // kind::f16 instruction descriptor: D FP32 (bits 4-5 = 1), A and B bf16
+  // (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
+  constexpr unsigned IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(NDP >> 3) << 17) |
+                             ((unsigned)(kChunk >> 4) << 24);
+  static_assert(NDP % 16 == 0 && NDP >= 16 && NDP <= 256, "N of an M = 128 MMA: multiple of 16 in [16, 256]");
+  static_assert(2 * NDP <= NCOLS, "two accumulators");
+  static_assert(kChunk == 128, "one TMEM lane and one thread per pair");
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned short *sA = reinterpret_cast<unsigned short *>(smem_raw);
+  unsigned short *sB = sA + 3 * A_ELEMS;
+  __shared__ int s_src[kChunk];
+  __shared__ __align__(8) unsigned long long s_bar;
+  __shared__ unsigned s_tmem;
+  const int total = *nchunks;
+  const int j0 = (int)((long long)total * blockIdx.x / gridDim.x);
+  const int j1 = (int)((long long)total * (blockIdx.x + 1) / gridDim.x);
+  if (j0 >= j1) return;
+  const unsigned bar = smem_u32(&s_bar);
+  if (threadIdx.x < 32) {  // warp 0 owns the accumulators' columns
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                 "r"(NCOLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  int4 ch = chunks[j0];  // this thread's pair of the first chunk
+  int q = (int)threadIdx.x < ch.z ? sval[ch.y + threadIdx.x] : -1;
+  s_src[threadIdx.x] = q >= 0 ? ssrc[ch.y + threadIdx.x] : -1;
+  int cur_cls = -1;
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const unsigned tmem = s_tmem;
+  mma_gather<NDP>(sA, sB, s_src, ch.z, ch.x, cur_cls, Kb, Msb);
+  mma_tiles_ready();
+  for (int j = j0; j < j1; j++) {
+    const int cnt = ch.z, qc = q;
+    if (threadIdx.x == 0) {
+      const unsigned a0 = smem_u32(sA), b0 = smem_u32(sB);
+      // pieces (of the sources, of the operator): hi.hi into D0, the rest into D1
+      const int pa[6] = {0, 0, 2, 1, 0, 1}, pb[6] = {0, 2, 0, 1, 1, 0};
+#pragma unroll
+      for (int t = 0; t < 6; t++)
+#pragma unroll
+        for (int k = 0; k < NDP / 16; k++) {  // 16 inputs = two core matrices = 256 bytes per step
+          const unsigned long long da = umma_desc(a0 + (unsigned)(pa[t] * A_ELEMS * 2 + k * 256), 128, SBO);
+          const unsigned long long db = umma_desc(b0 + (unsigned)(pb[t] * B_ELEMS * 2 + k * 256), 128, SBO);
+          umma_bf16(tmem + (t == 0 ? 0u : D1), da, db, IDESC, (t > 1 || k > 0) ? 1u : 0u);
+        }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                   : "memory");
+    }
+    int sc = -1;  // the next chunk's indices while the products run
+    if (j + 1 < j1) {
+      ch = chunks[j + 1];
+      q = (int)threadIdx.x < ch.z ? sval[ch.y + threadIdx.x] : -1;
+      sc = q >= 0 ? ssrc[ch.y + threadIdx.x] : -1;
+    }
+    bool done = true;  // one poller per warp
+    if ((threadIdx.x & 31) == 0) done = mbar_wait_bounded(bar, (unsigned)((j - j0) & 1));
+    done = __shfl_sync(0xffffffffu, done, 0);
+    tc_fence_after();
+    if (!__syncthreads_and(done)) {  // products done: the tiles and s_src are free
+      if (threadIdx.x == 0) atomicOr(err, kErrMmaTimeout);
+      break;
+    }
+    if (j + 1 < j1) {
+      s_src[threadIdx.x] = sc;
+      __syncthreads();
+      mma_gather<NDP>(sA, sB, s_src, ch.z, ch.x, cur_cls, Kb, Msb);
+    }
+    {  // chunk j's accumulators -> Y, while the gather is in flight
+      const int warp = threadIdx.x >> 5;  // row threadIdx.x = TMEM lane threadIdx.x
+      const unsigned taddr = tmem + ((unsigned)(warp * 32) << 16);
+      float *y = (int)threadIdx.x < cnt ? Y + (long long)qc * NDP : nullptr;
+#pragma unroll
+      for (int c0 = 0; c0 < NDP; c0 += 16) {
+        unsigned r[16], v[16];
+        tmem_ld16(taddr + (unsigned)c0, r);
+        tmem_ld16(taddr + D1 + (unsigned)c0, v);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (y) {
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            float o[8];
+#pragma unroll
+            for (int e = 0; e < 8; e++) o[e] = __uint_as_float(r[8 * h + e]) + __uint_as_float(v[8 * h + e]);
+            st_global_v8(y + c0 + 8 * h, o);
+          }
+        }
+      }
+    }
+    mma_tiles_ready();
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOLS) : "memory");
   }
 }
 
@@ -494,14 +809,18 @@ bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int
   int *cs = alt ? g.cs_alt.p : g.cs.p;
   k_class_ids<<<(ncls + 255) / 256, 256, 0, st>>>(cs, ncls, g.hid.p);
   EXA_CHECK_LAUNCH();
-  g.K.ensure((long long)ncls * NDP * NDP);
+  const bool tc = g.tensor_cores;
+  if (tc) g.Kb.ensure((long long)ncls * 3 * NDP * NDP);
+  else g.K.ensure((long long)ncls * NDP * NDP);
   {
     const size_t smem = tri(2 * P - 1) * sizeof(double2);
-    k_build_K<<<ncls, 256, smem, st>>>(t, ck, P, g.K.p);
+    k_build_K<<<ncls, 256, smem, st>>>(t, ck, P, tc ? nullptr : g.K.p, tc ? g.Kb.p : nullptr);
     EXA_CHECK_LAUNCH();
   }
-  g.Msr.ensure(nc * NDP);
-  k_scale_M_real<<<kNumSMs * 8, 256, 0, st>>>(t, a.M64, a.cell_x, nc, P, g.Msr.p);
+  if (tc) g.Msb.ensure(nc * 3 * NDP);
+  else g.Msr.ensure(nc * NDP);
+  k_scale_M_real<<<kNumSMs * 8, 256, 0, st>>>(t, a.M64, a.cell_x, nc, P, tc ? nullptr : g.Msr.p,
+                                              tc ? g.Msb.p : nullptr);
   EXA_CHECK_LAUNCH();
   // ---- pairs of frequent classes, sorted by class
   g.taken.ensure(n_m2l);
@@ -530,16 +849,33 @@ bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int
   EXA_CHECK_LAUNCH();
   ChunkScan cs2{g.cstart.p, g.cbase.p, ncls};
   launch_scan<256, 8>(cs2, nullptr, ncls, ncls, C.scan, C.err.p, st);
+  const long long chunks_max = n_m2l / kChunk + ncls + 1;
+  if (tc) {
+    g.chunks.ensure(chunks_max);
+    g.ssrc.ensure(n_m2l);
+    k_chunk_table<<<(ncls + 255) / 256, 256, 0, st>>>(g.cstart.p, g.cbase.p, ncls, g.chunks.p);
+    EXA_CHECK_LAUNCH();
+    const int grid = (int)std::min<long long>(kNumSMs * 8, (n_m2l + 255) / 256);
+    k_sorted_sources<<<grid, 256, 0, st>>>(sv, a.m2l_src, g.cstart.p + ncls, g.ssrc.p);
+    EXA_CHECK_LAUNCH();
+  }
   // ---- products per class chunk, then per-target sums
   g.Y.ensure(n_m2l * NDP);
-  const long long chunks_max = n_m2l / kChunk + ncls + 1;
   switch (NDP) {
 #define EXA_GEMM_CASE(N)                                                                                      \
   case N: {                                                                                                   \
-    const size_t smem = (size_t)(N * N + kChunk * (N + 4)) * sizeof(float);                                   \
-    set_smem(k_m2l_class_gemm<N>, smem);                                                                      \
-    k_m2l_class_gemm<N><<<(unsigned)chunks_max, 128, smem, st>>>(sk, sv, g.cstart.p, g.cbase.p, ncls,        \
-                                                                 a.m2l_src, g.K.p, g.Msr.p, g.Y.p);           \
+    if (tc) {                                                                                                 \
+      const size_t smem = mma_smem_bytes(N);                                                                  \
+      set_smem(k_m2l_class_mma<N>, smem);                                                                     \
+      const long long grid = std::min<long long>(chunks_max, (long long)kNumSMs * mma_ctas_per_sm(N));        \
+      k_m2l_class_mma<N><<<(unsigned)grid, 128, smem, st>>>(g.chunks.p, g.cbase.p + ncls, sv, g.ssrc.p,       \
+                                                            g.Kb.p, g.Msb.p, g.Y.p, C.err.p);                 \
+    } else {                                                                                                  \
+      const size_t smem = (size_t)(N * N + kChunk * (N + 4)) * sizeof(float);                                 \
+      set_smem(k_m2l_class_gemm<N>, smem);                                                                    \
+      k_m2l_class_gemm<N><<<(unsigned)chunks_max, 128, smem, st>>>(sk, sv, g.cstart.p, g.cbase.p, ncls,      \
+                                                                   a.m2l_src, g.K.p, g.Msr.p, g.Y.p);         \
+    }                                                                                                         \
     EXA_CHECK_LAUNCH();                                                                                       \
     k_m2l_class_reduce<N><<<kNumSMs * 8, 256, 0, st>>>(a.m2l_off, nc, g.taken.p, g.Y.p, a.cell_x, t, P, a.L64); \
     EXA_CHECK_LAUNCH();                                                                                       \

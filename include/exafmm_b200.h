@@ -56,9 +56,11 @@ int exafmm_set_params(exafmm_ctx *ctx, int P, double theta, int ncrit, int nspaw
 /* Mixed form only: which operators run in FP32 and which M2L pairs may
  * (target level >= min_level, |level difference| <= max_dl); the rest runs in
  * FP64.  m2l_fp32: 0 = FP64; 1 = FP32, with the pairs of frequent offset
- * classes evaluated as dense per-class products when the system is large
- * enough for that to pay (P = 8 or 10); 2 = FP32 pair by pair only; 3 = FP32
- * with the per-class products at any size.  p2p_fp32: 0 or 1.
+ * classes evaluated as dense per-class products on the tensor cores (three
+ * bf16 pieces per operand, FP32 accumulation) when the system is large
+ * enough for that to pay (P = 8 or 10); 2 = FP32 pair by pair only; 3 = as 1
+ * with the per-class products at any size; 4 and 5 = as 1 and 3 with the
+ * per-class products in FP32 on the CUDA cores.  p2p_fp32: 0 or 1.
  * Defaults: 1, 1, 4, 3.  No counterpart in the reference (its precision is a
  * compile-time switch, EXAFMM_SINGLE). */
 int exafmm_set_mixed_policy(exafmm_ctx *ctx, int m2l_fp32, int p2p_fp32, int min_level, int max_dl);
