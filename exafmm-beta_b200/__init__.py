@@ -22,6 +22,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libexafmm_b200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "exafmm_b200.h")
+MD_HEADER = os.path.join(os.path.dirname(HERE), "include", "exafmm_md.h")
 
 FP64 = 0
 MIXED = 1
@@ -41,10 +42,13 @@ def build(force: bool = False) -> str:
 
 
 def exported_symbols() -> list[str]:
-    """Every function declared in include/exafmm_b200.h."""
+    """Every function declared in include/exafmm_b200.h and include/exafmm_md.h."""
     import re
     text = open(HEADER).read()
-    return sorted(set(re.findall(r"\b(exafmm_[a-z0-9_]+)\s*\(", text)))
+    names = set(re.findall(r"\b(exafmm_[a-z0-9_]+)\s*\(", text))
+    md = open(MD_HEADER).read()
+    names |= set(re.findall(r"^\s*(?:void|bool|int|const char \*)\s*([A-Za-z_]\w*)\s*\(", md, re.M))
+    return sorted(names)
 
 
 def lib() -> ctypes.CDLL:
@@ -112,6 +116,10 @@ def lib() -> ctypes.CDLL:
         "exafmm_ewald": (_c_int, [_vp, _c_ll, _c_int, _c_double, _c_double, _c_double, _c_double, _vp]),
         "exafmm_ewald_error": (ctypes.c_char_p, []),
         "exafmm_dipole_correction": (_c_int, [_vp, _vp, _c_ll]),
+        "exafmm_write_list": (_c_int, [_vp, ctypes.c_char_p, _c_int]),
+        "exafmm_write_time": (_c_int, [_vp, ctypes.c_char_p, _c_int]),
+        "exafmm_write_time_events": (_c_int, [ctypes.c_char_p, _c_int, _c_int, _vp, _vp]),
+        "exafmm_morton_key": (ctypes.c_ulonglong, [_vp, _vp, _c_double, _c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -291,6 +299,19 @@ class Fmm:
 
     PHASES = ("bounds", "tree", "upward", "lists", "m2l", "p2p", "downward", "total")
 
+    # ---- records in the reference's file formats ----
+    def write_list(self, path: str = "./", rank: int = 0) -> str:
+        """Traversal::writeList (EXAFMM_COUNT_LIST): path + 'list%06d.dat' with each cell's
+        ICELL and P2P / M2L list sizes from the last traversal.  Returns the file name."""
+        self._check(lib().exafmm_write_list(self._h, path.encode(), int(rank)))
+        return f"{path}list{int(rank):06d}.dat"
+
+    def write_time(self, path: str = "./", rank: int = 0) -> str:
+        """logger::writeTime: path + 'time%06d.dat' with the phase times summed since the last
+        call, under the reference's event names; clears them.  Returns the file name."""
+        self._check(lib().exafmm_write_time(self._h, path.encode(), int(rank)))
+        return f"{path}time{int(rank):06d}.dat"
+
     def phase_times(self) -> dict:
         """Device milliseconds of each phase of the last solve (CUDA events on its stream)."""
         t = np.zeros(8)
@@ -302,6 +323,22 @@ class Fmm:
 def _kcheck(rc):
     if rc != 0:
         raise FmmError(lib().exafmm_kernel_error().decode())
+
+
+def write_time_events(events: dict, path: str = "./", rank: int = 0) -> str:
+    """logger::writeTime of `events` (name -> seconds) into path + 'time%06d.dat'."""
+    names = (ctypes.c_char_p * max(len(events), 1))(*[k.encode() for k in events])
+    vals = np.array(list(events.values()) or [0.0], dtype=np.float64)
+    if lib().exafmm_write_time_events(path.encode(), int(rank), len(events), ctypes.cast(names, _vp), _p(vals)):
+        raise FmmError(f"cannot write {path}time{int(rank):06d}.dat")
+    return f"{path}time{int(rank):06d}.dat"
+
+
+def morton_key(X, Xmin, diameter: float, level: int) -> int:
+    """BuildTree::getKey (include/build_tree.h:111-120) as the compiled reference evaluates it."""
+    X = _f64(X).reshape(3)
+    Xmin = _f64(Xmin).reshape(3)
+    return int(lib().exafmm_morton_key(_p(X), _p(Xmin), float(diameter), int(level)))
 
 
 def ewald(xyzq, ksize, alpha, sigma, cutoff, cycle, trg=None) -> np.ndarray:

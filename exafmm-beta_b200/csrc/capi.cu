@@ -1,6 +1,7 @@
 // extern "C" surface of the engine (include/exafmm_b200.h) and the solve driver.
 #include <atomic>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <stdexcept>
 #include <vector>
@@ -9,6 +10,7 @@
 #include "drift.cuh"
 #include "fmm.h"
 #include "harmonics.cuh"
+#include "records.h"
 
 namespace exafmm_b200 {
 
@@ -31,17 +33,50 @@ void direct_fp64(const double4 *tgt, long long nt, const double4 *src, long long
 
 namespace {
 
+// Phase events of the last solve: ev[0..7] bound bounds, tree, upward, lists,
+// m2l, p2p, downward; link splits the tree build (growTree / linkTree), lat
+// brackets the periodic lattice.  After each complete solve (pending) the times
+// are added under the reference's logger event names to `timer`, which
+// exafmm_write_time writes out and clears (logger::writeTime).
 struct Timing {
   cudaEvent_t ev[8] = {};
+  cudaEvent_t link = nullptr, lat[2] = {};
   bool live = false;
+  bool pending = false;    // a complete solve whose times are not in `timer` yet
+  bool periodic = false;   // that solve ran the periodic lattice
+  std::map<std::string, double> timer;
   void init() {
     if (live) return;
     for (auto &e : ev) EXA_CUDA(cudaEventCreate(&e));
+    EXA_CUDA(cudaEventCreate(&link));
+    for (auto &e : lat) EXA_CUDA(cudaEventCreate(&e));
     live = true;
   }
+  double seconds(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.f;
+    EXA_CUDA(cudaEventElapsedTime(&ms, a, b));
+    return 1e-3 * ms;
+  }
+  // Event names of include/bound_box.h:12, build_tree.h:187-207, up_down_pass.h:50-74,
+  // traversal.h:234-350 ("Traverse" includes "Traverse periodic", as there).
+  void fold() {
+    if (!pending) return;
+    EXA_CUDA(cudaEventSynchronize(ev[7]));
+    timer["Get bounds"] += seconds(ev[0], ev[1]);
+    timer["Grow tree"] += seconds(ev[1], link);
+    timer["Link tree"] += seconds(link, ev[2]);
+    timer["Upward pass"] += seconds(ev[2], ev[3]);
+    timer["Traverse"] += seconds(ev[3], ev[6]);
+    if (periodic) timer["Traverse periodic"] += seconds(lat[0], lat[1]);
+    timer["Downward pass"] += seconds(ev[6], ev[7]);
+    pending = false;
+  }
   ~Timing() {
-    if (live)
+    if (live) {
       for (auto &e : ev) cudaEventDestroy(e);
+      cudaEventDestroy(link);
+      for (auto &e : lat) cudaEventDestroy(e);
+    }
   }
 };
 
@@ -107,7 +142,9 @@ struct Engine {
   }
 
   void build(const double *bounds6) {
+    tm.fold();  // the previous solve's times, before its events are reused
     tm.init();
+    C.ev_link = tm.link;
     EXA_CUDA(cudaEventRecord(tm.ev[0], C.stream));
     if (bounds6) set_bounds(C, bounds6);
     else compute_bounds(C);
@@ -197,10 +234,12 @@ struct Engine {
       } else {
         m2l_fp64(a);
       }
+      EXA_CUDA(cudaEventRecord(tm.lat[0], C.stream));
       if (C.prm.images > 1) {  // Traversal::traversePeriodic
         lat.ensure(lattice_scratch_terms(C.prm.P));
         lattice_fp64(a, C.prm.images, C.prm.theta, lat.p);
       }
+      EXA_CUDA(cudaEventRecord(tm.lat[1], C.stream));
       EXA_CUDA(cudaEventRecord(tm.ev[5], C.stream));
       if (mixed && C.prm.mixed_p2p) {
         x32.ensure(2 * C.tree.n);  // hi and lo float4 per body
@@ -212,6 +251,8 @@ struct Engine {
       }
     } else {
       EXA_CUDA(cudaEventRecord(tm.ev[4], C.stream));
+      EXA_CUDA(cudaEventRecord(tm.lat[0], C.stream));
+      EXA_CUDA(cudaEventRecord(tm.lat[1], C.stream));
       EXA_CUDA(cudaEventRecord(tm.ev[5], C.stream));
     }
     EXA_CUDA(cudaEventRecord(tm.ev[6], C.stream));
@@ -227,6 +268,8 @@ struct Engine {
       l2p_fp64(a);
     }
     EXA_CUDA(cudaEventRecord(tm.ev[7], C.stream));
+    tm.pending = true;
+    tm.periodic = C.prm.images > 0;
   }
 
   void results(double *dst, cudaMemcpyKind kind);
@@ -590,6 +633,42 @@ int exafmm_get_expansions(exafmm_ctx *ctx, double *Mh, double *Lh) {
 }
 
 void *exafmm_stream(exafmm_ctx *ctx) { return ctx ? (void *)ctx->E.C.stream : nullptr; }
+
+int exafmm_write_list(exafmm_ctx *ctx, const char *path, int rank) {
+  return guarded(ctx, [&] {
+    Engine &E = ctx->E;
+    if (!E.lists_ok) throw std::runtime_error("no interaction lists (traverse first)");
+    cudaSetDevice(E.C.device);
+    const long long nc = E.C.tree.ncells;
+    std::vector<int> m2l_off(nc + 1, 0), p2p_off(nc + 1, 0);
+    std::vector<int2> pl(nc);
+    std::vector<double4> x(nc);
+    if (nc) {
+      EXA_CUDA(cudaMemcpy(m2l_off.data(), E.lists.m2l_off.p, (nc + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+      EXA_CUDA(cudaMemcpy(p2p_off.data(), E.lists.p2p_off.p, (nc + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+      EXA_CUDA(cudaMemcpy(pl.data(), E.C.tree.cell_pl.p, nc * sizeof(int2), cudaMemcpyDeviceToHost));
+      EXA_CUDA(cudaMemcpy(x.data(), E.C.tree.cell_x.p, nc * sizeof(double4), cudaMemcpyDeviceToHost));
+    }
+    // BuildTree::nodes2cells (include/build_tree.h:132): getKey(C->X, X0 - R0, 2 C->R, level)
+    std::vector<unsigned long long> icell(nc);
+    for (long long c = 0; c < nc; c++) {
+      const double X[3] = {x[c].x, x[c].y, x[c].z};
+      const double Xmin[3] = {x[0].x - x[0].w, x[0].y - x[0].w, x[0].z - x[0].w};
+      icell[c] = morton_key(X, Xmin, 2 * x[c].w, pl[c].y);
+    }
+    write_list_file(path, rank, nc, icell.data(), p2p_off.data(), m2l_off.data());
+  });
+}
+
+int exafmm_write_time(exafmm_ctx *ctx, const char *path, int rank) {
+  return guarded(ctx, [&] {
+    Engine &E = ctx->E;
+    cudaSetDevice(E.C.device);
+    E.tm.fold();
+    write_time_file(path, rank, E.tm.timer);
+    E.tm.timer.clear();
+  });
+}
 
 int exafmm_phase_times(exafmm_ctx *ctx, double *ms8) {
   return guarded(ctx, [&] {

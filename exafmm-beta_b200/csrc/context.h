@@ -55,6 +55,7 @@ struct Context {
   long long dev_bytes = 0;     // device bytes held by this context's buffers (declared first: outlives them)
   Params prm;
   cudaStream_t stream = nullptr;
+  cudaEvent_t ev_link = nullptr;  // when set, recorded between growing the octree and linking the cells
   int device = 0;
   DBuf<int> err;               // device error word
   int *err_host = nullptr;     // pinned mirror

@@ -142,6 +142,19 @@ int exafmm_direct(const double *targets, long long nt, const double *sources, lo
   });
 }
 
+int exafmm_direct_range(const double *targets, long long nt, const double *sources, long long ns, int prange,
+                        double cycle, double *trg) {
+  return run([&] {
+    if (prange < 0) throw std::runtime_error("negative image range");
+    Mini m;
+    const double4 *t = m.up((const double4 *)targets, nt);
+    const double4 *s = m.up((const double4 *)sources, ns);
+    double4 *r = m.up((const double4 *)trg, nt);
+    direct_fp64(t, nt, s, ns, prange, cycle, r, m.st);
+    m.down((double4 *)trg, r, nt);
+  });
+}
+
 int exafmm_kernel_p2m(int P, const double *X, long long n, const double *xyzq, double *Mh) {
   return run([&] {
     check_P(P);

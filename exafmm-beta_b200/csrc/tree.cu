@@ -521,6 +521,7 @@ void build_tree(Context &C) {
     k_emit<<<node_grid, 256, 0, st>>>(a, l);
     EXA_CHECK_LAUNCH();
   }
+  if (C.ev_link) EXA_CUDA(cudaEventRecord(C.ev_link, st));  // BuildTree: growTree done, linkTree next
   for (int l = kMaxLevels; l >= 0; l--) {
     k_nnode<<<node_grid, 256, 0, st>>>(a, l);
     EXA_CHECK_LAUNCH();

@@ -123,6 +123,26 @@ void *exafmm_stream(exafmm_ctx *ctx);
 /* Device time (ms, CUDA events on the context's stream) of the phases of the
  * last solve: bounds, tree, upward, lists, m2l, p2p, downward, total. */
 int exafmm_phase_times(exafmm_ctx *ctx, double *ms8);
+/* Solve records in the reference's file formats.  exafmm_write_list writes
+ * path + "list%06d.dat" (rank) as Traversal::writeList does under
+ * EXAFMM_COUNT_LIST (include/traversal.h:412-421): per cell, in cell order, the
+ * Morton key ICELL (BuildTree::getKey, include/build_tree.h:111-120), the P2P
+ * and the M2L list sizes of the last traversal.  exafmm_write_time writes
+ * path + "time%06d.dat" as logger::writeTime does (include/logger.h:116-127):
+ * the solve phases timed since the last call, summed, in seconds, under the
+ * reference's event names (Get bounds, Grow tree, Link tree, Upward pass,
+ * Traverse, Traverse periodic when periodic, Downward pass), then clears them.
+ * exafmm_write_time_events writes given events in that format (events with the
+ * same name add up, as logger::stopTimer accumulates).  path is a directory
+ * prefix ending in '/' ("./" if null). */
+int exafmm_write_list(exafmm_ctx *ctx, const char *path, int rank);
+int exafmm_write_time(exafmm_ctx *ctx, const char *path, int rank);
+int exafmm_write_time_events(const char *path, int rank, int count, const char *const *names, const double *seconds);
+/* BuildTree::getKey (include/build_tree.h:111-120) of center X at level, cube
+ * corner Xmin and cell diameter, with the compiled reference's 32-bit shift
+ * semantics (keys of levels >= 11 wrap as they do there). */
+unsigned long long exafmm_morton_key(const double *X, const double *Xmin, double diameter, int level);
+
 /* Device memory held by the context's grow-only buffers, in bytes (no
  * counterpart in the reference; used by the request server's admission). */
 int exafmm_device_bytes(exafmm_ctx *ctx, long long *bytes);
@@ -134,6 +154,11 @@ long long exafmm_launch_count(void);
  * Host arrays; trg accumulates. */
 int exafmm_direct(const double *targets, long long nt, const double *sources, long long ns, int images,
                   double theta, double cycle, double *trg);
+/* The same sum over the images -prange..prange in each direction (the range
+ * the MD wrappers' direct sums use, wrappers/gromacs.cxx:289-301: prange =
+ * sum of 3^i over the image levels). */
+int exafmm_direct_range(const double *targets, long long nt, const double *sources, long long ns, int prange,
+                        double cycle, double *trg);
 
 /* Ewald summation (include/ewald.h:7-197, as examples/ewald.cxx drives it), FP64
  * on the device: wave part over the integer waves |k| <= ksize of

@@ -54,6 +54,7 @@ class TreeRun:
     M: np.ndarray | None
     L: np.ndarray | None
     times: np.ndarray | None = None
+    icell: np.ndarray | None = None   # Cell::ICELL (the reference only)
 
 
 class _Lib:
@@ -241,12 +242,29 @@ class Reference(_Lib):
                              _vp, _c_int])
         self._f("get_cells", None, [_vp, _vp, _vp, _vp])
         self._f("get_times", None, [_vp, _vp])
+        self._f("write_list", None, [_vp, ctypes.c_char_p])
+        self._f("write_time", None, [_c_int, _vp, _vp, ctypes.c_char_p])
 
     def _get_cells(self, h, ci, cr):
         self.lib.ref_get_cells(h, _ptr(ci), _ptr(cr), None)
 
+    def icell(self, h, nc):
+        out = np.zeros(nc, dtype=np.uint64)
+        ci = np.zeros((nc, 5), dtype=np.int32)
+        cr = np.zeros((nc, 4))
+        self.lib.ref_get_cells(h, _ptr(ci), _ptr(cr), _ptr(out))
+        return out
+
+    def write_time(self, events: dict, path: str) -> None:
+        """logger::writeTime of `events` (name -> seconds) into path + 'time000000.dat'."""
+        names = (ctypes.c_char_p * len(events))(*[k.encode() for k in events])
+        vals = np.array(list(events.values()), dtype=np.float64)
+        self.lib.ref_write_time(len(events), names, _ptr(vals), path.encode())
+
     def solve(self, xyzq, P=10, theta=0.4, ncrit=64, nspawn=5000, images=0, cycle=2 * np.pi,
-              bounds=None, threads=1, record_lists=True, dipole_correction=False, expansions=False) -> TreeRun:
+              bounds=None, threads=1, record_lists=True, dipole_correction=False, expansions=False,
+              list_path=None) -> TreeRun:
+        """One solve; with list_path, also Traversal::writeList into list_path + 'list000000.dat'."""
         xyzq = _as_xyzq(xyzq)
         b = None if bounds is None else np.asarray(bounds, np.float64)
         h = self.lib.ref_run(len(xyzq), _ptr(xyzq), P, theta, ncrit, nspawn, images, cycle, threads,
@@ -256,6 +274,9 @@ class Reference(_Lib):
             t = np.zeros(8)
             self.lib.ref_get_times(h, _ptr(t))
             run.times = t
+            run.icell = self.icell(h, len(run.cells_int))
+            if list_path is not None:
+                self.lib.ref_write_list(h, list_path.encode())
             return run
         finally:
             self.lib.ref_free(h)

@@ -138,6 +138,7 @@ void * ref_run(int n, const double * xyzq, int P, double theta, int ncrit, int n
   run->cells = buildTree.buildTree(run->bodies, buffer, run->bounds);
   double t2 = logger::get_time();
   upDownPass.upwardPass(run->cells);
+  traversal.initListCount(run->cells);  // examples/fmm.cxx:67
   double t3 = logger::get_time();
   kernel.C0 = run->cells.begin();
   kernel.log = record_lists ? &run->log : nullptr;
@@ -232,6 +233,25 @@ void ref_get_expansions(void * h, double * M, double * L) {
     }
     c++;
   }
+}
+
+// Traversal::writeList (include/traversal.h:412-421) of the run's cells into
+// path + "list%06d.dat" (rank 0), as examples/fmm.cxx:88 calls it.
+void ref_write_list(void * h, const char * path) {
+  Run * run = (Run *)h;
+  Traversal traversal(kernelFor(run->P), 0.4, 0, 0, path);
+  traversal.writeList(run->cells, 0);
+}
+
+// logger::writeTime (include/logger.h:116-127) of the given events into
+// path + "time%06d.dat" (rank 0).
+void ref_write_time(int count, const char * const * names, const double * seconds, const char * path) {
+  logger::timer.clear();
+  for (int i = 0; i < count; i++) logger::timer[names[i]] = seconds[i];
+  const char * saved = logger::path;
+  logger::path = path;
+  logger::writeTime(0);
+  logger::path = saved;
 }
 
 void ref_get_times(void * h, double * t) {

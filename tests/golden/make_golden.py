@@ -7,7 +7,7 @@ commits no golden values of its own (its .reg regression files are written at
 run time), so these fixtures are what pins both the CPU restatement (oracle/)
 and the GPU engine to the reference's behaviour.
 
-Run from the repository root:  python tests/golden/make_golden.py
+Run from the repository root:  python tests/golden/make_golden.py [solve periodic kat records md]
 """
 from __future__ import annotations
 
@@ -105,15 +105,115 @@ def make_periodic_case(ref: Reference, name, gen, n, seed, P, theta, ncrit, nspa
     print(f"{name}: cells={nc} m2l={len(data['m2l'])} (+{lattice.sum()} lattice) p2p={len(run.p2p)}")
 
 
-def main():
+# Records in the reference's file formats: Traversal::writeList (EXAFMM_COUNT_LIST)
+# of a tree 19 levels deep (a Plummer sphere plus a tight cluster, so cell keys
+# of levels >= 11 wrap as the compiled reference computes them) and of a
+# periodic case, and logger::writeTime of fixed events.
+RECORD_EVENTS = {"Get bounds": 0.00123, "Grow tree": 1.5e-05, "Link tree": 0.25, "Upward pass": 12.5,
+                 "Traverse": 3.0, "Traverse periodic": 0.0, "Downward pass": 1e-07, "Total FMM": 123456.789}
+
+
+def records_input():
+    x = datasets.plummer(5000, 21)
+    rng = np.random.default_rng(22)
+    c = np.zeros((200, 4))
+    c[:, :3] = np.array([0.3, -0.2, 0.1]) + 1e-4 * rng.standard_normal((200, 3))
+    c[:, 3] = 1.0 / 5200
+    return np.vstack([x, c])
+
+
+def make_records(ref: Reference):
+    import tempfile
+    out = {}
+    for tag, x, kw in (("deep", records_input(), dict(P=6, theta=0.4, ncrit=8, nspawn=5000, images=0)),
+                       ("periodic", datasets.cube(600, 31) * np.array([np.pi, np.pi, np.pi, 1.0]),
+                        dict(P=6, theta=0.4, ncrit=16, nspawn=5000, images=2, cycle=2 * np.pi))):
+        d = tempfile.mkdtemp() + "/"
+        run = ref.solve(x, threads=1, record_lists=False, list_path=d, **kw)
+        with open(d + "list000000.dat", "rb") as f:
+            text = f.read()
+        out[f"{tag}_xyzq"] = x
+        out[f"{tag}_params"] = np.array([kw["P"], kw["theta"], kw["ncrit"], kw["nspawn"], kw["images"],
+                                         kw.get("cycle", 2 * np.pi)])
+        out[f"{tag}_icell"] = run.icell
+        out[f"{tag}_cells_real"] = run.cells_real
+        out[f"{tag}_list"] = np.frombuffer(text, dtype=np.uint8)
+        print(f"records {tag}: cells={len(run.cells_int)} list bytes={len(text)}")
+    d = tempfile.mkdtemp() + "/"
+    ref.write_time(RECORD_EVENTS, d)
+    with open(d + "time000000.dat", "rb") as f:
+        out["time_text"] = np.frombuffer(f.read(), dtype=np.uint8)
+    out["time_names"] = np.array(list(RECORD_EVENTS.keys()))
+    out["time_values"] = np.array(list(RECORD_EVENTS.values()))
+    np.savez_compressed(os.path.join(OUT, "records.npz"), **out)
+
+
+# The MD ABI (wrappers/gromacs.cxx, driven as wrappers/test_gromacs.cxx drives it):
+# 1000 random charges with zero net charge in [-cycle/2, cycle/2)^3, cycle = 2 pi,
+# images 3, Ewald ksize 11, alpha 10/cycle, sigma 0.25/pi, cutoff cycle/2.  The
+# wrapper needs MPI, which is not here, so its single-rank recipe runs through
+# the harness: bodies shifted by -cycle/2 and wrapped (vec.h wrap), bounds of
+# BoundBox::getBounds narrowed by Partition::octsection with one rank, FMM with
+# P 10, theta 0.5, ncrit 32, nspawn 1000 and the dipole correction, and Ewald on
+# the wrapped, unshifted bodies.
+def md_wrap(X, w):
+    X = X.copy()
+    for d in range(3):
+        lo = X[:, d] < -w / 2
+        X[lo, d] += w
+        hi = X[:, d] > w / 2
+        X[hi, d] -= w
+    return X
+
+
+def make_md(ref: Reference):
+    rng = np.random.default_rng(41)
+    n = 1000
+    cycle32 = np.float32(2 * np.pi)
+    x32 = (rng.uniform(size=(n, 3)) * cycle32 - cycle32 / np.float32(2)).astype(np.float32)
+    q32 = (rng.uniform(size=n) - 0.5).astype(np.float32)
+    q32 = (q32 - np.float32(q32.astype(np.float64).mean())).astype(np.float32)
+    c = float(cycle32)
+    # FMM_Coulomb's bodies and bounds
+    X = md_wrap(x32.astype(np.float64) - c / 2, c)
+    xyzq = np.column_stack([X, q32.astype(np.float64)])
+    g = ref.solve(xyzq, P=10, theta=0.5, ncrit=32, nspawn=1000, images=0, record_lists=False).bounds
+    part = (g[3:] - g[:3]) / 1
+    local = np.concatenate([g[:3] + 0 * part, g[:3] + 1 * part])
+    fmm = ref.solve(xyzq, P=10, theta=0.5, ncrit=32, nspawn=1000, images=3, cycle=c, bounds=local,
+                    record_lists=False, dipole_correction=True)
+    # Ewald_Coulomb's bodies
+    Xe = md_wrap(x32.astype(np.float64), c)
+    ew = ref.ewald(np.column_stack([Xe, q32.astype(np.float64)]), 11, 10 / c, 0.25 / np.pi, c / 2, c)
+    # at cutoff L/2 the reference's real part takes each pair's image from its leaf
+    # cells' centers and drops some pairs; the nearest-image sum is the oracle's
+    from bindings import Oracle
+    ew_nearest = Oracle().ewald(np.column_stack([Xe, q32.astype(np.float64)]), 11, 10 / c, 0.25 / np.pi, c / 2, c)
+    np.savez_compressed(os.path.join(OUT, "md_gromacs.npz"), x=x32, q=q32, cycle=np.array([c]), bounds=local,
+                        perm=fmm.perm, fmm_trg=fmm.trg, ewald_trg=ew, ewald_nearest_trg=ew_nearest)
+    e_fmm, e_ew = np.sum(fmm.trg[:, 0] * q32), np.sum(ew[:, 0] * q32)
+    acc = np.sqrt(np.sum((fmm.trg[:, 1:] - ew[:, 1:]) ** 2) / np.sum(ew[:, 1:] ** 2))
+    print(f"md_gromacs: energy fmm {e_fmm:.8e} ewald {e_ew:.8e} rel {abs(e_fmm - e_ew) / abs(e_ew):.2e}, "
+          f"force rel-L2 {acc:.2e}")
+
+
+def main(which=("solve", "periodic", "kat", "records", "md")):
     build(reference=True)
     ref = Reference()
-    for c in CASES:
-        make_case(ref, *c)
-    for c in PERIODIC_CASES:
-        make_periodic_case(ref, *c)
-    make_kat(ref)
+    if "solve" in which:
+        for c in CASES:
+            make_case(ref, *c)
+    if "periodic" in which:
+        for c in PERIODIC_CASES:
+            make_periodic_case(ref, *c)
+    if "kat" in which:
+        make_kat(ref)
+    if "records" in which:
+        make_records(ref)
+    if "md" in which:
+        make_md(ref)
 
 
 if __name__ == "__main__":
-    main()
+    # optional arguments: a subset of solve, periodic, kat, records, md
+    main(tuple(sys.argv[1:]) or ("solve", "periodic", "kat", "records", "md"))
