@@ -116,6 +116,9 @@ def lib() -> ctypes.CDLL:
         "exafmm_ewald": (_c_int, [_vp, _c_ll, _c_int, _c_double, _c_double, _c_double, _c_double, _vp]),
         "exafmm_ewald_error": (ctypes.c_char_p, []),
         "exafmm_dipole_correction": (_c_int, [_vp, _vp, _c_ll]),
+        "exafmm_set_sources": (_c_int, [_vp, _vp, _c_ll]),
+        "exafmm_get_source_cells": (_c_int, [_vp, ctypes.POINTER(_c_ll), _vp, _vp, _vp]),
+        "exafmm_direct_range": (_c_int, [_vp, _c_ll, _vp, _c_ll, _c_int, _c_double, _vp]),
         "exafmm_write_list": (_c_int, [_vp, ctypes.c_char_p, _c_int]),
         "exafmm_write_time": (_c_int, [_vp, ctypes.c_char_p, _c_int]),
         "exafmm_write_time_events": (_c_int, [ctypes.c_char_p, _c_int, _c_int, _vp, _vp]),
@@ -199,6 +202,28 @@ class Fmm:
         self._check(lib().exafmm_set_mixed_policy(self._h, int(m2l_fp32), int(p2p_fp32), min_level, max_dl))
 
     # ---- solve steps (examples/fmm.cxx:163-179) ----
+    def set_sources(self, xyzq=None):
+        """Separate source bodies (examples/fmm.cxx -j IneJ): later solves evaluate the field
+        of these sources at this context's bodies (free space, FP64).  None: sources are
+        the bodies again."""
+        if xyzq is None:
+            self._check(lib().exafmm_set_sources(self._h, None, 0))
+            return
+        xyzq = _f64(xyzq, 4)
+        self._check(lib().exafmm_set_sources(self._h, _p(xyzq), len(xyzq)))
+
+    def source_cells(self):
+        """The source tree: (cells_int, cells_real, perm) as cells() / perm()."""
+        nc = _c_ll()
+        self._check(lib().exafmm_get_source_cells(self._h, ctypes.byref(nc), None, None, None))
+        ints = np.zeros((nc.value, 5), dtype=np.int32)
+        reals = np.zeros((nc.value, 4))
+        self._check(lib().exafmm_get_source_cells(self._h, None, _p(ints), _p(reals), None))
+        nb = int(ints[0, 4]) if nc.value else 0
+        perm = np.zeros(nb, dtype=np.int32)
+        self._check(lib().exafmm_get_source_cells(self._h, None, None, None, _p(perm)))
+        return ints, reals, perm
+
     def set_bodies(self, xyzq):
         xyzq = _f64(xyzq, 4)
         self.n = len(xyzq)

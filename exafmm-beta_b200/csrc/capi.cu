@@ -95,6 +95,14 @@ struct Engine {
   DBuf<double4> trg, out;
   Timing tm;
   bool tree_ok = false, up_ok = false, lists_ok = false;
+  // Separate source bodies (examples/fmm.cxx -j IneJ, :61-73): their own tree
+  // and multipoles, on the same stream as the targets.
+  std::unique_ptr<Engine> jsrc;
+  bool is_source = false;  // this engine is another one's source tree (owns its pinned error word)
+
+  ~Engine() {
+    if (is_source && C.err_host) cudaFreeHost(C.err_host);
+  }
 
   FmmArgs args() {
     FmmArgs a;
@@ -141,14 +149,58 @@ struct Engine {
     tree_ok = up_ok = lists_ok = false;
   }
 
+  void set_sources(const double *xyzq, long long n) {
+    if (!xyzq) {  // back to sources == targets
+      jsrc.reset();
+    } else {
+      if (n <= 0) throw std::runtime_error("separate sources need at least one body");
+      if (!jsrc) {
+        std::unique_ptr<Engine> e(new Engine);
+        e->is_source = true;
+        e->C.device = C.device;
+        e->C.stream = C.stream;
+        e->C.err.ensure(1);
+        EXA_CUDA(cudaMemsetAsync(e->C.err.p, 0, sizeof(int), C.stream));
+        EXA_CUDA(cudaMallocHost((void **)&e->C.err_host, sizeof(int)));
+        jsrc = std::move(e);
+      }
+      jsrc->C.prm = C.prm;
+      jsrc->set_bodies(xyzq, n, cudaMemcpyHostToDevice);
+    }
+    tree_ok = up_ok = lists_ok = false;
+  }
+
+  // The source tree on the targets' bounds (examples/fmm.cxx:69).
+  void build_sources(const double *d_bounds6, const Params &prm) {
+    tm.init();
+    C.prm = prm;
+    C.tree.bounds.ensure(6);
+    EXA_CUDA(cudaMemcpyAsync(C.tree.bounds.p, d_bounds6, 6 * sizeof(double), cudaMemcpyDeviceToDevice, C.stream));
+    grow_tree();
+    tree_ok = true;
+    up_ok = lists_ok = false;
+  }
+
   void build(const double *bounds6) {
     tm.fold();  // the previous solve's times, before its events are reused
     tm.init();
     C.ev_link = tm.link;
     EXA_CUDA(cudaEventRecord(tm.ev[0], C.stream));
-    if (bounds6) set_bounds(C, bounds6);
-    else compute_bounds(C);
+    if (bounds6) {
+      set_bounds(C, bounds6);
+    } else {
+      compute_bounds(C);
+      if (jsrc) extend_bounds(C, jsrc->C.tree.xyzq.p, jsrc->C.tree.n);  // examples/fmm.cxx:62-64
+    }
     EXA_CUDA(cudaEventRecord(tm.ev[1], C.stream));
+    grow_tree();
+    if (jsrc) jsrc->build_sources(C.tree.bounds.p, C.prm);
+    EXA_CUDA(cudaEventRecord(tm.ev[2], C.stream));
+    tree_ok = true;
+    up_ok = lists_ok = false;
+  }
+
+  void grow_tree() {
     for (int attempt = 0;; attempt++) {
       build_tree(C);
       sync_tree(C);
@@ -161,9 +213,6 @@ struct Engine {
       break;
     }
     check_err("build_tree");
-    EXA_CUDA(cudaEventRecord(tm.ev[2], C.stream));
-    tree_ok = true;
-    up_ok = lists_ok = false;
   }
 
   void build_tree_grow(long long cap) {
@@ -196,8 +245,32 @@ struct Engine {
       p2m_fp64(a);
       for (int l = C.tree.depth - 1; l >= 0; l--) m2m_fp64(a, l, C.tree.lvl_host[l]);
     }
+    if (jsrc) jsrc->upward();  // examples/fmm.cxx:70
     EXA_CUDA(cudaEventRecord(tm.ev[3], C.stream));
     up_ok = true;
+  }
+
+  // Traversal::traverse(cells, jcells) and the FP64 operators across the two trees.
+  void traverse_separate_sources() {
+    if (C.prm.precision != kFP64) throw std::runtime_error("separate sources: FP64 precision only");
+    if (C.prm.images != 0) throw std::runtime_error("separate sources: free space only (images = 0)");
+    const long long nc = C.tree.ncells;
+    const int NT = tri(C.prm.P);
+    for (int attempt = 0; !traverse(C, lists, &jsrc->C.tree); attempt++)
+      if (attempt > 8) throw std::runtime_error("traversal capacity growth did not converge");
+    check_err("traverse");
+    EXA_CUDA(cudaEventRecord(tm.ev[4], C.stream));
+    EXA_CUDA(cudaMemsetAsync(L.p, 0, nc * NT * sizeof(double2), C.stream));
+    FmmArgs a = args();
+    a.src_cell_b = jsrc->C.tree.cell_b.p;
+    a.src_cell_x = jsrc->C.tree.cell_x.p;
+    a.src_xt = jsrc->C.tree.xyzq_tree.p;
+    a.src_M64 = jsrc->M.p;
+    m2l_fp64(a);
+    EXA_CUDA(cudaEventRecord(tm.lat[0], C.stream));
+    EXA_CUDA(cudaEventRecord(tm.lat[1], C.stream));
+    EXA_CUDA(cudaEventRecord(tm.ev[5], C.stream));
+    p2p_fp64(a);
   }
 
   void traverse_and_evaluate() {
@@ -206,7 +279,9 @@ struct Engine {
     const int NT = tri(C.prm.P);
     trg.ensure(C.tree.n);
     if (C.tree.n) EXA_CUDA(cudaMemsetAsync(trg.p, 0, C.tree.n * sizeof(double4), C.stream));
-    if (nc > 0) {
+    if (nc > 0 && jsrc) {
+      traverse_separate_sources();
+    } else if (nc > 0) {
       for (int attempt = 0; !traverse(C, lists); attempt++)
         if (attempt > 8) throw std::runtime_error("traversal capacity growth did not converge");
       check_err("traverse");
@@ -364,6 +439,38 @@ int guarded_free(F &&f, std::string &err) {
   }
 }
 thread_local std::string g_kernel_error;
+
+// Cell table in the reference's layout: ints (IPARENT, ICHILD, NCHILD, IBODY, NBODY),
+// reals (X, Y, Z, R).
+void copy_cells(Engine &E, int *ints, double *reals) {
+  {
+    const long long nc = E.C.tree.ncells;
+    std::vector<int4> b(nc);
+    std::vector<int2> pl(nc);
+    std::vector<double4> x(nc);
+    if (nc) {
+      EXA_CUDA(cudaMemcpy(b.data(), E.C.tree.cell_b.p, nc * sizeof(int4), cudaMemcpyDeviceToHost));
+      EXA_CUDA(cudaMemcpy(pl.data(), E.C.tree.cell_pl.p, nc * sizeof(int2), cudaMemcpyDeviceToHost));
+      EXA_CUDA(cudaMemcpy(x.data(), E.C.tree.cell_x.p, nc * sizeof(double4), cudaMemcpyDeviceToHost));
+    }
+    for (long long c = 0; c < nc; c++) {
+      if (ints) {
+        ints[5 * c + 0] = pl[c].x;
+        ints[5 * c + 1] = b[c].z;
+        ints[5 * c + 2] = b[c].w;
+        ints[5 * c + 3] = b[c].x;
+        ints[5 * c + 4] = b[c].y;
+      }
+      if (reals) {
+        reals[4 * c + 0] = x[c].x;
+        reals[4 * c + 1] = x[c].y;
+        reals[4 * c + 2] = x[c].z;
+        reals[4 * c + 3] = x[c].w;
+      }
+    }
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -488,6 +595,7 @@ int exafmm_get_bounds(exafmm_ctx *ctx, double *b6) {
   return guarded(ctx, [&] {
     cudaSetDevice(ctx->E.C.device);
     compute_bounds(ctx->E.C);
+    if (ctx->E.jsrc) extend_bounds(ctx->E.C, ctx->E.jsrc->C.tree.xyzq.p, ctx->E.jsrc->C.tree.n);
     EXA_CUDA(cudaMemcpyAsync(b6, ctx->E.C.tree.bounds.p, 6 * sizeof(double), cudaMemcpyDeviceToHost,
                              ctx->E.C.stream));
     EXA_CUDA(cudaStreamSynchronize(ctx->E.C.stream));
@@ -558,33 +666,29 @@ int exafmm_tree_info(exafmm_ctx *ctx, long long *ncells, int *depth, long long *
 
 int exafmm_get_cells(exafmm_ctx *ctx, int *ints, double *reals) {
   return guarded(ctx, [&] {
+    if (!ctx->E.tree_ok) throw std::runtime_error("no tree");
+    cudaSetDevice(ctx->E.C.device);
+    copy_cells(ctx->E, ints, reals);
+  });
+}
+
+int exafmm_set_sources(exafmm_ctx *ctx, const double *xyzq, long long n) {
+  return guarded(ctx, [&] {
+    cudaSetDevice(ctx->E.C.device);
+    ctx->E.set_sources(xyzq, n);
+  });
+}
+
+int exafmm_get_source_cells(exafmm_ctx *ctx, long long *ncells, int *ints, double *reals, int *perm) {
+  return guarded(ctx, [&] {
     Engine &E = ctx->E;
-    if (!E.tree_ok) throw std::runtime_error("no tree");
+    if (!E.jsrc) throw std::runtime_error("no separate sources");
+    if (!E.tree_ok || !E.jsrc->tree_ok) throw std::runtime_error("no tree");
     cudaSetDevice(E.C.device);
-    const long long nc = E.C.tree.ncells;
-    std::vector<int4> b(nc);
-    std::vector<int2> pl(nc);
-    std::vector<double4> x(nc);
-    if (nc) {
-      EXA_CUDA(cudaMemcpy(b.data(), E.C.tree.cell_b.p, nc * sizeof(int4), cudaMemcpyDeviceToHost));
-      EXA_CUDA(cudaMemcpy(pl.data(), E.C.tree.cell_pl.p, nc * sizeof(int2), cudaMemcpyDeviceToHost));
-      EXA_CUDA(cudaMemcpy(x.data(), E.C.tree.cell_x.p, nc * sizeof(double4), cudaMemcpyDeviceToHost));
-    }
-    for (long long c = 0; c < nc; c++) {
-      if (ints) {
-        ints[5 * c + 0] = pl[c].x;
-        ints[5 * c + 1] = b[c].z;
-        ints[5 * c + 2] = b[c].w;
-        ints[5 * c + 3] = b[c].x;
-        ints[5 * c + 4] = b[c].y;
-      }
-      if (reals) {
-        reals[4 * c + 0] = x[c].x;
-        reals[4 * c + 1] = x[c].y;
-        reals[4 * c + 2] = x[c].z;
-        reals[4 * c + 3] = x[c].w;
-      }
-    }
+    if (ncells) *ncells = E.jsrc->C.tree.ncells;
+    copy_cells(*E.jsrc, ints, reals);
+    if (perm && E.jsrc->C.tree.n)
+      EXA_CUDA(cudaMemcpy(perm, E.jsrc->C.tree.perm.p, E.jsrc->C.tree.n * sizeof(int), cudaMemcpyDeviceToHost));
   });
 }
 

@@ -68,6 +68,8 @@ struct Context {
 // Tree construction (tree.cu).
 void compute_bounds(Context &C);
 void set_bounds(Context &C, const double *bounds6_host);
+// BoundBox::getBounds(bodies, bounds): C's bounds extended by n bodies x (device).
+void extend_bounds(Context &C, const double4 *x, long long n);
 void build_tree(Context &C);
 void sync_tree(Context &C);  // reads cell count, depth and the error word
 

@@ -21,6 +21,12 @@ struct FmmArgs {
   const int *p2p_off = nullptr, *p2p_src = nullptr;
   double2 *M64 = nullptr, *L64 = nullptr;
   double4 *trg64 = nullptr;            // results in tree order
+  // separate source bodies (their own tree): the source side of M2L and P2P
+  // (null: the sources are the targets)
+  const int4 *src_cell_b = nullptr;
+  const double4 *src_cell_x = nullptr;
+  const double4 *src_xt = nullptr;
+  const double2 *src_M64 = nullptr;
 };
 
 void p2m_fp64(const FmmArgs &a);
@@ -111,6 +117,6 @@ struct ListBufs {
 // Runs the traversal into lists (unsorted), then groups them by target cell.
 // Returns false when a capacity was exceeded; the capacities are then grown to
 // the counts the traversal reported and the caller reruns it.
-bool traverse(Context &C, ListBufs &lb);
+bool traverse(Context &C, ListBufs &lb, const TreeBufs *sources = nullptr);
 
 }  // namespace exafmm_b200

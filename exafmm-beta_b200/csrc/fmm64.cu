@@ -191,8 +191,8 @@ __device__ __forceinline__ void m2l_accumulate(const DevTables &t, const int (&o
 // sign s = +1 (m < 0), (-1)^m (0 <= m <= k), (-1)^k (m > k).
 template <int MAXO>
 __global__ void k_m2l(DevTables t, const int *off, const int *src, long long ncells, const double4 *cell_x,
-                      const double2 *M, double2 *L, double cycle, const int2 *cell_pl, int skip_min_level,
-                      int skip_max_dl) {
+                      const double4 *cell_xj, const double2 *M, double2 *L, double cycle, const int2 *cell_pl,
+                      int skip_min_level, int skip_max_dl) {
   extern __shared__ double2 sh[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int P = t.P, NT = t.nterm, NS = tri(2 * P - 1);
@@ -223,7 +223,7 @@ __global__ void k_m2l(DevTables t, const int *off, const int *src, long long nce
       }
       double sx, sy, sz;
       image_shift(img, cycle, sx, sy, sz);
-      const double4 Xj = cell_x[cj];
+      const double4 Xj = cell_xj[cj];
       const double dx = Xi.x - Xj.x - sx, dy = Xi.y - Xj.y - sy, dz = Xi.z - Xj.z - sz;
       for (int o = lane; o < NT; o += 32) Mp[o] = cscale(M[(long long)cj * NT + o], t.anm[o]);
       if (lane < 2 * P - 1) singular_column(t, lane, 2 * P - 1, dx, dy, dz, t.ainv, S);
@@ -372,7 +372,7 @@ __global__ void k_l2p(DevTables t, const int4 *cell_b, const double4 *cell_x, co
 // pot += q/r, grad += q (x_j - x_i)/r^3 with r = 0 pairs skipped (laplace.h:150-235).
 template <int TPL>
 __global__ void k_p2p(const int *off, const int *src, long long ncells, const int4 *cell_b, const double4 *xt,
-                      double4 *trg, double cycle) {
+                      const int4 *cell_bj, const double4 *xtj, double4 *trg, double cycle) {
   __shared__ double4 sbuf[kWarpsPerBlock][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (long long c = (long long)blockIdx.x * kWarpsPerBlock + warp; c < ncells; c += (long long)gridDim.x * kWarpsPerBlock) {
@@ -396,11 +396,11 @@ __global__ void k_p2p(const int *off, const int *src, long long ncells, const in
         const int cj = packed & 0x3ffffff, img = packed >> 26;
         double sx, sy, sz;
         image_shift(img, cycle, sx, sy, sz);
-        const int4 cjb = cell_b[cj];
+        const int4 cjb = cell_bj[cj];
         for (int sb = 0; sb < cjb.y; sb += 32) {
           const int ns = min(32, cjb.y - sb);
           if (lane < ns) {
-            double4 s = xt[cjb.x + sb + lane];
+            double4 s = xtj[cjb.x + sb + lane];
             s.x += sx;
             s.y += sy;
             s.z += sz;
@@ -655,7 +655,8 @@ void m2l_fp64(const FmmArgs &a, int skip_min_level, int skip_max_dl) {
   EXA_MAXO_SWITCH(maxo_for(a.P), {
     set_smem(k_m2l<MO>, smem);
     k_m2l<MO><<<blocks_for(a.ncells), 32 * kWarpsPerBlock, smem, a.stream>>>(
-        t, a.m2l_off, a.m2l_src, a.ncells, a.cell_x, a.M64, a.L64, a.cycle, pl, skip_min_level, skip_max_dl);
+        t, a.m2l_off, a.m2l_src, a.ncells, a.cell_x, a.src_cell_x ? a.src_cell_x : a.cell_x,
+        a.src_M64 ? a.src_M64 : a.M64, a.L64, a.cycle, pl, skip_min_level, skip_max_dl);
   });
   EXA_CHECK_LAUNCH();
 }
@@ -682,15 +683,17 @@ void l2p_fp64(const FmmArgs &a) {
 
 void p2p_fp64(const FmmArgs &a) {
   const int tpl = (a.ncrit + 31) / 32;
+  const int4 *bj = a.src_cell_b ? a.src_cell_b : a.cell_b;
+  const double4 *xj = a.src_xt ? a.src_xt : a.xt;
   if (tpl <= 1)
     k_p2p<1><<<blocks_for(a.ncells), 32 * kWarpsPerBlock, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b,
-                                                                          a.xt, a.trg64, a.cycle);
+                                                                          a.xt, bj, xj, a.trg64, a.cycle);
   else if (tpl <= 2)
     k_p2p<2><<<blocks_for(a.ncells), 32 * kWarpsPerBlock, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b,
-                                                                          a.xt, a.trg64, a.cycle);
+                                                                          a.xt, bj, xj, a.trg64, a.cycle);
   else
     k_p2p<4><<<blocks_for(a.ncells), 32 * kWarpsPerBlock, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b,
-                                                                          a.xt, a.trg64, a.cycle);
+                                                                          a.xt, bj, xj, a.trg64, a.cycle);
   EXA_CHECK_LAUNCH();
 }
 

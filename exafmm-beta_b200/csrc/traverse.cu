@@ -23,8 +23,11 @@ constexpr int kImgShift = 26;
 constexpr int kCellMask = (1 << kImgShift) - 1;
 
 struct PairCtx {
-  const int4 *cell_b;
+  const int4 *cell_b;      // target cells
   const double4 *cell_x;
+  const int4 *cell_bj;     // source cells (the same table unless sources have their own tree)
+  const double4 *cell_xj;
+  int same;                // one tree: Ci == Cj is possible (splitCell splits both then)
   double theta;
   int nspawn;
   double cycle;
@@ -34,9 +37,9 @@ enum Mode : int { kM2L = 0, kP2P = 1, kSplitI = 2, kSplitJ = 3, kSplitBoth = 4 }
 
 __device__ __forceinline__ int decide(const PairCtx &c, int2 pr, int4 &bi, int4 &bj) {
   const int ci = pr.x, cj = pr.y & kCellMask, img = pr.y >> kImgShift;
-  const double4 Xi = c.cell_x[ci], Xj = c.cell_x[cj];
+  const double4 Xi = c.cell_x[ci], Xj = c.cell_xj[cj];
   bi = c.cell_b[ci];
-  bj = c.cell_b[cj];
+  bj = c.cell_bj[cj];
   const double sx = (double)(img / 9 - 1) * c.cycle;
   const double sy = (double)((img / 3) % 3 - 1) * c.cycle;
   const double sz = (double)(img % 3 - 1) * c.cycle;
@@ -50,7 +53,7 @@ __device__ __forceinline__ int decide(const PairCtx &c, int2 pr, int4 &bi, int4 
   if (bi.w == 0 && bj.w == 0) return bj.y == 0 ? kM2L : kP2P;
   if (bj.w == 0) return kSplitI;
   if (bi.w == 0) return kSplitJ;
-  if (bi.y + bj.y >= c.nspawn || ci == cj) return kSplitBoth;
+  if (bi.y + bj.y >= c.nspawn || (c.same && ci == cj)) return kSplitBoth;
   return (Xi.w >= Xj.w) ? kSplitI : kSplitJ;
 }
 
@@ -179,8 +182,9 @@ void group_by_target(Context &C, const int2 *pairs, long long n, long long ncell
 
 }  // namespace
 
-bool traverse(Context &C, ListBufs &lb) {
+bool traverse(Context &C, ListBufs &lb, const TreeBufs *sources) {
   const long long ncells = C.tree.ncells;
+  const TreeBufs &S = sources ? *sources : C.tree;
   cudaStream_t st = C.stream;
   // capacities for this tree (a reused context may hold a larger one now)
   lb.m2l_cap = std::max(lb.m2l_cap, 256 * ncells + 1024);
@@ -191,11 +195,14 @@ bool traverse(Context &C, ListBufs &lb) {
   lb.m2l.ensure(lb.m2l_cap);
   lb.p2p.ensure(lb.p2p_cap);
   lb.cnt.ensure(3 * (kMaxSweeps + 1));
-  k_trav_init<<<1, 32, 0, st>>>(lb.q0.p, lb.cnt.p, C.prm.images, ncells);
+  k_trav_init<<<1, 32, 0, st>>>(lb.q0.p, lb.cnt.p, C.prm.images, std::min<long long>(ncells, S.ncells));
   EXA_CHECK_LAUNCH();
   PairScan ps;
   ps.c.cell_b = C.tree.cell_b.p;
   ps.c.cell_x = C.tree.cell_x.p;
+  ps.c.cell_bj = S.cell_b.p;
+  ps.c.cell_xj = S.cell_x.p;
+  ps.c.same = sources == nullptr;
   ps.c.theta = C.prm.theta;
   ps.c.nspawn = C.prm.nspawn;
   ps.c.cycle = C.prm.cycle;
@@ -207,9 +214,10 @@ bool traverse(Context &C, ListBufs &lb) {
   ps.p2p_cap = lb.p2p_cap;
   ps.err = C.err.p;
   // Every split takes one side of a pair a level deeper and leaf pairs are
-  // decided where they are met, so a tree of depth d needs at most 2d + 1
-  // sweeps; two more are launched, and the queue after the last must be empty.
-  const int nsw = std::min(kMaxSweeps, 2 * (C.tree.depth + 1) + 2);
+  // decided where they are met, so trees of depths di and dj need at most
+  // di + dj + 1 sweeps; two more are launched, and the queue after the last
+  // must be empty.
+  const int nsw = std::min(kMaxSweeps, (C.tree.depth + 1) + (S.depth + 1) + 2);
   for (int s = 0; s < nsw; s++) {
     ps.sweep = s;
     ps.qin = (s & 1) ? lb.q1.p : lb.q0.p;

@@ -76,18 +76,32 @@ __global__ void k_bounds(const double4 *x, long long n, unsigned long long *enc)
 // whose estimate lies within twice that of the extreme estimate can hold the
 // exact extreme; only those evaluate the closed form.
 // enc[0..5]: exact result, enc[6..11]: estimates, enc[12]: max |x| over all coordinates.
-__global__ void k_bounds_estimate(const double4 *x, long long n, unsigned long long *enc) {
+// With init6 (BoundBox::getBounds(bodies, bounds), bound_box.h:28-36) the
+// running bounds start from init6 instead of the first body: every body then
+// drifts n - 1 - j times and init6 itself n times.
+__global__ void k_bounds_estimate(const double4 *x, long long n, unsigned long long *enc, const double *init6) {
   unsigned long long lo[3] = {~0ull, ~0ull, ~0ull}, hi[3] = {0, 0, 0}, amax = 0;
   for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
     const double4 b = x[j];
     const double v[3] = {b.x, b.y, b.z};
-    const double kc = (double)((j == 0) ? n : n - 1 - j) * 1e-5;
+    const double kc = (double)((j == 0 && !init6) ? n : n - 1 - j) * 1e-5;
     for (int d = 0; d < 3; d++) {
       const unsigned long long a = order_enc(v[d] - kc), c = order_enc(v[d] + kc);
       lo[d] = a < lo[d] ? a : lo[d];
       hi[d] = c > hi[d] ? c : hi[d];
       const unsigned long long ab = order_enc(fabs(v[d]));
       amax = ab > amax ? ab : amax;
+    }
+  }
+  if (init6 && blockIdx.x == 0 && threadIdx.x == 0) {
+    const double kc = (double)n * 1e-5;
+    for (int d = 0; d < 3; d++) {
+      const unsigned long long a = order_enc(init6[d] - kc), c = order_enc(init6[3 + d] + kc);
+      lo[d] = a < lo[d] ? a : lo[d];
+      hi[d] = c > hi[d] ? c : hi[d];
+      const unsigned long long a1 = order_enc(fabs(init6[d])), a2 = order_enc(fabs(init6[3 + d]));
+      amax = a1 > amax ? a1 : amax;
+      amax = a2 > amax ? a2 : amax;
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
@@ -109,7 +123,7 @@ __global__ void k_bounds_estimate(const double4 *x, long long n, unsigned long l
   }
 }
 
-__global__ void k_bounds_exact(const double4 *x, long long n, unsigned long long *enc) {
+__global__ void k_bounds_exact(const double4 *x, long long n, unsigned long long *enc, const double *init6) {
   const double span = order_dec(enc[12]) + (double)n * 1e-5;
   const double B = (double)n * ldexp(1.0, ilogb(span > 1e-300 ? span : 1e-300) - 52) + 1e-300;
   double elo[3], ehi[3];
@@ -120,11 +134,18 @@ __global__ void k_bounds_exact(const double4 *x, long long n, unsigned long long
   for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
     const double4 b = x[j];
     const double v[3] = {b.x, b.y, b.z};
-    const long long k = (j == 0) ? n : n - 1 - j;
+    const long long k = (j == 0 && !init6) ? n : n - 1 - j;
     const double kc = (double)k * 1e-5;
     for (int d = 0; d < 3; d++) {
       if (v[d] - kc <= elo[d]) atomicMin(&enc[d], order_enc(drift_down(v[d], k)));
       if (v[d] + kc >= ehi[d]) atomicMax(&enc[3 + d], order_enc(drift_up(v[d], k)));
+    }
+  }
+  if (init6 && blockIdx.x == 0 && threadIdx.x == 0) {
+    const double kc = (double)n * 1e-5;
+    for (int d = 0; d < 3; d++) {
+      if (init6[d] - kc <= elo[d]) atomicMin(&enc[d], order_enc(drift_down(init6[d], n)));
+      if (init6[3 + d] + kc >= ehi[d]) atomicMax(&enc[3 + d], order_enc(drift_up(init6[3 + d], n)));
     }
   }
 }
@@ -422,12 +443,26 @@ void compute_bounds(Context &C) {
   k_bounds_init<<<1, 32, 0, C.stream>>>(T.bounds_enc.p);
   EXA_CHECK_LAUNCH();
   if (T.n > 0) {
-    k_bounds_estimate<<<grid_for(T.n, 256), 256, 0, C.stream>>>(T.xyzq.p, T.n, T.bounds_enc.p);
+    k_bounds_estimate<<<grid_for(T.n, 256), 256, 0, C.stream>>>(T.xyzq.p, T.n, T.bounds_enc.p, nullptr);
     EXA_CHECK_LAUNCH();
-    k_bounds_exact<<<grid_for(T.n, 256), 256, 0, C.stream>>>(T.xyzq.p, T.n, T.bounds_enc.p);
+    k_bounds_exact<<<grid_for(T.n, 256), 256, 0, C.stream>>>(T.xyzq.p, T.n, T.bounds_enc.p, nullptr);
     EXA_CHECK_LAUNCH();
   }
   k_bounds_final<<<1, 32, 0, C.stream>>>(T.bounds_enc.p, T.n, T.bounds.p);
+  EXA_CHECK_LAUNCH();
+}
+
+void extend_bounds(Context &C, const double4 *x, long long n) {
+  TreeBufs &T = C.tree;
+  if (n <= 0) return;  // no bodies: the bounds stay as they are
+  T.bounds_enc.ensure(16);
+  k_bounds_init<<<1, 32, 0, C.stream>>>(T.bounds_enc.p);
+  EXA_CHECK_LAUNCH();
+  k_bounds_estimate<<<grid_for(n, 256), 256, 0, C.stream>>>(x, n, T.bounds_enc.p, T.bounds.p);
+  EXA_CHECK_LAUNCH();
+  k_bounds_exact<<<grid_for(n, 256), 256, 0, C.stream>>>(x, n, T.bounds_enc.p, T.bounds.p);
+  EXA_CHECK_LAUNCH();
+  k_bounds_final<<<1, 32, 0, C.stream>>>(T.bounds_enc.p, n, T.bounds.p);
   EXA_CHECK_LAUNCH();
 }
 

@@ -65,13 +65,27 @@ int exafmm_set_params(exafmm_ctx *ctx, int P, double theta, int ncrit, int nspaw
  * compile-time switch, EXAFMM_SINGLE). */
 int exafmm_set_mixed_policy(exafmm_ctx *ctx, int m2l_fp32, int p2p_fp32, int min_level, int max_dl);
 
+/* Separate source bodies (examples/fmm.cxx -j IneJ, :37-47, :61-73): the next
+ * solves evaluate the field of these n sources (n x 4: x, y, z, q, caller
+ * order) at the context's bodies.  As there, the bounds are the targets'
+ * extended by the sources (BoundBox::getBounds(jbodies, bounds)), each set gets
+ * a tree on those bounds and its upward pass, and the traversal runs target
+ * cells against source cells.  Free space, FP64 precision.  xyzq == NULL
+ * returns to sources == targets. */
+int exafmm_set_sources(exafmm_ctx *ctx, const double *xyzq, long long n);
+/* The source tree of the last build: cell count, cell table (as
+ * exafmm_get_cells) and the sources' tree-order permutation; any output may be NULL. */
+int exafmm_get_source_cells(exafmm_ctx *ctx, long long *ncells, int *ints, double *reals, int *perm);
+
 /* Bodies in caller order (Dataset::initBodies / Bodies, include/types.h:72-86).
  * The _device form takes a device pointer to n x 4 doubles on the context's device. */
 int exafmm_set_bodies(exafmm_ctx *ctx, const double *xyzq, long long n);
 int exafmm_set_bodies_device(exafmm_ctx *ctx, const double *d_xyzq, long long n);
 
 /* BoundBox::getBounds(Bodies&) (include/bound_box.h:11-25), including its
- * sequential 1e-5 drift, evaluated on the device in closed form. */
+ * sequential 1e-5 drift, evaluated on the device in closed form; with separate
+ * sources, extended by them as getBounds(jbodies, bounds) does
+ * (bound_box.h:28-36), which is what the solve uses. */
 int exafmm_get_bounds(exafmm_ctx *ctx, double *bounds6);
 
 /* BuildTree::buildTree(bodies, buffer, bounds) (include/build_tree.h:186-209).

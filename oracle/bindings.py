@@ -243,6 +243,9 @@ class Reference(_Lib):
         self._f("get_cells", None, [_vp, _vp, _vp, _vp])
         self._f("get_times", None, [_vp, _vp])
         self._f("write_list", None, [_vp, ctypes.c_char_p])
+        self._f("run_inej", _vp, [_c_int, _vp, _c_int, _vp, _c_int, _c_double, _c_int, _c_int, _c_int])
+        self._f("num_jcells", _c_int, [_vp])
+        self._f("get_jcells", None, [_vp, _vp, _vp, _vp])
         self._f("write_time", None, [_c_int, _vp, _vp, ctypes.c_char_p])
 
     def _get_cells(self, h, ci, cr):
@@ -278,6 +281,23 @@ class Reference(_Lib):
             if list_path is not None:
                 self.lib.ref_write_list(h, list_path.encode())
             return run
+        finally:
+            self.lib.ref_free(h)
+
+    def solve_inej(self, xyzq, jxyzq, P=10, theta=0.4, ncrit=64, nspawn=5000, record_lists=True):
+        """examples/fmm.cxx with -j IneJ: targets xyzq, separate sources jxyzq (free space).
+        Returns the target-side TreeRun and (jcells_int, jcells_real, jperm) of the source tree."""
+        xyzq, jxyzq = _as_xyzq(xyzq), _as_xyzq(jxyzq)
+        h = self.lib.ref_run_inej(len(xyzq), _ptr(xyzq), len(jxyzq), _ptr(jxyzq), P, theta, ncrit, nspawn,
+                                  int(record_lists))
+        try:
+            run = self._collect(h, len(xyzq), P, lists=record_lists)
+            nj = self.lib.ref_num_jcells(h)
+            ji = np.zeros((nj, 5), dtype=np.int32)
+            jr = np.zeros((nj, 4))
+            jp = np.zeros(len(jxyzq), dtype=np.int32)
+            self.lib.ref_get_jcells(h, _ptr(ji), _ptr(jr), _ptr(jp))
+            return run, (ji, jr, jp)
         finally:
             self.lib.ref_free(h)
 

@@ -38,19 +38,20 @@ namespace exafmm_laplace {
   class Kernel : public RefKernelBase {
   public:
     PairLog * log = nullptr;
-    C_iter C0;
+    C_iter C0;    // first target cell
+    C_iter Cj0;   // first source cell (C0 unless the sources have their own tree)
     Kernel(int P, real_t eps2, complex_t wavek) : RefKernelBase(P, eps2, wavek) {}
     void M2L(C_iter Ci, C_iter Cj) {
       if (log) {
         log->m2l.push_back(int(Ci - C0));
-        log->m2l.push_back(int(Cj - C0));
+        log->m2l.push_back(int(Cj - Cj0));
       }
       RefKernelBase::M2L(Ci, Cj);
     }
     void P2P(C_iter Ci, C_iter Cj) {
       if (log) {
         log->p2p.push_back(int(Ci - C0));
-        log->p2p.push_back(int(Cj - C0));
+        log->p2p.push_back(int(Cj - Cj0));
       }
       RefKernelBase::P2P(Ci, Cj);
     }
@@ -98,6 +99,8 @@ namespace {
     Bounds bounds;
     Bodies bodies;            // tree order after buildTree
     Cells cells;
+    Bodies jbodies;           // separate sources (IneJ), tree order
+    Cells jcells;
     PairLog log;
     double times[8] = {0};    // bounds, grow, link, up, traverse, down, total, dipole
   };
@@ -141,6 +144,7 @@ void * ref_run(int n, const double * xyzq, int P, double theta, int ncrit, int n
   traversal.initListCount(run->cells);  // examples/fmm.cxx:67
   double t3 = logger::get_time();
   kernel.C0 = run->cells.begin();
+  kernel.Cj0 = run->cells.begin();
   kernel.log = record_lists ? &run->log : nullptr;
   if (threads > 1) {
     omp_set_num_threads(threads);
@@ -170,6 +174,59 @@ void * ref_run(int n, const double * xyzq, int P, double theta, int ncrit, int n
   run->times[6] = t5 - t0;
   run->times[7] = t6 - t5;
   return run;
+}
+
+// Separate source bodies (examples/fmm.cxx -j IneJ, :61-73): bounds of the
+// targets extended by the sources (BoundBox::getBounds(jbodies, bounds)), a
+// tree for each on those bounds, both upward passes, traverse(cells, jcells),
+// downward pass of the targets.  Free space.
+void * ref_run_inej(int n, const double * xyzq, int nj, const double * jxyzq, int P, double theta, int ncrit,
+                    int nspawn, int record_lists) {
+  Run * run = new Run;
+  run->n = n;
+  run->P = P;
+  Kernel & kernel = kernelFor(P);
+  loadBodies(run->bodies, n, xyzq);
+  loadBodies(run->jbodies, nj, jxyzq);
+  Bodies buffer;
+  buffer.reserve(std::max(n, nj));
+  BoundBox boundBox;
+  BuildTree buildTree(ncrit);
+  UpDownPass upDownPass(kernel);
+  Traversal traversal(kernel, theta, nspawn, 0, "./");
+  vec3 vcycle = 2 * M_PI;
+  run->bounds = boundBox.getBounds(run->bodies);
+  run->bounds = boundBox.getBounds(run->jbodies, run->bounds);
+  run->cells = buildTree.buildTree(run->bodies, buffer, run->bounds);
+  upDownPass.upwardPass(run->cells);
+  traversal.initListCount(run->cells);
+  run->jcells = buildTree.buildTree(run->jbodies, buffer, run->bounds);
+  upDownPass.upwardPass(run->jcells);
+  kernel.C0 = run->cells.begin();
+  kernel.Cj0 = run->jcells.begin();
+  kernel.log = record_lists ? &run->log : nullptr;
+  traversal.traverse(run->cells, run->jcells, vcycle, true);
+  kernel.log = nullptr;
+  upDownPass.downwardPass(run->cells);
+  return run;
+}
+
+int ref_num_jcells(void * h) { return int(((Run *)h)->jcells.size()); }
+
+void ref_get_jcells(void * h, int * ints, double * reals, int * jperm) {
+  Run * run = (Run *)h;
+  int c = 0;
+  for (auto & C : run->jcells) {
+    ints[5 * c + 0] = C.IPARENT;
+    ints[5 * c + 1] = C.ICHILD;
+    ints[5 * c + 2] = C.NCHILD;
+    ints[5 * c + 3] = C.IBODY;
+    ints[5 * c + 4] = C.NBODY;
+    for (int d = 0; d < 3; d++) reals[4 * c + d] = C.X[d];
+    reals[4 * c + 3] = C.R;
+    c++;
+  }
+  for (size_t i = 0; i < run->jbodies.size(); i++) jperm[i] = run->jbodies[i].IBODY;
 }
 
 int ref_num_cells(void * h) { return int(((Run *)h)->cells.size()); }

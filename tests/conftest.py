@@ -61,11 +61,15 @@ def golden_cases():
     the MD ABI are separate)."""
     other = ("kernel_kat.npz", "records.npz", "md_gromacs.npz")
     return sorted(p for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if os.path.basename(p) not in other and not os.path.basename(p).startswith("periodic_"))
+                  if os.path.basename(p) not in other and not os.path.basename(p).startswith(("periodic_", "inej_")))
 
 
 def periodic_golden_cases():
     return sorted(glob.glob(os.path.join(GOLDEN, "periodic_*.npz")))
+
+
+def inej_golden_cases():
+    return sorted(glob.glob(os.path.join(GOLDEN, "inej_*.npz")))
 
 
 def load_golden(path):

@@ -7,7 +7,7 @@ commits no golden values of its own (its .reg regression files are written at
 run time), so these fixtures are what pins both the CPU restatement (oracle/)
 and the GPU engine to the reference's behaviour.
 
-Run from the repository root:  python tests/golden/make_golden.py [solve periodic kat records md]
+Run from the repository root:  python tests/golden/make_golden.py [solve periodic kat records md inej]
 """
 from __future__ import annotations
 
@@ -197,7 +197,31 @@ def make_md(ref: Reference):
           f"force rel-L2 {acc:.2e}")
 
 
-def main(which=("solve", "periodic", "kat", "records", "md")):
+# Separate source bodies (examples/fmm.cxx -j IneJ): (name, target generator, n,
+# seed, source generator, n, seed, split, P, theta, ncrit, nspawn).  split applies
+# fmm.cxx's transform (targets x -> (x + pi) / 2, sources x -> (x - pi) / 2).
+INEJ_CASES = [
+    ("inej_split_cube", "cube", 2000, 31, "cube", 1500, 32, True, 6, 0.4, 16, 5000),
+    ("inej_overlap_plummer", "plummer", 3000, 33, "plummer", 2500, 34, False, 8, 0.35, 32, 5000),
+    ("inej_overlap_cube_nspawn", "cube", 1500, 35, "sphere", 2000, 36, False, 4, 0.5, 8, 100),
+]
+
+
+def make_inej(ref: Reference, name, gen, n, seed, jgen, nj, jseed, split, P, theta, ncrit, nspawn):
+    x = getattr(datasets, gen)(n, seed)
+    jx = getattr(datasets, jgen)(nj, jseed)
+    if split:
+        x[:, 0] = (x[:, 0] + np.pi) * 0.5
+        jx[:, 0] = (jx[:, 0] - np.pi) * 0.5
+    run, (ji, jr, jp) = ref.solve_inej(x, jx, P=P, theta=theta, ncrit=ncrit, nspawn=nspawn)
+    data = dict(xyzq=x, jxyzq=jx, params=np.array([P, theta, ncrit, nspawn], dtype=np.float64), bounds=run.bounds,
+                perm=run.perm, cells_int=run.cells_int, cells_real=run.cells_real, jcells_int=ji, jcells_real=jr,
+                jperm=jp, m2l=sorted_pairs(run.m2l), p2p=sorted_pairs(run.p2p), trg=run.trg)
+    np.savez_compressed(os.path.join(OUT, name + ".npz"), **data)
+    print(f"{name}: cells={len(run.cells_int)} jcells={len(ji)} m2l={len(run.m2l)} p2p={len(run.p2p)}")
+
+
+def main(which=("solve", "periodic", "kat", "records", "md", "inej")):
     build(reference=True)
     ref = Reference()
     if "solve" in which:
@@ -212,8 +236,11 @@ def main(which=("solve", "periodic", "kat", "records", "md")):
         make_records(ref)
     if "md" in which:
         make_md(ref)
+    if "inej" in which:
+        for c in INEJ_CASES:
+            make_inej(ref, *c)
 
 
 if __name__ == "__main__":
-    # optional arguments: a subset of solve, periodic, kat, records, md
-    main(tuple(sys.argv[1:]) or ("solve", "periodic", "kat", "records", "md"))
+    # optional arguments: a subset of solve, periodic, kat, records, md, inej
+    main(tuple(sys.argv[1:]) or ("solve", "periodic", "kat", "records", "md", "inej"))

@@ -1,0 +1,85 @@
+"""Separate source bodies (examples/fmm.cxx -j IneJ) on the GPU against fixtures the
+reference wrote (tests/golden/make_golden.py inej): extended bounds, both trees and
+the cross-tree interaction lists bit for bit, FP64 results within the plain
+method's bar."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import inej_golden_cases, load_golden, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-11
+
+
+def _sorted(p):
+    p = np.asarray(p)[:, :2]
+    return p[np.lexsort((p[:, 1], p[:, 0]))] if len(p) else p.reshape(0, 2)
+
+
+@pytest.mark.parametrize("path", inej_golden_cases(), ids=lambda p: os.path.basename(p)[:-4])
+def test_separate_sources_match_reference(ex, path):
+    g = load_golden(path)
+    P, theta, ncrit, nspawn = g["params"]
+    f = ex.Fmm(P=int(P), theta=float(theta), ncrit=int(ncrit), nspawn=int(nspawn))
+    f.set_bodies(g["xyzq"])
+    f.set_sources(g["jxyzq"])
+    assert np.array_equal(f.get_bounds(), g["bounds"])
+    f.solve()
+    trg = f.results()
+    assert np.array_equal(f.perm(), g["perm"])
+    ci, cr = f.cells()
+    assert np.array_equal(ci, g["cells_int"])
+    assert np.array_equal(cr, g["cells_real"])
+    ji, jr, jp = f.source_cells()
+    assert np.array_equal(ji, g["jcells_int"])
+    assert np.array_equal(jr, g["jcells_real"])
+    assert np.array_equal(jp, g["jperm"])
+    m2l, p2p = f.lists()
+    assert np.array_equal(_sorted(m2l), g["m2l"])
+    assert np.array_equal(_sorted(p2p), g["p2p"])
+    assert rel_l2(trg[:, 0], g["trg"][:, 0]) < TOL
+    assert rel_l2(trg[:, 1:], g["trg"][:, 1:]) < TOL
+    f.close()
+
+
+def test_separate_sources_against_direct_and_reset(ex, datasets):
+    x = datasets.cube(3000, seed=8)
+    jx = datasets.plummer(4000, seed=9)
+    f = ex.Fmm(P=10, theta=0.4, ncrit=64)
+    f.set_bodies(x)
+    f.set_sources(jx)
+    f.solve()
+    trg = f.results()
+    idx = datasets.strided_sample(len(x), 256)
+    direct = ex.direct(x[idx], jx)
+    assert rel_l2(trg[idx, 0], direct[:, 0]) < 1e-5
+    assert rel_l2(trg[idx, 1:], direct[:, 1:]) < 1e-4
+    # sources back to the bodies themselves: the same as a fresh context
+    f.set_sources(None)
+    f.solve()
+    self_trg = f.results()
+    g = ex.Fmm(P=10, theta=0.4, ncrit=64)
+    g.set_bodies(x)
+    g.solve()
+    assert np.array_equal(self_trg, g.results())
+    f.close()
+    g.close()
+
+
+def test_separate_sources_need_fp64_free_space(ex, datasets):
+    x = datasets.cube(500, seed=1)
+    f = ex.Fmm(P=6, precision=ex.MIXED)
+    f.set_bodies(x)
+    f.set_sources(x[:100])
+    with pytest.raises(ex.FmmError, match="FP64"):
+        f.solve()
+    f.close()
+    f = ex.Fmm(P=6, images=1)
+    f.set_bodies(x)
+    f.set_sources(x[:100])
+    with pytest.raises(ex.FmmError, match="free space"):
+        f.solve()
+    f.close()
