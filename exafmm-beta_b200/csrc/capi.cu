@@ -87,6 +87,7 @@ struct Engine {
   ListBufs lists;
   DBuf<double2> M, L;
   DBuf<unsigned char> Ms;  // scaled multipoles for the unrolled M2L (FP32 or FP64)
+  DBuf<unsigned char> Ms64;  // FP64 scaled multipoles for the FP64 part of the mixed form
   DBuf<float4> x32;        // bodies as two-float pairs relative to the root center (mixed P2P)
   M2LGemmBufs gemm;         // class-grouped tile M2L (mixed form)
   DBuf<double2> lat;        // periodic lattice: supercell multipoles and warp partials
@@ -301,7 +302,19 @@ struct Engine {
         Ms.ensure(nc * NT * sizeof(float2));
         scale_multipoles(a, true, Ms.p);
         m2l_fast(left, true, Ms.p, C.prm.mixed_min_level, C.prm.mixed_max_dl);
-        m2l_fp64(a, C.prm.mixed_min_level, C.prm.mixed_max_dl);  // root levels, large size ratios
+        // root levels and large size ratios in FP64: few target cells with many
+        // sources each, which the unrolled kernel's lanes-over-sources form spreads out
+        if (m2l_fast_supported(C.prm.P, false)) {
+          m2l_complement(C, a, gemm, lists.n_m2l, C.prm.mixed_min_level, C.prm.mixed_max_dl);
+          FmmArgs comp = a;
+          comp.m2l_off = gemm.comp_off.p;
+          comp.m2l_src = gemm.comp_src.p;
+          Ms64.ensure(nc * NT * sizeof(double2));
+          scale_multipoles(a, false, Ms64.p);
+          m2l_fast(comp, false, Ms64.p);
+        } else {
+          m2l_fp64(a, C.prm.mixed_min_level, C.prm.mixed_max_dl);
+        }
       } else if (m2l_fast_supported(C.prm.P, false)) {
         Ms.ensure(nc * NT * sizeof(double2));
         scale_multipoles(a, false, Ms.p);

@@ -49,7 +49,7 @@ bool m2l_fast_supported(int P, bool mixed);
 // Ms = A_n^m M_n^m / R^n per cell, FP32 (mixed) or FP64.
 void scale_multipoles(const FmmArgs &a, bool mixed, void *Ms);
 // In mixed mode only pairs with target level >= min_level and |level difference|
-// <= max_dl are taken (the generic FP64 kernel handles the rest).
+// <= max_dl are taken (FP64 takes the rest, compacted by m2l_complement).
 // taken: pairs another kernel evaluates (skipped here), or null.
 bool m2l_fast(const FmmArgs &a, bool mixed, const void *Ms, int min_level = 0, int max_dl = 0,
               const unsigned char *taken = nullptr);
@@ -78,11 +78,14 @@ struct M2LGemmBufs {
   DBuf<float> Y;                      // per list entry: the pair's contribution (real dofs)
   DBuf<int> cnt;
   DBuf<int> left_cnt, left_off, left_src;
+  DBuf<int> comp_cnt, comp_off, comp_src;  // pairs outside the mixed policy (FP64), per target
   bool force = false;         // use the class products whatever the size (parity tests)
   bool tensor_cores = true;   // tcgen05 bf16x3 products, else FP32 on the CUDA cores
 };
 bool m2l_gemm_supported(int P);
 bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int min_level, int max_dl);
+// The pairs outside the mixed policy compacted into g.comp_off / g.comp_src (CSR by target, list order).
+long long m2l_complement(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int min_level, int max_dl);
 
 // Periodic lattice of root images (traversePeriodic), FP64, into L of the root.
 // scratch holds lattice_scratch_terms(P) complex values.

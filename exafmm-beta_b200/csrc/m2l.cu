@@ -146,6 +146,7 @@ k_m2l_part(M2LCtx g, DevTables t, double2 *L) {
         if (g.mode == 1 && !mixed_regular(g, lt, ls)) live = false;
         if (g.taken && g.taken[q]) live = false;
       }
+      if (!__any_sync(0xffffffffu, live)) continue;  // warp-uniform: a batch with nothing to add
       T x = T(1), y = T(0), z = T(0);
       if (live) {
         const double4 Xs = g.cell_x[cj];

@@ -320,6 +320,51 @@ __global__ void k_left_fill(const int *off, const int *src, long long ncells, co
   }
 }
 
+// The pairs outside the mixed policy (root levels, large size ratios), which
+// stay FP64: counted per target, then compacted in list order.
+__global__ void k_complement_count(const int *off, const int *src, long long ncells, const int2 *cell_pl,
+                                   int min_level, int max_dl, int *cnt) {
+  const int lane = threadIdx.x & 31;
+  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long c = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < ncells; c += warps) {
+    const int b = off[c], e = off[c + 1];
+    const int lt = cell_pl[c].y;
+    int k = 0;
+    if (lt < min_level) {
+      k = e - b;  // every pair of a root-level target
+    } else {
+      for (int q = b + lane; q < e; q += 32)
+        if (!policy_pair(lt, cell_pl[src[q] & 0x3ffffff].y, min_level, max_dl)) k++;
+      for (int o = 16; o > 0; o >>= 1) k += __shfl_xor_sync(0xffffffffu, k, o);
+    }
+    if (lane == 0) cnt[c] = k;
+  }
+}
+
+__global__ void k_complement_fill(const int *off, const int *src, long long ncells, const int2 *cell_pl,
+                                  int min_level, int max_dl, const int *off2, int *src2) {
+  const int lane = threadIdx.x & 31;
+  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long c = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < ncells; c += warps) {
+    const int b = off[c], e = off[c + 1];
+    const int lt = cell_pl[c].y;
+    int at = off2[c];
+    if (off2[c + 1] == at) continue;
+    for (int base = b; base < e; base += 32) {
+      const int q = base + lane;
+      bool keep = false;
+      int v = 0;
+      if (q < e) {
+        v = src[q];
+        keep = lt < min_level || !policy_pair(lt, cell_pl[v & 0x3ffffff].y, min_level, max_dl);
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, keep);
+      if (keep) src2[at + __popc(m & ((1u << lane) - 1u))] = v;
+      at += __popc(m);
+    }
+  }
+}
+
 // 5. Class ranges in the class-sorted pairs, and chunks of kChunk pairs.
 constexpr int kChunk = 128;
 
@@ -889,6 +934,23 @@ bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int
     default: return false;
   }
   return true;
+}
+
+long long m2l_complement(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int min_level, int max_dl) {
+  const long long nc = a.ncells;
+  cudaStream_t st = a.stream;
+  g.comp_cnt.ensure(nc);
+  g.comp_off.ensure(nc + 1);
+  g.comp_src.ensure(n_m2l > 0 ? n_m2l : 1);
+  const int grid = (int)std::max<long long>(1, std::min<long long>(kNumSMs * 8, (nc + 7) / 8));
+  k_complement_count<<<grid, 256, 0, st>>>(a.m2l_off, a.m2l_src, nc, a.cell_pl, min_level, max_dl, g.comp_cnt.p);
+  EXA_CHECK_LAUNCH();
+  LeftScan ls{g.comp_cnt.p, g.comp_off.p, nc};
+  launch_scan<256, 8>(ls, nullptr, nc, nc, C.scan, C.err.p, st);
+  k_complement_fill<<<grid, 256, 0, st>>>(a.m2l_off, a.m2l_src, nc, a.cell_pl, min_level, max_dl, g.comp_off.p,
+                                          g.comp_src.p);
+  EXA_CHECK_LAUNCH();
+  return nc;
 }
 
 }  // namespace exafmm_b200
