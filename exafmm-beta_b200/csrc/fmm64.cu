@@ -86,6 +86,20 @@ __global__ void k_p2m(DevTables t, const int4 *cell_b, const double4 *cell_x, co
   }
 }
 
+// acc + sum over terms [b, e) of src[a] * (Y[b] * w), conjugations per flag (DevTables::m2m_ops).
+__device__ __forceinline__ double2 trans_sum(const TransOp *ops, int b, int e, const double2 *src, const double2 *Y,
+                                             double2 a) {
+  for (int i = b; i < e; i++) {
+    const TransOp op = ops[i];
+    double2 s = src[op.a & 0xffff];
+    if (op.a >> 16) s.y = -s.y;
+    double2 z = Y[op.b & 0xffff];
+    if (op.b >> 16) z.y = -z.y;
+    a = cfma(s, cscale(z, op.w), a);
+  }
+  return a;
+}
+
 // ---------------------------------------------------------------- M2M
 // One child's contribution to the lane's parent coefficients (laplace.h:254-290):
 // Y = regular harmonics of X_parent - X_child, Mc = the child's multipole.
@@ -96,25 +110,7 @@ __device__ __forceinline__ void m2m_accumulate(const DevTables &t, const int (&o
   for (int u = 0; u < MAXO; u++) {
     const int j = oj[u], k = ok[u];
     if (j < 0) continue;
-    double2 a = acc[u];
-    const double ajk = t.anm[tri(j) + k];
-    for (int n = 0; n <= j; n++) {
-      for (int m = -n; m <= n; m++) {
-        const int km = k - m;
-        if (km > j - n || -km > j - n) continue;
-        const double w = t.anm[tri(n) + (m < 0 ? -m : m)] * t.anm[tri(j - n) + (km < 0 ? -km : km)] / ajk;
-        const double2 Z = m >= 0 ? Y[tri(n) + m] : cconj(Y[tri(n) - m]);
-        if (m < k) {
-          const double ph = (m < 0 && (m & 1)) ? -1.0 : 1.0;
-          const double2 src = Mc[tri(j - n) + km];
-          a = cfma(src, cscale(Z, ph * sgn_pow(n) * w), a);
-        } else {
-          const double2 src = cconj(Mc[tri(j - n) - km]);
-          a = cfma(src, cscale(Z, sgn_pow(k + n + m) * w), a);
-        }
-      }
-    }
-    acc[u] = a;
+    acc[u] = trans_sum(t.m2m_ops, t.m2m_start[tri(j) + k], t.m2m_start[tri(j) + k + 1], Mc, Y, acc[u]);
   }
 }
 
@@ -273,23 +269,8 @@ __global__ void k_l2l(DevTables t, const long long *lvl, int level, const int *n
     for (int u = 0; u < MAXO; u++) {
       const int j = oj[u], k = ok[u];
       if (j < 0) continue;
-      double2 a = make_double2(0.0, 0.0);
-      const double ajk = t.anm[tri(j) + k];
-      for (int n = j; n < P; n++) {
-        for (int m = -n; m <= n; m++) {
-          const int mk = m - k;
-          if (mk > n - j || -mk > n - j) continue;
-          const double w = t.anm[tri(n - j) + (mk < 0 ? -mk : mk)] * ajk / t.anm[tri(n) + (m < 0 ? -m : m)];
-          const double2 Yv = mk >= 0 ? Y[tri(n - j) + mk] : cconj(Y[tri(n - j) - mk]);
-          if (m < 0) {
-            a = cfma(cconj(Lp[tri(n) - m]), cscale(Yv, sgn_pow(k) * w), a);
-          } else {
-            const double ph = (mk < 0 && (mk & 1)) ? -1.0 : 1.0;
-            a = cfma(Lp[tri(n) + m], cscale(Yv, ph * w), a);
-          }
-        }
-      }
       const int o = tri(j) + k;
+      const double2 a = trans_sum(t.l2l_ops, t.l2l_start[o], t.l2l_start[o + 1], Lp, Y, make_double2(0.0, 0.0));
       double2 *dst = &L[(long long)c * NT + o];
       *dst = cadd(*dst, a);
     }

@@ -19,6 +19,12 @@
 namespace exafmm_b200 {
 
 // Device-side tables for one expansion order P (all FP64, n < 2P).
+struct TransOp {
+  double w;
+  int a;  // source coefficient index | conj << 16
+  int b;  // harmonic index | conj << 16
+};
+
 struct DevTables {
   int P;
   int nterm;            // P(P+1)/2
@@ -27,6 +33,14 @@ struct DevTables {
   const double *ra;     // a_n^m, index n*(n+1)/2+m
   const double *rb;     // b_n^m
   const double *rd;     // sqrt((2m-1)/(2m)), rd[0] = 1
+  // Translation terms of M2M and L2L (laplace.h:254-290, 324-357) per output
+  // coefficient o = tri(j) + k: terms [m2m_start[o], m2m_start[o + 1]) of
+  // m2m_ops, each acc += src[a] * (Y[b] * w) with src or Y conjugated where
+  // the flag in bit 16 of a or b is set; the sign and phase of the term are in w.
+  const TransOp *m2m_ops;
+  const int *m2m_start;
+  const TransOp *l2l_ops;
+  const int *l2l_start;
 };
 
 // Host construction (tables.cu).

@@ -53,9 +53,69 @@ const DevTables &device_tables(int P) {
     g_allocs.push_back(p);
     return (const double *)p;
   };
+  // M2M and L2L term lists, in the order the terms are summed (n, then m)
+  auto aidx = [&](int n, int m) { return tri(n) + (m < 0 ? -m : m); };
+  std::vector<TransOp> m2m, l2l;
+  std::vector<int> m2m_start, l2l_start;
+  for (int j = 0; j < P; j++) {
+    for (int k = 0; k <= j; k++) {
+      m2m_start.push_back((int)m2m.size());
+      const double ajk = anm[tri(j) + k];
+      for (int n = 0; n <= j; n++) {
+        for (int m = -n; m <= n; m++) {
+          const int km = k - m;
+          if (km > j - n || -km > j - n) continue;
+          const double w = anm[aidx(n, m)] * anm[aidx(j - n, km)] / ajk;
+          TransOp op;
+          op.b = aidx(n, m) | ((m < 0 ? 1 : 0) << 16);
+          if (m < k) {
+            const double ph = (m < 0 && (m & 1)) ? -1.0 : 1.0;
+            op.a = tri(j - n) + km;
+            op.w = ph * ((n & 1) ? -1.0 : 1.0) * w;
+          } else {
+            op.a = (tri(j - n) - km) | (1 << 16);
+            op.w = (((k + n + m) & 1) ? -1.0 : 1.0) * w;
+          }
+          m2m.push_back(op);
+        }
+      }
+      l2l_start.push_back((int)l2l.size());
+      for (int n = j; n < P; n++) {
+        for (int m = -n; m <= n; m++) {
+          const int mk = m - k;
+          if (mk > n - j || -mk > n - j) continue;
+          const double w = anm[aidx(n - j, mk)] * ajk / anm[aidx(n, m)];
+          TransOp op;
+          op.b = aidx(n - j, mk) | ((mk < 0 ? 1 : 0) << 16);
+          if (m < 0) {
+            op.a = (tri(n) - m) | (1 << 16);
+            op.w = ((k & 1) ? -1.0 : 1.0) * w;
+          } else {
+            const double ph = (mk < 0 && (mk & 1)) ? -1.0 : 1.0;
+            op.a = tri(n) + m;
+            op.w = ph * w;
+          }
+          l2l.push_back(op);
+        }
+      }
+    }
+  }
+  m2m_start.push_back((int)m2m.size());
+  l2l_start.push_back((int)l2l.size());
+  auto upload_raw = [&](const void *src, size_t bytes) {
+    void *p = nullptr;
+    EXA_CUDA(cudaMalloc(&p, bytes ? bytes : 1));
+    if (bytes) EXA_CUDA(cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice));
+    g_allocs.push_back(p);
+    return p;
+  };
   DevTables t;
   t.P = P;
   t.nterm = tri(P);
+  t.m2m_ops = (const TransOp *)upload_raw(m2m.data(), m2m.size() * sizeof(TransOp));
+  t.m2m_start = (const int *)upload_raw(m2m_start.data(), m2m_start.size() * sizeof(int));
+  t.l2l_ops = (const TransOp *)upload_raw(l2l.data(), l2l.size() * sizeof(TransOp));
+  t.l2l_start = (const int *)upload_raw(l2l_start.data(), l2l_start.size() * sizeof(int));
   t.anm = upload(anm);
   t.ainv = upload(ainv);
   t.ra = upload(ra);
