@@ -81,11 +81,26 @@ struct PairScan {
     else v.a = (unsigned long long)bi.w * bj.w;
     return v;
   }
-  __device__ void emit(long long i, const T &, const T &excl) const {
+  __device__ void emit(long long i, const T &v, const T &excl) const {
     if (i >= q_cap || stopped()) return;
     const int2 pr = qin[i];
-    int4 bi, bj;
-    const int mode = decide(c, pr, bi, bj);
+    // value() decided this pair: M2L and P2P show in v.b; a split needs the
+    // child ranges again and, in the last rule of decide(), the radii
+    int4 bi = make_int4(0, 0, 0, 0), bj = make_int4(0, 0, 0, 0);
+    int mode;
+    if (v.b >> 32) {
+      mode = kM2L;
+    } else if (v.b) {
+      mode = kP2P;
+    } else {
+      const int ci = pr.x, cj = pr.y & kCellMask;
+      bi = c.cell_b[ci];
+      bj = c.cell_bj[cj];
+      if (bj.w == 0) mode = kSplitI;
+      else if (bi.w == 0) mode = kSplitJ;
+      else if (bi.y + bj.y >= c.nspawn || (c.same && ci == cj)) mode = kSplitBoth;
+      else mode = (c.cell_x[ci].w >= c.cell_xj[cj].w) ? kSplitI : kSplitJ;
+    }
     const int img = pr.y & ~kCellMask;
     if (mode == kM2L) {
       const long long at = cnt[3 * sweep + 1] + (long long)(excl.b >> 32);

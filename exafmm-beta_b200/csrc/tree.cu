@@ -40,38 +40,9 @@ __global__ void k_bounds_init(unsigned long long *enc) {
   else if (t < 13) enc[t] = 0ull;                 // running maxima, max |x|
 }
 
-// Each body contributes g^(N-1-j)(X_j) to the min and the mirrored drift to the
-// max; body 0 also carries the initial value, which is drifted N times.
-__global__ void k_bounds(const double4 *x, long long n, unsigned long long *enc) {
-  unsigned long long lo[3] = {~0ull, ~0ull, ~0ull}, hi[3] = {0, 0, 0};
-  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
-    const double4 b = x[j];
-    const double v[3] = {b.x, b.y, b.z};
-    const long long k = (j == 0) ? n : n - 1 - j;
-    for (int d = 0; d < 3; d++) {
-      unsigned long long a = order_enc(drift_down(v[d], k));
-      unsigned long long c = order_enc(drift_up(v[d], k));
-      lo[d] = a < lo[d] ? a : lo[d];
-      hi[d] = c > hi[d] ? c : hi[d];
-    }
-  }
-  for (int d = 0; d < 3; d++) {
-    for (int o = 16; o > 0; o >>= 1) {
-      unsigned long long a = __shfl_xor_sync(0xffffffffu, lo[d], o);
-      unsigned long long c = __shfl_xor_sync(0xffffffffu, hi[d], o);
-      lo[d] = a < lo[d] ? a : lo[d];
-      hi[d] = c > hi[d] ? c : hi[d];
-    }
-  }
-  if ((threadIdx.x & 31) == 0) {
-    for (int d = 0; d < 3; d++) {
-      atomicMin(&enc[d], lo[d]);
-      atomicMax(&enc[3 + d], hi[d]);
-    }
-  }
-}
-
-// Two-pass form of k_bounds.  The unrounded estimate x_j -/+ k_j * 1e-5 is
+// BoundBox::getBounds in closed form: each body contributes g^(N-1-j)(X_j) to
+// the min and the mirrored drift to the max; body 0 also carries the initial
+// value, which is drifted N times.  Two passes: the unrounded estimate x_j -/+ k_j * 1e-5 is
 // within k * ulp(max|x| + N * 1e-5) of the exact drifted value, so only bodies
 // whose estimate lies within twice that of the extreme estimate can hold the
 // exact extreme; only those evaluate the closed form.
