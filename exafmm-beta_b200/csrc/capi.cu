@@ -332,7 +332,7 @@ struct Engine {
       if (mixed && C.prm.mixed_p2p) {
         x32.ensure(2 * C.tree.n);  // hi and lo float4 per body
         rel_bodies32(a, x32.p);
-        work.ensure(1);
+        work.ensure(2);  // work counters of the two P2P kernels
         p2p_mixed(a, x32.p, C.prm.images > 0, work.p);
       } else {
         p2p_fp64(a);

@@ -162,25 +162,26 @@ __device__ __forceinline__ void stage_dummy(Stage &sm, int k) {
   D[o] = 0.f;
 }
 
-constexpr int kTPL = 2;  // targets per lane
-
-// Targets of one lane: t[u] = packed (hx, hy, hz, lx, ly, lz), each value in both halves.
+// Targets of one lane (TPL of them): t[u] = packed (hx, hy, hz, lx, ly, lz), each value in both halves.
+template <int TPL>
 struct Targets {
-  f2p t[kTPL][6];
+  f2p t[TPL][6];
 };
 
+template <int TPL>
 struct Sums {
-  Kahan k[kTPL][4];  // potential, gradient x, y, z
+  Kahan k[TPL][4];  // potential, gradient x, y, z
 };
 
 // One pair step: two staged sources (pair p) against the lane's targets.
-__device__ __forceinline__ void pair_step(const Stage &sm, int p, const Targets &T, f2p (&pp)[kTPL],
-                                          f2p (&px)[kTPL], f2p (&py)[kTPL], f2p (&pz)[kTPL]) {
+template <int TPL>
+__device__ __forceinline__ void pair_step(const Stage &sm, int p, const Targets<TPL> &T, f2p (&pp)[TPL],
+                                          f2p (&px)[TPL], f2p (&py)[TPL], f2p (&pz)[TPL]) {
   const float4 A = sm.A[p], B = sm.B[p], C = sm.C[p], D = sm.D[p];
   const f2p shx = pk2(A.x, A.y), shy = pk2(A.z, A.w), shz = pk2(B.x, B.y), w = pk2(B.z, B.w);
   const f2p slx = pk2(C.x, C.y), sly = pk2(C.z, C.w), slz = pk2(D.x, D.y);
 #pragma unroll
-  for (int u = 0; u < kTPL; u++) {
+  for (int u = 0; u < TPL; u++) {
     const f2p dx = add2(sub2(T.t[u][0], shx), sub2(T.t[u][3], slx));
     const f2p dy = add2(sub2(T.t[u][1], shy), sub2(T.t[u][4], sly));
     const f2p dz = add2(sub2(T.t[u][2], shz), sub2(T.t[u][5], slz));
@@ -200,9 +201,9 @@ __device__ __forceinline__ void pair_step(const Stage &sm, int p, const Targets 
 
 // Streams the bodies of the P2P list entries [qb, qe) through the warp and
 // accumulates their action on the lane's targets into `acc`.
-template <int S, bool PERIODIC>
+template <int S, int TPL, bool PERIODIC>
 __device__ __forceinline__ void p2p_stream(Stage &sm, const int *src, const int4 *cell_b, const float4 *x32,
-                                           double cycle, int qb, int qe, const Targets &T, Sums &acc) {
+                                           double cycle, int qb, int qe, const Targets<TPL> &T, Sums<TPL> &acc) {
   constexpr int G = 32 / S, CH = 32 * G;
   const int lane = threadIdx.x & 31, g = lane / S;
   int q = qb, o = 0, qw = qb - 64;
@@ -245,16 +246,16 @@ __device__ __forceinline__ void p2p_stream(Stage &sm, const int *src, const int4
     __syncwarp();
 
     // ---- evaluate: group g takes pairs g, g + G, g + 2G, ... ----
-    f2p pp[kTPL], px[kTPL], py[kTPL], pz[kTPL];
+    f2p pp[TPL], px[TPL], py[TPL], pz[TPL];
 #pragma unroll
-    for (int u = 0; u < kTPL; u++) pp[u] = px[u] = py[u] = pz[u] = 0ull;
+    for (int u = 0; u < TPL; u++) pp[u] = px[u] = py[u] = pz[u] = 0ull;
     for (int s = 0; s < steps; s += 2) {
       pair_step(sm, g + G * s, T, pp, px, py, pz);
       pair_step(sm, g + G * (s + 1), T, pp, px, py, pz);
     }
     __syncwarp();
 #pragma unroll
-    for (int u = 0; u < kTPL; u++) {
+    for (int u = 0; u < TPL; u++) {
       const float2 a = unpk2(pp[u]), bx = unpk2(px[u]), by = unpk2(py[u]), bz = unpk2(pz[u]);
       acc.k[u][0].add(a.x + a.y);
       acc.k[u][1].add(bx.x + bx.y);
@@ -264,14 +265,14 @@ __device__ __forceinline__ void p2p_stream(Stage &sm, const int *src, const int4
   }
 }
 
-template <int S, bool PERIODIC>
+template <int S, int TPL, bool PERIODIC>
 __device__ __forceinline__ void p2p_leaf(Stage &sm, int4 cb, int b, int e, const int *src, const int4 *cell_b,
                                          const float4 *x32, double4 *trg, double cycle) {
   const int lane = threadIdx.x & 31, g = lane / S, j = lane % S;
-  for (int tb = 0; tb < cb.y; tb += S * kTPL) {
-    Targets T;
+  for (int tb = 0; tb < cb.y; tb += S * TPL) {
+    Targets<TPL> T;
 #pragma unroll
-    for (int u = 0; u < kTPL; u++) {
+    for (int u = 0; u < TPL; u++) {
       const int i = tb + j + S * u;
       float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h;
       if (i < cb.y) {
@@ -285,11 +286,11 @@ __device__ __forceinline__ void p2p_leaf(Stage &sm, int4 cb, int b, int e, const
       T.t[u][4] = pk2(l.y, l.y);
       T.t[u][5] = pk2(l.z, l.z);
     }
-    Sums acc;
-    p2p_stream<S, PERIODIC>(sm, src, cell_b, x32, cycle, b, e, T, acc);
+    Sums<TPL> acc;
+    p2p_stream<S, TPL, PERIODIC>(sm, src, cell_b, x32, cycle, b, e, T, acc);
     // combine the groups (lanes j, j + S, j + 2S, ... hold the same targets) in FP64
 #pragma unroll
-    for (int u = 0; u < kTPL; u++) {
+    for (int u = 0; u < TPL; u++) {
       double v[4];
 #pragma unroll
       for (int k = 0; k < 4; k++) v[k] = (double)acc.k[u][k].s - (double)acc.k[u][k].c;
@@ -310,11 +311,21 @@ __device__ __forceinline__ void p2p_leaf(Stage &sm, int4 cb, int b, int e, const
   }
 }
 
+// Target slots of a leaf: S lanes x TPL targets per lane.  Leaves of 9-12,
+// 17-24, 33-48 and 65-96 bodies fill three targets per lane (12, 24, 48, 96
+// slots) better than two (16, 32, 64, 128); the rest take two.  The two
+// kinds run as separate kernels, so the three-target code's registers do not
+// lower the occupancy of the two-target one.
+__device__ __forceinline__ bool three_per_lane(int n) {
+  return (n > 8 && n <= 12) || (n > 16 && n <= 24) || (n > 32 && n <= 48) || (n > 64 && n <= 96);
+}
+
 // Persistent one-warp blocks, as many as fit on the GPU; each takes target
 // cells in order from a counter until none is left, so leaves of very
-// different cost balance out without the launch of one block per cell.
-template <bool PERIODIC>
-__global__ void __launch_bounds__(32, 16)
+// different cost balance out without the launch of one block per cell.  Each
+// kernel evaluates the leaves of its kind and skips the others.
+template <bool PERIODIC, int TPL>
+__global__ void __launch_bounds__(32, TPL == 2 ? 16 : 12)
 k_p2p32(const int *off, const int *src, long long ncells, const int4 *cell_b, const float4 *x32, double4 *trg,
         double cycle, unsigned long long *next) {
   __shared__ Stage sm;
@@ -326,14 +337,15 @@ k_p2p32(const int *off, const int *src, long long ncells, const int4 *cell_b, co
     const int b = off[c], e = off[c + 1];
     if (b == e) continue;
     const int4 cb = cell_b[c];
-    if (cb.y <= 8)
-      p2p_leaf<4, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
-    else if (cb.y <= 16)
-      p2p_leaf<8, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
-    else if (cb.y <= 32)
-      p2p_leaf<16, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
+    if (three_per_lane(cb.y) != (TPL == 3)) continue;
+    if (cb.y <= 4 * TPL)
+      p2p_leaf<4, TPL, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
+    else if (cb.y <= 8 * TPL)
+      p2p_leaf<8, TPL, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
+    else if (cb.y <= 16 * TPL)
+      p2p_leaf<16, TPL, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
     else
-      p2p_leaf<32, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
+      p2p_leaf<32, TPL, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
     __syncwarp();  // the stage buffer is free before the next cell's first fill
   }
 }
@@ -350,13 +362,22 @@ void rel_bodies32(const FmmArgs &a, float4 *x32) {
 
 void p2p_mixed(const FmmArgs &a, const float4 *x32, bool periodic, unsigned long long *counter) {
   if (a.ncells <= 0) return;
-  EXA_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), a.stream));
-  const unsigned grid = (unsigned)std::min<long long>(a.ncells, (long long)kNumSMs * 16);
-  if (periodic)
-    k_p2p32<true><<<grid, 32, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b, x32, a.trg64, a.cycle, counter);
-  else
-    k_p2p32<false><<<grid, 32, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b, x32, a.trg64, a.cycle,
+  EXA_CUDA(cudaMemsetAsync(counter, 0, 2 * sizeof(unsigned long long), a.stream));
+  const unsigned g2 = (unsigned)std::min<long long>(a.ncells, (long long)kNumSMs * 16);
+  const unsigned g3 = (unsigned)std::min<long long>(a.ncells, (long long)kNumSMs * 12);
+  if (periodic) {
+    k_p2p32<true, 2><<<g2, 32, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b, x32, a.trg64, a.cycle,
                                               counter);
+    EXA_CHECK_LAUNCH();
+    k_p2p32<true, 3><<<g3, 32, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b, x32, a.trg64, a.cycle,
+                                              counter + 1);
+  } else {
+    k_p2p32<false, 2><<<g2, 32, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b, x32, a.trg64, a.cycle,
+                                               counter);
+    EXA_CHECK_LAUNCH();
+    k_p2p32<false, 3><<<g3, 32, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b, x32, a.trg64, a.cycle,
+                                               counter + 1);
+  }
   EXA_CHECK_LAUNCH();
 }
 
