@@ -884,7 +884,7 @@ bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int
   k_left_fill<<<kNumSMs * 8, 256, 0, st>>>(a.m2l_off, a.m2l_src, nc, g.taken.p, a.cell_pl, min_level, max_dl,
                                            g.left_off.p, g.left_src.p);
   EXA_CHECK_LAUNCH();
-  const int end_bit = std::min(32, (bits_for(ncls + 1) + 7) / 8 * 8);
+  const int end_bit = std::min(32, bits_for(ncls + 1));  // class ids; the untaken key 0xffffffff sorts last
   alt = radix_sort_u32(g.skey.p, g.pval.p, g.skey_alt.p, g.pval_alt.p, n_m2l, 0, end_bit, C.sort, C.err.p, st);
   const unsigned *sk = alt ? g.skey_alt.p : g.skey.p;
   const int *sv = alt ? g.pval_alt.p : g.pval.p;

@@ -182,9 +182,8 @@ void group_by_target(Context &C, const int2 *pairs, long long n, long long ncell
   if (n > 0) {
     k_split_pairs<<<kNumSMs * 8, 256, 0, st>>>(pairs, n, lb.key.p, lb.val.p);
     EXA_CHECK_LAUNCH();
-    int bits = bits_for(ncells);
-    int end = ((bits + 7) / 8) * 8;
-    bool alt = radix_sort_u32(lb.key.p, lb.val.p, lb.key_alt.p, lb.val_alt.p, n, 0, end, C.sort, C.err.p, st);
+    const int bits = bits_for(ncells);  // target cell ids
+    bool alt = radix_sort_u32(lb.key.p, lb.val.p, lb.key_alt.p, lb.val_alt.p, n, 0, bits, C.sort, C.err.p, st);
     unsigned *k = alt ? lb.key_alt.p : lb.key.p;
     int *v = alt ? lb.val_alt.p : lb.val.p;
     EXA_CUDA(cudaMemcpyAsync(src.p, v, n * sizeof(int), cudaMemcpyDeviceToDevice, st));
