@@ -1,5 +1,6 @@
 // Internal host-side interfaces of the engine (not part of the C ABI).
 #pragma once
+#include <algorithm>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -72,9 +73,11 @@ void launch_scan(const Producer &prod, const long long *n_dev, long long n_host,
   constexpr int TILE = BLOCK * ITEMS;
   long long tiles = (max_items + TILE - 1) / TILE + 1;
   ScanScratch s = w.prepare(st, err, tiles, sizeof(typename Producer::T));
-  // enough tiles for the most items the scan can see (the count on the device
-  // is at most max_items), so small scans do not occupy the whole GPU
-  int grid = kNumSMs * 4;
+  // as many blocks as an SM holds by threads (at most 16), so that tiles
+  // waiting on their look-back overlap with others' work; but no more than
+  // the most items the scan can see need (the count on the device is at most
+  // max_items), so small scans do not occupy the whole GPU
+  int grid = kNumSMs * std::min(16, 2048 / BLOCK);
   const long long bound = n_dev ? max_items : n_host;
   const long long need = (bound + TILE - 1) / TILE;
   if (need < grid) grid = need > 0 ? (int)need : 1;

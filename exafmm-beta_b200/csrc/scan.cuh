@@ -122,7 +122,7 @@ scan_kernel(Producer prod, const long long *n_ptr, long long n_const, ScanScratc
           unsigned f = flags[p];
           if ((f >> 2) != epoch || (f & 3u) == 0) {
             if (++spins > kSpinLimit) { atomicOr(s.error, 16); break; }
-            __nanosleep(64);
+            if (spins > 64) __nanosleep(64);  // short waits poll at full rate
             continue;
           }
           __threadfence();
