@@ -236,7 +236,7 @@ bool traverse(Context &C, ListBufs &lb, const TreeBufs *sources) {
     ps.sweep = s;
     ps.qin = (s & 1) ? lb.q1.p : lb.q0.p;
     ps.qout = (s & 1) ? lb.q0.p : lb.q1.p;
-    launch_scan<128, 4>(ps, lb.cnt.p + 3 * s, 0, lb.q_cap, C.scan, C.err.p, st);
+    launch_scan<256, 8>(ps, lb.cnt.p + 3 * s, 0, lb.q_cap, C.scan, C.err.p, st);  // 2048-pair tiles
   }
   long long cnt[3 * (kMaxSweeps + 1)];
   EXA_CUDA(cudaMemcpyAsync(cnt, lb.cnt.p, 3 * (nsw + 1) * sizeof(long long), cudaMemcpyDeviceToHost, st));
