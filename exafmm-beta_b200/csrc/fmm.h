@@ -81,6 +81,7 @@ struct M2LGemmBufs {
   DBuf<int> comp_cnt, comp_off, comp_src;  // pairs outside the mixed policy (FP64), per target
   bool force = false;         // use the class products whatever the size (parity tests)
   bool tensor_cores = true;   // tcgen05 bf16x3 products, else FP32 on the CUDA cores
+  bool tma = true;            // P = 8 on the tensor cores: source pieces gathered by TMA
 };
 bool m2l_gemm_supported(int P);
 bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int min_level, int max_dl);

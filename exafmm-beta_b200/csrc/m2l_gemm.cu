@@ -32,6 +32,7 @@
 // tcgen05.mma into an FP32 accumulator in tensor memory: the terms left out
 // weigh about 2^-24, FP32 rounding.  The CUDA-core one (k_m2l_class_gemm) is a
 // plain FP32 product.
+#include <cuda.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -166,7 +167,8 @@ __global__ void k_class_ids(const int *cs_sorted, int ncls, int *hid) {
 // 3. Operator of each class: FP32 k-major, Kt[class][input dof][output dof]
 // (CUDA-core engine), or three bf16 pieces of it per class, each an operand
 // image of NDP output rows x NDP inputs in the core_off layout (tensor cores).
-__global__ void k_build_K(DevTables t, const unsigned long long *ck, int P, float *Kt, unsigned short *Kb) {
+__global__ void k_build_K(DevTables t, const unsigned long long *ck, int P, float *Kt, unsigned short *Kb,
+                          bool swizzled) {
   extern __shared__ double2 S[];  // S'_p^q, q >= 0, at d / R_t
   const int NT = t.nterm, ND = nd_of(P), NDP = ndp_of(P);
   const unsigned long long key = ck[blockIdx.x];
@@ -179,8 +181,11 @@ __global__ void k_build_K(DevTables t, const unsigned long long *ck, int P, floa
     singular_column(t, threadIdx.x, 2 * P - 1, ux * to_rt, uy * to_rt, uz * to_rt, t.ainv, S);
   __syncthreads();
   for (int e = threadIdx.x; e < NDP * NDP; e += blockDim.x) {
-    int c, r;  // input and output dof; with Kb, e walks the core_off layout so the stores are contiguous
-    if (Kb) {
+    int c, r;  // input and output dof; with Kb, e walks the operand image so the stores are contiguous
+    if (Kb && swizzled) {  // 128-byte-swizzled image (NDP = 64): row r, 16-byte chunk (c / 8) ^ (r % 8)
+      r = e >> 6;
+      c = ((((e >> 3) & 7) ^ (r & 7)) << 3) | (e & 7);
+    } else if (Kb) {
       const int ci = e >> 6, w = e & 63;
       r = (ci / (NDP >> 3)) * 8 + (w >> 3);
       c = (ci % (NDP >> 3)) * 8 + (w & 7);
@@ -221,7 +226,7 @@ __global__ void k_build_K(DevTables t, const unsigned long long *ck, int P, floa
     if (Kb) {
       unsigned short h[3];
       split_bf16x3(val, h);
-      unsigned short *dst = Kb + (long long)blockIdx.x * 3 * NDP * NDP + e;  // e == core_off(r, c, NDP)
+      unsigned short *dst = Kb + (long long)blockIdx.x * 3 * NDP * NDP + e;  // e == the operand offset of (r, c)
 #pragma unroll
       for (int p = 0; p < 3; p++) dst[p * NDP * NDP] = h[p];
     }
@@ -746,6 +751,185 @@ k_m2l_class_mma(const int4 *chunks, const int *nchunks, const int *sval, const i
   }
 }
 
+// ---- the P = 8 products with the source pieces gathered by TMA
+// The operands in the canonical 128-byte-swizzle K-major layout: NDP = 64
+// inputs per row = 128 bytes, row r at r * 128, its 16-byte chunk c stored at
+// chunk position c ^ (r % 8), 8-row atoms of 1024 bytes (1024-byte aligned).
+// TMA writes the source rows in this layout itself (tensor map swizzle 128B);
+// the operator image is written so by k_build_K: entry (row, k) at bf16 offset
+// row * 64 + (((k / 8) ^ (row % 8)) * 8) + k % 8.
+
+// Shared-memory matrix descriptor of a K-major, 128-byte-swizzled operand:
+// start address, stride byte offset 1024 (8-row atoms), leading byte offset
+// unused (1), version 1, layout SWIZZLE_128B (2 at bit 61).
+__device__ __forceinline__ unsigned long long umma_desc_sw128(unsigned addr) {
+  return (unsigned long long)((addr >> 4) & 0x3fffu) | (1ull << 16) | ((unsigned long long)(1024 >> 4) << 32) |
+         (1ull << 46) | (2ull << 61);
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// Four source rows (cells y0..y3, 64 bf16 from column x) into 4 x 128 bytes at dst.
+__device__ __forceinline__ void tma_gather4(unsigned dst, const CUtensorMap *map, unsigned bar, int x, int y0, int y1,
+                                            int y2, int y3) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5, %6, %7}], [%2];" ::"r"(dst),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(bar), "r"(x), "r"(y0), "r"(y1), "r"(y2), "r"(y3)
+      : "memory");
+}
+
+constexpr size_t kTmaSmem = 3 * (kChunk + 64) * 64 * 2 + 1024;  // A and B pieces, plus alignment slack
+
+// As k_m2l_class_mma<64>, with the chunk's source pieces (3 x 128 rows x
+// 128 bytes) brought in by 96 tile::gather4 loads (three per lane of warp 0)
+// completing on an mbarrier, instead of 3,072 cp.async of all threads.
+__global__ void __launch_bounds__(128)
+k_m2l_class_mma_tma(const __grid_constant__ CUtensorMap msb_map, const int4 *chunks, const int *nchunks,
+                    const int *sval, const int *ssrc, const unsigned short *Kb, float *Y, int *err) {
+  constexpr int NDP = 64;
+  constexpr int A_ELEMS = kChunk * NDP, B_ELEMS = NDP * NDP;
+  constexpr int NCOLS = mma_cols(NDP);
+  constexpr unsigned D1 = NCOLS / 2;
+  constexpr unsigned IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(NDP >> 3) << 17) |
+                             ((unsigned)(kChunk >> 4) << 24);
+  constexpr unsigned A_BYTES = 3 * A_ELEMS * 2;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned short *sA = reinterpret_cast<unsigned short *>(
+      (reinterpret_cast<unsigned long long>(smem_raw) + 1023) & ~1023ull);
+  unsigned short *sB = sA + 3 * A_ELEMS;
+  __shared__ int s_src[kChunk];
+  __shared__ __align__(8) unsigned long long s_bar, s_tbar;
+  __shared__ unsigned s_tmem;
+  const int total = *nchunks;
+  const int j0 = (int)((long long)total * blockIdx.x / gridDim.x);
+  const int j1 = (int)((long long)total * (blockIdx.x + 1) / gridDim.x);
+  if (j0 >= j1) return;
+  const unsigned bar = smem_u32(&s_bar), tbar = smem_u32(&s_tbar);
+  if (threadIdx.x < 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                 "r"(NCOLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tbar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  int4 ch = chunks[j0];
+  int q = (int)threadIdx.x < ch.z ? sval[ch.y + threadIdx.x] : -1;
+  s_src[threadIdx.x] = q >= 0 ? ssrc[ch.y + threadIdx.x] : -1;
+  int cur_cls = -1;
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const unsigned tmem = s_tmem;
+  const unsigned a0 = smem_u32(sA), b0 = smem_u32(sB);
+  // one chunk's loads: the operator pieces if the class changed (cp.async, all
+  // threads), the source pieces by TMA (thread 0); rows past the chunk repeat
+  // its first source (their products are not stored)
+  auto issue_loads = [&](int cls, int cnt) {
+    if (cls != cur_cls) {
+      const unsigned short *Kg = Kb + (long long)cls * 3 * B_ELEMS;
+      for (int i = threadIdx.x; i < 3 * B_ELEMS / 8; i += 128) cp_async16(sB + 8 * i, Kg + 8 * i);
+      cur_cls = cls;
+    }
+    cp_async_commit();
+    if (threadIdx.x < 32) {  // warp 0: lane g issues row group g of the three pieces
+      if (threadIdx.x == 0) mbar_expect_tx(tbar, A_BYTES);
+      __syncwarp();
+      const int g = threadIdx.x, f = s_src[0];
+      int y[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) y[u] = 4 * g + u < cnt ? s_src[4 * g + u] : f;
+#pragma unroll
+      for (int p = 0; p < 3; p++)
+        tma_gather4(a0 + (unsigned)(p * A_ELEMS * 2 + g * 512), &msb_map, tbar, p * NDP, y[0], y[1], y[2], y[3]);
+    }
+  };
+  issue_loads(ch.x, ch.z);
+  bool ok = true;
+  for (int j = j0; j < j1; j++) {
+    const int cnt = ch.z, qc = q, it = j - j0;
+    // this chunk's tiles: the source pieces (TMA) and the operator (cp.async)
+    bool got = true;
+    if ((threadIdx.x & 31) == 0) got = mbar_wait_bounded(tbar, (unsigned)(it & 1));
+    got = __shfl_sync(0xffffffffu, got, 0);
+    cp_async_wait_all();
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    if (!__syncthreads_and(got)) {
+      ok = false;
+      break;
+    }
+    tc_fence_after();
+    if (threadIdx.x == 0) {
+      const int pa[6] = {0, 0, 2, 1, 0, 1}, pb[6] = {0, 2, 0, 1, 1, 0};
+#pragma unroll
+      for (int t = 0; t < 6; t++)
+#pragma unroll
+        for (int k = 0; k < NDP / 16; k++) {  // 16 inputs = 32 bytes along the swizzled rows
+          const unsigned long long da = umma_desc_sw128(a0 + (unsigned)(pa[t] * A_ELEMS * 2 + k * 32));
+          const unsigned long long db = umma_desc_sw128(b0 + (unsigned)(pb[t] * B_ELEMS * 2 + k * 32));
+          umma_bf16(tmem + (t == 0 ? 0u : D1), da, db, IDESC, (t > 1 || k > 0) ? 1u : 0u);
+        }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                   : "memory");
+    }
+    int sc = -1;
+    if (j + 1 < j1) {
+      ch = chunks[j + 1];
+      q = (int)threadIdx.x < ch.z ? sval[ch.y + threadIdx.x] : -1;
+      sc = q >= 0 ? ssrc[ch.y + threadIdx.x] : -1;
+    }
+    bool done = true;
+    if ((threadIdx.x & 31) == 0) done = mbar_wait_bounded(bar, (unsigned)(it & 1));
+    done = __shfl_sync(0xffffffffu, done, 0);
+    tc_fence_after();
+    if (!__syncthreads_and(done)) {  // products done: the tiles and s_src are free
+      ok = false;
+      break;
+    }
+    if (j + 1 < j1) {
+      s_src[threadIdx.x] = sc;
+      __syncthreads();
+      issue_loads(ch.x, ch.z);
+    }
+    {  // chunk j's accumulators -> Y, while the next loads are in flight
+      const int warp = threadIdx.x >> 5;
+      const unsigned taddr = tmem + ((unsigned)(warp * 32) << 16);
+      float *yrow = (int)threadIdx.x < cnt ? Y + (long long)qc * NDP : nullptr;
+#pragma unroll
+      for (int c0 = 0; c0 < NDP; c0 += 16) {
+        unsigned r[16], v[16];
+        tmem_ld16(taddr + (unsigned)c0, r);
+        tmem_ld16(taddr + D1 + (unsigned)c0, v);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (yrow) {
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            float o[8];
+#pragma unroll
+            for (int e = 0; e < 8; e++) o[e] = __uint_as_float(r[8 * h + e]) + __uint_as_float(v[8 * h + e]);
+            st_global_v8(yrow + c0 + 8 * h, o);
+          }
+        }
+      }
+    }
+  }
+  if (!ok && (threadIdx.x & 31) == 0) atomicOr(err, kErrMmaTimeout);
+  cp_async_wait_all();
+  tc_fence_before();
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOLS) : "memory");
+  }
+}
+
 // 7. Per target: its taken pairs' contributions summed in list order in FP64,
 // scaled by (-1)^j A_j^k R_t^{-(j+1)}, added to L.
 template <int NDP>
@@ -795,6 +979,41 @@ int bits_for(long long v) {
 template <typename F>
 void set_smem(F f, size_t bytes) {
   if (bytes > 48 * 1024) EXA_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled from the driver (no link-time dependency on libcuda).
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+
+// The bf16 source pieces Msb[cell][3 x 64] as a 2-D tensor (192 x ncells,
+// rows 384 bytes apart), read in boxes of one row x 64 elements (128 bytes)
+// into the 128-byte-swizzled layout.
+bool msb_tensor_map(CUtensorMap *map, const unsigned short *Msb, long long ncells) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn || ncells <= 0 || ncells > 0x7fffffffLL) return false;
+  if ((reinterpret_cast<unsigned long long>(Msb) & 15ull) != 0) return false;
+  const cuuint64_t dims[2] = {3 * 64, (cuuint64_t)ncells};
+  const cuuint64_t strides[1] = {3 * 64 * sizeof(unsigned short)};
+  const cuuint32_t box[2] = {64, 1};
+  const cuuint32_t estr[2] = {1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void *)Msb, dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 }  // namespace
@@ -855,15 +1074,19 @@ bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int
   k_class_ids<<<(ncls + 255) / 256, 256, 0, st>>>(cs, ncls, g.hid.p);
   EXA_CHECK_LAUNCH();
   const bool tc = g.tensor_cores;
+  // P = 8 on the tensor cores: source pieces gathered by TMA (its tensor map made below)
+  CUtensorMap msb_map;
+  bool use_tma = tc && NDP == 64 && g.tma && encode_tiled() != nullptr;
   if (tc) g.Kb.ensure((long long)ncls * 3 * NDP * NDP);
   else g.K.ensure((long long)ncls * NDP * NDP);
   {
     const size_t smem = tri(2 * P - 1) * sizeof(double2);
-    k_build_K<<<ncls, 256, smem, st>>>(t, ck, P, tc ? nullptr : g.K.p, tc ? g.Kb.p : nullptr);
+    k_build_K<<<ncls, 256, smem, st>>>(t, ck, P, tc ? nullptr : g.K.p, tc ? g.Kb.p : nullptr, use_tma);
     EXA_CHECK_LAUNCH();
   }
   if (tc) g.Msb.ensure(nc * 3 * NDP);
   else g.Msr.ensure(nc * NDP);
+  if (use_tma && !msb_tensor_map(&msb_map, g.Msb.p, nc)) throw std::runtime_error("TMA tensor map of the multipoles");
   k_scale_M_real<<<kNumSMs * 8, 256, 0, st>>>(t, a.M64, a.cell_x, nc, P, tc ? nullptr : g.Msr.p,
                                               tc ? g.Msb.p : nullptr);
   EXA_CHECK_LAUNCH();
@@ -909,7 +1132,12 @@ bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int
   switch (NDP) {
 #define EXA_GEMM_CASE(N)                                                                                      \
   case N: {                                                                                                   \
-    if (tc) {                                                                                                 \
+    if (use_tma) {                                                                                            \
+      set_smem(k_m2l_class_mma_tma, kTmaSmem);                                                                \
+      const long long grid = std::min<long long>(chunks_max, (long long)kNumSMs * 3);                         \
+      k_m2l_class_mma_tma<<<(unsigned)grid, 128, kTmaSmem, st>>>(msb_map, g.chunks.p, g.cbase.p + ncls, sv,  \
+                                                                 g.ssrc.p, g.Kb.p, g.Y.p, C.err.p);           \
+    } else if (tc) {                                                                                          \
       const size_t smem = mma_smem_bytes(N);                                                                  \
       set_smem(k_m2l_class_mma<N>, smem);                                                                     \
       const long long grid = std::min<long long>(chunks_max, (long long)kNumSMs * mma_ctas_per_sm(N));        \
