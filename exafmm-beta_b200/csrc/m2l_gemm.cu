@@ -180,11 +180,14 @@ __global__ void k_build_K(DevTables t, const unsigned long long *ck, int P, floa
   if ((int)threadIdx.x < 2 * P - 1)
     singular_column(t, threadIdx.x, 2 * P - 1, ux * to_rt, uy * to_rt, uz * to_rt, t.ainv, S);
   __syncthreads();
-  for (int e = threadIdx.x; e < NDP * NDP; e += blockDim.x) {
+  const int KB = (NDP + 63) / 64;  // 128-byte K-blocks of the swizzled image
+  const int img = swizzled ? KB * NDP * 64 : NDP * NDP;
+  for (int e = threadIdx.x; e < img; e += blockDim.x) {
     int c, r;  // input and output dof; with Kb, e walks the operand image so the stores are contiguous
-    if (Kb && swizzled) {  // 128-byte-swizzled image (NDP = 64): row r, 16-byte chunk (c / 8) ^ (r % 8)
-      r = e >> 6;
-      c = ((((e >> 3) & 7) ^ (r & 7)) << 3) | (e & 7);
+    if (Kb && swizzled) {  // 128-byte-swizzled image: K-block c / 64, row r, 16-byte chunk ((c % 64) / 8) ^ (r % 8)
+      const int kb = e / (NDP * 64), w = e - kb * NDP * 64;
+      r = w >> 6;
+      c = kb * 64 + (((((w >> 3) & 7) ^ (r & 7))) << 3) + (w & 7);
     } else if (Kb) {
       const int ci = e >> 6, w = e & 63;
       r = (ci / (NDP >> 3)) * 8 + (w >> 3);
@@ -226,9 +229,9 @@ __global__ void k_build_K(DevTables t, const unsigned long long *ck, int P, floa
     if (Kb) {
       unsigned short h[3];
       split_bf16x3(val, h);
-      unsigned short *dst = Kb + (long long)blockIdx.x * 3 * NDP * NDP + e;  // e == the operand offset of (r, c)
+      unsigned short *dst = Kb + (long long)blockIdx.x * 3 * img + e;  // e == the operand offset of (r, c)
 #pragma unroll
-      for (int p = 0; p < 3; p++) dst[p * NDP * NDP] = h[p];
+      for (int p = 0; p < 3; p++) dst[p * img] = h[p];
     }
   }
 }
@@ -781,21 +784,31 @@ __device__ __forceinline__ void tma_gather4(unsigned dst, const CUtensorMap *map
       : "memory");
 }
 
-constexpr size_t kTmaSmem = 3 * (kChunk + 64) * 64 * 2 + 1024;  // A and B pieces, plus alignment slack
+// 128-byte K-blocks per operand row, and the kernel's shared memory (A and B
+// pieces in K-blocks, plus alignment slack).
+__host__ __device__ constexpr int tma_kblocks(int NDP) { return (NDP + 63) / 64; }
+__host__ __device__ constexpr size_t tma_smem_bytes(int NDP) {
+  return (size_t)3 * tma_kblocks(NDP) * (kChunk + NDP) * 128 + 1024;
+}
 
-// As k_m2l_class_mma<64>, with the chunk's source pieces (3 x 128 rows x
-// 128 bytes) brought in by 96 tile::gather4 loads (three per lane of warp 0)
-// completing on an mbarrier, instead of 3,072 cp.async of all threads.
+// As k_m2l_class_mma<NDP>, with the chunk's source pieces (3 x KB x 128 rows
+// x 128 bytes, KB = 1 at P = 8, 2 at P = 10) brought in by 96 KB
+// tile::gather4 loads (3 KB per lane of warp 0) completing on an mbarrier,
+// instead of cp.async of all threads.  At NDP = 112 the second K-block holds
+// inputs 64-127 of a row: past 112 it reads the next piece (or zeros past the
+// row's end), which no MMA step reaches (the last one ends at input 112).
+template <int NDP>
 __global__ void __launch_bounds__(128)
 k_m2l_class_mma_tma(const __grid_constant__ CUtensorMap msb_map, const int4 *chunks, const int *nchunks,
                     const int *sval, const int *ssrc, const unsigned short *Kb, float *Y, int *err) {
-  constexpr int NDP = 64;
-  constexpr int A_ELEMS = kChunk * NDP, B_ELEMS = NDP * NDP;
+  constexpr int KB = tma_kblocks(NDP);
+  constexpr int A_ELEMS = KB * kChunk * 64, B_ELEMS = KB * NDP * 64;  // one piece of each, in K-blocks
   constexpr int NCOLS = mma_cols(NDP);
   constexpr unsigned D1 = NCOLS / 2;
   constexpr unsigned IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(NDP >> 3) << 17) |
                              ((unsigned)(kChunk >> 4) << 24);
   constexpr unsigned A_BYTES = 3 * A_ELEMS * 2;
+  static_assert(NDP % 16 == 0 && NDP <= 128, "one or two 128-byte K-blocks");
   extern __shared__ unsigned char smem_raw[];
   unsigned short *sA = reinterpret_cast<unsigned short *>(
       (reinterpret_cast<unsigned long long>(smem_raw) + 1023) & ~1023ull);
@@ -838,7 +851,7 @@ k_m2l_class_mma_tma(const __grid_constant__ CUtensorMap msb_map, const int4 *chu
       cur_cls = cls;
     }
     cp_async_commit();
-    if (threadIdx.x < 32) {  // warp 0: lane g issues row group g of the three pieces
+    if (threadIdx.x < 32) {  // warp 0: lane g issues row group g of every piece and K-block
       if (threadIdx.x == 0) mbar_expect_tx(tbar, A_BYTES);
       __syncwarp();
       const int g = threadIdx.x, f = s_src[0];
@@ -847,7 +860,10 @@ k_m2l_class_mma_tma(const __grid_constant__ CUtensorMap msb_map, const int4 *chu
       for (int u = 0; u < 4; u++) y[u] = 4 * g + u < cnt ? s_src[4 * g + u] : f;
 #pragma unroll
       for (int p = 0; p < 3; p++)
-        tma_gather4(a0 + (unsigned)(p * A_ELEMS * 2 + g * 512), &msb_map, tbar, p * NDP, y[0], y[1], y[2], y[3]);
+#pragma unroll
+        for (int kb = 0; kb < KB; kb++)
+          tma_gather4(a0 + (unsigned)(p * A_ELEMS * 2 + kb * kChunk * 128 + g * 512), &msb_map, tbar,
+                      p * NDP + 64 * kb, y[0], y[1], y[2], y[3]);
     }
   };
   issue_loads(ch.x, ch.z);
@@ -871,9 +887,12 @@ k_m2l_class_mma_tma(const __grid_constant__ CUtensorMap msb_map, const int4 *chu
 #pragma unroll
       for (int t = 0; t < 6; t++)
 #pragma unroll
-        for (int k = 0; k < NDP / 16; k++) {  // 16 inputs = 32 bytes along the swizzled rows
-          const unsigned long long da = umma_desc_sw128(a0 + (unsigned)(pa[t] * A_ELEMS * 2 + k * 32));
-          const unsigned long long db = umma_desc_sw128(b0 + (unsigned)(pb[t] * B_ELEMS * 2 + k * 32));
+        for (int k = 0; k < NDP / 16; k++) {  // 16 inputs = 32 bytes along the swizzled rows of K-block k / 4
+          const int kb = k >> 2, kk = k & 3;
+          const unsigned long long da =
+              umma_desc_sw128(a0 + (unsigned)(pa[t] * A_ELEMS * 2 + kb * kChunk * 128 + kk * 32));
+          const unsigned long long db =
+              umma_desc_sw128(b0 + (unsigned)(pb[t] * B_ELEMS * 2 + kb * NDP * 128 + kk * 32));
           umma_bf16(tmem + (t == 0 ? 0u : D1), da, db, IDESC, (t > 1 || k > 0) ? 1u : 0u);
         }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
@@ -1000,20 +1019,33 @@ EncodeTiledFn encode_tiled() {
   return fn;
 }
 
-// The bf16 source pieces Msb[cell][3 x 64] as a 2-D tensor (192 x ncells,
-// rows 384 bytes apart), read in boxes of one row x 64 elements (128 bytes)
-// into the 128-byte-swizzled layout.
-bool msb_tensor_map(CUtensorMap *map, const unsigned short *Msb, long long ncells) {
+// The bf16 source pieces Msb[cell][3 x NDP] as a 2-D tensor (3 NDP x ncells),
+// read in boxes of one row x 64 elements (128 bytes) into the 128-byte-swizzled
+// layout.
+bool msb_tensor_map(CUtensorMap *map, const unsigned short *Msb, long long ncells, int NDP) {
   EncodeTiledFn fn = encode_tiled();
   if (!fn || ncells <= 0 || ncells > 0x7fffffffLL) return false;
   if ((reinterpret_cast<unsigned long long>(Msb) & 15ull) != 0) return false;
-  const cuuint64_t dims[2] = {3 * 64, (cuuint64_t)ncells};
-  const cuuint64_t strides[1] = {3 * 64 * sizeof(unsigned short)};
+  const cuuint64_t dims[2] = {(cuuint64_t)(3 * NDP), (cuuint64_t)ncells};
+  const cuuint64_t strides[1] = {(cuuint64_t)(3 * NDP * sizeof(unsigned short))};
   const cuuint32_t box[2] = {64, 1};
   const cuuint32_t estr[2] = {1, 1};
   return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void *)Msb, dims, strides, box, estr,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int NDP>
+void tma_launch(const CUtensorMap &map, M2LGemmBufs &g, const int *sv, long long chunks_max, int ncls, int *err,
+                cudaStream_t st) {
+  if constexpr (NDP == 64) {  // the two-K-block form (NDP = 112) measured slower than cp.async at P = 10
+    constexpr size_t smem = tma_smem_bytes(NDP);
+    set_smem(k_m2l_class_mma_tma<NDP>, smem);
+    const int per_sm = (int)(233472 / (smem + 640 + 1024));
+    const long long grid = std::min<long long>(chunks_max, (long long)kNumSMs * per_sm);
+    k_m2l_class_mma_tma<NDP><<<(unsigned)grid, 128, smem, st>>>(map, g.chunks.p, g.cbase.p + ncls, sv, g.ssrc.p,
+                                                                g.Kb.p, g.Y.p, err);
+  }
 }
 
 }  // namespace
@@ -1074,10 +1106,12 @@ bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int
   k_class_ids<<<(ncls + 255) / 256, 256, 0, st>>>(cs, ncls, g.hid.p);
   EXA_CHECK_LAUNCH();
   const bool tc = g.tensor_cores;
-  // P = 8 on the tensor cores: source pieces gathered by TMA (its tensor map made below)
+  // P = 8 on the tensor cores: source pieces gathered by TMA (its tensor map made below).
+  // At P = 10 (two 128-byte K-blocks, one CTA per SM either way) the cp.async
+  // form is a little faster (M2L 16.4 vs 16.8 ms on a 1M-charge periodic box).
   CUtensorMap msb_map;
   bool use_tma = tc && NDP == 64 && g.tma && encode_tiled() != nullptr;
-  if (tc) g.Kb.ensure((long long)ncls * 3 * NDP * NDP);
+  if (tc) g.Kb.ensure((long long)ncls * 3 * (use_tma ? tma_kblocks(NDP) * NDP * 64 : NDP * NDP));
   else g.K.ensure((long long)ncls * NDP * NDP);
   {
     const size_t smem = tri(2 * P - 1) * sizeof(double2);
@@ -1086,7 +1120,8 @@ bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int
   }
   if (tc) g.Msb.ensure(nc * 3 * NDP);
   else g.Msr.ensure(nc * NDP);
-  if (use_tma && !msb_tensor_map(&msb_map, g.Msb.p, nc)) throw std::runtime_error("TMA tensor map of the multipoles");
+  if (use_tma && !msb_tensor_map(&msb_map, g.Msb.p, nc, NDP))
+    throw std::runtime_error("TMA tensor map of the multipoles");
   k_scale_M_real<<<kNumSMs * 8, 256, 0, st>>>(t, a.M64, a.cell_x, nc, P, tc ? nullptr : g.Msr.p,
                                               tc ? g.Msb.p : nullptr);
   EXA_CHECK_LAUNCH();
@@ -1133,10 +1168,7 @@ bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int
 #define EXA_GEMM_CASE(N)                                                                                      \
   case N: {                                                                                                   \
     if (use_tma) {                                                                                            \
-      set_smem(k_m2l_class_mma_tma, kTmaSmem);                                                                \
-      const long long grid = std::min<long long>(chunks_max, (long long)kNumSMs * 3);                         \
-      k_m2l_class_mma_tma<<<(unsigned)grid, 128, kTmaSmem, st>>>(msb_map, g.chunks.p, g.cbase.p + ncls, sv,  \
-                                                                 g.ssrc.p, g.Kb.p, g.Y.p, C.err.p);           \
+      tma_launch<N>(msb_map, g, sv, chunks_max, ncls, C.err.p, st);                                           \
     } else if (tc) {                                                                                          \
       const size_t smem = mma_smem_bytes(N);                                                                  \
       set_smem(k_m2l_class_mma<N>, smem);                                                                     \
