@@ -964,13 +964,27 @@ __global__ void k_m2l_class_reduce(const int *off, long long ncells, const unsig
     bool any = false;
 #pragma unroll
     for (int u = 0; u < PER; u++) acc[u] = 0.0;
-    for (int q = b; q < e; q++) {
-      if (!taken[q]) continue;
-      any = true;
-      const float *y = Y + (long long)q * NDP;
+    // eight pairs' flags and columns loaded before they are added (in list order)
+    constexpr int G = 8;
+    for (int q0 = b; q0 < e; q0 += G) {
+      bool tk[G];
+      float v[G][PER];
 #pragma unroll
-      for (int u = 0; u < PER; u++)
-        if (lane + 32 * u < NDP) acc[u] += (double)y[lane + 32 * u];
+      for (int i = 0; i < G; i++) tk[i] = q0 + i < e && taken[q0 + i];
+#pragma unroll
+      for (int i = 0; i < G; i++) {
+        const float *y = Y + (long long)(q0 + i) * NDP;
+#pragma unroll
+        for (int u = 0; u < PER; u++) v[i][u] = (tk[i] && lane + 32 * u < NDP) ? y[lane + 32 * u] : 0.f;
+      }
+#pragma unroll
+      for (int i = 0; i < G; i++) {
+        if (!tk[i]) continue;
+        any = true;
+#pragma unroll
+        for (int u = 0; u < PER; u++)
+          if (lane + 32 * u < NDP) acc[u] += (double)v[i][u];
+      }
     }
     if (!any) continue;
     const double rt = cell_x[c].w;
