@@ -33,22 +33,52 @@ __device__ __forceinline__ void image_shift(int img, double cycle, double &sx, d
 
 // ---------------------------------------------------------------- P2M
 // M_n^m = sum_b q_b conj(Y_n^m(x_b - X_c)) (laplace.h:237-252); lanes take
-// bodies, every coefficient is reduced across the warp.
+// bodies.  The terms come out of the recurrence in (m, n) order; each lane
+// stages its body's terms for a window of 16 of them in shared memory, then
+// lane l adds component l / 16 of window term l % 16 over the bodies (four
+// running sums over the bodies mod 4, added pairwise): one load and one add a
+// body and double, where a shuffle tree costs five of each.  The cell's sums
+// are kept in that (m, n) order and written out at tri(n) + m.
+constexpr int kP2mWin = 16;
+constexpr int kP2mRow = kP2mWin + 1;  // odd stride in double2: lane rows hit distinct banks
+
+__device__ __forceinline__ void p2m_flush(const double2 *stage, double *acc, int lane, int cols, int rows) {
+  __syncwarp();
+  const int j = lane & (kP2mWin - 1);
+  if (j < cols) {
+    const double *col = reinterpret_cast<const double *>(stage) + 2 * j + (lane >> 4);
+    constexpr int RS = 2 * kP2mRow;
+    double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    int r = 0;
+    for (; r + 4 <= rows; r += 4) {
+      a0 += col[r * RS];
+      a1 += col[(r + 1) * RS];
+      a2 += col[(r + 2) * RS];
+      a3 += col[(r + 3) * RS];
+    }
+    for (; r < rows; r++) a0 += col[r * RS];
+    acc[2 * j + (lane >> 4)] += (a0 + a1) + (a2 + a3);
+  }
+  __syncwarp();
+}
+
 __global__ void k_p2m(DevTables t, const int4 *cell_b, const double4 *cell_x, const double4 *xt, double2 *M,
                       long long ncells) {
   extern __shared__ double2 sh[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int P = t.P, NT = t.nterm;
-  double2 *acc = sh + warp * NT;
+  double2 *acc = sh + warp * (NT + 32 * kP2mRow);  // (m, n) order
+  double2 *stage = acc + NT;
+  double2 *mine = stage + lane * kP2mRow;
+  double *accd = reinterpret_cast<double *>(acc);
   for (long long c = (long long)blockIdx.x * kWarpsPerBlock + warp; c < ncells;
        c += (long long)gridDim.x * kWarpsPerBlock) {
     const int4 cb = cell_b[c];
     if (cb.w != 0) continue;
     const double4 X = cell_x[c];
-    for (int o = lane; o < NT; o += 32) acc[o] = make_double2(0.0, 0.0);
-    __syncwarp();
+    for (int s = lane; s < NT; s += 32) acc[s] = make_double2(0.0, 0.0);
     for (int base = 0; base < cb.y; base += 32) {
-      const int i = base + lane;
+      const int i = base + lane, rows = min(32, cb.y - base);
       double x = 0, y = 0, z = 0, q = 0;
       if (i < cb.y) {
         const double4 b = xt[cb.x + i];
@@ -59,6 +89,7 @@ __global__ void k_p2m(DevTables t, const int4 *cell_b, const double4 *cell_x, co
       }
       const double r2 = x * x + y * y + z * z;
       double2 w = make_double2(q, 0.0);  // q * diagonal, with e^{-i m beta}
+      int k = 0, win = 0;
       for (int m = 0; m < P; m++) {
         if (m > 0) {
           const double f = -t.rd[m];
@@ -66,10 +97,11 @@ __global__ void k_p2m(DevTables t, const int4 *cell_b, const double4 *cell_x, co
         }
         double2 prev = make_double2(0.0, 0.0), cur = w;
         for (int n = m; n < P; n++) {
-          const double re = warp_sum(cur.x), im = warp_sum(cur.y);
-          if (lane == 0) {
-            acc[tri(n) + m].x += re;
-            acc[tri(n) + m].y += im;
+          mine[k] = cur;
+          if (++k == kP2mWin) {
+            p2m_flush(stage, accd + 2 * win, lane, kP2mWin, rows);
+            win += kP2mWin;
+            k = 0;
           }
           if (n + 1 < P) {
             const double a = t.ra[tri(n) + m], b = t.rb[tri(n) + m];
@@ -79,9 +111,17 @@ __global__ void k_p2m(DevTables t, const int4 *cell_b, const double4 *cell_x, co
           }
         }
       }
+      if (k) p2m_flush(stage, accd + 2 * win, lane, k, rows);
     }
     __syncwarp();
-    for (int o = lane; o < NT; o += 32) M[c * NT + o] = acc[o];
+    for (int s = lane; s < NT; s += 32) {
+      int m = 0, r = s;
+      while (r >= P - m) {
+        r -= P - m;
+        m++;
+      }
+      M[c * NT + tri(m + r) + m] = acc[s];
+    }
     __syncwarp();
   }
 }
@@ -318,18 +358,19 @@ __global__ void k_l2p(DevTables t, const int4 *cell_b, const double4 *cell_x, co
           const double2 Lnm = Lc[tri(n) + m];
           pot += wm * (Lnm.x * cur.x - Lnm.y * cur.y);
           if (n + 1 < P) {
+            const int o = tri(n) + m;
             const double2 L1 = Lc[tri(n + 1) + m];
-            gz += wm * sqrt((double)((n + 1) * (n + 1) - m * m)) * (L1.x * cur.x - L1.y * cur.y);
+            gz += t.l2p_gz[o] * (L1.x * cur.x - L1.y * cur.y);
             if (m + 1 <= n + 1) {
               const double2 L2 = Lc[tri(n + 1) + m + 1];
-              l11 = cfma(L2, cscale(cur, sqrt(0.5 * (double)((n + m + 2) * (n + m + 1)))), l11);
+              l11 = cfma(L2, cscale(cur, t.l2p_s1[o]), l11);
             }
             if (m == 1) {
               const double2 L0 = Lc[tri(n + 1)];
-              l11 = cfma(L0, cscale(cconj(cur), -sqrt(0.5 * (double)((n + 1) * n))), l11);
+              l11 = cfma(L0, cscale(cconj(cur), t.l2p_s2[o]), l11);
             } else if (m >= 2) {
               const double2 Lu = cconj(Lc[tri(n + 1) + m - 1]);
-              l11 = cfma(Lu, cscale(cconj(cur), -sqrt(0.5 * (double)((n + 2 - m) * (n + 1 - m)))), l11);
+              l11 = cfma(Lu, cscale(cconj(cur), t.l2p_s2[o]), l11);
             }
             const double a = t.ra[tri(n) + m], bb = t.rb[tri(n) + m];
             double2 nxt = make_double2(a * z * cur.x - bb * r2 * prev.x, a * z * cur.y - bb * r2 * prev.y);
@@ -612,7 +653,7 @@ void set_smem(F f, size_t bytes) {
 
 void p2m_fp64(const FmmArgs &a) {
   const DevTables &t = device_tables(a.P);
-  size_t smem = kWarpsPerBlock * t.nterm * sizeof(double2);
+  size_t smem = kWarpsPerBlock * (t.nterm + 32 * kP2mRow) * sizeof(double2);
   set_smem(k_p2m, smem);
   k_p2m<<<blocks_for(a.ncells), 32 * kWarpsPerBlock, smem, a.stream>>>(t, a.cell_b, a.cell_x, a.xt, a.M64, a.ncells);
   EXA_CHECK_LAUNCH();

@@ -41,6 +41,12 @@ struct DevTables {
   const int *m2m_start;
   const TransOp *l2l_ops;
   const int *l2l_start;
+  // L2P factors per (n, m), index tri(n) + m, n + 1 < P (laplace.h:359-388 as
+  // restated in k_l2p): w_m sqrt((n+1)^2 - m^2), sqrt((n+m+2)(n+m+1)/2), and
+  // -sqrt((n+1)n/2) (m = 1) or -sqrt((n+2-m)(n+1-m)/2) (m >= 2).
+  const double *l2p_gz;
+  const double *l2p_s1;
+  const double *l2p_s2;
 };
 
 // Host construction (tables.cu).

@@ -102,6 +102,17 @@ const DevTables &device_tables(int P) {
   }
   m2m_start.push_back((int)m2m.size());
   l2l_start.push_back((int)l2l.size());
+  std::vector<double> gz(tri(P) + 1, 0.0), s1(tri(P) + 1, 0.0), s2(tri(P) + 1, 0.0);
+  for (int n = 0; n + 1 < P; n++) {
+    for (int m = 0; m <= n; m++) {
+      const int o = tri(n) + m;
+      const double wm = (m == 0) ? 1.0 : 2.0;
+      gz[o] = wm * sqrt((double)((n + 1) * (n + 1) - m * m));
+      s1[o] = sqrt(0.5 * (double)((n + m + 2) * (n + m + 1)));
+      if (m == 1) s2[o] = -sqrt(0.5 * (double)((n + 1) * n));
+      else if (m >= 2) s2[o] = -sqrt(0.5 * (double)((n + 2 - m) * (n + 1 - m)));
+    }
+  }
   auto upload_raw = [&](const void *src, size_t bytes) {
     void *p = nullptr;
     EXA_CUDA(cudaMalloc(&p, bytes ? bytes : 1));
@@ -116,6 +127,9 @@ const DevTables &device_tables(int P) {
   t.m2m_start = (const int *)upload_raw(m2m_start.data(), m2m_start.size() * sizeof(int));
   t.l2l_ops = (const TransOp *)upload_raw(l2l.data(), l2l.size() * sizeof(TransOp));
   t.l2l_start = (const int *)upload_raw(l2l_start.data(), l2l_start.size() * sizeof(int));
+  t.l2p_gz = upload(gz);
+  t.l2p_s1 = upload(s1);
+  t.l2p_s2 = upload(s2);
   t.anm = upload(anm);
   t.ainv = upload(ainv);
   t.ra = upload(ra);
