@@ -23,6 +23,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libexafmm_b200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "exafmm_b200.h")
 MD_HEADER = os.path.join(os.path.dirname(HERE), "include", "exafmm_md.h")
+MDD_HEADER = os.path.join(os.path.dirname(HERE), "include", "exafmm_md_distributed.h")
+# The MD-code ABIs (wrappers/gromacs.cxx and wrappers/md_distributed.cxx shapes):
+# separate libraries over libexafmm_b200.so, since their FMM_* names overlap.
+MD_GROMACS_LIB_PATH = os.path.join(HERE, "libexafmm_md_gromacs.so")
+MD_DISTRIBUTED_LIB_PATH = os.path.join(HERE, "libexafmm_md_distributed.so")
 
 FP64 = 0
 MIXED = 1
@@ -42,13 +47,17 @@ def build(force: bool = False) -> str:
 
 
 def exported_symbols() -> list[str]:
-    """Every function declared in include/exafmm_b200.h and include/exafmm_md.h."""
+    """Every function declared in include/exafmm_b200.h (libexafmm_b200.so)."""
     import re
     text = open(HEADER).read()
-    names = set(re.findall(r"\b(exafmm_[a-z0-9_]+)\s*\(", text))
-    md = open(MD_HEADER).read()
-    names |= set(re.findall(r"^\s*(?:void|bool|int|const char \*)\s*([A-Za-z_]\w*)\s*\(", md, re.M))
-    return sorted(names)
+    return sorted(set(re.findall(r"\b(exafmm_[a-z0-9_]+)\s*\(", text)))
+
+
+def md_exported_symbols(header: str) -> list[str]:
+    """Every function an MD-code ABI header (MD_HEADER or MDD_HEADER) declares."""
+    import re
+    text = open(header).read()
+    return sorted(set(re.findall(r"^\s*(?:void|bool|int|const char \*)\s*([A-Za-z_]\w*)\s*\(", text, re.M)))
 
 
 def lib() -> ctypes.CDLL:

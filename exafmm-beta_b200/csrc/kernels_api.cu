@@ -57,6 +57,51 @@ __global__ void k_direct(const double4 *tgt, long long nt, const double4 *src, l
   }
 }
 
+// The MD wrappers' cutoff sum (wrappers/md_distributed.cxx:407-461): every
+// source at every image -prange..prange whose separation is below the cutoff;
+// image shifts rounded to float as the reference's Xperiodic[3] is.
+__global__ void k_direct_cutoff(const double4 *tgt, long long nt, const double4 *src, long long ns, int prange,
+                                double3 cycle, double cutoff2, double4 *trg) {
+  __shared__ double4 tile[256];
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double4 xi = make_double4(0, 0, 0, 0);
+  if (i < nt) xi = tgt[i];
+  double pot = 0, ax = 0, ay = 0, az = 0;
+  for (int ix = -prange; ix <= prange; ix++)
+    for (int iy = -prange; iy <= prange; iy++)
+      for (int iz = -prange; iz <= prange; iz++) {
+        const double sx = (double)(float)(ix * cycle.x), sy = (double)(float)(iy * cycle.y),
+                     sz = (double)(float)(iz * cycle.z);
+        for (long long base = 0; base < ns; base += 256) {
+          __syncthreads();
+          if (base + threadIdx.x < ns) tile[threadIdx.x] = src[base + threadIdx.x];
+          __syncthreads();
+          const int cnt = (int)min((long long)256, ns - base);
+          for (int s = 0; s < cnt; s++) {
+            const double4 sj = tile[s];
+            const double dx = xi.x - sj.x - sx, dy = xi.y - sj.y - sy, dz = xi.z - sj.z - sz;
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 < cutoff2 && r2 != 0.0) {
+              const double inv = 1.0 / sqrt(r2);
+              const double s3 = sj.w * inv * inv * inv;
+              pot += sj.w * inv;
+              ax += dx * s3;
+              ay += dy * s3;
+              az += dz * s3;
+            }
+          }
+        }
+      }
+  if (i < nt) {
+    double4 r = trg[i];
+    r.x += pot;
+    r.y -= ax;
+    r.z -= ay;
+    r.w -= az;
+    trg[i] = r;
+  }
+}
+
 // Device staging for one operator call.
 struct Mini {
   cudaStream_t st = nullptr;
@@ -151,6 +196,25 @@ int exafmm_direct_range(const double *targets, long long nt, const double *sourc
     const double4 *s = m.up((const double4 *)sources, ns);
     double4 *r = m.up((const double4 *)trg, nt);
     direct_fp64(t, nt, s, ns, prange, cycle, r, m.st);
+    m.down((double4 *)trg, r, nt);
+  });
+}
+
+int exafmm_direct_cutoff(const double *targets, long long nt, const double *sources, long long ns, int prange,
+                         const double *cycle3, double cutoff, double *trg) {
+  return run([&] {
+    if (prange < 0) throw std::runtime_error("negative image range");
+    if (!cycle3) throw std::runtime_error("null cycle");
+    if (!(cutoff >= 0)) throw std::runtime_error("negative cutoff");
+    if (nt == 0) return;
+    Mini m;
+    const double4 *t = m.up((const double4 *)targets, nt);
+    const double4 *s = m.up((const double4 *)sources, ns);
+    double4 *r = m.up((const double4 *)trg, nt);
+    k_direct_cutoff<<<(int)((nt + 255) / 256), 256, 0, m.st>>>(t, nt, s, ns, prange,
+                                                              make_double3(cycle3[0], cycle3[1], cycle3[2]),
+                                                              cutoff * cutoff, r);
+    EXA_CHECK_LAUNCH();
     m.down((double4 *)trg, r, nt);
   });
 }

@@ -1,15 +1,17 @@
 // MD-code ABI in the shape of the reference's GROMACS wrapper
 // (wrappers/gromacs.cxx:39-363), one process and one GPU; declared in
-// include/exafmm_md.h.  Host code over the engine's own C ABI: one solve
-// context holds the tree, expansions and lists of the periodic system.
+// include/exafmm_md.h, built as libexafmm_md_gromacs.so.  Host code over the
+// engine's own C ABI: one solve context holds the tree, expansions and lists of
+// the periodic system.
 #include <cmath>
 #include <cstdio>
 #include <stdexcept>
 #include <string>
 #include <vector>
 
-#include "../../include/exafmm_b200.h"
-#include "../../include/exafmm_md.h"
+#include "../../../include/exafmm_b200.h"
+#include "../../../include/exafmm_md.h"
+#include "md_common.h"
 
 namespace {
 
@@ -34,33 +36,17 @@ struct MdState {
 MdState *g_md = nullptr;
 std::string g_error;
 
-// vec.h:534-553 wrap / unwrap with a scalar period: a coordinate below -w/2 or
-// above w/2 moves by one period, and the moved dimensions are flagged.
+// vec.h:534-553 wrap / unwrap with a scalar period.
 int wrap3(double v[3], double w) {
-  int iw = 0;
-  for (int i = 0; i < 3; i++) {
-    if (v[i] < -w / 2) {
-      v[i] += w;
-      iw |= 1 << i;
-    }
-    if (v[i] > w / 2) {
-      v[i] -= w;
-      iw |= 1 << i;
-    }
-  }
-  return iw;
+  const double ww[3] = {w, w, w};
+  return exafmm_md::wrap3(v, ww);
 }
 void unwrap3(double v[3], double w, int iw) {
-  for (int i = 0; i < 3; i++)
-    if ((iw >> i) & 1) v[i] += (v[i] > 0 ? -w : w);
+  const double ww[3] = {w, w, w};
+  exafmm_md::unwrap3(v, ww, iw);
 }
 
-void check(int rc, const char *what) {
-  if (rc == 0) return;
-  std::string m = what;
-  if (g_md && g_md->ctx) m += std::string(": ") + exafmm_last_error(g_md->ctx);
-  throw std::runtime_error(m);
-}
+void check(int rc, const char *what) { exafmm_md::check(g_md ? g_md->ctx : nullptr, rc, what); }
 
 MdState &state() {
   if (!g_md || !g_md->ctx) throw std::runtime_error("FMM_Init has not been called");
@@ -69,13 +55,7 @@ MdState &state() {
 
 template <typename F>
 void guarded(const char *name, F &&f) {
-  try {
-    g_error.clear();
-    f();
-  } catch (const std::exception &e) {
-    g_error = std::string(name) + ": " + e.what();
-    std::fprintf(stderr, "exafmm %s\n", g_error.c_str());
-  }
+  exafmm_md::guarded(g_error, name, f);
 }
 
 // Bodies of FMM_Partition / FMM_Coulomb: X = x - cycle / 2, wrapped into the box.
@@ -147,11 +127,7 @@ void FMM_Partition(int *n, int *ibody, int *icell, float *x, float *q, float cyc
     // (include/partition.h:185-207): Xmin stays, Xmax = Xmin + 1 * (Xmax - Xmin)
     double g[6];
     check(exafmm_get_bounds(s.ctx, g), "get_bounds");
-    for (int d = 0; d < 3; d++) {
-      const double part = (g[3 + d] - g[d]) / 1;
-      s.bounds[d] = g[d] + 0 * part;
-      s.bounds[3 + d] = g[d] + (0 + 1) * part;
-    }
+    exafmm_md::octsection_one_rank(g, s.bounds);
     s.have_bounds = true;
     check(exafmm_build_tree(s.ctx, s.bounds), "build_tree");
     std::vector<int> perm(N);

@@ -173,6 +173,12 @@ int exafmm_direct(const double *targets, long long nt, const double *sources, lo
  * sum of 3^i over the image levels). */
 int exafmm_direct_range(const double *targets, long long nt, const double *sources, long long ns, int prange,
                         double cycle, double *trg);
+/* The cutoff direct sum of wrappers/md_distributed.cxx:407-461 (FMM_Cutoff):
+ * pairs at images -prange..prange per direction (shifts i * cycle3[d] rounded
+ * to float, as there) closer than cutoff; FP64 on the device.  Host arrays;
+ * trg accumulates (potential, gradient). */
+int exafmm_direct_cutoff(const double *targets, long long nt, const double *sources, long long ns, int prange,
+                         const double *cycle3, double cutoff, double *trg);
 
 /* Ewald summation (include/ewald.h:7-197, as examples/ewald.cxx drives it), FP64
  * on the device: wave part over the integer waves |k| <= ksize of

@@ -1,6 +1,9 @@
 /* MD-code ABI in the shape of the reference's GROMACS wrapper
  * (wrappers/gromacs.cxx:39-363, driven by wrappers/test_gromacs.cxx), for one
- * process and one GPU.  Same names, argument meaning and call order:
+ * process and one GPU, in libexafmm_md_gromacs.so (the distributed wrapper's
+ * ABI, include/exafmm_md_distributed.h, reuses some of these names under other
+ * signatures and lives in its own library).  Same names, argument meaning and
+ * call order:
  *
  *   FMM_Init(images, threads, verbose, path);
  *   FMM_Partition(&n, ibody, icell, x, q, cycle);   once, or when bodies moved far

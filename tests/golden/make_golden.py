@@ -197,6 +197,39 @@ def make_md(ref: Reference):
           f"force rel-L2 {acc:.2e}")
 
 
+# wrappers/md_distributed.cxx's recipe as wrappers/test_md_distributed.cxx drives
+# it (images 3, theta 0.4, cutoff L/2, cycle 2 pi, Ewald ksize 11, alpha 10/L,
+# sigma 1/(4 pi)) on seeded bodies: the bodies wrapped without a shift,
+# Set_Index's tree in the bounds of getBounds, FMM_Partition's in those bounds
+# narrowed by the one-rank octsection, FMM_FMM's solve in the latter with the
+# dipole correction, and Ewald on the wrapped bodies.
+def make_md_distributed(ref: Reference):
+    from bindings import Oracle
+    rng = np.random.default_rng(43)
+    n = 1000
+    c = 2 * np.pi
+    x = rng.uniform(size=(n, 3)) * c - c / 2
+    x[:7] += c * np.array([1.0, -1.0, 0.0])  # a few bodies given at another image
+    q = rng.uniform(size=n) - 0.5
+    q -= q.mean()
+    X = md_wrap(x, c)
+    xyzq = np.column_stack([X, q])
+    idx = ref.solve(xyzq, P=10, theta=0.4, ncrit=32, nspawn=1000, images=0, record_lists=False)
+    g = idx.bounds
+    part = (g[3:] - g[:3]) / 1
+    local = np.concatenate([g[:3] + 0 * part, g[:3] + 1 * part])
+    fmm = ref.solve(xyzq, P=10, theta=0.4, ncrit=32, nspawn=1000, images=3, cycle=c, bounds=local,
+                    record_lists=False, dipole_correction=True)
+    ew = ref.ewald(xyzq, 11, 10 / c, 0.25 / np.pi, c / 2, c)
+    ew_nearest = Oracle().ewald(xyzq, 11, 10 / c, 0.25 / np.pi, c / 2, c)
+    np.savez_compressed(os.path.join(OUT, "md_distributed.npz"), x=x, q=q, cycle=np.array([c]),
+                        index_bounds=g, index_perm=idx.perm, index_cells=idx.cells_int, bounds=local,
+                        perm=fmm.perm, fmm_trg=fmm.trg, ewald_trg=ew, ewald_nearest_trg=ew_nearest)
+    e_fmm, e_ew = np.sum(fmm.trg[:, 0] * q), np.sum(ew[:, 0] * q)
+    print(f"md_distributed: cells={len(idx.cells_int)} energy fmm {e_fmm:.8e} ewald {e_ew:.8e} "
+          f"rel {abs(e_fmm - e_ew) / abs(e_ew):.2e}")
+
+
 # Separate source bodies (examples/fmm.cxx -j IneJ): (name, target generator, n,
 # seed, source generator, n, seed, split, P, theta, ncrit, nspawn).  split applies
 # fmm.cxx's transform (targets x -> (x + pi) / 2, sources x -> (x - pi) / 2).
@@ -236,6 +269,7 @@ def main(which=("solve", "periodic", "kat", "records", "md", "inej")):
         make_records(ref)
     if "md" in which:
         make_md(ref)
+        make_md_distributed(ref)
     if "inej" in which:
         for c in INEJ_CASES:
             make_inej(ref, *c)

@@ -19,6 +19,23 @@ def test_library_exports_every_declared_symbol(ex):
     assert set(declared) <= names
 
 
+@pytest.mark.parametrize("which", ["gromacs", "distributed"])
+def test_md_libraries_export_their_abi(ex, which):
+    """Each MD-code ABI lives in its own library (their FMM_* names overlap) that
+    exports every function its header declares; the engine library exports none."""
+    path, header = {"gromacs": (ex.MD_GROMACS_LIB_PATH, ex.MD_HEADER),
+                    "distributed": (ex.MD_DISTRIBUTED_LIB_PATH, ex.MDD_HEADER)}[which]
+    declared = ex.md_exported_symbols(header)
+    assert {"FMM_Init", "FMM_Finalize", "FMM_Partition", "FMM_Error"} <= set(declared)
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True).stdout
+    names = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    assert set(declared) <= names
+    L = ctypes.CDLL(path)
+    assert all(hasattr(L, s) for s in declared)
+    engine = subprocess.run(["nm", "-D", "--defined-only", ex.LIB_PATH], capture_output=True, text=True).stdout
+    assert "FMM_Init" not in engine
+
+
 @pytest.mark.parametrize("seed", range(6))
 def test_closed_form_drift_matches_stepwise_recurrence(ex, oracle, seed):
     """BoundBox::getBounds's running min/max drift (include/bound_box.h:19-20),

@@ -1,6 +1,6 @@
 """The MD ABI of include/exafmm_md.h (the reference's GROMACS wrapper shape,
-wrappers/gromacs.cxx) through its C symbols, as wrappers/test_gromacs.cxx calls
-them: FMM_Init -> FMM_Partition -> FMM_Coulomb, Ewald_Coulomb, Direct_Coulomb.
+wrappers/gromacs.cxx) through the C symbols of libexafmm_md_gromacs.so, as
+wrappers/test_gromacs.cxx calls them: FMM_Init -> FMM_Partition -> FMM_Coulomb, Ewald_Coulomb, Direct_Coulomb.
 Pinned to the reference's own solve of the same recipe (tests/golden/md_gromacs.npz)."""
 import ctypes
 import os
@@ -18,7 +18,7 @@ _i = ctypes.POINTER(ctypes.c_int)
 
 @pytest.fixture(scope="module")
 def md(ex):
-    L = ctypes.CDLL(ex.LIB_PATH)
+    L = ctypes.CDLL(ex.MD_GROMACS_LIB_PATH)
     L.FMM_Init.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_bool, ctypes.c_char_p]
     L.FMM_Finalize.argtypes = []
     L.FMM_Partition.argtypes = [_i, _i, _i, _f, _f, ctypes.c_float]
