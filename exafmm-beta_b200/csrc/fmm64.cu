@@ -262,7 +262,7 @@ __global__ void k_m2l(DevTables t, const int *off, const int *src, long long nce
       const double4 Xj = cell_xj[cj];
       const double dx = Xi.x - Xj.x - sx, dy = Xi.y - Xj.y - sy, dz = Xi.z - Xj.z - sz;
       for (int o = lane; o < NT; o += 32) Mp[o] = cscale(M[(long long)cj * NT + o], t.anm[o]);
-      if (lane < 2 * P - 1) singular_column(t, lane, 2 * P - 1, dx, dy, dz, t.ainv, S);
+      for (int m = lane; m < 2 * P - 1; m += 32) singular_column(t, m, 2 * P - 1, dx, dy, dz, t.ainv, S);
       __syncwarp();
       m2l_accumulate<MAXO>(t, oj, ok, Mp, S, acc);
       __syncwarp();
@@ -511,7 +511,7 @@ __global__ void k_lattice_m2l(DevTables t, const double2 *Msup, double cycle, in
     // d = X_root - X_root - Xperiodic
     const double dx = -(double)(ix * nb + cx) * cycle, dy = -(double)(iy * nb + cy) * cycle,
                  dz = -(double)(iz * nb + cz) * cycle;
-    if (lane < 2 * P - 1) singular_column(t, lane, 2 * P - 1, dx, dy, dz, t.ainv, S);
+    for (int m = lane; m < 2 * P - 1; m += 32) singular_column(t, m, 2 * P - 1, dx, dy, dz, t.ainv, S);
     __syncwarp();
     m2l_accumulate<MAXO>(t, oj, ok, Mp, S, acc);
     __syncwarp();
