@@ -1,8 +1,9 @@
 // Stable LSD radix sort (digits of 8 to 10 bits) of key/value pairs, and the scan work
 // buffers.  Each pass: per-tile digit histograms, one device-wide scan of the
 // digit-major count table, then a stable scatter in which every warp ranks its
-// own contiguous chunk with __match_any_sync and the warps of a tile are ordered
-// by a shared prefix table.
+// own contiguous chunk with __match_any_sync, the warps of a tile are ordered
+// by a shared prefix table, and the tile is written out through shared memory
+// in digit order (coalesced bucket runs).
 #include <algorithm>
 
 #include "engine.h"
@@ -71,18 +72,36 @@ struct CountScan {
   __device__ void total(const T &) const {}
 };
 
+// Shared memory of one scatter tile: the tile's keys and values in digit
+// order, per-warp digit counts, the tile's global offsets and its digit starts.
+template <typename K, int BITS>
+constexpr size_t scatter_smem_bytes() {
+  return (size_t)kSortTile * (sizeof(K) + sizeof(int)) + (size_t)(kSortWarps + 2) * (1 << BITS) * sizeof(unsigned);
+}
+
+// Stable scatter of one tile.  Items are ranked within their warp's chunk
+// (__match_any_sync) and across warps, placed in shared memory in digit order,
+// then written out bucket run by bucket run, so consecutive threads store to
+// consecutive addresses of a bucket instead of each lane to a different one.
 template <typename K, int BITS>
 __global__ void __launch_bounds__(kSortThreads)
 radix_scatter(const K *keys_in, const int *vals_in, K *keys_out, int *vals_out, long long n, int shift,
               unsigned mask, const unsigned *offsets, int ntiles) {
   constexpr int B = 1 << BITS;
-  __shared__ unsigned wcnt[kSortWarps][B];
-  __shared__ unsigned toff[B];
+  constexpr int PER = (B + kSortThreads - 1) / kSortThreads;  // digits per thread in the tile scan
+  extern __shared__ __align__(16) unsigned char sort_smem[];
+  K *skey = reinterpret_cast<K *>(sort_smem);
+  int *sval = reinterpret_cast<int *>(skey + kSortTile);
+  unsigned (*wcnt)[B] = reinterpret_cast<unsigned (*)[B]>(sval + kSortTile);
+  unsigned *toff = &wcnt[kSortWarps][0];  // global start of each digit's run of this tile
+  unsigned *tstart = toff + B;            // start of each digit within the tile
+  __shared__ unsigned wsum[kSortWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int i = threadIdx.x; i < kSortWarps * B; i += blockDim.x) (&wcnt[0][0])[i] = 0;
   for (int d = threadIdx.x; d < B; d += blockDim.x) toff[d] = offsets[(long long)d * ntiles + blockIdx.x];
   __syncthreads();
-  const long long base = (long long)blockIdx.x * kSortTile + warp * (32 * kSortItems);
+  const long long tile0 = (long long)blockIdx.x * kSortTile;
+  const long long base = tile0 + warp * (32 * kSortItems);
   K key[kSortItems];
   int val[kSortItems];
   unsigned rank[kSortItems];
@@ -103,13 +122,41 @@ radix_scatter(const K *keys_in, const int *vals_in, K *keys_out, int *vals_out, 
     rank[it] = b + r;
   }
   __syncthreads();
-  // Exclusive prefix over warps, per digit.
+  // Exclusive prefix over warps, per digit; the digit's tile total goes to tstart.
   for (int d = threadIdx.x; d < B; d += blockDim.x) {
     unsigned run = 0;
     for (int w = 0; w < kSortWarps; w++) {
       unsigned c = wcnt[w][d];
       wcnt[w][d] = run;
       run += c;
+    }
+    tstart[d] = run;
+  }
+  __syncthreads();
+  // Exclusive scan of the digit totals over the tile: PER consecutive digits a thread.
+  {
+    unsigned v[PER], sum = 0;
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+      const int d = threadIdx.x * PER + k;
+      v[k] = d < B ? tstart[d] : 0u;
+      sum += v[k];
+    }
+    unsigned incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    unsigned before = incl - sum;
+    for (int w = 0; w < warp; w++) before += wsum[w];
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+      const int d = threadIdx.x * PER + k;
+      if (d < B) tstart[d] = before;
+      before += v[k];
     }
   }
   __syncthreads();
@@ -118,10 +165,19 @@ radix_scatter(const K *keys_in, const int *vals_in, K *keys_out, int *vals_out, 
     const long long i = base + it * 32 + lane;
     if (i < n) {
       const unsigned dig = (unsigned)(key[it] >> shift) & mask;
-      const unsigned pos = toff[dig] + wcnt[warp][dig] + rank[it];
-      keys_out[pos] = key[it];
-      vals_out[pos] = val[it];
+      const unsigned loc = tstart[dig] + wcnt[warp][dig] + rank[it];
+      skey[loc] = key[it];
+      sval[loc] = val[it];
     }
+  }
+  __syncthreads();
+  const int tile_n = (int)min((long long)kSortTile, n - tile0);
+  for (int j = threadIdx.x; j < tile_n; j += blockDim.x) {
+    const K k = skey[j];
+    const unsigned dig = (unsigned)(k >> shift) & mask;
+    const unsigned pos = toff[dig] + (unsigned)j - tstart[dig];
+    keys_out[pos] = k;
+    vals_out[pos] = sval[j];
   }
 }
 
@@ -134,7 +190,10 @@ void radix_pass(const K *kin, const int *vin, K *kout, int *vout, long long n, i
   CountScan cs{w.counts.p};
   const long long cells = (long long)(1 << BITS) * ntiles;
   launch_scan<256, 8>(cs, nullptr, cells, cells, w.scan, err, st);
-  radix_scatter<K, BITS><<<ntiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, shift, mask, w.counts.p, ntiles);
+  constexpr size_t smem = scatter_smem_bytes<K, BITS>();
+  EXA_CUDA(cudaFuncSetAttribute(radix_scatter<K, BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  radix_scatter<K, BITS><<<ntiles, kSortThreads, smem, st>>>(kin, vin, kout, vout, n, shift, mask, w.counts.p,
+                                                             ntiles);
   EXA_CHECK_LAUNCH();
 }
 
