@@ -216,7 +216,8 @@ bool radix_sort_impl(K *keys, int *vals, K *keys_alt, int *vals_alt, long long n
   bool in_alt = false;
   for (int shift = begin_bit; shift < end_bit; shift += bits) {
     const int width = std::min(bits, end_bit - shift);
-    if (width > 8) radix_pass<K, 10>(kin, vin, kout, vout, n, shift, width, ntiles, w, err, st);
+    if (width > 9) radix_pass<K, 10>(kin, vin, kout, vout, n, shift, width, ntiles, w, err, st);
+    else if (width > 8) radix_pass<K, 9>(kin, vin, kout, vout, n, shift, width, ntiles, w, err, st);
     else radix_pass<K, 8>(kin, vin, kout, vout, n, shift, width, ntiles, w, err, st);
     K *tk = kin; kin = kout; kout = tk;
     int *tv = vin; vin = vout; vout = tv;
