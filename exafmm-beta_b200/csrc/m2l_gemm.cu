@@ -131,7 +131,10 @@ __global__ void k_pair_class(const int *off, const int *src, long long ncells, c
           const unsigned long long key = class_key(dl, (long long)fx, (long long)fy, (long long)fz);
           long long h = (long long)(mix64(key) & (unsigned long long)hmask);
           for (int p = 0; p < kProbe; p++) {
-            const unsigned long long old = atomicCAS(&hk[h], kEmpty, key);
+            // a slot's key, once set, never changes: read it at L2 and CAS only
+            // while the slot is still empty
+            unsigned long long old = __ldcg(&hk[h]);
+            if (old == kEmpty) old = atomicCAS(&hk[h], kEmpty, key);
             if (old == kEmpty || old == key) {
               atomicAdd(&hc[h], 1u);
               slot = (int)h;
