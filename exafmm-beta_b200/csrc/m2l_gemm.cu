@@ -953,32 +953,34 @@ k_m2l_class_mma_tma(const __grid_constant__ CUtensorMap msb_map, const int4 *chu
 }
 
 // 7. Per target: its taken pairs' contributions summed in list order in FP64,
-// scaled by (-1)^j A_j^k R_t^{-(j+1)}, added to L.
+// scaled by (-1)^j A_j^k R_t^{-(j+1)}, added to L.  Lane l holds entries
+// 2l, 2l + 1 (+ 64 u) of the column and loads them as one 8-byte word.
 template <int NDP>
 __global__ void k_m2l_class_reduce(const int *off, long long ncells, const unsigned char *taken, const float *Y,
                                    const double4 *cell_x, DevTables t, int P, double2 *L) {
-  constexpr int PER = (NDP + 31) / 32;
+  constexpr int PER = (NDP + 63) / 64;
   const int lane = threadIdx.x & 31;
   const int NT = t.nterm, ND = nd_of(P);
   const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
   for (long long c = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < ncells; c += warps) {
     const int b = off[c], e = off[c + 1];
-    double acc[PER];
+    double acc[PER][2];
     bool any = false;
 #pragma unroll
-    for (int u = 0; u < PER; u++) acc[u] = 0.0;
-    // eight pairs' flags and columns loaded before they are added (in list order)
-    constexpr int G = 8;
+    for (int u = 0; u < PER; u++) acc[u][0] = acc[u][1] = 0.0;
+    // G pairs' flags and columns loaded before they are added (in list order)
+    constexpr int G = NDP > 64 ? 8 : 16;
     for (int q0 = b; q0 < e; q0 += G) {
       bool tk[G];
-      float v[G][PER];
+      float2 v[G][PER];
 #pragma unroll
       for (int i = 0; i < G; i++) tk[i] = q0 + i < e && taken[q0 + i];
 #pragma unroll
       for (int i = 0; i < G; i++) {
-        const float *y = Y + (long long)(q0 + i) * NDP;
+        const float2 *y = reinterpret_cast<const float2 *>(Y + (long long)(q0 + i) * NDP);
 #pragma unroll
-        for (int u = 0; u < PER; u++) v[i][u] = (tk[i] && lane + 32 * u < NDP) ? y[lane + 32 * u] : 0.f;
+        for (int u = 0; u < PER; u++)
+          v[i][u] = (tk[i] && 2 * lane + 64 * u < NDP) ? y[lane + 32 * u] : make_float2(0.f, 0.f);
       }
 #pragma unroll
       for (int i = 0; i < G; i++) {
@@ -986,22 +988,28 @@ __global__ void k_m2l_class_reduce(const int *off, long long ncells, const unsig
         any = true;
 #pragma unroll
         for (int u = 0; u < PER; u++)
-          if (lane + 32 * u < NDP) acc[u] += (double)v[i][u];
+          if (2 * lane + 64 * u < NDP) {
+            acc[u][0] += (double)v[i][u].x;
+            acc[u][1] += (double)v[i][u].y;
+          }
       }
     }
     if (!any) continue;
     const double rt = cell_x[c].w;
 #pragma unroll
     for (int u = 0; u < PER; u++) {
-      const int d = lane + 32 * u;
-      if (d >= ND) continue;
-      int j, k, part;
-      dof_decode(d, NT, j, k, part);
-      const int o = tri(j) + k;
-      const double v = acc[u] * sgn_pow(j) * t.anm[o] * pow(rt, -(double)(j + 1));
-      double2 *dst = &L[c * NT + o];
-      if (part == 0) dst->x += v;
-      else dst->y += v;
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int d = 2 * lane + 64 * u + h;
+        if (d >= ND) continue;
+        int j, k, part;
+        dof_decode(d, NT, j, k, part);
+        const int o = tri(j) + k;
+        const double v = acc[u][h] * sgn_pow(j) * t.anm[o] * pow(rt, -(double)(j + 1));
+        double2 *dst = &L[c * NT + o];
+        if (part == 0) dst->x += v;
+        else dst->y += v;
+      }
     }
   }
 }
