@@ -1,10 +1,12 @@
 """Seeded body generators for the benchmark workloads, plus the reference's own.
 
 The reference's generators (include/dataset.h) draw with drand48 from fixed
-shapes ([-pi, pi]^3 cube, radius-pi sphere, Plummer scaled by 3*pi/16).  The
-workloads this engine is measured on use different shapes, so they are
-generated here with numpy's PCG64 from an explicit seed and handed, as the
-same (n, 4) array, to both the GPU engine and the CPU checkers.
+shapes ([-pi, pi]^3 cube, radius-pi sphere, octant, Plummer scaled by
+3*pi/16, [-1, 1]^3 lattice); `reference_bodies` reproduces them bit for bit
+(`drand48` is the POSIX stream).  The workloads this engine is measured on use
+different shapes, so they are generated here with numpy's PCG64 from an
+explicit seed and handed, as the same (n, 4) array, to both the GPU engine and
+the CPU checkers.
 
 Every generator returns float64 (n, 4): x, y, z, charge.
 """
@@ -101,3 +103,143 @@ def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
     num = float(np.sum((np.asarray(a) - np.asarray(b)) ** 2))
     den = float(np.sum(np.asarray(b) ** 2))
     return float(np.sqrt(num / den)) if den > 0 else float(np.sqrt(num))
+
+
+# ---------------------------------------------------------------------------
+# The reference's own generators, Dataset::initBodies (include/dataset.h:29-257),
+# bit for bit: the same drand48 streams, the same IEEE arithmetic in the same
+# order, pow / sin / cos from the C math library (Python's math module).
+
+_DRAND_A = 0x5DEECE66D
+_DRAND_C = 0xB
+_MASK48 = (1 << 48) - 1
+_LO24 = (1 << 24) - 1
+
+
+def _mulmod48(x, y):
+    """x * y mod 2^48 for uint64 values below 2^48 (24-bit halves, no overflow)."""
+    xl, xh = x & _LO24, x >> np.uint64(24)
+    yl, yh = y & _LO24, y >> np.uint64(24)
+    return (xl * yl + (((xh * yl + xl * yh) & _LO24) << np.uint64(24))) & _MASK48
+
+
+def drand48(seed: int, count: int) -> np.ndarray:
+    """The first `count` values of drand48() after srand48(seed) (POSIX: the
+    48-bit congruence X <- (0x5DEECE66D X + 11) mod 2^48 from X = seed << 16 |
+    0x330E, the low 32 bits of seed; each value is the new X / 2^48).  Computed
+    in blocks: a block of B values is the previous one advanced by a^B, c_B."""
+    x = (((int(seed) & 0xFFFFFFFF) << 16) | 0x330E) & _MASK48
+    if count <= 0:
+        return np.zeros(0)
+    B = min(count, 4096)
+    first = np.empty(B, np.uint64)
+    for i in range(B):
+        x = (_DRAND_A * x + _DRAND_C) & _MASK48
+        first[i] = x
+    aB, cB = 1, 0
+    for _ in range(B):  # X_{k+B} = aB X_k + cB
+        aB, cB = (_DRAND_A * aB) & _MASK48, (_DRAND_A * cB + _DRAND_C) & _MASK48
+    out = np.empty(count, np.uint64)
+    out[:B] = first
+    a, c = np.uint64(aB), np.uint64(cB)
+    for k in range(B, count, B):
+        m = min(B, count - k)
+        out[k:k + m] = (_mulmod48(out[k - B:k - B + m], a) + c) & _MASK48
+    return out.astype(np.float64) * 2.0 ** -48
+
+
+def _split_range(begin: int, end: int, i: int, num_split: int):
+    """Dataset::splitRange (include/dataset.h:18-26)."""
+    size = end - begin
+    inc, rem = size // num_split, size % num_split
+    begin += i * inc + min(i, rem)
+    end = begin + inc + (1 if rem > i else 0)
+    return begin, end
+
+
+def _ref_lattice(n: int, mpirank: int, mpisize: int) -> np.ndarray:
+    import math
+    nx = int(math.pow(n * mpisize, 1.0 / 3))
+    b, e = _split_range(0, nx, mpirank, mpisize)
+    ix, iy, iz = np.meshgrid(np.arange(nx), np.arange(nx), np.arange(b, e), indexing="ij")
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return np.stack([(g.reshape(-1) / float(nx - 1)) * 2 - 1 for g in (ix, iy, iz)], axis=1)
+
+
+def _ref_positions(kind: str, n: int, seed: int, num_split: int) -> np.ndarray:
+    import math
+    X = np.zeros((n, 3))
+    for s in range(num_split):
+        b, e = _split_range(0, n, s, num_split)
+        m = e - b
+        if kind == "c":  # cube (dataset.h:52-66)
+            X[b:e] = (drand48(seed + s, 3 * m).reshape(m, 3) * 2) * math.pi - math.pi
+        elif kind == "s":  # sphere (dataset.h:68-86)
+            Y = drand48(seed + s, 3 * m).reshape(m, 3) * 2 - 1
+            r = np.sqrt((Y[:, 0] * Y[:, 0] + Y[:, 1] * Y[:, 1]) + Y[:, 2] * Y[:, 2])
+            X[b:e] = Y * (math.pi / r)[:, None]
+        elif kind == "o":  # octant (dataset.h:88-103)
+            d = drand48(seed + s, 2 * m).reshape(m, 2)
+            th = (d[:, 0] * math.pi) * 0.5
+            ph = (d[:, 1] * math.pi) * 0.5
+            st = np.array([math.sin(v) for v in th])
+            ct = np.array([math.cos(v) for v in th])
+            sp = np.array([math.sin(v) for v in ph])
+            cp = np.array([math.cos(v) for v in ph])
+            X[b:e, 0] = ((2 * math.pi) * st) * cp - math.pi
+            X[b:e, 1] = ((2 * math.pi) * st) * sp - math.pi
+            X[b:e, 2] = (2 * math.pi) * ct - math.pi
+        elif kind == "p":  # plummer (dataset.h:105-137): triples until R < 100
+            scale = 3.0 * math.pi / 16.0
+            tries = m + m // 500 + 16
+            while True:
+                d = drand48(seed + s, 3 * tries).reshape(tries, 3)
+                R = np.array([1.0 / math.sqrt(math.pow(v, -2.0 / 3.0) - 1.0) for v in d[:, 0]])
+                keep = np.nonzero(R < 100.0)[0]
+                if len(keep) >= m:
+                    break
+                tries *= 2
+            keep = keep[:m]
+            R, X2, X3 = R[keep], d[keep, 1], d[keep, 2]
+            Z = (1.0 - 2.0 * X2) * R
+            w = np.sqrt(R * R - Z * Z)
+            ang = (2.0 * math.pi) * X3
+            X[b:e, 0] = (w * np.array([math.cos(v) for v in ang])) * scale
+            X[b:e, 1] = (w * np.array([math.sin(v) for v in ang])) * scale
+            X[b:e, 2] = Z * scale
+    return X
+
+
+def _ref_charges(n: int, seed: int, num_split: int) -> np.ndarray:
+    """Dataset::initSource for Laplace (dataset.h:141-154): drand48() - 0.5 per
+    split, minus the split's average summed in body order."""
+    q = np.zeros(n)
+    for s in range(num_split):
+        b, e = _split_range(0, n, s, num_split)
+        v = drand48(seed + s, e - b) - 0.5
+        avg = 0.0
+        for x in v.tolist():
+            avg += x
+        avg /= (e - b)
+        q[b:e] = v - avg
+    return q
+
+
+def reference_bodies(n: int, distribution: str, mpirank: int = 0, mpisize: int = 1,
+                     num_split: int = 1) -> np.ndarray:
+    """Dataset::initBodies(numBodies, distribution, mpirank, mpisize, numSplit)
+    (include/dataset.h:229-257) as float64 (m, 4): x, y, z, charge.  The
+    distribution is chosen by its first letter as there: lattice (m = the
+    largest whole cube root of n * mpisize, cubed, this rank's slab of it),
+    cube, sphere, octant or plummer, seeded with mpirank (+ the split index);
+    the charges restart the same drand48 stream (initSource).  Targets start at
+    zero (initTarget) in this engine's results."""
+    kind = distribution[:1]
+    if kind == "l":
+        X = _ref_lattice(n, mpirank, mpisize)
+    elif kind in ("c", "s", "o", "p"):
+        X = _ref_positions(kind, n, mpirank, num_split)
+    else:
+        raise ValueError(f"Unknown data distribution {distribution}")
+    q = _ref_charges(len(X), mpirank, num_split)
+    return np.column_stack([X, q])

@@ -59,7 +59,7 @@ def reference():
 def golden_cases():
     """Free-space solve fixtures (periodic ones, the operator chain, the record formats and
     the MD ABI are separate)."""
-    other = ("kernel_kat.npz", "records.npz", "md_gromacs.npz", "md_distributed.npz")
+    other = ("kernel_kat.npz", "records.npz", "md_gromacs.npz", "md_distributed.npz", "datasets_reference.npz")
     return sorted(p for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
                   if os.path.basename(p) not in other and not os.path.basename(p).startswith(("periodic_", "inej_")))
 

@@ -7,7 +7,7 @@ commits no golden values of its own (its .reg regression files are written at
 run time), so these fixtures are what pins both the CPU restatement (oracle/)
 and the GPU engine to the reference's behaviour.
 
-Run from the repository root:  python tests/golden/make_golden.py [solve periodic kat records md inej]
+Run from the repository root:  python tests/golden/make_golden.py [solve periodic kat records md inej datasets]
 """
 from __future__ import annotations
 
@@ -254,7 +254,33 @@ def make_inej(ref: Reference, name, gen, n, seed, jgen, nj, jseed, split, P, the
     print(f"{name}: cells={len(run.cells_int)} jcells={len(ji)} m2l={len(run.m2l)} p2p={len(run.p2p)}")
 
 
-def main(which=("solve", "periodic", "kat", "records", "md", "inej")):
+# Dataset::initBodies (include/dataset.h:229-257) from the reference compiled
+# without fast-math (oracle/_ref/libexafmm_ref_dataset.so):
+# (distribution, n, mpirank, mpisize, numSplit).
+DATASET_CASES = [("lattice", 1000, 0, 1, 1), ("lattice", 300, 1, 2, 1), ("cube", 1000, 0, 1, 1),
+                 ("cube", 997, 2, 1, 3), ("sphere", 1000, 1, 1, 1), ("octant", 1000, 0, 1, 2),
+                 ("plummer", 2000, 0, 1, 1), ("plummer", 777, 5, 1, 4)]
+
+
+def make_datasets():
+    import ctypes
+    lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libexafmm_ref_dataset.so"))
+    lib.ref_dataset_init_bodies.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+    lib.ref_drand48.argtypes = [ctypes.c_long, ctypes.c_int, ctypes.c_void_p]
+    data = {}
+    for dist, n, rank, size, ns in DATASET_CASES:
+        buf = np.zeros((n * size + 8, 4))
+        m = lib.ref_dataset_init_bodies(n, dist.encode(), rank, size, ns, buf.ctypes.data, len(buf))
+        data[f"{dist}_{n}_{rank}_{size}_{ns}"] = buf[:m].copy()
+    d = np.zeros(5000)
+    lib.ref_drand48(12345, 5000, d.ctypes.data)
+    data["drand48_12345"] = d
+    np.savez_compressed(os.path.join(OUT, "datasets_reference.npz"), **data)
+    print("datasets_reference:", ", ".join(f"{k} {v.shape}" for k, v in data.items()))
+
+
+def main(which=("solve", "periodic", "kat", "records", "md", "inej", "datasets")):
     build(reference=True)
     ref = Reference()
     if "solve" in which:
@@ -273,8 +299,10 @@ def main(which=("solve", "periodic", "kat", "records", "md", "inej")):
     if "inej" in which:
         for c in INEJ_CASES:
             make_inej(ref, *c)
+    if "datasets" in which:
+        make_datasets()
 
 
 if __name__ == "__main__":
-    # optional arguments: a subset of solve, periodic, kat, records, md, inej
-    main(tuple(sys.argv[1:]) or ("solve", "periodic", "kat", "records", "md", "inej"))
+    # optional arguments: a subset of solve, periodic, kat, records, md, inej, datasets
+    main(tuple(sys.argv[1:]) or ("solve", "periodic", "kat", "records", "md", "inej", "datasets"))
