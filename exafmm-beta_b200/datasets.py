@@ -243,3 +243,53 @@ def reference_bodies(n: int, distribution: str, mpirank: int = 0, mpisize: int =
         raise ValueError(f"Unknown data distribution {distribution}")
     q = _ref_charges(len(X), mpirank, num_split)
     return np.column_stack([X, q])
+
+
+# Dataset's text files (include/dataset.h:162-204, 259-287): one value a line in
+# the C++ stream's default format (%g, 6 significant digits); sources are x, y,
+# z, q per body, targets the four target values.  Reads go on from a byte
+# position and return the position after the last value read (the reference
+# keeps it in the Dataset object, one position for both files).
+
+def _write_values(fname: str, a: np.ndarray) -> str:
+    with open(fname, "w") as f:
+        f.write("".join(f"{v:g}\n" for v in np.asarray(a, dtype=np.float64).reshape(-1).tolist()))
+    return fname
+
+
+def _read_values(fname: str, count: int, position: int):
+    import re
+    with open(fname, "rb") as f:
+        f.seek(position)
+        data = f.read()
+    vals, end = [], 0
+    for m in re.finditer(rb"\S+", data):
+        if len(vals) == count:
+            break
+        vals.append(float(m.group()))
+        end = m.end()
+    if len(vals) < count:
+        raise ValueError(f"{fname}: {len(vals)} values from byte {position}, {count} wanted")
+    return np.array(vals), position + end
+
+
+def write_sources(xyzq: np.ndarray, rank: int = 0, path: str = "./") -> str:
+    """Dataset::writeSources: path + 'source%04d.dat' (rank)."""
+    return _write_values(f"{path}source{rank:04d}.dat", np.asarray(xyzq)[:, :4])
+
+
+def read_sources(n: int, rank: int = 0, path: str = "./", position: int = 0):
+    """Dataset::readSources of n bodies from byte `position`: ((n, 4) x, y, z, q; next position)."""
+    v, pos = _read_values(f"{path}source{rank:04d}.dat", 4 * n, position)
+    return v.reshape(n, 4), pos
+
+
+def write_targets(trg: np.ndarray, rank: int = 0, path: str = "./") -> str:
+    """Dataset::writeTargets: path + 'target%04d.dat' (rank)."""
+    return _write_values(f"{path}target{rank:04d}.dat", np.asarray(trg)[:, :4])
+
+
+def read_targets(n: int, rank: int = 0, path: str = "./", position: int = 0):
+    """Dataset::readTargets of n bodies from byte `position`: ((n, 4) targets; next position)."""
+    v, pos = _read_values(f"{path}target{rank:04d}.dat", 4 * n, position)
+    return v.reshape(n, 4), pos

@@ -30,6 +30,43 @@ int ref_dataset_init_bodies(int n, const char *distribution, int mpirank, int mp
   return m;
 }
 
+// Dataset::writeSources / writeTargets (include/dataset.h:186-204, 276-287)
+// of n bodies given as n x 4 (x, y, z, q) and n x 4 targets, into the current
+// directory as the reference names them (source%04d.dat, target%04d.dat).
+void ref_dataset_write(int n, const double *xyzq, const double *trg, int mpirank) {
+  Dataset data;
+  Bodies bodies(n);
+  for (int i = 0; i < n; i++) {
+    for (int d = 0; d < 3; d++) bodies[i].X[d] = xyzq[4 * i + d];
+    bodies[i].SRC = xyzq[4 * i + 3];
+    for (int d = 0; d < 4; d++) bodies[i].TRG[d] = trg[4 * i + d];
+  }
+  data.writeSources(bodies, mpirank);
+  data.writeTargets(bodies, mpirank);
+}
+
+// Dataset::readSources twice on one Dataset object, then readTargets twice on
+// another (include/dataset.h:162-184, 259-274): successive reads of n bodies
+// each from the current directory, each going on from the object's file
+// position.  src_out holds 2 x n x (x, y, z, q), trg_out 2 x n x 4.
+void ref_dataset_read(int n, int mpirank, double *src_out, double *trg_out) {
+  Dataset data, tdata;
+  for (int r = 0; r < 2; r++) {
+    Bodies bodies(n);
+    data.readSources(bodies, mpirank);
+    for (int i = 0; i < n; i++) {
+      for (int d = 0; d < 3; d++) src_out[(r * n + i) * 4 + d] = bodies[i].X[d];
+      src_out[(r * n + i) * 4 + 3] = bodies[i].SRC;
+    }
+  }
+  for (int r = 0; r < 2; r++) {
+    Bodies bodies(n);
+    tdata.readTargets(bodies, mpirank);
+    for (int i = 0; i < n; i++)
+      for (int d = 0; d < 4; d++) trg_out[(r * n + i) * 4 + d] = bodies[i].TRG[d];
+  }
+}
+
 // n draws of drand48 after srand48(seed), the sequence every generator uses.
 void ref_drand48(long seed, int n, double *out) {
   srand48(seed);

@@ -70,3 +70,38 @@ def test_charges_have_zero_mean_per_split(datasets):
         assert abs(x[b:e, 3].sum()) < 1e-12
     with pytest.raises(ValueError):
         datasets.reference_bodies(10, "gaussian")
+
+
+def test_source_target_files_match_reference(datasets, ref_lib, tmp_path, monkeypatch):
+    """Dataset::writeSources / writeTargets byte for byte, and successive
+    readSources / readTargets going on from the returned file position."""
+    monkeypatch.chdir(tmp_path)
+    rng = np.random.default_rng(8)
+    n = 300
+    x = datasets.reference_bodies(2 * n, "plummer", 0)
+    x[:5, :3] *= np.array([1e-7, 1e6, -3e-12])
+    x[5, 3] = 0.0
+    trg = rng.standard_normal((2 * n, 4)) * np.logspace(-9, 9, 2 * n)[:, None]
+    lib = ref_lib
+    lib.ref_dataset_write.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+    lib.ref_dataset_read.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    lib.ref_dataset_write(2 * n, np.ascontiguousarray(x).ctypes.data, np.ascontiguousarray(trg).ctypes.data, 3)
+    ref_src = open("source0003.dat", "rb").read()
+    ref_trg = open("target0003.dat", "rb").read()
+    mine = tmp_path / "mine"
+    mine.mkdir()
+    datasets.write_sources(x, 3, str(mine) + "/")
+    datasets.write_targets(trg, 3, str(mine) + "/")
+    assert (mine / "source0003.dat").read_bytes() == ref_src
+    assert (mine / "target0003.dat").read_bytes() == ref_trg
+    src_out = np.zeros((2 * n, 4))
+    trg_out = np.zeros((2 * n, 4))
+    lib.ref_dataset_read(n, 3, src_out.ctypes.data, trg_out.ctypes.data)
+    a, pos = datasets.read_sources(n, 3)
+    b, pos = datasets.read_sources(n, 3, position=pos)
+    np.testing.assert_array_equal(np.vstack([a, b]), src_out)
+    c, pos = datasets.read_targets(n, 3)
+    d, pos = datasets.read_targets(n, 3, position=pos)
+    np.testing.assert_array_equal(np.vstack([c, d]), trg_out)
+    with pytest.raises(ValueError):
+        datasets.read_sources(2 * n + 1, 3)
