@@ -5,6 +5,7 @@
 // by a shared prefix table, and the tile is written out through shared memory
 // in digit order (coalesced bucket runs).
 #include <algorithm>
+#include <atomic>
 
 #include "engine.h"
 
@@ -181,6 +182,21 @@ radix_scatter(const K *keys_in, const int *vals_in, K *keys_out, int *vals_out, 
   }
 }
 
+// The scatter's shared-memory opt-in, once per device and kernel: the call
+// is a driver round trip that solving threads would otherwise make on every
+// pass.
+template <typename K, int BITS>
+void scatter_smem_optin() {
+  static std::atomic<unsigned long long> done{0};
+  int dev = 0;
+  EXA_CUDA(cudaGetDevice(&dev));
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (done.load(std::memory_order_acquire) & bit) return;
+  EXA_CUDA(cudaFuncSetAttribute(radix_scatter<K, BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)scatter_smem_bytes<K, BITS>()));
+  done.fetch_or(bit, std::memory_order_release);
+}
+
 template <typename K, int BITS>
 void radix_pass(const K *kin, const int *vin, K *kout, int *vout, long long n, int shift, int width, int ntiles,
                 SortWork &w, int *err, cudaStream_t st) {
@@ -191,7 +207,7 @@ void radix_pass(const K *kin, const int *vin, K *kout, int *vout, long long n, i
   const long long cells = (long long)(1 << BITS) * ntiles;
   launch_scan<256, 8>(cs, nullptr, cells, cells, w.scan, err, st);
   constexpr size_t smem = scatter_smem_bytes<K, BITS>();
-  EXA_CUDA(cudaFuncSetAttribute(radix_scatter<K, BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  scatter_smem_optin<K, BITS>();
   radix_scatter<K, BITS><<<ntiles, kSortThreads, smem, st>>>(kin, vin, kout, vout, n, shift, mask, w.counts.p,
                                                              ntiles);
   EXA_CHECK_LAUNCH();
