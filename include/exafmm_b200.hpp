@@ -1,0 +1,621 @@
+/* C++ facade of the reference's solve API over the C ABI (exafmm_b200.h), so
+ * that a driver written like examples/fmm.cxx compiles against this header
+ * with its class names, members and call sequence:
+ *
+ *   Bodies bodies = data.initBodies(N, "plummer", 0);
+ *   Bounds bounds = boundBox.getBounds(bodies);
+ *   Cells cells = buildTree.buildTree(bodies, buffer, bounds);  // bodies now in tree order
+ *   upDownPass.upwardPass(cells);
+ *   traversal.initListCount(cells); traversal.initWeight(cells);
+ *   traversal.traverse(cells, cells, cycle, args.dual);          // or (cells, jcells, ...)
+ *   upDownPass.downwardPass(cells);                              // Body::TRG += potential, gradient
+ *
+ * Types and classes follow include/types.h:23-119, bound_box.h:11-38,
+ * build_tree.h:183-209, up_down_pass.h:46-99, traversal.h:291-421,
+ * dataset.h:29-298, verify.h:42-107 and kernels/laplace.h:116-388
+ * (namespace exafmm_laplace, real_t = double).
+ *
+ * One engine context, shared by every object of the process (the reference's
+ * objects likewise share one body vector), holds the device tree, expansions
+ * and lists; it is created on first use on the current CUDA device.  What
+ * differs from the reference, by design:
+ *  - the expansions stay in device memory (Cell::M and Cell::L are left
+ *    empty; exafmm_get_expansions reads them), and Cell::ICELL is 0;
+ *  - traverse evaluates M2L and P2P on the device and downwardPass adds all
+ *    of a body's potential and gradient to Body::TRG at once (the reference
+ *    adds P2P during traverse and L2P in downwardPass);
+ *  - a second buildTree on other bodies makes them the source tree of the
+ *    next traverse (examples/fmm.cxx -j: cells, jcells), in FP64;
+ *  - the periodic solve needs cycle[0] == cycle[1] == cycle[2];
+ *  - Kernel's eps2 must be 0 and wavek is not used (Laplace);
+ *  - Args (the command line) and the logger are not provided.
+ * Errors throw std::runtime_error with the engine's message. */
+#ifndef EXAFMM_B200_HPP
+#define EXAFMM_B200_HPP
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstdlib>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "exafmm_b200.h"
+
+namespace exafmm_laplace {
+
+typedef double real_t;
+typedef std::complex<real_t> complex_t;
+
+// include/vec.h:13-235 in the parts a driver uses.
+template <int N, typename T>
+class vec {
+  T d[N];
+
+ public:
+  vec() {}
+  vec(const T &v) { for (int i = 0; i < N; i++) d[i] = v; }
+  vec &operator=(const T &v) { for (int i = 0; i < N; i++) d[i] = v; return *this; }
+  T &operator[](int i) { return d[i]; }
+  const T &operator[](int i) const { return d[i]; }
+  vec &operator+=(const vec &v) { for (int i = 0; i < N; i++) d[i] += v[i]; return *this; }
+  vec &operator-=(const vec &v) { for (int i = 0; i < N; i++) d[i] -= v[i]; return *this; }
+  vec &operator*=(const T &v) { for (int i = 0; i < N; i++) d[i] *= v; return *this; }
+  vec &operator/=(const T &v) { for (int i = 0; i < N; i++) d[i] /= v; return *this; }
+  vec operator+(const vec &v) const { vec r = *this; return r += v; }
+  vec operator-(const vec &v) const { vec r = *this; return r -= v; }
+  vec operator+(const T &v) const { vec r; for (int i = 0; i < N; i++) r[i] = d[i] + v; return r; }
+  vec operator-(const T &v) const { vec r; for (int i = 0; i < N; i++) r[i] = d[i] - v; return r; }
+  vec operator*(const T &v) const { vec r = *this; return r *= v; }
+  vec operator/(const T &v) const { vec r = *this; return r /= v; }
+  friend T norm(const vec &v) { T s = 0; for (int i = 0; i < N; i++) s += v[i] * v[i]; return s; }
+  friend vec min(const vec &a, const vec &b) { vec r; for (int i = 0; i < N; i++) r[i] = a[i] < b[i] ? a[i] : b[i]; return r; }
+  friend vec max(const vec &a, const vec &b) { vec r; for (int i = 0; i < N; i++) r[i] = a[i] > b[i] ? a[i] : b[i]; return r; }
+};
+typedef vec<3, real_t> vec3;
+typedef vec<4, real_t> vec4;
+typedef vec<3, int> ivec3;
+
+struct Bounds {
+  vec3 Xmin;
+  vec3 Xmax;
+};
+
+struct Source {
+  vec3 X;
+  real_t SRC;
+};
+
+struct Body : public Source {
+  int IBODY;
+  int IRANK;
+  int64_t ICELL;
+  real_t WEIGHT;
+  vec4 TRG;
+};
+typedef std::vector<Body> Bodies;
+typedef Bodies::iterator B_iter;
+
+struct CellBase {
+  int IPARENT;
+  int ICHILD;
+  int NCHILD;
+  int IBODY;
+  int NBODY;
+  uint64_t ICELL;
+  real_t WEIGHT;
+  vec3 X;
+  real_t R;
+  B_iter BODY;
+};
+struct Cell : public CellBase {
+  std::vector<complex_t> M;
+  std::vector<complex_t> L;
+};
+typedef std::vector<Cell> Cells;
+typedef Cells::iterator C_iter;
+
+namespace facade_detail {
+
+// The process's engine context and the parameters the objects set on it.
+struct Engine {
+  exafmm_ctx *ctx = nullptr;
+  int P = 10, ncrit = 64, nspawn = 5000, images = 0;
+  double theta = 0.4, cycle = 2 * M_PI;
+  int precision = EXAFMM_FP64;
+  Bodies *targets = nullptr, *sources = nullptr;  // the bodies of the last trees
+  std::vector<int> perm, jperm;                   // tree slot -> caller index at buildTree
+  bool evaluated = false;
+
+  exafmm_ctx *context() {
+    if (!ctx && exafmm_create(&ctx, P, theta, ncrit, nspawn, images, cycle, precision, -1) != 0)
+      throw std::runtime_error(std::string("exafmm: ") + exafmm_create_error());
+    return ctx;
+  }
+  void check(int rc, const char *what) {
+    if (rc != 0) throw std::runtime_error(std::string("exafmm ") + what + ": " + exafmm_last_error(ctx));
+  }
+  void params() { check(exafmm_set_params(context(), P, theta, ncrit, nspawn, images, cycle), "set_params"); }
+};
+
+// One engine for the process.  It is not destroyed at exit (the CUDA runtime
+// may be gone by then); the process's exit releases it.
+inline Engine &engine() {
+  static Engine *e = new Engine;
+  return *e;
+}
+
+inline std::vector<double> pack(const Bodies &b) {
+  std::vector<double> x(4 * b.size());
+  for (size_t i = 0; i < b.size(); i++) {
+    for (int d = 0; d < 3; d++) x[4 * i + d] = b[i].X[d];
+    x[4 * i + 3] = b[i].SRC;
+  }
+  return x;
+}
+
+inline void reorder(Bodies &b, const std::vector<int> &perm) {
+  Bodies t(b.size());
+  for (size_t i = 0; i < b.size(); i++) t[i] = b[perm[i]];
+  b.swap(t);
+}
+
+inline Cells cells_of(std::vector<int> &ci, std::vector<double> &cr, long long nc, Bodies &bodies) {
+  Cells cells(nc);
+  for (long long c = 0; c < nc; c++) {
+    Cell &C = cells[c];
+    C.IPARENT = ci[5 * c + 0];
+    C.ICHILD = ci[5 * c + 1];
+    C.NCHILD = ci[5 * c + 2];
+    C.IBODY = ci[5 * c + 3];
+    C.NBODY = ci[5 * c + 4];
+    C.ICELL = 0;
+    C.WEIGHT = 1;
+    for (int d = 0; d < 3; d++) C.X[d] = cr[4 * c + d];
+    C.R = cr[4 * c + 3];
+    C.BODY = bodies.begin() + C.IBODY;
+  }
+  return cells;
+}
+
+}  // namespace facade_detail
+
+// kernels/laplace.h:116-148 and the per-cell operators (:150-388), each on the
+// device through exafmm_kernel_*, accumulating into the cells' M, L and the
+// bodies' TRG as the reference's do.  Xperiodic shifts the source cell in P2P
+// and M2L.
+class Kernel {
+ public:
+  const int P;
+  const int NTERM;
+  real_t eps2;
+  complex_t wavek;
+  vec3 Xperiodic;
+
+  Kernel(int _P, real_t _eps2, complex_t _wavek) : P(_P), NTERM(_P * (_P + 1) / 2), eps2(_eps2), wavek(_wavek) {
+    if (_eps2 != 0) throw std::runtime_error("exafmm: the Laplace engine has no softening (eps2 must be 0)");
+    Xperiodic = 0;
+    facade_detail::engine().P = _P;
+  }
+
+  void P2P(C_iter Ci, C_iter Cj) const {
+    std::vector<double> xi = packs(Ci), xj = packs(Cj), trg(4 * Ci->NBODY, 0.0);
+    const double xp[3] = {Xperiodic[0], Xperiodic[1], Xperiodic[2]};
+    op(exafmm_kernel_p2p(Ci->NBODY, xi.data(), Cj->NBODY, xj.data(), xp, trg.data()), "P2P");
+    for (int i = 0; i < Ci->NBODY; i++)
+      for (int k = 0; k < 4; k++) Ci->BODY[i].TRG[k] += trg[4 * i + k];
+  }
+  void P2M(C_iter C) const {
+    sized(C->M);
+    std::vector<double> x = packs(C), Xc = xyz(C->X);
+    op(exafmm_kernel_p2m(P, Xc.data(), C->NBODY, x.data(), (double *)C->M.data()), "P2M");
+  }
+  void M2M(C_iter Ci, C_iter C0) const {
+    sized(Ci->M);
+    std::vector<double> Xc, Mc;
+    for (C_iter Cj = C0 + Ci->ICHILD; Cj != C0 + Ci->ICHILD + Ci->NCHILD; Cj++) {
+      sized(Cj->M);
+      for (int d = 0; d < 3; d++) Xc.push_back(Cj->X[d]);
+      const double *m = (const double *)Cj->M.data();
+      Mc.insert(Mc.end(), m, m + 2 * NTERM);
+    }
+    std::vector<double> Xp = xyz(Ci->X);
+    op(exafmm_kernel_m2m(P, Xp.data(), Ci->NCHILD, Xc.data(), Mc.data(), (double *)Ci->M.data()), "M2M");
+  }
+  void M2L(C_iter Ci, C_iter Cj) const {
+    sized(Ci->L);
+    sized(Cj->M);
+    std::vector<double> Xi = xyz(Ci->X), Xj = xyz(Cj->X);
+    const double xp[3] = {Xperiodic[0], Xperiodic[1], Xperiodic[2]};
+    op(exafmm_kernel_m2l(P, Xi.data(), Xj.data(), (const double *)Cj->M.data(), (double *)Ci->L.data(), xp), "M2L");
+  }
+  void L2L(C_iter Ci, C_iter C0) const {
+    C_iter Cj = C0 + Ci->IPARENT;
+    sized(Ci->L);
+    sized(Cj->L);
+    std::vector<double> Xc = xyz(Ci->X), Xp = xyz(Cj->X);
+    op(exafmm_kernel_l2l(P, Xc.data(), Xp.data(), (const double *)Cj->L.data(), (double *)Ci->L.data()), "L2L");
+  }
+  void L2P(C_iter Ci) const {
+    sized(Ci->L);
+    std::vector<double> x = packs(Ci), X = xyz(Ci->X), trg(4 * Ci->NBODY, 0.0);
+    op(exafmm_kernel_l2p(P, X.data(), (const double *)Ci->L.data(), Ci->NBODY, x.data(), trg.data()), "L2P");
+    for (int i = 0; i < Ci->NBODY; i++)
+      for (int k = 0; k < 4; k++) Ci->BODY[i].TRG[k] += trg[4 * i + k];
+  }
+
+ private:
+  void sized(std::vector<complex_t> &E) const {
+    if ((int)E.size() != NTERM) E.assign(NTERM, complex_t(0, 0));
+  }
+  static std::vector<double> xyz(const vec3 &X) { return {X[0], X[1], X[2]}; }
+  static std::vector<double> packs(C_iter C) {
+    std::vector<double> x(4 * C->NBODY);
+    for (int i = 0; i < C->NBODY; i++) {
+      for (int d = 0; d < 3; d++) x[4 * i + d] = C->BODY[i].X[d];
+      x[4 * i + 3] = C->BODY[i].SRC;
+    }
+    return x;
+  }
+  static void op(int rc, const char *what) {
+    if (rc != 0) throw std::runtime_error(std::string("exafmm ") + what + ": " + exafmm_kernel_error());
+  }
+};
+
+// include/bound_box.h:11-38 (the body forms), with the running 1e-5 drift.
+class BoundBox {
+ public:
+  Bounds getBounds(Bodies &bodies) {
+    Bounds b;
+    if (bodies.empty()) {
+      b.Xmin = b.Xmax = 0;
+      return b;
+    }
+    facade_detail::Engine &e = facade_detail::engine();
+    std::vector<double> x = facade_detail::pack(bodies);
+    e.targets = e.sources = nullptr;  // a new solve: the next buildTree makes the targets
+    e.check(exafmm_set_sources(e.context(), nullptr, 0), "set_sources");
+    e.check(exafmm_set_bodies(e.context(), x.data(), (long long)bodies.size()), "set_bodies");
+    double g[6];
+    e.check(exafmm_get_bounds(e.context(), g), "get_bounds");
+    last_ = &bodies;
+    return to_bounds(g);
+  }
+  // getBounds(jbodies, getBounds(bodies)): the bounds of bodies extended by
+  // jbodies as the reference's running update does (examples/fmm.cxx:62-64).
+  Bounds getBounds(Bodies &jbodies, Bounds bounds) {
+    facade_detail::Engine &e = facade_detail::engine();
+    if (!last_) throw std::runtime_error("exafmm: getBounds(jbodies, bounds) extends the last getBounds(bodies)");
+    std::vector<double> x = facade_detail::pack(*last_), jx = facade_detail::pack(jbodies);
+    e.check(exafmm_set_bodies(e.context(), x.data(), (long long)last_->size()), "set_bodies");
+    e.check(exafmm_set_sources(e.context(), jx.data(), (long long)jbodies.size()), "set_sources");
+    double g[6];
+    e.check(exafmm_get_bounds(e.context(), g), "get_bounds");
+    e.check(exafmm_set_sources(e.context(), nullptr, 0), "set_sources");
+    (void)bounds;
+    return to_bounds(g);
+  }
+
+ private:
+  Bodies *last_ = nullptr;
+  static Bounds to_bounds(const double *g) {
+    Bounds b;
+    for (int d = 0; d < 3; d++) {
+      b.Xmin[d] = g[d];
+      b.Xmax[d] = g[3 + d];
+    }
+    return b;
+  }
+};
+
+// include/build_tree.h:183-209: the octree of bodies in the given bounds; the
+// bodies come back in tree order (their IBODY kept), the cells in the
+// reference's order with BODY into them.  buffer is not used.
+class BuildTree {
+ public:
+  explicit BuildTree(int ncrit) { facade_detail::engine().ncrit = ncrit; }
+
+  Cells buildTree(Bodies &bodies, Bodies &buffer, Bounds bounds) {
+    (void)buffer;
+    facade_detail::Engine &e = facade_detail::engine();
+    e.params();
+    const double b6[6] = {bounds.Xmin[0], bounds.Xmin[1], bounds.Xmin[2], bounds.Xmax[0], bounds.Xmax[1], bounds.Xmax[2]};
+    std::vector<double> x = facade_detail::pack(bodies);
+    long long nc = 0;
+    std::vector<int> ci;
+    std::vector<double> cr;
+    if (e.targets && e.targets != &bodies) {  // a second tree: the sources of the next traverse
+      e.check(exafmm_set_sources(e.context(), x.data(), (long long)bodies.size()), "set_sources");
+      e.check(exafmm_build_tree(e.context(), b6), "build_tree");
+      e.check(exafmm_get_source_cells(e.context(), &nc, nullptr, nullptr, nullptr), "get_source_cells");
+      ci.resize(5 * nc);
+      cr.resize(4 * nc);
+      e.jperm.resize(bodies.size());
+      e.check(exafmm_get_source_cells(e.context(), &nc, ci.data(), cr.data(), e.jperm.data()), "get_source_cells");
+      facade_detail::reorder(bodies, e.jperm);
+      e.sources = &bodies;
+    } else {
+      e.check(exafmm_set_sources(e.context(), nullptr, 0), "set_sources");
+      e.check(exafmm_set_bodies(e.context(), x.data(), (long long)bodies.size()), "set_bodies");
+      e.check(exafmm_build_tree(e.context(), b6), "build_tree");
+      e.check(exafmm_tree_info(e.context(), &nc, nullptr, nullptr, nullptr), "tree_info");
+      ci.resize(5 * nc);
+      cr.resize(4 * nc);
+      e.perm.resize(bodies.size());
+      if (nc) e.check(exafmm_get_cells(e.context(), ci.data(), cr.data()), "get_cells");
+      if (!bodies.empty()) e.check(exafmm_get_perm(e.context(), e.perm.data()), "get_perm");
+      facade_detail::reorder(bodies, e.perm);
+      e.targets = &bodies;
+      e.sources = nullptr;
+    }
+    e.evaluated = false;
+    return facade_detail::cells_of(ci, cr, nc, bodies);
+  }
+};
+
+// include/up_down_pass.h:46-99.
+class UpDownPass {
+ public:
+  explicit UpDownPass(Kernel &kernel) : kernel_(kernel) {}
+
+  void upwardPass(Cells &cells) {
+    facade_detail::Engine &e = facade_detail::engine();
+    if (cells.empty()) return;
+    e.check(exafmm_upward(e.context()), "upward");  // the targets' tree and, once built, the sources'
+  }
+  void downwardPass(Cells &cells) {
+    facade_detail::Engine &e = facade_detail::engine();
+    if (cells.empty() || !e.targets) return;
+    e.check(exafmm_downward(e.context()), "downward");
+    std::vector<double> trg(4 * e.targets->size());
+    e.check(exafmm_get_results(e.context(), trg.data()), "get_results");
+    Bodies &b = *e.targets;
+    for (size_t i = 0; i < b.size(); i++)  // results come in the caller's order of buildTree
+      for (int k = 0; k < 4; k++) b[i].TRG[k] += trg[4 * e.perm[i] + k];
+  }
+  vec3 getDipole(Bodies &bodies, vec3 X0) {
+    vec3 dipole = 0;
+    for (B_iter B = bodies.begin(); B != bodies.end(); B++) dipole += (B->X - X0) * B->SRC;
+    return dipole;
+  }
+  void dipoleCorrection(Bodies &bodies, vec3 dipole, int numBodies, vec3 cycle) {
+    const real_t coef = 4 * M_PI / (3 * cycle[0] * cycle[1] * cycle[2]);
+    for (B_iter B = bodies.begin(); B != bodies.end(); B++) {
+      B->TRG[0] -= coef * norm(dipole) / numBodies / B->SRC;
+      for (int d = 0; d < 3; d++) B->TRG[d + 1] -= coef * dipole[d];
+    }
+  }
+
+ private:
+  Kernel &kernel_;
+};
+
+// include/traversal.h:291-421.
+class Traversal {
+ public:
+  Traversal(Kernel &kernel, real_t theta, int nspawn, int images, const char *path = "./")
+      : kernel_(kernel), path_(path ? path : "./") {
+    facade_detail::Engine &e = facade_detail::engine();
+    e.theta = theta;
+    e.nspawn = nspawn;
+    e.images = images;
+  }
+  void initListCount(Cells &) {}  // the engine counts the lists of every traversal
+  void initWeight(Cells &) {}
+
+  // icells == jcells: the bodies' own field; jcells from a second buildTree:
+  // the field of those sources.  dual and remote are the reference's
+  // defaults (dual tree traversal, all sources local).
+  void traverse(Cells &icells, Cells &jcells, vec3 cycle, bool dual = true, real_t remote = 1) {
+    (void)dual;
+    (void)remote;
+    facade_detail::Engine &e = facade_detail::engine();
+    if (icells.empty()) return;
+    if (cycle[0] != cycle[1] || cycle[0] != cycle[2]) throw std::runtime_error("exafmm: the cycle must be cubic");
+    if (&icells != &jcells && e.sources == nullptr && !jcells.empty() && jcells.front().BODY != icells.front().BODY)
+      throw std::runtime_error("exafmm: jcells must come from a buildTree after the targets' one");
+    e.cycle = cycle[0];
+    e.params();
+    e.check(exafmm_traverse(e.context()), "traverse");
+    e.evaluated = true;
+  }
+  // include/traversal.h:355-377: all of jbodies onto bodies over the image
+  // range of the traversal's images and theta, added to bodies' TRG.
+  void direct(Bodies &bodies, Bodies &jbodies, vec3 cycle) {
+    facade_detail::Engine &e = facade_detail::engine();
+    std::vector<double> x = facade_detail::pack(bodies), jx = facade_detail::pack(jbodies), trg(4 * bodies.size(), 0.0);
+    if (exafmm_direct(x.data(), (long long)bodies.size(), jx.data(), (long long)jbodies.size(), e.images, e.theta,
+                      cycle[0], trg.data()) != 0)
+      throw std::runtime_error(std::string("exafmm direct: ") + exafmm_kernel_error());
+    for (size_t i = 0; i < bodies.size(); i++)
+      for (int k = 0; k < 4; k++) bodies[i].TRG[k] += trg[4 * i + k];
+  }
+  // include/traversal.h:412-421 (list%06d.dat of the last traversal).
+  void writeList(Cells &, int mpirank) {
+    facade_detail::Engine &e = facade_detail::engine();
+    e.check(exafmm_write_list(e.context(), path_.c_str(), mpirank), "write_list");
+  }
+
+ private:
+  Kernel &kernel_;
+  std::string path_;
+};
+
+// include/dataset.h:29-298 for Laplace: the generators with the same drand48
+// streams and arithmetic, initSource, initTarget and sampleBodies.
+class Dataset {
+ public:
+  Bodies initBodies(int numBodies, const char *distribution, int mpirank = 0, int mpisize = 1, int numSplit = 1) {
+    Bodies bodies;
+    switch (distribution[0]) {
+      case 'l': bodies = lattice(numBodies, mpirank, mpisize); break;
+      case 'c': bodies = cube(numBodies, mpirank, numSplit); break;
+      case 's': bodies = sphere(numBodies, mpirank, numSplit); break;
+      case 'o': bodies = octant(numBodies, mpirank, numSplit); break;
+      case 'p': bodies = plummer(numBodies, mpirank, numSplit); break;
+      default: throw std::runtime_error(std::string("Unknown data distribution ") + distribution);
+    }
+    initSource(bodies, mpirank, numSplit);
+    initTarget(bodies);
+    return bodies;
+  }
+  void initSource(Bodies &bodies, int seed, int numSplit) {
+    for (int s = 0; s < numSplit; s++, seed++) {
+      int b = 0, e = (int)bodies.size();
+      split(b, e, s, numSplit);
+      srand48(seed);
+      real_t avg = 0;
+      for (int i = b; i < e; i++) {
+        bodies[i].SRC = drand48() - .5;
+        avg += bodies[i].SRC;
+      }
+      avg /= (e - b);
+      for (int i = b; i < e; i++) bodies[i].SRC -= avg;
+    }
+  }
+  void initTarget(Bodies &bodies) {
+    for (size_t i = 0; i < bodies.size(); i++) {
+      bodies[i].TRG = 0;
+      bodies[i].IBODY = (int)i;
+      bodies[i].ICELL = 0;
+      bodies[i].WEIGHT = 1;
+    }
+  }
+  void sampleBodies(Bodies &bodies, int numTargets) {
+    if (numTargets < (int)bodies.size()) {
+      const int stride = (int)bodies.size() / numTargets;
+      for (int i = 0; i < numTargets; i++) bodies[i] = bodies[i * stride];
+      bodies.resize(numTargets);
+    }
+  }
+
+ private:
+  static void split(int &begin, int &end, int i, int n) {
+    const int size = end - begin, inc = size / n, rem = size % n;
+    begin += i * inc + std::min(i, rem);
+    end = begin + inc + (rem > i ? 1 : 0);
+  }
+  static Bodies fresh(int n) {
+    Bodies b(n);
+    for (auto &B : b) {
+      B.X = 0;
+      B.SRC = 0;
+      B.IRANK = 0;
+    }
+    return b;
+  }
+  Bodies lattice(int n, int rank, int size) {
+    const int nx = int(std::pow(n * size, 1. / 3));
+    int b = 0, e = nx;
+    split(b, e, rank, size);
+    Bodies bodies = fresh(nx * nx * (e - b));
+    size_t k = 0;
+    for (int ix = 0; ix < nx; ix++)
+      for (int iy = 0; iy < nx; iy++)
+        for (int iz = b; iz < e; iz++, k++) {
+          bodies[k].X[0] = (ix / real_t(nx - 1)) * 2 - 1;
+          bodies[k].X[1] = (iy / real_t(nx - 1)) * 2 - 1;
+          bodies[k].X[2] = (iz / real_t(nx - 1)) * 2 - 1;
+        }
+    return bodies;
+  }
+  Bodies cube(int n, int seed, int numSplit) {
+    Bodies bodies = fresh(n);
+    for (int s = 0; s < numSplit; s++, seed++) {
+      int b = 0, e = n;
+      split(b, e, s, numSplit);
+      srand48(seed);
+      for (int i = b; i < e; i++)
+        for (int d = 0; d < 3; d++) bodies[i].X[d] = drand48() * 2 * M_PI - M_PI;
+    }
+    return bodies;
+  }
+  Bodies sphere(int n, int seed, int numSplit) {
+    Bodies bodies = fresh(n);
+    for (int s = 0; s < numSplit; s++, seed++) {
+      int b = 0, e = n;
+      split(b, e, s, numSplit);
+      srand48(seed);
+      for (int i = b; i < e; i++) {
+        for (int d = 0; d < 3; d++) bodies[i].X[d] = drand48() * 2 - 1;
+        const real_t r = std::sqrt(norm(bodies[i].X));
+        for (int d = 0; d < 3; d++) bodies[i].X[d] *= M_PI / r;
+      }
+    }
+    return bodies;
+  }
+  Bodies octant(int n, int seed, int numSplit) {
+    Bodies bodies = fresh(n);
+    for (int s = 0; s < numSplit; s++, seed++) {
+      int b = 0, e = n;
+      split(b, e, s, numSplit);
+      srand48(seed);
+      for (int i = b; i < e; i++) {
+        const real_t th = drand48() * M_PI * 0.5, ph = drand48() * M_PI * 0.5;
+        bodies[i].X[0] = 2 * M_PI * std::sin(th) * std::cos(ph) - M_PI;
+        bodies[i].X[1] = 2 * M_PI * std::sin(th) * std::sin(ph) - M_PI;
+        bodies[i].X[2] = 2 * M_PI * std::cos(th) - M_PI;
+      }
+    }
+    return bodies;
+  }
+  Bodies plummer(int n, int seed, int numSplit) {
+    Bodies bodies = fresh(n);
+    for (int s = 0; s < numSplit; s++, seed++) {
+      int b = 0, e = n;
+      split(b, e, s, numSplit);
+      srand48(seed);
+      int i = b;
+      while (i < e) {
+        const real_t X1 = drand48(), X2 = drand48(), X3 = drand48();
+        const real_t R = 1.0 / std::sqrt(std::pow(X1, -2.0 / 3.0) - 1.0);
+        if (R < 100.0) {
+          const real_t Z = (1.0 - 2.0 * X2) * R;
+          real_t X = std::sqrt(R * R - Z * Z) * std::cos(2.0 * M_PI * X3);
+          real_t Y = std::sqrt(R * R - Z * Z) * std::sin(2.0 * M_PI * X3);
+          const real_t scale = 3.0 * M_PI / 16.0;
+          bodies[i].X[0] = X * scale;
+          bodies[i].X[1] = Y * scale;
+          bodies[i].X[2] = Z * scale;
+          i++;
+        }
+      }
+    }
+    return bodies;
+  }
+};
+
+// include/verify.h:42-107: squared norms and differences of the targets.
+class Verify {
+ public:
+  explicit Verify(const char * = "./") {}
+  double getNrmScalar(Bodies &b) {
+    double v = 0;
+    for (auto &B : b) v += std::abs(B.TRG[0] * B.TRG[0]);
+    return v;
+  }
+  double getDifScalar(Bodies &b, Bodies &b2) {
+    double v = 0;
+    for (size_t i = 0; i < b.size(); i++) v += std::abs((b[i].TRG[0] - b2[i].TRG[0]) * (b[i].TRG[0] - b2[i].TRG[0]));
+    return v;
+  }
+  double getNrmVector(Bodies &b) {
+    double v = 0;
+    for (auto &B : b) v += std::abs(B.TRG[1] * B.TRG[1] + B.TRG[2] * B.TRG[2] + B.TRG[3] * B.TRG[3]);
+    return v;
+  }
+  double getDifVector(Bodies &b, Bodies &b2) {
+    double v = 0;
+    for (size_t i = 0; i < b.size(); i++)
+      v += std::abs((b[i].TRG[1] - b2[i].TRG[1]) * (b[i].TRG[1] - b2[i].TRG[1]) +
+                    (b[i].TRG[2] - b2[i].TRG[2]) * (b[i].TRG[2] - b2[i].TRG[2]) +
+                    (b[i].TRG[3] - b2[i].TRG[3]) * (b[i].TRG[3] - b2[i].TRG[3]));
+    return v;
+  }
+};
+
+}  // namespace exafmm_laplace
+
+#endif

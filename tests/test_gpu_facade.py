@@ -1,0 +1,67 @@
+"""The C++ facade include/exafmm_b200.hpp run on the GPU: a driver in the shape
+of examples/fmm.cxx (tests/facade/fmm_driver.cpp) against the engine's own
+path on the same bodies.  Same engine, same bounds and trees, so the bodies'
+order, the cells and the potentials and gradients agree exactly; the driver's
+own check against the direct sum (examples/fmm.cxx:107-124) is reported too."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from test_facade import compile_facade
+
+pytestmark = pytest.mark.gpu
+
+
+def read_driver(path):
+    with open(path, "rb") as f:
+        n = int(np.frombuffer(f.read(8), np.int64)[0])
+        bodies = np.frombuffer(f.read(8 * 9 * n), np.float64).reshape(n, 9)
+        nc = int(np.frombuffer(f.read(8), np.int64)[0])
+        cells = np.frombuffer(f.read(4 * 5 * nc), np.int32).reshape(nc, 5)
+        err = np.frombuffer(f.read(16), np.float64)
+    return bodies, cells, err
+
+
+@pytest.fixture(scope="module")
+def driver(ex, tmp_path_factory):
+    return compile_facade("fmm_driver.cpp", str(tmp_path_factory.mktemp("facade") / "fmm_driver"), ex)
+
+
+@pytest.mark.parametrize("n,dist,P,theta,ncrit,nspawn,images,inej", [
+    (20000, "plummer", 8, 0.35, 32, 5000, 0, 0),
+    (6000, "cube", 6, 0.4, 16, 1000, 1, 0),
+    (5000, "cube", 6, 0.4, 16, 5000, 0, 1),
+])
+def test_facade_driver_matches_engine(ex, datasets, driver, tmp_path, n, dist, P, theta, ncrit, nspawn, images, inej):
+    out = str(tmp_path / "out.bin")
+    r = subprocess.run([driver, out, str(n), dist, str(P), str(theta), str(ncrit), str(nspawn), str(images), str(inej)],
+                       capture_output=True, text=True, cwd=str(tmp_path), timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    bodies, cells, err = read_driver(out)
+    x = datasets.reference_bodies(n, dist, 0)
+    jx = None
+    if inej:
+        x[:, 0] = (x[:, 0] + np.pi) * 0.5
+        jx = datasets.reference_bodies(n, dist, 1)
+        jx[:, 0] = (jx[:, 0] - np.pi) * 0.5
+    f = ex.Fmm(P=P, theta=theta, ncrit=ncrit, nspawn=nspawn, images=images, cycle=2 * np.pi)
+    f.set_bodies(x)
+    if inej:
+        f.set_sources(jx)
+    f.solve()
+    trg = f.results()
+    perm = f.perm()
+    ints, _ = f.cells()
+    f.close()
+    # the bodies come back in the tree's order, with their IBODY and results
+    np.testing.assert_array_equal(bodies[:, 4].astype(np.int64), perm)
+    np.testing.assert_array_equal(bodies[:, :4], x[perm])
+    np.testing.assert_array_equal(cells, ints)
+    np.testing.assert_array_equal(bodies[:, 5:], trg[perm])
+    assert os.path.exists(tmp_path / "list000000.dat")
+    # examples/fmm.cxx's accuracy check on 100 sampled targets (the method's
+    # truncation at these P and theta; images 1 is the 27 nearest cells' sum
+    # for both)
+    assert err[0] < 1e-3 and err[1] < 1e-2, err
