@@ -23,8 +23,9 @@ def compile_facade(src, out, ex):
     return out
 
 
-def test_fmm_driver_compiles_and_links(ex, tmp_path):
-    exe = compile_facade("fmm_driver.cpp", str(tmp_path / "fmm_driver"), ex)
+@pytest.mark.parametrize("src", ["fmm_driver.cpp", "kernel_driver.cpp"])
+def test_drivers_compile_and_link(ex, tmp_path, src):
+    exe = compile_facade(src, str(tmp_path / src[:-4]), ex)
     assert os.path.exists(exe)
 
 

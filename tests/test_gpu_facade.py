@@ -65,3 +65,24 @@ def test_facade_driver_matches_engine(ex, datasets, driver, tmp_path, n, dist, P
     # truncation at these P and theta; images 1 is the 27 nearest cells' sum
     # for both)
     assert err[0] < 1e-3 and err[1] < 1e-2, err
+
+
+def test_facade_kernel_chain_matches_reference(ex, tmp_path):
+    """examples/kernel.cxx's chain through the facade's Kernel, against the
+    reference's own values (tests/golden/kernel_kat.npz)."""
+    from conftest import GOLDEN, load_golden, rel_l2
+    exe = compile_facade("kernel_driver.cpp", str(tmp_path / "kernel_driver"), ex)
+    g = load_golden(os.path.join(GOLDEN, "kernel_kat.npz"))
+    for P in (4, 8, 10, 14):
+        out = str(tmp_path / f"k{P}.bin")
+        r = subprocess.run([exe, out, str(P)], capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0, r.stderr
+        nt = P * (P + 1) // 2
+        raw = np.fromfile(out, dtype=np.float64)
+        E = raw[:8 * nt].view(np.complex128).reshape(4, nt)
+        trg, direct = raw[8 * nt:8 * nt + 4], raw[8 * nt + 4:]
+        for k, name in enumerate(("Mj", "MJ", "LI", "Li")):
+            ref = g[f"P{P}_{name}"]
+            assert np.abs(E[k] - ref).max() <= 1e-13 * np.abs(ref).max(), (P, name)
+        assert rel_l2(trg, g[f"P{P}_trg"].reshape(-1)) < 1e-13
+        assert rel_l2(direct, g[f"P{P}_direct"].reshape(-1)) < 1e-15
