@@ -12,7 +12,7 @@
  *
  * Types and classes follow include/types.h:23-119, bound_box.h:11-38,
  * build_tree.h:183-209, up_down_pass.h:46-99, traversal.h:291-421,
- * dataset.h:29-298, verify.h:42-107 and kernels/laplace.h:116-388
+ * dataset.h:29-298, verify.h:9-175 and kernels/laplace.h:116-388
  * (namespace exafmm_laplace, real_t = double).
  *
  * One engine context, shared by every object of the process (the reference's
@@ -38,6 +38,10 @@
 #include <complex>
 #include <cstdint>
 #include <cstdlib>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <map>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -587,10 +591,80 @@ class Dataset {
   }
 };
 
-// include/verify.h:42-107: squared norms and differences of the targets.
+// include/verify.h:9-175: squared norms and differences of the targets, and
+// the regression files (path + "accuracy.reg", or path + "time_" + $WORKERNAME
+// + ".reg"): the running average of the values over the iterations passes if
+// no record exists for the key or it stays within the record times
+// (1 + 1e-16 + 0.01 iteration), and for accuracy below 5e-4 (5e-3 for the
+// second value); a pass stores the average as the key's record.
 class Verify {
  public:
-  explicit Verify(const char * = "./") {}
+  bool verbose = false;
+  double average = 0, average2 = 0;
+
+  Verify() : path_("./") {}
+  explicit Verify(const char *path) : path_(path ? path : "./") {}
+
+  double getSumScalar(Bodies &b) {
+    double v = 0;
+    for (auto &B : b) v += B.TRG[0] * B.SRC;
+    return v;
+  }
+  void print(std::string title, double v) {
+    if (verbose)
+      std::cout << std::setw(20) << std::left << title << " : " << std::setprecision(7) << std::scientific << v
+                << std::endl;
+  }
+  bool regression(uint64_t key, bool time, int iteration, double value, double value2 = 0) {
+    typedef std::map<uint64_t, double> Record;
+    bool pass = false;
+    const bool second = value2 != 0;
+    Record record, record2;
+    std::string name = path_;
+    if (time) {
+      name += "time_";
+      const char *host = std::getenv("WORKERNAME");
+      if (host) name += std::string(host) + ".reg";  // no name: the stream stops at "time_" there
+    } else {
+      name += "accuracy.reg";
+    }
+    {
+      std::ifstream file(name.c_str());
+      int numKeys;
+      if (file.good() && (file >> numKeys)) {
+        for (int i = 0; i < numKeys; i++) {
+          uint64_t k;
+          file >> k;
+          file >> record[k];
+          if (second) file >> record2[k];
+        }
+      }
+    }
+    average = (average * iteration + value) / (iteration + 1);
+    if (second) average2 = (average2 * iteration + value2) / (iteration + 1);
+    double threshold = record[key] * (1 + 1e-16 + iteration * .01);
+    if ((record[key] == 0 || average <= threshold) && (average < 5e-4 || time)) {
+      pass = true;
+      record[key] = average;
+    }
+    if (second) {
+      threshold = record2[key] * (1 + 1e-16 + iteration * .01);
+      if ((record2[key] == 0 || average2 <= threshold) && (average2 < 5e-3 || time)) {
+        record2[key] = average2;
+      } else {
+        pass = false;
+      }
+    }
+    std::ofstream file(name.c_str());
+    file << record.size() << std::endl;
+    Record::iterator R2 = second ? record2.begin() : record.begin();
+    for (Record::iterator R = record.begin(); R != record.end(); R++, R2++) {
+      file << R->first << " " << R->second;
+      if (second) file << " " << R2->second;
+      file << std::endl;
+    }
+    return pass;
+  }
   double getNrmScalar(Bodies &b) {
     double v = 0;
     for (auto &B : b) v += std::abs(B.TRG[0] * B.TRG[0]);
@@ -614,6 +688,9 @@ class Verify {
                     (b[i].TRG[3] - b2[i].TRG[3]) * (b[i].TRG[3] - b2[i].TRG[3]));
     return v;
   }
+
+ private:
+  std::string path_;
 };
 
 }  // namespace exafmm_laplace

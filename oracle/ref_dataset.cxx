@@ -10,6 +10,7 @@
 
 #include "types.h"
 #include "dataset.h"
+#include "verify.h"
 
 using namespace exafmm_laplace;
 
@@ -65,6 +66,16 @@ void ref_dataset_read(int n, int mpirank, double *src_out, double *trg_out) {
     for (int i = 0; i < n; i++)
       for (int d = 0; d < 4; d++) trg_out[(r * n + i) * 4 + d] = bodies[i].TRG[d];
   }
+}
+
+// Verify::regression (include/verify.h:118-175) over a sequence of calls on one
+// Verify object whose path is `path`: calls i uses keys[i], time[i],
+// iteration[i], value[i], value2[i]; pass[i] receives its result.
+void ref_verify_sequence(const char *path, int n, const unsigned long long *keys, const int *time,
+                         const int *iteration, const double *value, const double *value2, int *pass) {
+  Verify verify(path);
+  verify.verbose = false;
+  for (int i = 0; i < n; i++) pass[i] = verify.regression(keys[i], time[i] != 0, iteration[i], value[i], value2[i]);
 }
 
 // n draws of drand48 after srand48(seed), the sequence every generator uses.

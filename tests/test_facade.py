@@ -40,3 +40,42 @@ def test_facade_dataset_matches_reference(ex, tmp_path):
         mine = np.fromfile(out, dtype=np.float64).reshape(-1, 4)
         assert mine.shape == ref.shape, key
         np.testing.assert_array_equal(mine, ref, err_msg=key)
+
+
+def test_facade_verify_regression_matches_reference(ex, tmp_path, monkeypatch):
+    """Verify::regression of the facade against the reference's own
+    (include/verify.h:118-175, compiled in oracle/_ref/libexafmm_ref_dataset.so):
+    the same pass / fail answers and byte-identical regression files over a
+    sequence of accuracy (two values) and time calls on one object."""
+    import ctypes
+    ref_path = os.path.join(ROOT, "oracle", "_ref", "libexafmm_ref_dataset.so")
+    if not os.path.exists(ref_path):
+        pytest.skip("oracle/_ref was not built here (needs the reference tree)")
+    lib = ctypes.CDLL(ref_path)
+    lib.ref_verify_sequence.argtypes = [ctypes.c_char_p, ctypes.c_int] + [ctypes.c_void_p] * 6
+    monkeypatch.setenv("WORKERNAME", "box")
+    calls = [  # key, time, iteration, value, value2
+        (3, 0, 0, 1e-5, 2e-4), (3, 0, 1, 1.05e-5, 2.1e-4), (3, 0, 2, 9e-5, 2e-4), (77, 0, 0, 6e-4, 1e-4),
+        (77, 0, 0, 3e-4, 6e-3), (3, 0, 0, 1e-5, 1e-4), (12345678901, 0, 3, 2e-6, 3e-5),
+        (5, 1, 0, 0.25, 0.0), (5, 1, 1, 0.24, 0.0), (5, 1, 0, 0.5, 0.0), (9, 1, 2, 1.5, 0.0), (5, 1, 0, 0.2, 0.0),
+    ]
+    ref_dir, my_dir = tmp_path / "ref", tmp_path / "mine"
+    ref_dir.mkdir()
+    my_dir.mkdir()
+    keys = np.array([c[0] for c in calls], np.uint64)
+    tm = np.array([c[1] for c in calls], np.int32)
+    it = np.array([c[2] for c in calls], np.int32)
+    v = np.array([c[3] for c in calls])
+    v2 = np.array([c[4] for c in calls])
+    ref_pass = np.zeros(len(calls), np.int32)
+    lib.ref_verify_sequence((str(ref_dir) + "/").encode(), len(calls), keys.ctypes.data, tm.ctypes.data,
+                            it.ctypes.data, v.ctypes.data, v2.ctypes.data, ref_pass.ctypes.data)
+    exe = compile_facade("verify_driver.cpp", str(tmp_path / "verify_driver"), ex)
+    args = [exe, str(my_dir) + "/"]
+    for c in calls:
+        args += [str(c[0]), str(c[1]), str(c[2]), repr(c[3]), repr(c[4])]
+    out = subprocess.run(args, capture_output=True, text=True, check=True).stdout.split()
+    assert [int(t) for t in out] == ref_pass.tolist()
+    assert 0 < ref_pass.sum() < len(calls)  # both outcomes exercised
+    for name in ("accuracy.reg", "time_box.reg"):
+        assert (my_dir / name).read_bytes() == (ref_dir / name).read_bytes(), name
