@@ -28,7 +28,8 @@
  *    next traverse (examples/fmm.cxx -j: cells, jcells), in FP64;
  *  - the periodic solve needs cycle[0] == cycle[1] == cycle[2];
  *  - Kernel's eps2 must be 0 and wavek is not used (Laplace);
- *  - Args (the command line) and the logger are not provided.
+ *  - Args (the command line) is not provided; logger keeps host wall-clock
+ *    timers and the time file, not PAPI counters or traces.
  * Errors throw std::runtime_error with the engine's message. */
 #ifndef EXAFMM_B200_HPP
 #define EXAFMM_B200_HPP
@@ -37,7 +38,9 @@
 #include <cmath>
 #include <complex>
 #include <cstdint>
+#include <cstdio>
 #include <cstdlib>
+#include <ctime>
 #include <fstream>
 #include <iomanip>
 #include <iostream>
@@ -446,6 +449,82 @@ class Traversal {
   Kernel &kernel_;
   std::string path_;
 };
+
+// include/logger.h:39-138: event timers (host wall clock) and the time file.
+// writeTime writes path + "time%06d.dat" with the driver's timers and the
+// engine's phases since the last write (Get bounds, Grow tree, Link tree,
+// Upward pass, Traverse, Traverse periodic, Downward pass), as the
+// reference's file holds its own phases; the PAPI, tracer and DAG hooks do
+// nothing here.
+namespace logger {
+inline int stringLength = 20;
+inline int decimal = 7;
+inline bool verbose = false;
+inline const char *path = "./";
+inline std::map<std::string, double> timer, beginTimer;
+
+inline double get_time() {
+  struct timespec ts;
+  clock_gettime(CLOCK_REALTIME, &ts);
+  return double(ts.tv_sec) + double(ts.tv_nsec) * 1e-9;
+}
+inline void printTitle(std::string title) {
+  if (verbose) {
+    title += " ";
+    std::cout << "--- " << std::setw(stringLength) << std::left << std::setfill('-') << title << std::setw(10) << "-"
+              << std::setfill(' ') << std::endl;
+  }
+}
+inline void startTimer(std::string event) { beginTimer[event] = get_time(); }
+inline void printTime(std::string event) {
+  if (verbose)
+    std::cout << std::setw(stringLength) << std::left << event << " : " << std::setprecision(decimal) << std::fixed
+              << timer[event] << " s" << std::endl;
+}
+inline double stopTimer(std::string event, int print = 1) {
+  const double t = get_time() - beginTimer[event];
+  timer[event] += t;
+  if (verbose && print) printTime(event);
+  return t;
+}
+inline void writeTime(int mpirank = 0) {
+  std::map<std::string, double> all = timer;
+  facade_detail::Engine &e = facade_detail::engine();
+  char name[32];
+  std::snprintf(name, sizeof(name), "time%06d.dat", mpirank);
+  if (e.ctx && exafmm_write_time(e.ctx, path, mpirank) == 0) {  // the engine's phases, then merged
+    std::ifstream f((std::string(path) + name).c_str());
+    std::string line;
+    while (std::getline(f, line)) {
+      if (line.size() <= (size_t)stringLength) continue;
+      std::string ev = line.substr(0, stringLength);
+      ev.erase(ev.find_last_not_of(' ') + 1);
+      all[ev] += std::atof(line.c_str() + stringLength + 1);
+    }
+  }
+  std::vector<std::string> names;
+  std::vector<const char *> cnames;
+  std::vector<double> secs;
+  for (auto &kv : all) {
+    names.push_back(kv.first);
+    secs.push_back(kv.second);
+  }
+  for (auto &n : names) cnames.push_back(n.c_str());
+  if (exafmm_write_time_events(path, mpirank, (int)names.size(), cnames.data(), secs.data()) != 0)
+    throw std::runtime_error("exafmm: cannot write the time file");
+  timer.clear();
+}
+inline void resetTimer(std::string event) { timer.erase(event); }
+inline void resetTimer() { timer.clear(); }
+inline void startPAPI() {}
+inline void stopPAPI() {}
+inline void printPAPI() {}
+inline void initTracer() {}
+inline void writeTracer(int = 0) {}
+inline void startDAG() {}
+inline void stopDAG() {}
+inline void writeDAG() {}
+}  // namespace logger
 
 // include/dataset.h:29-298 for Laplace: the generators with the same drand48
 // streams and arithmetic, initSource, initTarget and sampleBodies.

@@ -4,7 +4,9 @@
 // P, theta, ncrit, nspawn, images, IneJ (0/1).  Writes, in binary: N, then per
 // body in the order the facade leaves them X[3], SRC, IBODY, TRG[4]; the cell
 // count and each cell's IPARENT ICHILD NCHILD IBODY NBODY; then the relative
-// errors against the direct sum on 100 sampled targets.
+// errors against the direct sum on 100 sampled targets.  Also writes the list
+// file and the time file (the solve timed as "Total FMM") in the working
+// directory.
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -46,6 +48,7 @@ int main(int argc, char **argv) {
         B->X[0] *= 0.5;
       }
     }
+    logger::startTimer("Total FMM");
     bounds = boundBox.getBounds(bodies);
     if (IneJ) bounds = boundBox.getBounds(jbodies, bounds);
     cells = buildTree.buildTree(bodies, buffer, bounds);
@@ -61,6 +64,8 @@ int main(int argc, char **argv) {
       jbodies = bodies;
     }
     upDownPass.downwardPass(cells);
+    logger::stopTimer("Total FMM");
+    logger::writeTime(0);
     traversal.writeList(cells, 0);
   } catch (const std::exception &e) {
     std::fprintf(stderr, "%s\n", e.what());

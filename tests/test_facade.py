@@ -79,3 +79,17 @@ def test_facade_verify_regression_matches_reference(ex, tmp_path, monkeypatch):
     assert 0 < ref_pass.sum() < len(calls)  # both outcomes exercised
     for name in ("accuracy.reg", "time_box.reg"):
         assert (my_dir / name).read_bytes() == (ref_dir / name).read_bytes(), name
+
+
+def test_facade_logger_time_file(ex, tmp_path):
+    """logger's timers accumulate per event and writeTime writes them in the
+    reference's time file format (the same writer as exafmm_write_time,
+    byte-compared with the reference in test_gpu_records.py), then clears."""
+    exe = compile_facade("logger_driver.cpp", str(tmp_path / "logger_driver"), ex)
+    subprocess.run([exe, str(tmp_path) + "/"], check=True)
+    lines = (tmp_path / "time000002.dat").read_text().splitlines()
+    names = [ln[:20].rstrip() for ln in lines]
+    vals = [float(ln[21:]) for ln in lines]
+    assert names == ["Direct sum", "Total FMM"]
+    assert 0.015 < vals[0] < 0.5 and 0.05 < vals[1] < 1.0
+    assert (tmp_path / "time000003.dat").read_text() == ""

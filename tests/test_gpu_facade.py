@@ -61,6 +61,10 @@ def test_facade_driver_matches_engine(ex, datasets, driver, tmp_path, n, dist, P
     np.testing.assert_array_equal(cells, ints)
     np.testing.assert_array_equal(bodies[:, 5:], trg[perm])
     assert os.path.exists(tmp_path / "list000000.dat")
+    # the time file: the driver's timer with the engine's phases, as the reference writes it
+    names = [ln[:20].rstrip() for ln in (tmp_path / "time000000.dat").read_text().splitlines()]
+    assert {"Total FMM", "Get bounds", "Grow tree", "Upward pass", "Traverse", "Downward pass"} <= set(names)
+    assert names == sorted(names)
     # examples/fmm.cxx's accuracy check on 100 sampled targets (the method's
     # truncation at these P and theta; images 1 is the 27 nearest cells' sum
     # for both)
