@@ -178,6 +178,53 @@ def run_reference_arm(args, rank: int):
     print(json.dumps(line), flush=True)
 
 
+def replica_value(local_seconds: float, units_per_rank: float, world: int, dist=None, device="cuda"):
+    """Replicas only: every rank solves its own systems.  The job's time is the
+    slowest rank's (one MAX all-reduce of a scalar, no data-path collective);
+    the value is the units all ranks processed over that time."""
+    import torch
+    t = torch.tensor([float(local_seconds)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    tmax = float(t.item())
+    return tmax, units_per_rank * world / tmax
+
+
+def agree_ncrit(best: int, world: int, dist=None, device="cuda") -> int:
+    """Every rank solves on rank 0's tuned ncrit (the same trees everywhere)."""
+    import torch
+    t = torch.tensor([int(best)], dtype=torch.int64, device=device)
+    if world > 1:
+        dist.broadcast(t, 0)
+    return int(t.item())
+
+
+def torchrun_command(argv: list[str], gpus: int, port: int) -> list[str]:
+    """The launch of `gpus` replica ranks of this script on one node."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={gpus}",
+            "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + list(argv)
+
+
+def _free_port() -> int:
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def check_world(gpus: int, env=None) -> str:
+    """'spawn' when --gpus N > 1 was given without a rank environment (this
+    process then launches the ranks itself), 'run' otherwise; a rank
+    environment whose size differs from --gpus is an error."""
+    env = os.environ if env is None else env
+    if "WORLD_SIZE" not in env:
+        return "spawn" if gpus > 1 else "run"
+    world = int(env["WORLD_SIZE"])
+    if world != gpus:
+        raise SystemExit(f"bench.py: --gpus {gpus} but WORLD_SIZE={world}; launch one rank per GPU")
+    return "run"
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -196,6 +243,9 @@ def main():
                          "with images=3 against Ewald")
     ap.add_argument("--workers", type=int, default=16, help="contexts (streams) of the batch / serve runtime")
     args = ap.parse_args()
+    if check_world(args.gpus) == "spawn":
+        r = subprocess.run(["timeout", "-k", "60", "3600"] + torchrun_command(sys.argv[1:], args.gpus, _free_port()))
+        sys.exit(r.returncode)
     if args.workload != "solve":
         return run_runtime_workload(args)
 
@@ -251,12 +301,7 @@ def main():
             solve_device(f, dout)
             tuned[cand] = f.phase_times()["total"]
             f.close()
-        best = [min(tuned, key=tuned.get)]
-        if world > 1:  # every rank must use the same ncrit
-            tb = torch.tensor(best, device="cuda")
-            dist.broadcast(tb, 0)
-            best = [int(tb.item())]
-        ncrit = best[0]
+        ncrit = agree_ncrit(min(tuned, key=tuned.get), world, dist)
 
     fmm = make(prec, ncrit)
     stream = torch.cuda.ExternalStream(fmm.stream())
@@ -283,12 +328,10 @@ def main():
     launches = pkg.launch_count() - launches0
     ms = ev0.elapsed_time(ev1)
     clk = clocks.summary()
-    t = torch.tensor([ms], device="cuda")
+    s_max, value = replica_value(ms / 1e3, n * args.steps, world, dist)
+    ms_max = 1e3 * s_max
     if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
-    ms_max = float(t.item())
-    value = n * world * args.steps / (ms_max / 1e3)
 
     # ---- e2e: public API from pinned host memory ----
     if world > 1:
@@ -303,10 +346,7 @@ def main():
         fmm.results(out=hout_np)
     e1.record(stream)
     torch.cuda.synchronize()
-    te = torch.tensor([e0.elapsed_time(e1)], device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = n * world * args.steps / (float(te.item()) / 1e3)
+    _, e2e_value = replica_value(e0.elapsed_time(e1) / 1e3, n * args.steps, world, dist)
 
     # ---- plain FP64 run of the same input, and the three-way error split ----
     plain = None
@@ -322,10 +362,8 @@ def main():
             solve_device(f64, dref)
         p1.record(s64)
         torch.cuda.synchronize()
-        tp = torch.tensor([p0.elapsed_time(p1)], device="cuda")
-        if world > 1:
-            dist.all_reduce(tp, op=dist.ReduceOp.MAX)
-        plain_ms = float(tp.item()) / args.steps
+        tp_s, _ = replica_value(p0.elapsed_time(p1) / 1e3, n * args.steps, world, dist)
+        plain_ms = 1e3 * tp_s / args.steps
         mixed_out, plain_out = dout.cpu().numpy(), dref.cpu().numpy()
         idx = datasets.strided_sample(n, 4096)
         direct = pkg.direct(x[idx], x)
@@ -462,9 +500,7 @@ def run_runtime_workload(args):
     if world > 1:
         import torch.distributed as dist
         if args.workload in ("batch", "periodic"):  # whole-job bodies/s over the slowest rank's time
-            t = torch.tensor([line["_time"]], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            line["value"] = line["_units"] * world / float(t.item())
+            _, line["value"] = replica_value(line["_time"], line["_units"], world, dist)
         else:  # latency: the worst rank's p99
             t = torch.tensor([line["value"]], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)

@@ -8,17 +8,23 @@
 // doubles.  The only other device memory used is a 128-byte file-scope array,
 // which every GPU that loads this library holds until the process exits.
 //
-// Set-up: the first call on each device looks up the device address of that
-// array (cudaGetSymbolAddress) with the device current; make that first call
-// before any stream capture.  All calls share the one array, and each call
-// starts by clearing it, so calls whose work overlaps on the GPU (different
-// streams, or different host threads on the same device) race and must be
-// ordered by the caller.
+// Set-up: the first call in each CUDA context looks up the device address of
+// that array (cudaGetSymbolAddress) with the context current; make that first
+// call before any stream capture.  The address belongs to the context that
+// loaded this library's module, so it is remembered per context (by the
+// driver's unique context id), not per device ordinal: after cudaDeviceReset,
+// or when a host framework makes its own context current, the next call looks
+// the address up again.  All calls share the one array, and each call starts
+// by clearing it, so calls whose work overlaps on the GPU (different streams,
+// or different host threads on the same device) race and must be ordered by
+// the caller.
 //
 // This entry point has no counterpart in the reference.  It runs the same
 // two-pass algorithm as the context-based exafmm_get_bounds: an unrounded
 // estimate per body, then the exact drift only for bodies whose estimate lies
 // within the estimate's error bound of the extreme.
+#include <cuda.h>
+
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -37,7 +43,30 @@ static __device__ __align__(256) unsigned long long g_bounds_scratch[kBoundsScra
 constexpr long long kNoAllocMaxBodies = (1LL << 31) - 1;
 
 std::mutex g_mutex;
-unsigned long long *g_scratch_ptr[64] = {};
+// Scratch address per CUDA context, keyed by the driver's context id (unique
+// for the life of the process, unlike a context handle, which a new context
+// may reuse).  Up to kCtxSlots contexts are remembered; more are looked up on
+// every call.
+constexpr int kCtxSlots = 64;
+struct CtxSlot {
+  unsigned long long id;
+  unsigned long long *ptr;
+};
+CtxSlot g_slots[kCtxSlots] = {};
+int g_nslots = 0;
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+
+template <typename F>
+F driver_entry(const char *name) {
+  void *p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPointByVersion(name, &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !p)
+    throw std::runtime_error(std::string("driver entry point not found: ") + name);
+  return (F)p;
+}
 
 __device__ __forceinline__ unsigned long long enc(double d) {
   unsigned long long u = (unsigned long long)__double_as_longlong(d);
@@ -110,21 +139,32 @@ __global__ void k_na_final(const unsigned long long *s, long long n, double *out
   if (t < 6) out[t] = (n > 0) ? dec(s[t]) : 0.0;
 }
 
-// Device address of the scratch array for the current device, looked up once.
-unsigned long long *scratch_for_current_device() {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) throw std::runtime_error(std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-  if (dev < 0 || dev >= 64) throw std::runtime_error("device ordinal out of range");
+// Device address of the scratch array in the current context, looked up once
+// per context.
+unsigned long long *scratch_for_current_context() {
   std::lock_guard<std::mutex> lock(g_mutex);
-  if (!g_scratch_ptr[dev]) {
-    unsigned long long *p = nullptr;
-    e = cudaGetSymbolAddress((void **)&p, g_bounds_scratch);
-    if (e != cudaSuccess || !p)
-      throw std::runtime_error(std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-    g_scratch_ptr[dev] = p;
-  }
-  return g_scratch_ptr[dev];
+  static CtxGetCurrentFn get_current = driver_entry<CtxGetCurrentFn>("cuCtxGetCurrent");
+  static CtxGetIdFn get_id = driver_entry<CtxGetIdFn>("cuCtxGetId");
+  auto current_id = [&](unsigned long long *id) {
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS) throw std::runtime_error("cuCtxGetCurrent failed");
+    if (!ctx) return false;
+    if (get_id(ctx, id) != CUDA_SUCCESS) throw std::runtime_error("cuCtxGetId failed");
+    return true;
+  };
+  unsigned long long id = 0;
+  const bool have = current_id(&id);
+  if (have)
+    for (int k = 0; k < g_nslots; k++)
+      if (g_slots[k].id == id) return g_slots[k].ptr;
+  // Unknown context, or none current yet: the lookup runs in (and, when none
+  // was current, first makes current) the runtime's context for this device.
+  unsigned long long *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress((void **)&p, g_bounds_scratch);
+  if (e != cudaSuccess || !p)
+    throw std::runtime_error(std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+  if ((have || current_id(&id)) && g_nslots < kCtxSlots) g_slots[g_nslots++] = CtxSlot{id, p};
+  return p;
 }
 
 }  // namespace
@@ -135,14 +175,17 @@ using namespace exafmm_b200;
 extern "C" {
 
 // Status: 0 done (results are ready once `stream` reaches this point),
-// 2 n outside [0, 2^31 - 1], 3 null pointer, 4 CUDA error (symbol lookup or
-// launch).  Nothing is launched unless the status is 0 or 4.
+// 2 n outside [0, 2^31 - 1], 3 null pointer, 4 CUDA error raised by this call
+// (context or symbol lookup, or one of its launches), 5 a CUDA error was
+// already pending on this thread when the call began (left pending for its
+// owner; nothing is launched).
 int exafmm_get_bounds_noalloc(const double *d_xyzq, long long n, double *d_bounds6, void *stream) {
   if (n < 0 || n > kNoAllocMaxBodies) return 2;
   if (!d_bounds6 || (n > 0 && !d_xyzq)) return 3;
+  if (cudaPeekAtLastError() != cudaSuccess) return 5;
   try {
     cudaStream_t st = (cudaStream_t)stream;
-    unsigned long long *s = scratch_for_current_device();
+    unsigned long long *s = scratch_for_current_context();
     k_na_clear<<<1, 32, 0, st>>>(s);  // the array keeps the previous call's contents
     EXA_CHECK_LAUNCH();
     if (n > 0) {

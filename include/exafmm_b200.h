@@ -264,10 +264,13 @@ const char *exafmm_server_error(void);
  * cudaStream_t; NULL is the legacy default stream).  Needs no context and
  * allocates nothing: its only scratch is a 128-byte array built into the
  * library, held by every GPU that loads it until the process exits.  The first
- * call on a device looks up that array's address, so make it before any stream
- * capture.  All calls share the array, so calls that overlap on the GPU race.
- * Returns 0, or 2 when n is outside [0, 2^31 - 1], 3 for a null pointer,
- * 4 for a CUDA error. */
+ * call in each CUDA context (per device, and again after cudaDeviceReset or
+ * under a caller's own context) looks up that array's address, so make it
+ * before any stream capture.  All calls share the array, so calls that overlap
+ * on the GPU race.  Returns 0, or 2 when n is outside [0, 2^31 - 1], 3 for a
+ * null pointer, 4 for a CUDA error raised by this call, 5 when a CUDA error
+ * was already pending on the calling thread (it is left pending, and nothing
+ * is launched). */
 int exafmm_get_bounds_noalloc(const double *d_xyzq, long long n, double *d_bounds6, void *stream);
 
 /* Host-side closed form of the bounds drift: fl(x -/+ 1e-5) applied k times

@@ -19,16 +19,16 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libexafmm_ref.so")
-REFERENCE_ROOT = os.environ.get("EXAFMM_REFERENCE_ROOT", "/root/reference")
 
 _c_int, _c_double, _vp = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
 
 
-def build(reference: bool = True) -> None:
-    """Compile liboracle.so and, when the reference tree is present, the harness."""
+def build(reference_root: str | None = None) -> None:
+    """Compile liboracle.so and, when reference_root names an exafmm-beta
+    source tree that exists, the reference harness compiled in place from it."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
-    if reference and os.path.isdir(os.path.join(REFERENCE_ROOT, "include")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE_ROOT={REFERENCE_ROOT}"], check=True)
+    if reference_root and os.path.isdir(os.path.join(reference_root, "include")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE_ROOT={reference_root}"], check=True)
 
 
 def _ptr(a: np.ndarray | None):
