@@ -1,5 +1,7 @@
 // Solve context: every device buffer one FMM solve touches, owned per caller.
 #pragma once
+#include <vector>
+
 #include "engine.h"
 
 namespace exafmm_b200 {
@@ -49,7 +51,34 @@ struct TreeBufs {
   int ncells = 0;
   int depth = 0;
   long long lvl_host[2 * (kMaxLevels + 1)];
+
+  // Forest of independent systems (exafmm_set_systems).  nsys == 0 is the
+  // plain path: one system, root cell 0.  Otherwise the bodies of system s are
+  // [sys_off[s], sys_off[s+1]) in caller order and in tree order alike; each
+  // non-empty system has a root node at level 0 (root node k belongs to system
+  // root_sys[k]) and its cells are [sys_cell[s], sys_cell[s+1]), laid out as
+  // that system's solo tree would be, shifted by sys_cell[s].
+  int nsys = 0;
+  int nroots = 0;
+  long long ntiles = 0;                 // body tiles of at most kForestTile bodies, none across systems
+  std::vector<long long> sys_off_host;  // nsys + 1
+  std::vector<int> sys_cell_host;       // nsys + 1 (valid after sync_tree)
+  DBuf<long long> sys_off;
+  DBuf<int> sys_root;                   // per system: its root node, or -1 when it has no bodies
+  DBuf<int> root_sys;                   // per root node: its system
+  DBuf<int> tile_sys;
+  DBuf<long long> tile_beg;
+  DBuf<unsigned long long> sys_enc;     // 16 words per system (bounds reduction)
+  DBuf<double> sys_bounds;              // Xmin[3], Xmax[3] per system
+  DBuf<double4> sys_box;                // X0, R0 per system
+  DBuf<int> sys_cell;
+  DBuf<int> nd_sys;                     // node -> system
+  DBuf<unsigned> fs_key, fs_key_alt;    // second sort pass: system of each key-sorted body
+  DBuf<int> fs_idx, fs_idx_alt;
 };
+
+// Bodies per tile of the forest's per-system reductions.
+constexpr int kForestTile = 4096;
 
 struct Context {
   long long dev_bytes = 0;     // device bytes held by this context's buffers (declared first: outlives them)

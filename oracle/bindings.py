@@ -179,7 +179,7 @@ class Oracle(_Lib):
     prefix = "oracle_"
 
     def __init__(self, path: str = ORACLE_SO):
-        build(reference=False)  # incremental; keeps the .so in step with exafmm_oracle.c
+        build()  # incremental; keeps the .so in step with exafmm_oracle.c
         super().__init__(path)
 
     def _sig(self):

@@ -7,7 +7,10 @@ commits no golden values of its own (its .reg regression files are written at
 run time), so these fixtures are what pins both the CPU restatement (oracle/)
 and the GPU engine to the reference's behaviour.
 
-Run from the repository root:  python tests/golden/make_golden.py [solve periodic kat records md inej datasets]
+Run from the repository root, with EXAFMM_REFERENCE_ROOT naming the
+exafmm-beta source tree (read only):
+
+    EXAFMM_REFERENCE_ROOT=/root/reference python tests/golden/make_golden.py [solve periodic kat records md inej datasets]
 """
 from __future__ import annotations
 
@@ -281,7 +284,10 @@ def make_datasets():
 
 
 def main(which=("solve", "periodic", "kat", "records", "md", "inej", "datasets")):
-    build(reference=True)
+    root = os.environ.get("EXAFMM_REFERENCE_ROOT")
+    if not root or not os.path.isdir(os.path.join(root, "include")):
+        raise SystemExit("set EXAFMM_REFERENCE_ROOT to the exafmm-beta source tree")
+    build(reference_root=root)
     ref = Reference()
     if "solve" in which:
         for c in CASES:
