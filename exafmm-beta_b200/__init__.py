@@ -132,6 +132,9 @@ def lib() -> ctypes.CDLL:
         "exafmm_write_time": (_c_int, [_vp, ctypes.c_char_p, _c_int]),
         "exafmm_write_time_events": (_c_int, [ctypes.c_char_p, _c_int, _c_int, _vp, _vp]),
         "exafmm_morton_key": (ctypes.c_ulonglong, [_vp, _vp, _c_double, _c_int]),
+        "exafmm_set_systems": (_c_int, [_vp, _c_int, _vp, _vp]),
+        "exafmm_set_systems_device": (_c_int, [_vp, _c_int, _vp, _vp]),
+        "exafmm_get_systems": (_c_int, [_vp, _vp, _vp, _vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -173,6 +176,7 @@ class Fmm:
         self.P, self.theta, self.ncrit, self.nspawn, self.images, self.cycle = P, theta, ncrit, nspawn, images, cycle
         self.precision = precision
         self.n = 0
+        self.nsys = 0
 
     def _check(self, rc):
         if rc != 0:
@@ -236,11 +240,46 @@ class Fmm:
     def set_bodies(self, xyzq):
         xyzq = _f64(xyzq, 4)
         self.n = len(xyzq)
+        self.nsys = 0
         self._check(lib().exafmm_set_bodies(self._h, _p(xyzq), self.n))
 
     def set_bodies_device(self, ptr: int, n: int):
         self.n = n
+        self.nsys = 0
         self._check(lib().exafmm_set_bodies_device(self._h, _vp(ptr), n))
+
+    # ---- a forest of independent systems, solved together ----
+    def set_systems(self, systems):
+        """Independent systems (a list of (n_i, 4) arrays) solved as one forest:
+        each gets its own bounds, tree, lists and expansions, as a solo solve of
+        it would, with every phase launched once for all of them."""
+        sizes = np.ascontiguousarray([len(x) for x in systems], dtype=np.int64)
+        cat = _f64(np.concatenate([np.asarray(x, dtype=np.float64).reshape(-1, 4) for x in systems])
+                   if len(systems) else np.zeros((0, 4)), 4)
+        self.n, self.nsys = int(sizes.sum()), len(systems)
+        self._sizes = sizes
+        self._check(lib().exafmm_set_systems(self._h, self.nsys, _p(sizes), _p(cat)))
+
+    def set_systems_device(self, ptr: int, sizes):
+        """The same with the concatenated bodies already on the device."""
+        sizes = np.ascontiguousarray(sizes, dtype=np.int64)
+        self.n, self.nsys = int(sizes.sum()), len(sizes)
+        self._sizes = sizes
+        self._check(lib().exafmm_set_systems_device(self._h, self.nsys, _p(sizes), _vp(ptr)))
+
+    def systems(self) -> dict:
+        """Forest layout after a build: cell_base and body_off (nsys + 1 each), bounds (nsys, 6)."""
+        cb = np.zeros(self.nsys + 1, dtype=np.int64)
+        bo = np.zeros(self.nsys + 1, dtype=np.int64)
+        b = np.zeros((self.nsys, 6))
+        self._check(lib().exafmm_get_systems(self._h, _p(cb), _p(bo), _p(b)))
+        return {"cell_base": cb, "body_off": bo, "bounds": b}
+
+    def system_results(self, out: np.ndarray | None = None) -> list:
+        """Per-system (n_i, 4) views of the concatenated results."""
+        r = self.results(out)
+        off = np.concatenate([[0], np.cumsum(self._sizes)])
+        return [r[off[i]:off[i + 1]] for i in range(self.nsys)]
 
     def get_bounds(self) -> np.ndarray:
         b = np.zeros(6)

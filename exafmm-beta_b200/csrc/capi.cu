@@ -126,6 +126,11 @@ struct Engine {
     a.M64 = M.p;
     a.L64 = L.p;
     a.trg64 = trg.p;
+    if (C.tree.nsys) {
+      a.nsys = C.tree.nsys;
+      a.sys_off = C.tree.sys_off.p;
+      a.sys_box = C.tree.sys_box.p;
+    }
     return a;
   }
 
@@ -144,13 +149,79 @@ struct Engine {
   void set_bodies(const double *xyzq, long long n, cudaMemcpyKind kind) {
     if (n < 0) throw std::runtime_error("negative body count");
     if (n >= (1LL << 26)) throw std::runtime_error("more than 2^26 bodies per context is not supported");
+    C.tree.nsys = 0;  // one system
+    C.tree.nroots = 0;
     C.tree.n = n;
     C.tree.xyzq.ensure(n);
     if (n) EXA_CUDA(cudaMemcpyAsync(C.tree.xyzq.p, xyzq, n * sizeof(double4), kind, C.stream));
     tree_ok = up_ok = lists_ok = false;
   }
 
+  // A forest of count independent systems, bodies concatenated in system
+  // order (system s: n[s] bodies).  Every system gets its own bounds, tree,
+  // lists and expansions, as a solo solve of it would; they run together.
+  void set_systems(int count, const long long *n, const double *xyzq, cudaMemcpyKind kind) {
+    if (count < 1) throw std::runtime_error("a forest needs at least one system");
+    if (!n) throw std::runtime_error("null system sizes");
+    if (jsrc) throw std::runtime_error("a forest of systems cannot have separate sources");
+    if (C.prm.images != 0) throw std::runtime_error("a forest of systems is solved in free space (images = 0)");
+    TreeBufs &T = C.tree;
+    std::vector<long long> off(count + 1, 0);
+    std::vector<int> sys_root(count, -1), root_sys;
+    std::vector<int> tile_sys;
+    std::vector<long long> tile_beg;
+    for (int s = 0; s < count; s++) {
+      if (n[s] < 0) throw std::runtime_error("negative body count");
+      off[s + 1] = off[s] + n[s];
+      if (off[s + 1] >= (1LL << 26)) throw std::runtime_error("more than 2^26 bodies per context is not supported");
+      if (n[s] > 0) {
+        sys_root[s] = (int)root_sys.size();
+        root_sys.push_back(s);
+        for (long long b = off[s]; b < off[s + 1]; b += kForestTile) {
+          tile_sys.push_back(s);
+          tile_beg.push_back(b);
+        }
+      }
+    }
+    const long long total = off[count];
+    if (T.nsys == count && T.sys_off_host == off) {  // same layout as before: only the bodies change
+      T.n = total;
+      if (total) EXA_CUDA(cudaMemcpyAsync(T.xyzq.p, xyzq, total * sizeof(double4), kind, C.stream));
+      tree_ok = up_ok = lists_ok = false;
+      return;
+    }
+    T.nsys = count;
+    T.nroots = (int)root_sys.size();
+    T.ntiles = (long long)tile_sys.size();
+    T.sys_off_host = off;
+    T.sys_off.ensure(count + 1);
+    T.sys_root.ensure(count);
+    T.root_sys.ensure(std::max<size_t>(1, root_sys.size()));
+    T.tile_sys.ensure(std::max<size_t>(1, tile_sys.size()));
+    T.tile_beg.ensure(std::max<size_t>(1, tile_beg.size()));
+    // on the context's stream (its buffers are stream-ordered allocations);
+    // pageable host vectors, so the stream is synchronized before they go
+    cudaStream_t st = C.stream;
+    EXA_CUDA(cudaMemcpyAsync(T.sys_off.p, off.data(), (count + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
+    EXA_CUDA(cudaMemcpyAsync(T.sys_root.p, sys_root.data(), count * sizeof(int), cudaMemcpyHostToDevice, st));
+    if (!root_sys.empty())
+      EXA_CUDA(cudaMemcpyAsync(T.root_sys.p, root_sys.data(), root_sys.size() * sizeof(int), cudaMemcpyHostToDevice,
+                               st));
+    if (!tile_sys.empty()) {
+      EXA_CUDA(cudaMemcpyAsync(T.tile_sys.p, tile_sys.data(), tile_sys.size() * sizeof(int), cudaMemcpyHostToDevice,
+                               st));
+      EXA_CUDA(cudaMemcpyAsync(T.tile_beg.p, tile_beg.data(), tile_beg.size() * sizeof(long long),
+                               cudaMemcpyHostToDevice, st));
+    }
+    EXA_CUDA(cudaStreamSynchronize(st));
+    T.n = total;
+    T.xyzq.ensure(total);
+    if (total) EXA_CUDA(cudaMemcpyAsync(T.xyzq.p, xyzq, total * sizeof(double4), kind, C.stream));
+    tree_ok = up_ok = lists_ok = false;
+  }
+
   void set_sources(const double *xyzq, long long n) {
+    if (xyzq && C.tree.nsys) throw std::runtime_error("a forest of systems cannot have separate sources");
     if (!xyzq) {  // back to sources == targets
       jsrc.reset();
     } else {
@@ -187,6 +258,7 @@ struct Engine {
     tm.init();
     C.ev_link = tm.link;
     EXA_CUDA(cudaEventRecord(tm.ev[0], C.stream));
+    if (C.tree.nsys && bounds6) throw std::runtime_error("a forest computes each system's own bounds");
     if (bounds6) {
       set_bounds(C, bounds6);
     } else {
@@ -604,8 +676,43 @@ int exafmm_set_bodies_device(exafmm_ctx *ctx, const double *d_xyzq, long long n)
   });
 }
 
+int exafmm_set_systems(exafmm_ctx *ctx, int count, const long long *n, const double *xyzq) {
+  return guarded(ctx, [&] {
+    cudaSetDevice(ctx->E.C.device);
+    ctx->E.set_systems(count, n, xyzq, cudaMemcpyHostToDevice);
+    EXA_CUDA(cudaStreamSynchronize(ctx->E.C.stream));
+  });
+}
+
+int exafmm_set_systems_device(exafmm_ctx *ctx, int count, const long long *n, const double *d_xyzq) {
+  return guarded(ctx, [&] {
+    cudaSetDevice(ctx->E.C.device);
+    ctx->E.set_systems(count, n, d_xyzq, cudaMemcpyDeviceToDevice);
+  });
+}
+
+int exafmm_get_systems(exafmm_ctx *ctx, long long *cell_base, long long *body_off, double *bounds) {
+  return guarded(ctx, [&] {
+    Engine &E = ctx->E;
+    TreeBufs &T = E.C.tree;
+    if (!T.nsys) throw std::runtime_error("the context holds one system (exafmm_set_systems was not called)");
+    cudaSetDevice(E.C.device);
+    if (body_off)
+      for (int s = 0; s <= T.nsys; s++) body_off[s] = T.sys_off_host[s];
+    if ((cell_base || bounds) && !E.tree_ok) throw std::runtime_error("no tree");
+    if (cell_base)
+      for (int s = 0; s <= T.nsys; s++) cell_base[s] = T.sys_cell_host[s];
+    if (bounds) {
+      EXA_CUDA(cudaMemcpyAsync(bounds, T.sys_bounds.p, 6 * T.nsys * sizeof(double), cudaMemcpyDeviceToHost,
+                               E.C.stream));
+      EXA_CUDA(cudaStreamSynchronize(E.C.stream));
+    }
+  });
+}
+
 int exafmm_get_bounds(exafmm_ctx *ctx, double *b6) {
   return guarded(ctx, [&] {
+    if (ctx->E.C.tree.nsys) throw std::runtime_error("a forest has bounds per system (exafmm_get_systems)");
     cudaSetDevice(ctx->E.C.device);
     compute_bounds(ctx->E.C);
     if (ctx->E.jsrc) extend_bounds(ctx->E.C, ctx->E.jsrc->C.tree.xyzq.p, ctx->E.jsrc->C.tree.n);

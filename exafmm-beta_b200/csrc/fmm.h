@@ -27,6 +27,11 @@ struct FmmArgs {
   const double4 *src_cell_x = nullptr;
   const double4 *src_xt = nullptr;
   const double2 *src_M64 = nullptr;
+  // forest of systems: bodies of system s are [sys_off[s], sys_off[s+1]) in
+  // tree order, its root box sys_box[s] (null: one system, root cell 0)
+  int nsys = 0;
+  const long long *sys_off = nullptr;
+  const double4 *sys_box = nullptr;
 };
 
 void p2m_fp64(const FmmArgs &a);

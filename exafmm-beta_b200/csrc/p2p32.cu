@@ -114,6 +114,26 @@ __global__ void k_abs32(const double4 *xt, long long n, const double4 *cell_x, f
   }
 }
 
+// The same in a forest: each body relative to its own system's root center
+// (the center of its root cell, so each system's values equal its solo solve's).
+__global__ void k_abs32_forest(const double4 *xt, long long n, const long long *sys_off, int nsys,
+                               const double4 *sys_box, float4 *x32) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = nsys - 1;  // last s with sys_off[s] <= i
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (sys_off[mid] <= i) lo = mid;
+      else hi = mid - 1;
+    }
+    const double4 X0 = sys_box[lo];
+    const double4 b = xt[i];
+    const double dx = b.x - X0.x, dy = b.y - X0.y, dz = b.z - X0.z;
+    const float hx = (float)dx, hy = (float)dy, hz = (float)dz;
+    x32[2 * i] = make_float4(hx, hy, hz, (float)b.w);
+    x32[2 * i + 1] = make_float4((float)(dx - (double)hx), (float)(dy - (double)hy), (float)(dz - (double)hz), 0.f);
+  }
+}
+
 // (hi, lo) += s, with s split into two floats and the hi sum made exact by TwoSum.
 __device__ __forceinline__ void add_shift(float &hi, float &lo, double s) {
   const float sh = (float)s, sl = (float)(s - (double)sh);
@@ -356,7 +376,8 @@ void rel_bodies32(const FmmArgs &a, float4 *x32) {
   if (a.n <= 0) return;
   long long g = (a.n + 255) / 256;
   if (g > kNumSMs * 16) g = kNumSMs * 16;
-  k_abs32<<<(int)g, 256, 0, a.stream>>>(a.xt, a.n, a.cell_x, x32);
+  if (a.nsys) k_abs32_forest<<<(int)g, 256, 0, a.stream>>>(a.xt, a.n, a.sys_off, a.nsys, a.sys_box, x32);
+  else k_abs32<<<(int)g, 256, 0, a.stream>>>(a.xt, a.n, a.cell_x, x32);
   EXA_CHECK_LAUNCH();
 }
 

@@ -144,6 +144,19 @@ __global__ void k_trav_init(int2 *q, long long *cnt, int images, long long ncell
   }
 }
 
+// A forest starts from every system's root pair (Traversal::traverse of each
+// system, free space); pairs never cross systems from there.
+__global__ void k_trav_init_forest(int2 *q, long long *cnt, const int *nd_cell, int nroots) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    for (int s = 0; s < 3 * (kMaxSweeps + 1); s++) cnt[s] = 0;
+    cnt[0] = nroots;
+  }
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nroots; k += gridDim.x * blockDim.x) {
+    const int c = nd_cell[k];  // root node k's cell
+    q[k] = make_int2(c, c | (13 << kImgShift));
+  }
+}
+
 __global__ void k_split_pairs(const int2 *pairs, long long n, unsigned *key, int *val) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const int2 p = pairs[i];
@@ -209,7 +222,16 @@ bool traverse(Context &C, ListBufs &lb, const TreeBufs *sources) {
   lb.m2l.ensure(lb.m2l_cap);
   lb.p2p.ensure(lb.p2p_cap);
   lb.cnt.ensure(3 * (kMaxSweeps + 1));
-  k_trav_init<<<1, 32, 0, st>>>(lb.q0.p, lb.cnt.p, C.prm.images, std::min<long long>(ncells, S.ncells));
+  if (C.tree.nsys) {
+    if (sources || C.prm.images) throw_msg("a forest of systems is solved in free space with sources == targets");
+    lb.q_cap = std::max<long long>(lb.q_cap, C.tree.nroots);
+    lb.q0.ensure(lb.q_cap);
+    lb.q1.ensure(lb.q_cap);
+    k_trav_init_forest<<<std::max(1, std::min(kNumSMs, div_up(C.tree.nroots, 128))), 128, 0, st>>>(
+        lb.q0.p, lb.cnt.p, C.tree.nd_cell.p, C.tree.nroots);
+  } else {
+    k_trav_init<<<1, 32, 0, st>>>(lb.q0.p, lb.cnt.p, C.prm.images, std::min<long long>(ncells, S.ncells));
+  }
   EXA_CHECK_LAUNCH();
   PairScan ps;
   ps.c.cell_b = C.tree.cell_b.p;

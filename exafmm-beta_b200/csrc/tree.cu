@@ -127,8 +127,7 @@ __global__ void k_bounds_final(const unsigned long long *enc, long long n, doubl
 }
 
 // bounds2box (build_tree.h:168-180): center, then half-width scaled by 1.00001.
-__global__ void k_box(const double *bounds, double *box) {
-  if (threadIdx.x != 0) return;
+__device__ __forceinline__ double4 box_of(const double *bounds) {
   double R = 0;
   double X[3];
   for (int d = 0; d < 3; d++) X[d] = (bounds[3 + d] + bounds[d]) / 2;
@@ -138,10 +137,16 @@ __global__ void k_box(const double *bounds, double *box) {
     double b = bounds[3 + d] - X[d];
     R = (R < b) ? b : R;
   }
-  box[0] = X[0];
-  box[1] = X[1];
-  box[2] = X[2];
-  box[3] = __dmul_rn(R, 1.00001);
+  return make_double4(X[0], X[1], X[2], __dmul_rn(R, 1.00001));
+}
+
+__global__ void k_box(const double *bounds, double *box) {
+  if (threadIdx.x != 0) return;
+  const double4 b = box_of(bounds);
+  box[0] = b.x;
+  box[1] = b.y;
+  box[2] = b.z;
+  box[3] = b.w;
 }
 
 __device__ __forceinline__ double level_half(double R0, int level) {
@@ -150,22 +155,24 @@ __device__ __forceinline__ double level_half(double R0, int level) {
 }
 
 // One octant digit per level from the reference's center recurrence.
+__device__ __forceinline__ unsigned long long octant_key(const double4 b, double cx, double cy, double cz, double R0) {
+  unsigned long long key = 0;
+#pragma unroll 1
+  for (int l = 0; l < kMaxLevels; l++) {
+    const int ox = b.x > cx, oy = b.y > cy, oz = b.z > cz;
+    key = (key << 3) | (unsigned long long)(ox | (oy << 1) | (oz << 2));
+    const double r = level_half(R0, l);
+    cx = __dadd_rn(cx, r * (ox ? 1.0 : -1.0));
+    cy = __dadd_rn(cy, r * (oy ? 1.0 : -1.0));
+    cz = __dadd_rn(cz, r * (oz ? 1.0 : -1.0));
+  }
+  return key;
+}
+
 __global__ void k_keys(const double4 *x, long long n, const double *box, unsigned long long *keys, int *vals) {
   const double R0 = box[3];
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const double4 b = x[i];
-    double cx = box[0], cy = box[1], cz = box[2];
-    unsigned long long key = 0;
-#pragma unroll 1
-    for (int l = 0; l < kMaxLevels; l++) {
-      const int ox = b.x > cx, oy = b.y > cy, oz = b.z > cz;
-      key = (key << 3) | (unsigned long long)(ox | (oy << 1) | (oz << 2));
-      const double r = level_half(R0, l);
-      cx = __dadd_rn(cx, r * (ox ? 1.0 : -1.0));
-      cy = __dadd_rn(cy, r * (oy ? 1.0 : -1.0));
-      cz = __dadd_rn(cz, r * (oz ? 1.0 : -1.0));
-    }
-    keys[i] = key;
+    keys[i] = octant_key(x[i], box[0], box[1], box[2], R0);
     vals[i] = (int)i;
   }
 }
@@ -213,10 +220,17 @@ struct TreeArgs {
   double4 *cell_x;
   int *cell_node;
   const double *box;
+  int *nd_sys;            // forest: node -> system (null: one system, box)
+  const double4 *sys_box;  // forest: X0, R0 per system
   long long node_cap, cell_cap;
   int ncrit;
   int *err;
 };
+
+// Root half-width of the system a node belongs to.
+__device__ __forceinline__ double node_R0(const TreeArgs &a, long long node) {
+  return a.nd_sys ? a.sys_box[a.nd_sys[node]].w : a.box[3];
+}
 
 // Eight threads per node: thread o finds where octant o ends.
 __global__ void k_expand(TreeArgs a, int level) {
@@ -281,7 +295,6 @@ __global__ void k_emit(TreeArgs a, int level) {
   const long long cnt = a.lvl[level], start = a.lvl[kMaxLevels + 1 + level];
   const long long nstart = a.lvl[kMaxLevels + 1 + level + 1];
   const long long total = cnt * 8;
-  const double R0 = a.box[3];
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ((total + 31) / 32) * 32;
        t += (long long)gridDim.x * blockDim.x) {
     const bool live = t < total;
@@ -308,7 +321,8 @@ __global__ void k_emit(TreeArgs a, int level) {
         atomicOr(a.err, kErrCellOverflow);
       } else {
         const double4 X = a.nd_x[node];
-        const double r = level_half(R0, level);
+        const double r = level_half(node_R0(a, node), level);
+        if (a.nd_sys) a.nd_sys[child] = a.nd_sys[node];
         a.nd_begin[child] = s;
         a.nd_count[child] = e - s;
         a.nd_x[child] = make_double4(__dadd_rn(X.x, r * ((o & 1) ? 1.0 : -1.0)),
@@ -340,10 +354,10 @@ __global__ void k_nnode(TreeArgs a, int level) {
 __global__ void k_cells(TreeArgs a, int level) {
   const long long cnt = a.lvl[level], start = a.lvl[kMaxLevels + 1 + level];
   const long long nstart = (level < kMaxLevels) ? a.lvl[kMaxLevels + 1 + level + 1] : 0;
-  const double R0 = a.box[3];
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cnt; i += (long long)gridDim.x * blockDim.x) {
     const long long node = start + i;
     if (node >= a.node_cap) continue;
+    const double R0 = node_R0(a, node);
     const int c = a.nd_cell[node];
     if (c < 0 || c >= a.cell_cap) {
       atomicOr(a.err, kErrCellOverflow);
@@ -370,12 +384,14 @@ __global__ void k_cells(TreeArgs a, int level) {
 }
 
 // Restore input order inside each leaf: rank each body by its caller index.
-__global__ void k_leaf_order(const int *nd_count, const int *nd_begin, const int *nd_nchild, const int *nd_nnode,
+__global__ void k_leaf_order(const int *nd_count, const int *nd_begin, const int *nd_nchild, const long long *lvl,
                              int *perm, int ncrit, long long node_cap) {
   extern __shared__ int sh[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int *buf = sh + warp * ncrit;
-  const long long total = nd_nnode[0] < node_cap ? nd_nnode[0] : node_cap;
+  long long total = 0;  // every node of every level (the level counts are clamped to the capacity)
+  for (int l = 0; l <= kMaxLevels; l++) total += lvl[l];
+  total = total < node_cap ? total : node_cap;
   const int wpb = blockDim.x >> 5;
   for (long long node = (long long)blockIdx.x * wpb + warp; node < total; node += (long long)gridDim.x * wpb) {
     if (nd_nchild[node] != 0) continue;
@@ -398,6 +414,191 @@ __global__ void k_gather(const double4 *x, const int *perm, long long n, double4
     out[i] = x[perm[i]];
 }
 
+// ---------------------------------------------------------------- forest of systems
+// Independent systems side by side: every kernel below takes one tile of at
+// most kForestTile bodies of one system (tile_sys, tile_beg) or one system, and
+// reproduces per system exactly what the one-system kernels above compute.
+
+__global__ void k_fb_init(unsigned long long *enc, long long words) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < words; i += (long long)gridDim.x * blockDim.x) {
+    const int t = (int)(i & 15);
+    enc[i] = (t < 3 || (t >= 6 && t < 9)) ? ~0ull : 0ull;
+  }
+}
+
+// k_bounds_estimate per system (body j of a system of n drifts n - 1 - j
+// times, its first body n times).
+__global__ void k_fb_estimate(const double4 *x, const int *tile_sys, const long long *tile_beg,
+                              const long long *sys_off, unsigned long long *enc) {
+  const int s = tile_sys[blockIdx.x];
+  const long long s0 = sys_off[s], n = sys_off[s + 1] - s0, b = tile_beg[blockIdx.x];
+  const long long e = min(b + (long long)kForestTile, s0 + n);
+  unsigned long long lo[3] = {~0ull, ~0ull, ~0ull}, hi[3] = {0, 0, 0}, amax = 0;
+  for (long long g = b + threadIdx.x; g < e; g += blockDim.x) {
+    const double4 q = x[g];
+    const double v[3] = {q.x, q.y, q.z};
+    const long long j = g - s0;
+    const double kc = (double)(j == 0 ? n : n - 1 - j) * 1e-5;
+    for (int d = 0; d < 3; d++) {
+      const unsigned long long a = order_enc(v[d] - kc), c = order_enc(v[d] + kc);
+      lo[d] = a < lo[d] ? a : lo[d];
+      hi[d] = c > hi[d] ? c : hi[d];
+      const unsigned long long ab = order_enc(fabs(v[d]));
+      amax = ab > amax ? ab : amax;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    for (int d = 0; d < 3; d++) {
+      const unsigned long long a = __shfl_xor_sync(0xffffffffu, lo[d], o);
+      const unsigned long long c = __shfl_xor_sync(0xffffffffu, hi[d], o);
+      lo[d] = a < lo[d] ? a : lo[d];
+      hi[d] = c > hi[d] ? c : hi[d];
+    }
+    const unsigned long long m = __shfl_xor_sync(0xffffffffu, amax, o);
+    amax = m > amax ? m : amax;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    unsigned long long *es = enc + 16 * (long long)s;
+    for (int d = 0; d < 3; d++) {
+      atomicMin(&es[6 + d], lo[d]);
+      atomicMax(&es[9 + d], hi[d]);
+    }
+    atomicMax(&es[12], amax);
+  }
+}
+
+// k_bounds_exact per system.
+__global__ void k_fb_exact(const double4 *x, const int *tile_sys, const long long *tile_beg,
+                           const long long *sys_off, unsigned long long *enc) {
+  const int s = tile_sys[blockIdx.x];
+  const long long s0 = sys_off[s], n = sys_off[s + 1] - s0, b = tile_beg[blockIdx.x];
+  const long long e = min(b + (long long)kForestTile, s0 + n);
+  unsigned long long *es = enc + 16 * (long long)s;
+  const double span = order_dec(es[12]) + (double)n * 1e-5;
+  const double B = (double)n * ldexp(1.0, ilogb(span > 1e-300 ? span : 1e-300) - 52) + 1e-300;
+  double elo[3], ehi[3];
+  for (int d = 0; d < 3; d++) {
+    elo[d] = order_dec(es[6 + d]) + 2.0 * B;
+    ehi[d] = order_dec(es[9 + d]) - 2.0 * B;
+  }
+  for (long long g = b + threadIdx.x; g < e; g += blockDim.x) {
+    const double4 q = x[g];
+    const double v[3] = {q.x, q.y, q.z};
+    const long long j = g - s0;
+    const long long k = (j == 0) ? n : n - 1 - j;
+    const double kc = (double)k * 1e-5;
+    for (int d = 0; d < 3; d++) {
+      if (v[d] - kc <= elo[d]) atomicMin(&es[d], order_enc(drift_down(v[d], k)));
+      if (v[d] + kc >= ehi[d]) atomicMax(&es[3 + d], order_enc(drift_up(v[d], k)));
+    }
+  }
+}
+
+// Bounds (k_bounds_final) and root box (bounds2box) of every system.
+__global__ void k_fb_final(const unsigned long long *enc, const long long *sys_off, int nsys, double *bounds,
+                           double4 *sys_box) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nsys; s += gridDim.x * blockDim.x) {
+    const long long n = sys_off[s + 1] - sys_off[s];
+    double b[6];
+    for (int t = 0; t < 6; t++) {
+      b[t] = (n > 0) ? order_dec(enc[16 * (long long)s + t]) : 0.0;
+      bounds[6 * (long long)s + t] = b[t];
+    }
+    sys_box[s] = box_of(b);
+  }
+}
+
+__global__ void k_fkeys(const double4 *x, const int *tile_sys, const long long *tile_beg, const long long *sys_off,
+                        const double4 *sys_box, unsigned long long *keys, int *vals) {
+  const int s = tile_sys[blockIdx.x];
+  const long long b = tile_beg[blockIdx.x], e = min(b + (long long)kForestTile, sys_off[s + 1]);
+  const double4 box = sys_box[s];
+  for (long long g = b + threadIdx.x; g < e; g += blockDim.x) {
+    keys[g] = octant_key(x[g], box.x, box.y, box.z, box.w);
+    vals[g] = (int)g;
+  }
+}
+
+// System of each key-sorted body (bodies of system s are [sys_off[s], sys_off[s+1]) in caller order).
+__global__ void k_fsys(const int *perm, long long n, const long long *sys_off, int nsys, unsigned *skey, int *idx) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const long long c = perm[i];
+    int lo = 0, hi = nsys - 1;  // last s with sys_off[s] <= c
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (sys_off[mid] <= c) lo = mid;
+      else hi = mid - 1;
+    }
+    skey[i] = (unsigned)lo;
+    idx[i] = (int)i;
+  }
+}
+
+__global__ void k_fgather(const unsigned long long *keys_in, const int *perm_in, const int *idx, long long n,
+                          unsigned long long *keys_out, int *perm_out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int j = idx[i];
+    keys_out[i] = keys_in[j];
+    perm_out[i] = perm_in[j];
+  }
+}
+
+// One root node per non-empty system, in system order, at level 0.
+__global__ void k_froot(int nroots, const int *root_sys, const long long *sys_off, const double4 *sys_box,
+                        long long *lvl, int *nd_begin, int *nd_count, double4 *nd_x, int *nd_sys) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    for (int l = 0; l <= kMaxLevels; l++) {
+      lvl[l] = 0;
+      lvl[kMaxLevels + 1 + l] = 0;
+    }
+    lvl[0] = nroots;
+  }
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nroots; k += gridDim.x * blockDim.x) {
+    const int s = root_sys[k];
+    const double4 X = sys_box[s];
+    nd_begin[k] = (int)sys_off[s];
+    nd_count[k] = (int)(sys_off[s + 1] - sys_off[s]);
+    nd_x[k] = make_double4(X.x, X.y, X.z, 0.0);
+    nd_sys[k] = s;
+  }
+}
+
+// First cell of every system's tree: an exclusive scan of the root subtree
+// sizes in system order (one block).  A root cell is its own parent, as cell 0
+// is in the reference's layout, and its children start right after it.
+__global__ void __launch_bounds__(1024) k_froot_cells(int nsys, const int *sys_root, const int *nd_nnode,
+                                                      int *nd_cell, int *nd_pcell, int *nd_ichild, int *sys_cell,
+                                                      long long cell_cap, int *err) {
+  __shared__ long long part[1024];
+  const int t = threadIdx.x, per = (nsys + 1023) / 1024;
+  const int b = t * per, e = min(nsys, b + per);
+  long long sum = 0;
+  for (int s = b; s < e; s++) sum += sys_root[s] >= 0 ? nd_nnode[sys_root[s]] : 0;
+  part[t] = sum;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const long long v = t >= o ? part[t - o] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  long long base = part[t] - sum;
+  for (int s = b; s < e; s++) {
+    sys_cell[s] = (int)base;
+    const int k = sys_root[s];
+    if (k >= 0) {
+      nd_cell[k] = (int)base;
+      nd_pcell[k] = (int)base;
+      nd_ichild[k] = (int)base + 1;
+      base += nd_nnode[k];
+    }
+  }
+  if (t == 1023) {
+    sys_cell[nsys] = (int)part[1023];
+    if (part[1023] > cell_cap) atomicOr(err, kErrCellOverflow);
+  }
+}
+
 int grid_for(long long n, int block) {
   long long g = (n + block - 1) / block;
   if (g < 1) g = 1;
@@ -407,8 +608,33 @@ int grid_for(long long n, int block) {
 
 }  // namespace
 
+// Per-system bounds and root boxes of a forest (BoundBox::getBounds and
+// bounds2box of every system on its own).
+static void forest_bounds(Context &C) {
+  TreeBufs &T = C.tree;
+  cudaStream_t st = C.stream;
+  const long long words = 16LL * T.nsys;
+  T.sys_enc.ensure(words);
+  T.sys_bounds.ensure(6LL * T.nsys);
+  T.sys_box.ensure(T.nsys);
+  k_fb_init<<<grid_for(words, 256), 256, 0, st>>>(T.sys_enc.p, words);
+  EXA_CHECK_LAUNCH();
+  if (T.ntiles > 0) {
+    k_fb_estimate<<<(unsigned)T.ntiles, 256, 0, st>>>(T.xyzq.p, T.tile_sys.p, T.tile_beg.p, T.sys_off.p, T.sys_enc.p);
+    EXA_CHECK_LAUNCH();
+    k_fb_exact<<<(unsigned)T.ntiles, 256, 0, st>>>(T.xyzq.p, T.tile_sys.p, T.tile_beg.p, T.sys_off.p, T.sys_enc.p);
+    EXA_CHECK_LAUNCH();
+  }
+  k_fb_final<<<grid_for(T.nsys, 128), 128, 0, st>>>(T.sys_enc.p, T.sys_off.p, T.nsys, T.sys_bounds.p, T.sys_box.p);
+  EXA_CHECK_LAUNCH();
+}
+
 void compute_bounds(Context &C) {
   TreeBufs &T = C.tree;
+  if (T.nsys) {
+    forest_bounds(C);
+    return;
+  }
   T.bounds.ensure(6);
   T.bounds_enc.ensure(16);
   k_bounds_init<<<1, 32, 0, C.stream>>>(T.bounds_enc.p);
@@ -464,26 +690,62 @@ void build_tree(Context &C) {
   TreeBufs &T = C.tree;
   const long long n = T.n;
   const int ncrit = C.prm.ncrit;
+  const bool forest = T.nsys > 0;
   cudaStream_t st = C.stream;
   T.box.ensure(4);
   T.lvl.ensure(2 * (kMaxLevels + 1) + 4);
   // Node capacity for this system (a reused context may receive a larger one);
   // deeper trees than this estimate overflow, are flagged and rebuilt larger.
-  const long long est = 1024 + 8 * 4 * (n / (ncrit + 1) + 1);
+  const long long est = 1024 + 8 * 4 * (n / (ncrit + 1) + 1) + 8LL * T.nroots;
   if (est > T.node_cap) ensure_nodes(T, est);
   T.keys.ensure(n);
   T.keys_alt.ensure(n);
   T.perm.ensure(n);
   T.perm_alt.ensure(n);
   T.xyzq_tree.ensure(n);
-  k_box<<<1, 32, 0, st>>>(T.bounds.p, T.box.p);
-  EXA_CHECK_LAUNCH();
-  if (n > 0) {
+  if (forest) {
+    T.nd_sys.ensure(T.node_cap);
+    T.sys_cell.ensure(T.nsys + 1);
+  } else {
+    k_box<<<1, 32, 0, st>>>(T.bounds.p, T.box.p);
+    EXA_CHECK_LAUNCH();
+  }
+  if (n > 0 && !forest) {
     k_keys<<<grid_for(n, 256), 256, 0, st>>>(T.xyzq.p, n, T.box.p, T.keys.p, T.perm.p);
     EXA_CHECK_LAUNCH();
     bool alt = radix_sort_u64((uint64_t *)T.keys.p, T.perm.p, (uint64_t *)T.keys_alt.p, T.perm_alt.p, n, 0,
                               3 * kMaxLevels, C.sort, C.err.p, st);
     if (alt) {
+      std::swap(T.keys.p, T.keys_alt.p);
+      std::swap(T.perm.p, T.perm_alt.p);
+    }
+  } else if (n > 0) {
+    // keys of every body in its own system's box, sorted; then a stable pass
+    // on the system makes the order (system, key), each system's bodies in
+    // exactly the order its solo tree gives them
+    k_fkeys<<<(unsigned)T.ntiles, 256, 0, st>>>(T.xyzq.p, T.tile_sys.p, T.tile_beg.p, T.sys_off.p, T.sys_box.p,
+                                                T.keys.p, T.perm.p);
+    EXA_CHECK_LAUNCH();
+    bool alt = radix_sort_u64((uint64_t *)T.keys.p, T.perm.p, (uint64_t *)T.keys_alt.p, T.perm_alt.p, n, 0,
+                              3 * kMaxLevels, C.sort, C.err.p, st);
+    if (alt) {
+      std::swap(T.keys.p, T.keys_alt.p);
+      std::swap(T.perm.p, T.perm_alt.p);
+    }
+    if (T.nsys > 1) {
+      T.fs_key.ensure(n);
+      T.fs_key_alt.ensure(n);
+      T.fs_idx.ensure(n);
+      T.fs_idx_alt.ensure(n);
+      k_fsys<<<grid_for(n, 256), 256, 0, st>>>(T.perm.p, n, T.sys_off.p, T.nsys, T.fs_key.p, T.fs_idx.p);
+      EXA_CHECK_LAUNCH();
+      int bits = 0;
+      while ((1LL << bits) <= (long long)(T.nsys - 1)) bits++;
+      const bool alt2 = radix_sort_u32(T.fs_key.p, T.fs_idx.p, T.fs_key_alt.p, T.fs_idx_alt.p, n, 0, bits, C.sort,
+                                       C.err.p, st);
+      k_fgather<<<grid_for(n, 256), 256, 0, st>>>(T.keys.p, T.perm.p, alt2 ? T.fs_idx_alt.p : T.fs_idx.p, n,
+                                                  T.keys_alt.p, T.perm_alt.p);
+      EXA_CHECK_LAUNCH();
       std::swap(T.keys.p, T.keys_alt.p);
       std::swap(T.perm.p, T.perm_alt.p);
     }
@@ -505,12 +767,19 @@ void build_tree(Context &C) {
   a.cell_x = T.cell_x.p;
   a.cell_node = T.cell_node.p;
   a.box = T.box.p;
+  a.nd_sys = forest ? T.nd_sys.p : nullptr;
+  a.sys_box = forest ? T.sys_box.p : nullptr;
   a.node_cap = T.node_cap;
   a.cell_cap = T.cell_cap;
   a.ncrit = ncrit;
   a.err = C.err.p;
-  k_tree_root<<<1, 32, 0, st>>>(n, T.lvl.p, T.nd_begin.p, T.nd_count.p, T.nd_x.p, T.box.p, T.nd_cell.p,
-                                T.nd_pcell.p, T.nd_ichild.p);
+  if (forest) {
+    k_froot<<<grid_for(T.nroots, 128), 128, 0, st>>>(T.nroots, T.root_sys.p, T.sys_off.p, T.sys_box.p, T.lvl.p,
+                                                     T.nd_begin.p, T.nd_count.p, T.nd_x.p, T.nd_sys.p);
+  } else {
+    k_tree_root<<<1, 32, 0, st>>>(n, T.lvl.p, T.nd_begin.p, T.nd_count.p, T.nd_x.p, T.box.p, T.nd_cell.p,
+                                  T.nd_pcell.p, T.nd_ichild.p);
+  }
   EXA_CHECK_LAUNCH();
   // per-level kernels: eight threads per node at most node_cap nodes
   const int node_grid = (int)std::max<long long>(1, std::min<long long>(kNumSMs * 4, (8 * T.node_cap + 255) / 256));
@@ -532,6 +801,11 @@ void build_tree(Context &C) {
     k_nnode<<<node_grid, 256, 0, st>>>(a, l);
     EXA_CHECK_LAUNCH();
   }
+  if (forest) {
+    k_froot_cells<<<1, 1024, 0, st>>>(T.nsys, T.sys_root.p, T.nd_nnode.p, T.nd_cell.p, T.nd_pcell.p, T.nd_ichild.p,
+                                      T.sys_cell.p, T.cell_cap, C.err.p);
+    EXA_CHECK_LAUNCH();
+  }
   for (int l = 0; l <= kMaxLevels; l++) {
     k_cells<<<node_grid, 256, 0, st>>>(a, l);
     EXA_CHECK_LAUNCH();
@@ -539,7 +813,7 @@ void build_tree(Context &C) {
   if (n > 0) {
     const int wpb = 4;
     k_leaf_order<<<kNumSMs * 8, 32 * wpb, wpb * ncrit * sizeof(int), st>>>(T.nd_count.p, T.nd_begin.p,
-                                                                           T.nd_nchild.p, T.nd_nnode.p, T.perm.p,
+                                                                           T.nd_nchild.p, T.lvl.p, T.perm.p,
                                                                            ncrit, T.node_cap);
     EXA_CHECK_LAUNCH();
     k_gather<<<grid_for(n, 256), 256, 0, st>>>(T.xyzq.p, T.perm.p, n, T.xyzq_tree.p);
@@ -551,9 +825,16 @@ void sync_tree(Context &C) {
   TreeBufs &T = C.tree;
   EXA_CUDA(cudaMemcpyAsync(T.lvl_host, T.lvl.p, sizeof(T.lvl_host), cudaMemcpyDeviceToHost, C.stream));
   int nn = 0;
-  if (T.n > 0) EXA_CUDA(cudaMemcpyAsync(&nn, T.nd_nnode.p, sizeof(int), cudaMemcpyDeviceToHost, C.stream));
+  if (T.nsys) {
+    T.sys_cell_host.assign(T.nsys + 1, 0);
+    EXA_CUDA(cudaMemcpyAsync(T.sys_cell_host.data(), T.sys_cell.p, (T.nsys + 1) * sizeof(int),
+                             cudaMemcpyDeviceToHost, C.stream));
+  } else if (T.n > 0) {
+    EXA_CUDA(cudaMemcpyAsync(&nn, T.nd_nnode.p, sizeof(int), cudaMemcpyDeviceToHost, C.stream));
+  }
   EXA_CUDA(cudaMemcpyAsync(C.err_host, C.err.p, sizeof(int), cudaMemcpyDeviceToHost, C.stream));
   EXA_CUDA(cudaStreamSynchronize(C.stream));
+  if (T.nsys) nn = T.sys_cell_host[T.nsys];
   T.ncells = (T.n > 0) ? nn : 0;
   T.depth = 0;
   for (int l = 0; l <= kMaxLevels; l++)

@@ -82,6 +82,28 @@ int exafmm_get_source_cells(exafmm_ctx *ctx, long long *ncells, int *ints, doubl
 int exafmm_set_bodies(exafmm_ctx *ctx, const double *xyzq, long long n);
 int exafmm_set_bodies_device(exafmm_ctx *ctx, const double *d_xyzq, long long n);
 
+/* A forest of independent systems solved together (no counterpart in the
+ * reference, which solves one system per process, examples/fmm.cxx:163-179).
+ * count systems, system s holding n[s] bodies; xyzq holds them concatenated in
+ * system order (sum n[s] x 4 doubles, caller order inside each system).  The
+ * next build / solve gives every system its own bounds (BoundBox::getBounds),
+ * tree (BuildTree::buildTree), lists (Traversal::traverse from its own root
+ * pair) and expansions, exactly as a solo solve of that system gives them, but
+ * every phase runs once for all systems: one set of launches and host read
+ * backs per forest, not per system.  Results (exafmm_get_results) are
+ * concatenated the same way.  Cells of system s are [cell_base[s],
+ * cell_base[s+1]) of the context's cell table, in the layout of its solo tree
+ * shifted by cell_base[s]; IBODY and the permutation are offsets into the
+ * concatenated bodies.  Free space only (images = 0), sources == targets;
+ * empty systems are allowed.  exafmm_set_bodies returns to one system.  The
+ * _device form takes the concatenated bodies as a device pointer. */
+int exafmm_set_systems(exafmm_ctx *ctx, int count, const long long *n, const double *xyzq);
+int exafmm_set_systems_device(exafmm_ctx *ctx, int count, const long long *n, const double *d_xyzq);
+/* Layout of a forest after its build: cell_base (count + 1), body_off
+ * (count + 1) and each system's bounds (count x 6, as exafmm_get_bounds);
+ * any output may be NULL (body_off is known before a build). */
+int exafmm_get_systems(exafmm_ctx *ctx, long long *cell_base, long long *body_off, double *bounds);
+
 /* BoundBox::getBounds(Bodies&) (include/bound_box.h:11-25), including its
  * sequential 1e-5 drift, evaluated on the device in closed form; with separate
  * sources, extended by them as getBounds(jbodies, bounds) does
