@@ -242,6 +242,10 @@ def main():
                          "serve: Poisson request trace through the request server; periodic: water box "
                          "with images=3 against Ewald")
     ap.add_argument("--workers", type=int, default=16, help="contexts (streams) of the batch / serve runtime")
+    ap.add_argument("--buckets", type=int, default=3,
+                    help="batch: size groups solved as one forest each (0: one context per system)")
+    ap.add_argument("--min-level", type=int, default=None,
+                    help="mixed form: lowest target level of the FP32 M2L (batch default 2, solve default 4)")
     args = ap.parse_args()
     if check_world(args.gpus) == "spawn":
         r = subprocess.run(["timeout", "-k", "60", "3600"] + torchrun_command(sys.argv[1:], args.gpus, _free_port()))
@@ -440,20 +444,33 @@ SERVE = dict(name="serve_poisson_p6_8_10", count=60, lo=1000, hi=1_000_000, thet
              budget=150e9, repeat_frac=0.2, repeat_steps=50, loads=(0.5, 0.8))
 
 
-def _three_way(ex, datasets, xs, mixed, plain, sample=256, take=8):
-    """rel-L2 (pot, acc) of mixed vs direct, plain vs direct, mixed vs plain on `take`
-    systems spread over the sizes, each on `sample` strided targets."""
+def _three_way(ex, datasets, xs, mixed, plain, sample=256, take=None):
+    """rel-L2 (pot, acc) of mixed vs direct, plain vs direct and mixed vs plain per
+    system (every system, or `take` spread over the sizes), direct on `sample`
+    strided targets of each; returns the per-system lists and their maxima."""
     order = np.argsort([len(x) for x in xs])
-    pick = order[np.linspace(0, len(xs) - 1, min(take, len(xs))).astype(int)]
-    acc = {k: [] for k in ("mixed_vs_direct", "plain_vs_direct", "mixed_vs_plain")}
+    pick = order if take is None else order[np.linspace(0, len(xs) - 1, min(take, len(xs))).astype(int)]
+    per = {k: [] for k in ("mixed_vs_direct", "plain_vs_direct", "mixed_vs_plain")}
     for i in pick:
         x = xs[i]
+        if not len(x):
+            continue
         idx = datasets.strided_sample(len(x), sample)
         d = ex.direct(x[idx], x)
         for key, a, b in (("mixed_vs_direct", mixed[i][idx], d), ("plain_vs_direct", plain[i][idx], d),
                           ("mixed_vs_plain", mixed[i], plain[i])):
-            acc[key].append((datasets.rel_l2(a[:, 0], b[:, 0]), datasets.rel_l2(a[:, 1:], b[:, 1:])))
-    return {k: {"pot_max": max(v[0] for v in vals), "acc_max": max(v[1] for v in vals)} for k, vals in acc.items()}
+            per[key].append((int(i), datasets.rel_l2(a[:, 0], b[:, 0]), datasets.rel_l2(a[:, 1:], b[:, 1:])))
+    out = {}
+    for k, vals in per.items():
+        pot = np.array([v[1] for v in vals])
+        acc = np.array([v[2] for v in vals])
+        out[k] = {"pot_max": float(pot.max()), "pot_median": float(np.median(pot)),
+                  "acc_max": float(acc.max()), "acc_median": float(np.median(acc)),
+                  "pot_worst_system": int(vals[int(pot.argmax())][0])}
+    out["systems"] = len(per["mixed_vs_plain"])
+    out["direct_sample_per_system"] = sample
+    out["per_system_pot"] = {k: [float(v[1]) for v in vals] for k, vals in per.items()}
+    return out
 
 
 def _batch_cpu_baseline(xs, threads):
@@ -514,61 +531,139 @@ def run_runtime_workload(args):
 
 
 def _run_batch(args, pkg, datasets, workloads, prec, rank, world, local_rank):
+    """Batched uneven systems: each step solves all 512 systems, grouped by size
+    into `--buckets` forests (one context and stream each, running concurrently).
+    value: bodies resident on the device, timed by the batch's own device events
+    (from an event every forest's stream waits on to the last forest's copy out);
+    e2e: the same call with pinned host buffers, host clock around it."""
     import torch
     cfg = BATCH
     xs = workloads.batch_systems(cfg["count"], cfg["lo"], cfg["hi"], seed0=1000 + 100000 * rank)
-    nbodies = sum(len(x) for x in xs)
-    outs = [np.zeros((len(x), 4)) for x in xs]
-    b = pkg.Batch(P=cfg["P"], theta=cfg["theta"], ncrit=cfg["ncrit"], nspawn=cfg["nspawn"], precision=prec,
-                  device=local_rank, workers=args.workers)
-    b.autotune(True)   # the first warm-up step tunes ncrit per size class, then the table is frozen
-    for w in range(max(1, args.warmup)):
-        b.solve(xs, outs)
-        if w == 0:
-            b.autotune(False)
+    sizes = [len(x) for x in xs]
+    nbodies = sum(sizes)
+    min_level = 2 if args.min_level is None else args.min_level
+
+    def make(precision):
+        b = pkg.Batch(P=cfg["P"], theta=cfg["theta"], ncrit=cfg["ncrit"], nspawn=cfg["nspawn"], precision=precision,
+                      device=local_rank, workers=args.workers, forest=args.buckets)
+        if precision == pkg.MIXED:
+            b.set_mixed_policy(m2l_fp32=args.m2l_policy, min_level=min_level)
+        return b
+
+    dev_in = [torch.from_numpy(x).to(f"cuda:{local_rank}") for x in xs]
+    dev_out = [torch.empty_like(d) for d in dev_in]
+    in_ptrs, out_ptrs = [d.data_ptr() for d in dev_in], [d.data_ptr() for d in dev_out]
+
+    pool_out = [np.zeros_like(x) for x in xs]
+
+    def step(b):
+        if args.buckets > 0:
+            b.solve_device(sizes, in_ptrs, out_ptrs)
+            return b.elapsed_ms()
+        b.solve(xs, pool_out)  # one context per system takes host buffers
+        for d, o in zip(dev_out, pool_out):
+            d.copy_(torch.from_numpy(o))
+        return 0.0
+
+    b = make(prec)
+    forest = args.buckets > 0
+    if forest:  # the tuner tries one ncrit per call: three untimed tuning calls, then the table is frozen
+        b.autotune(True)
+        for _ in range(3):
+            step(b)
+        b.autotune(False)
+        warm = max(1, args.warmup - 3)
+    else:
+        b.autotune(True)
+        step(b)
+        b.autotune(False)
+        warm = max(1, args.warmup - 1)
+    for _ in range(warm):
+        step(b)
     torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
     launches0 = pkg.launch_count()
+    dev_ms = 0.0
     with ClockSampler(local_rank) as clocks:
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            b.solve(xs, outs)
+            dev_ms += step(b)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
     clk = clocks.summary()
     launches = pkg.launch_count() - launches0
-    dev_ms = float(b.times(len(xs)).sum())
+    if not forest:
+        dev_ms = 1e3 * dt  # one context per system: many streams, host clock around each call
+    group, group_ncrit = b.buckets(len(xs)) if forest else (np.zeros(len(xs), dtype=int), np.array([]))
+    mixed_out = [d.cpu().numpy() for d in dev_out]
+
+    # e2e: the public call from pinned host buffers, copies inside the timed region
+    hin = [torch.from_numpy(x).pin_memory() for x in xs]
+    hout = [torch.empty_like(h).pin_memory() for h in hin]
+    hin_ptrs, hout_ptrs = [h.data_ptr() for h in hin], [h.data_ptr() for h in hout]
+    hin_np, hout_np = [h.numpy() for h in hin], [h.numpy() for h in hout]
+
+    def host_call():
+        if forest:
+            b.solve_device(sizes, hin_ptrs, hout_ptrs)
+        else:
+            b.solve(hin_np, hout_np)
+
+    host_call()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        host_call()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    assert all(np.array_equal(m, h) for m, h in zip(mixed_out, hout_np))
+
+    value = nbodies * args.steps / (dev_ms / 1e3)
     line = {
         "metric": "batched FMM bodies/s (512 systems per step, N log-uniform [2e3, 2e5], P=10, theta=0.4)",
-        "value": nbodies * args.steps / dt, "unit": "bodies/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
+        "value": value, "unit": "bodies/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if prec == pkg.FP64 else "f32+kahan", "data": "synthetic",
         "config": {"workload": cfg["name"], "systems": cfg["count"], "bodies_per_step": nbodies,
                    "distribution": "even systems uniform in [-1,1]^3, odd on the unit sphere; q U[-1,1]",
-                   "P": cfg["P"], "theta": cfg["theta"], "ncrit_table": b.ncrit_table(), "workers": args.workers,
+                   "P": cfg["P"], "theta": cfg["theta"], "forest_groups": int(len(group_ncrit)),
+                   "group_ncrit": [int(v) for v in group_ncrit], "ncrit_table": b.ncrit_table(),
+                   "group_bodies": [int(sum(n for n, gi in zip(sizes, group) if gi == k))
+                                    for k in range(len(group_ncrit))],
+                   "mixed_min_level": min_level if prec == pkg.MIXED else None,
                    "precision": args.precision, "parallelism": f"replicas{world}",
-                   "timing": "host wall clock around each batch call, device synchronized on both sides "
-                             "(host buffers in and out, so value is end to end)",
-                   "l2": "each step streams 0.7 GB of bodies in and results out (larger than L2)"},
-        "e2e": {"value": nbodies * args.steps / dt, "unit": "bodies/s", "h2d_bytes_per_step": nbodies * 32,
-                "d2h_bytes_per_step": nbodies * 32},
-        "device_ms_per_step": dev_ms, "concurrency": dev_ms / (1e3 * dt / args.steps),
+                   "timing": ("device events of the batch call: an event every forest's stream waits on, to "
+                              "the last forest's results copied out" if forest else
+                              "host clock around each call, device synchronized on both sides"),
+                   "l2": "each step reads 0.7 GB of bodies and writes 0.7 GB of results (larger than L2)"},
+        "e2e": {"value": nbodies * args.steps / e2e_s, "unit": "bodies/s", "h2d_bytes_per_step": nbodies * 32,
+                "d2h_bytes_per_step": nbodies * 32,
+                "timing": "host clock around each call from pinned host buffers, device synchronized on both sides"},
         "gpu_launches": int(launches), "clocks": clk, "roofline": None,
-        "_time": dt, "_units": nbodies * args.steps,
+        "_time": dev_ms / 1e3, "_units": nbodies * args.steps,
     }
     if not args.no_plain and prec == pkg.MIXED:
-        bp = pkg.Batch(P=cfg["P"], theta=cfg["theta"], ncrit=cfg["ncrit"], nspawn=cfg["nspawn"],
-                       precision=pkg.FP64, device=local_rank, workers=args.workers)
+        bp = make(pkg.FP64)
         bp.set_ncrit_table(b.ncrit_table())  # the same trees, so mixed vs plain is precision only
-        plain = [np.zeros((len(x), 4)) for x in xs]
-        bp.solve(xs, plain)
+        step(bp)
         torch.cuda.synchronize()
+        kp = max(1, min(args.steps, 3))
+        tp = 0.0
         t0 = time.perf_counter()
-        bp.solve(xs, plain)
+        for _ in range(kp):
+            tp += step(bp)
         torch.cuda.synchronize()
-        tp = time.perf_counter() - t0
-        line["plain_fp64"] = {"value": nbodies / tp, "unit": "bodies/s", "ms_per_step": 1e3 * tp,
-                              "speedup_of_mixed": (nbodies * args.steps / dt) / (nbodies / tp),
-                              "rel_l2": _three_way(pkg, datasets, xs, outs, plain)}
+        if not forest:
+            tp = 1e3 * (time.perf_counter() - t0)
+        plain = [d.cpu().numpy() for d in dev_out]
+        plain_value = nbodies * kp / (tp / 1e3)
+        tw = _three_way(pkg, datasets, xs, mixed_out, plain)
+        per = tw.pop("per_system_pot")
+        line["plain_fp64"] = {"value": plain_value, "unit": "bodies/s", "ms_per_step": tp / kp,
+                              "speedup_of_mixed": value / plain_value, "rel_l2": tw}
+        line["per_system_rel_l2_pot"] = {k: [float(f"{v:.3e}") for v in vals] for k, vals in per.items()}
         bp.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = _batch_cpu_baseline(xs, os.cpu_count() or 1)

@@ -114,6 +114,11 @@ def lib() -> ctypes.CDLL:
         "exafmm_batch_autotune": (_c_int, [_vp, _c_int]),
         "exafmm_batch_ncrit_table": (_c_int, [_vp, _vp, _c_int]),
         "exafmm_batch_set_ncrit_table": (_c_int, [_vp, _vp, _c_int]),
+        "exafmm_batch_set_forest": (_c_int, [_vp, _c_int]),
+        "exafmm_batch_set_mixed_policy": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int]),
+        "exafmm_batch_elapsed": (_c_int, [_vp, _vp]),
+        "exafmm_batch_buckets": (_c_int, [_vp, _vp, _vp, _c_int]),
+        "exafmm_forest_buckets": (_c_int, [_c_int, _vp, _c_int, _vp]),
         "exafmm_server_create": (_c_int, [ctypes.POINTER(_vp), _c_int, _c_int, _c_double]),
         "exafmm_server_destroy": (_c_int, [_vp]),
         "exafmm_server_submit": (_c_int, [_vp, _vp, _c_ll, _vp, _c_int, _c_double, _c_int, _c_int, _c_int,
@@ -135,6 +140,8 @@ def lib() -> ctypes.CDLL:
         "exafmm_set_systems": (_c_int, [_vp, _c_int, _vp, _vp]),
         "exafmm_set_systems_device": (_c_int, [_vp, _c_int, _vp, _vp]),
         "exafmm_get_systems": (_c_int, [_vp, _vp, _vp, _vp]),
+        "exafmm_set_systems_list": (_c_int, [_vp, _c_int, _vp, _vp]),
+        "exafmm_get_results_list": (_c_int, [_vp, _vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -266,6 +273,36 @@ class Fmm:
         self.n, self.nsys = int(sizes.sum()), len(sizes)
         self._sizes = sizes
         self._check(lib().exafmm_set_systems_device(self._h, self.nsys, _p(sizes), _vp(ptr)))
+
+    def set_systems_list(self, systems):
+        """The same forest from one array per system (no concatenation on the host):
+        numpy arrays, or (device pointer, n) pairs."""
+        sizes, ptrs, keep = [], [], []
+        for x in systems:
+            if isinstance(x, tuple):
+                ptrs.append(int(x[0]))
+                sizes.append(int(x[1]))
+            else:
+                a = _f64(x, 4)
+                keep.append(a)
+                ptrs.append(a.ctypes.data if len(a) else 0)
+                sizes.append(len(a))
+        k = len(sizes)
+        self._sizes = np.asarray(sizes, dtype=np.int64)
+        self.n, self.nsys = int(self._sizes.sum()), k
+        n = (_c_ll * max(1, k))(*sizes)
+        px = (_vp * max(1, k))(*[p or None for p in ptrs])
+        self._check(lib().exafmm_set_systems_list(self._h, k, n, px))
+
+    def system_results_list(self, outs=None) -> list:
+        """Per-system results copied straight into `outs` (numpy arrays, or device
+        pointers), one copy per system."""
+        if outs is None:
+            outs = [np.zeros((int(k), 4)) for k in self._sizes]
+        ptrs = [o if isinstance(o, int) else (o.ctypes.data if len(o) else 0) for o in outs]
+        po = (_vp * max(1, len(ptrs)))(*[p or None for p in ptrs])
+        self._check(lib().exafmm_get_results_list(self._h, po))
+        return outs
 
     def systems(self) -> dict:
         """Forest layout after a build: cell_base and body_off (nsys + 1 each), bounds (nsys, 6)."""
@@ -487,12 +524,38 @@ class Batch:
     """Many independent systems per call, on a pool of solve contexts (one host
     thread and CUDA stream each)."""
 
-    def __init__(self, P=10, theta=0.4, ncrit=64, nspawn=5000, precision=FP64, device=-1, workers=8):
+    def __init__(self, P=10, theta=0.4, ncrit=64, nspawn=5000, precision=FP64, device=-1, workers=8, forest=0):
         h = _vp()
         rc = lib().exafmm_batch_create(ctypes.byref(h), P, theta, ncrit, nspawn, precision, device, workers)
         if rc != 0:
             raise FmmError(f"exafmm_batch_create failed ({rc})")
         self._h = h
+        if forest:
+            self.set_forest(forest)
+
+    def set_forest(self, buckets: int):
+        """buckets > 0: each call's systems are solved as at most `buckets` forests
+        (groups of whole size classes, one context each); 0: one system per context."""
+        if lib().exafmm_batch_set_forest(self._h, int(buckets)) != 0:
+            raise FmmError("invalid forest bucket count")
+
+    def set_mixed_policy(self, m2l_fp32=1, p2p_fp32=True, min_level=4, max_dl=3):
+        """Fmm.set_mixed_policy for every context of the batch."""
+        if lib().exafmm_batch_set_mixed_policy(self._h, int(m2l_fp32), int(p2p_fp32), min_level, max_dl) != 0:
+            raise FmmError("invalid mixed policy")
+
+    def elapsed_ms(self) -> float:
+        """Forest mode: device time of the last call (first copy in to last copy out)."""
+        v = _c_double()
+        lib().exafmm_batch_elapsed(self._h, ctypes.byref(v))
+        return v.value
+
+    def buckets(self, count: int):
+        """Forest mode: (group of each system, ncrit of each group) of the last call."""
+        of = np.zeros(max(1, count), dtype=np.int32)
+        nc = np.zeros(64, dtype=np.int32)
+        k = lib().exafmm_batch_buckets(self._h, _p(of), _p(nc), 64)
+        return of[:count], nc[:max(0, k)]
 
     def close(self):
         if getattr(self, "_h", None):
@@ -514,6 +577,16 @@ class Batch:
         if lib().exafmm_batch_set_ncrit_table(self._h, pairs, len(table)) != 0:
             raise FmmError("invalid ncrit table")
 
+    def solve_device(self, sizes, in_ptrs, out_ptrs):
+        """Forest mode with device memory: system i's n_i x 4 doubles at in_ptrs[i],
+        its results to out_ptrs[i]."""
+        k = len(sizes)
+        n = (_c_ll * max(1, k))(*[int(v) for v in sizes])
+        px = (_vp * max(1, k))(*[int(p) or None for p in in_ptrs])
+        po = (_vp * max(1, k))(*[int(p) or None for p in out_ptrs])
+        if lib().exafmm_batch_solve(self._h, k, n, px, po) != 0:
+            raise FmmError(lib().exafmm_batch_error(self._h).decode())
+
     def solve(self, systems, outs=None):
         """systems: list of (n_i, 4) float64 arrays; returns the list of (n_i, 4) results."""
         xs = [_f64(x, 4) for x in systems]
@@ -533,6 +606,16 @@ class Batch:
         t = np.zeros(count)
         lib().exafmm_batch_times(self._h, _p(t))
         return t
+
+
+def forest_buckets(sizes, buckets: int) -> np.ndarray:
+    """The batch's forest grouping of systems of these sizes (host only)."""
+    n = np.ascontiguousarray(sizes, dtype=np.int64)
+    out = np.zeros(max(1, len(n)), dtype=np.int32)
+    k = lib().exafmm_forest_buckets(len(n), _p(n), int(buckets), _p(out))
+    if k < 0:
+        raise FmmError("invalid forest grouping input")
+    return out[:len(n)]
 
 
 class Server:

@@ -160,7 +160,10 @@ struct Engine {
   // A forest of count independent systems, bodies concatenated in system
   // order (system s: n[s] bodies).  Every system gets its own bounds, tree,
   // lists and expansions, as a solo solve of it would; they run together.
-  void set_systems(int count, const long long *n, const double *xyzq, cudaMemcpyKind kind) {
+  // parts (optional): one pointer per system instead of the concatenation,
+  // host or device memory (copied with cudaMemcpyDefault, one copy each).
+  void set_systems(int count, const long long *n, const double *xyzq, cudaMemcpyKind kind,
+                   const double *const *parts = nullptr) {
     if (count < 1) throw std::runtime_error("a forest needs at least one system");
     if (!n) throw std::runtime_error("null system sizes");
     if (jsrc) throw std::runtime_error("a forest of systems cannot have separate sources");
@@ -186,7 +189,7 @@ struct Engine {
     const long long total = off[count];
     if (T.nsys == count && T.sys_off_host == off) {  // same layout as before: only the bodies change
       T.n = total;
-      if (total) EXA_CUDA(cudaMemcpyAsync(T.xyzq.p, xyzq, total * sizeof(double4), kind, C.stream));
+      copy_systems(xyzq, kind, parts);
       tree_ok = up_ok = lists_ok = false;
       return;
     }
@@ -216,8 +219,23 @@ struct Engine {
     EXA_CUDA(cudaStreamSynchronize(st));
     T.n = total;
     T.xyzq.ensure(total);
-    if (total) EXA_CUDA(cudaMemcpyAsync(T.xyzq.p, xyzq, total * sizeof(double4), kind, C.stream));
+    copy_systems(xyzq, kind, parts);
     tree_ok = up_ok = lists_ok = false;
+  }
+
+  void copy_systems(const double *xyzq, cudaMemcpyKind kind, const double *const *parts) {
+    TreeBufs &T = C.tree;
+    if (!parts) {
+      if (T.n) EXA_CUDA(cudaMemcpyAsync(T.xyzq.p, xyzq, T.n * sizeof(double4), kind, C.stream));
+      return;
+    }
+    for (int s = 0; s < T.nsys; s++) {
+      const long long k = T.sys_off_host[s + 1] - T.sys_off_host[s];
+      if (!k) continue;
+      if (!parts[s]) throw std::runtime_error("null bodies of system " + std::to_string(s));
+      EXA_CUDA(cudaMemcpyAsync(T.xyzq.p + T.sys_off_host[s], parts[s], k * sizeof(double4), cudaMemcpyDefault,
+                               C.stream));
+    }
   }
 
   void set_sources(const double *xyzq, long long n) {
@@ -432,7 +450,7 @@ struct Engine {
     tm.periodic = C.prm.images > 0;
   }
 
-  void results(double *dst, cudaMemcpyKind kind);
+  void results(double *dst, cudaMemcpyKind kind, double *const *parts = nullptr);
 
   void get_dipole(const double *X0, double *dipole3) {
     const double zero[3] = {0.0, 0.0, 0.0};
@@ -457,14 +475,26 @@ __global__ void k_unsort(const double4 *trg, const int *perm, long long n, doubl
 }
 }  // namespace
 
-void Engine::results(double *dst, cudaMemcpyKind kind) {
+// parts (a forest only): one destination per system, host or device memory.
+void Engine::results(double *dst, cudaMemcpyKind kind, double *const *parts) {
   if (!lists_ok) throw std::runtime_error("results before a solve");
   const long long n = C.tree.n;
   out.ensure(n);
   if (n) {
     k_unsort<<<kNumSMs * 4, 256, 0, C.stream>>>(trg.p, C.tree.perm.p, n, out.p);
     EXA_CHECK_LAUNCH();
-    EXA_CUDA(cudaMemcpyAsync(dst, out.p, n * sizeof(double4), kind, C.stream));
+    if (!parts) {
+      EXA_CUDA(cudaMemcpyAsync(dst, out.p, n * sizeof(double4), kind, C.stream));
+    } else {
+      const TreeBufs &T = C.tree;
+      for (int s = 0; s < T.nsys; s++) {
+        const long long k = T.sys_off_host[s + 1] - T.sys_off_host[s];
+        if (!k) continue;
+        if (!parts[s]) throw std::runtime_error("null results of system " + std::to_string(s));
+        EXA_CUDA(cudaMemcpyAsync(parts[s], out.p + T.sys_off_host[s], k * sizeof(double4), cudaMemcpyDefault,
+                                 C.stream));
+      }
+    }
   }
   EXA_CUDA(cudaStreamSynchronize(C.stream));
 }
@@ -688,6 +718,24 @@ int exafmm_set_systems_device(exafmm_ctx *ctx, int count, const long long *n, co
   return guarded(ctx, [&] {
     cudaSetDevice(ctx->E.C.device);
     ctx->E.set_systems(count, n, d_xyzq, cudaMemcpyDeviceToDevice);
+  });
+}
+
+int exafmm_set_systems_list(exafmm_ctx *ctx, int count, const long long *n, const double *const *xyzq) {
+  return guarded(ctx, [&] {
+    if (!xyzq) throw std::runtime_error("null body list");
+    cudaSetDevice(ctx->E.C.device);
+    ctx->E.set_systems(count, n, nullptr, cudaMemcpyDefault, xyzq);
+    EXA_CUDA(cudaStreamSynchronize(ctx->E.C.stream));
+  });
+}
+
+int exafmm_get_results_list(exafmm_ctx *ctx, double *const *trg) {
+  return guarded(ctx, [&] {
+    if (!trg) throw std::runtime_error("null result list");
+    if (!ctx->E.C.tree.nsys) throw std::runtime_error("the context holds one system (exafmm_set_systems was not called)");
+    cudaSetDevice(ctx->E.C.device);
+    ctx->E.results(nullptr, cudaMemcpyDefault, trg);
   });
 }
 

@@ -45,24 +45,34 @@ class NcritTuner {
  public:
   explicit NcritTuner(std::vector<int> cand) : cand_(std::move(cand)) {}
 
-  int pick(long long n, int fallback) {
+  int pick(long long n, int fallback) { return pick_class(size_class(n), fallback); }
+
+  void report(long long n, int ncrit, double ms) {
+    if (n > 0) report_class(size_class(n), ncrit, ms / (double)n);
+  }
+
+  // The same keyed by a class directly (a forest bucket is keyed by the
+  // lowest size class it holds), with the cost already per body.
+  int pick_class(int cls, int fallback) {
     std::lock_guard<std::mutex> lk(mu_);
     if (!enabled_) {
-      auto it = best_.find(size_class(n));
+      auto it = best_.find(cls);
       return it == best_.end() ? fallback : it->second;
     }
-    Class &c = cls_[size_class(n)];
+    Class &c = cls_[cls];
     if (c.trials.size() < cand_.size()) return cand_[c.trials.size()];
     return best_of(c);
   }
 
-  void report(long long n, int ncrit, double ms) {
+  void report_class(int cls, int ncrit, double ms_per_body) {
     std::lock_guard<std::mutex> lk(mu_);
-    if (!enabled_ || n <= 0) return;
-    Class &c = cls_[size_class(n)];
-    if (c.trials.size() < cand_.size() && ncrit == cand_[c.trials.size()]) c.trials.push_back(ms / (double)n);
-    if (c.trials.size() == cand_.size()) best_[size_class(n)] = best_of(c);
+    if (!enabled_) return;
+    Class &c = cls_[cls];
+    if (c.trials.size() < cand_.size() && ncrit == cand_[c.trials.size()]) c.trials.push_back(ms_per_body);
+    if (c.trials.size() == cand_.size()) best_[cls] = best_of(c);
   }
+
+  static int size_class(long long n) { return n <= 1 ? 0 : (int)std::floor(std::log2((double)n)); }
 
   void enable(bool on) {
     std::lock_guard<std::mutex> lk(mu_);
@@ -91,7 +101,6 @@ class NcritTuner {
   struct Class {
     std::vector<double> trials;  // ms per body, in candidate order
   };
-  static int size_class(long long n) { return n <= 1 ? 0 : (int)std::floor(std::log2((double)n)); }
   int best_of(const Class &c) const {
     size_t b = 0;
     for (size_t i = 1; i < c.trials.size(); i++)
@@ -115,6 +124,12 @@ struct SolveParams {
   int precision = EXAFMM_FP64;
 };
 
+// exafmm_set_mixed_policy's arguments, applied to every context a batch uses.
+struct MixedPolicy {
+  bool set = false;
+  int m2l_fp32 = 1, p2p_fp32 = 1, min_level = 4, max_dl = 3;
+};
+
 // One worker's context, created on first use and re-parameterized per system.
 struct Slot {
   exafmm_ctx *ctx = nullptr;
@@ -130,7 +145,35 @@ struct Slot {
     return b;
   }
   // Solve one system; returns the device time of the solve (ms).
-  double solve(int device, const SolveParams &p, const double *xyzq, long long n, double *trg) {
+  double solve(int device, const SolveParams &p, const double *xyzq, long long n, double *trg,
+               const MixedPolicy *pol = nullptr) {
+    prepare(device, p, pol);
+    check(exafmm_set_bodies(ctx, xyzq, n));
+    check(exafmm_solve(ctx));
+    check(exafmm_get_results(ctx, trg));
+    double ms[8];
+    check(exafmm_phase_times(ctx, ms));
+    return ms[7];
+  }
+
+  // Solve count systems as one forest (exafmm_set_systems_list): the
+  // context's stream first waits for `start`, and `done` is recorded on it
+  // after the results are copied out.  Returns the forest's solve time (ms).
+  double solve_forest(int device, const SolveParams &p, const MixedPolicy *pol, int count, const long long *n,
+                      const double *const *xyzq, double *const *trg, cudaEvent_t start, cudaEvent_t done) {
+    prepare(device, p, pol);
+    cudaStream_t st = (cudaStream_t)exafmm_stream(ctx);
+    if (cudaStreamWaitEvent(st, start, 0) != cudaSuccess) throw std::runtime_error("cudaStreamWaitEvent");
+    check(exafmm_set_systems_list(ctx, count, n, xyzq));
+    check(exafmm_solve(ctx));
+    check(exafmm_get_results_list(ctx, trg));
+    if (cudaEventRecord(done, st) != cudaSuccess) throw std::runtime_error("cudaEventRecord");
+    double ms[8];
+    check(exafmm_phase_times(ctx, ms));
+    return ms[7];
+  }
+
+  void prepare(int device, const SolveParams &p, const MixedPolicy *pol) {
     if (!ctx || p.precision != cur.precision) {
       release();
       if (exafmm_create(&ctx, p.P, p.theta, p.ncrit, p.nspawn, p.images, p.cycle, p.precision, device) != 0) {
@@ -143,12 +186,8 @@ struct Slot {
       check(exafmm_set_params(ctx, p.P, p.theta, p.ncrit, p.nspawn, p.images, p.cycle));
       cur = p;
     }
-    check(exafmm_set_bodies(ctx, xyzq, n));
-    check(exafmm_solve(ctx));
-    check(exafmm_get_results(ctx, trg));
-    double ms[8];
-    check(exafmm_phase_times(ctx, ms));
-    return ms[7];
+    if (pol && pol->set && p.precision == EXAFMM_MIXED)
+      check(exafmm_set_mixed_policy(ctx, pol->m2l_fp32, pol->p2p_fp32, pol->min_level, pol->max_dl));
   }
   void check(int rc) {
     if (rc != 0) throw std::runtime_error(exafmm_last_error(ctx));
@@ -162,11 +201,66 @@ struct exafmm_batch {
   int device = 0;
   int workers = 1;
   SolveParams prm;
+  MixedPolicy policy;
+  int forest_buckets = 0;       // 0: one context per system; k > 0: up to k forests by size
   std::vector<Slot> slots;
   NcritTuner tuner{{32, 64, 128}};
   std::vector<double> last_ms;  // per system of the last call, device ms
+  double last_elapsed_ms = 0;   // the last forest call, first copy in to last copy out, on the device
+  std::vector<int> last_bucket; // bucket of each system in the last forest call
+  std::vector<int> last_bucket_ncrit;
+  cudaStream_t timing = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_end = nullptr;
+  std::vector<cudaEvent_t> ev_done;
   std::string error;
+  ~exafmm_batch() {
+    slots.clear();
+    for (auto e : ev_done) cudaEventDestroy(e);
+    if (ev_start) cudaEventDestroy(ev_start);
+    if (ev_end) cudaEventDestroy(ev_end);
+    if (timing) cudaStreamDestroy(timing);
+  }
 };
+
+namespace {
+
+// Forest buckets: the non-empty systems' size classes (floor(log2 n)) in
+// increasing order, cut into at most `buckets` runs of whole classes with
+// about equal bodies each (bucket b's share ends at (b + 1) / buckets of all
+// bodies); empty systems join the first bucket.  Returns the
+// number of buckets and fills bucket_of[count] and, if given, the lowest class
+// of each bucket (its tuner key).
+int forest_buckets(int count, const long long *n, int buckets, int *bucket_of, std::vector<int> *key) {
+  std::map<int, long long> per_class;
+  long long total = 0;
+  for (int i = 0; i < count; i++)
+    if (n[i] > 0) {
+      per_class[NcritTuner::size_class(n[i])] += n[i];
+      total += n[i];
+    }
+  std::map<int, int> class_bucket;
+  std::vector<int> lowest;
+  int b = 0;
+  long long acc = 0;
+  for (auto &kv : per_class) {
+    // start the next bucket before this class when taking it would overshoot
+    // the current bucket's share by more than stopping here falls short of it
+    const double target = (double)total * (b + 1) / buckets;
+    if ((int)lowest.size() == b + 1 && b < buckets - 1 &&
+        (double)(acc + kv.second) - target > target - (double)acc)
+      b++;
+    if ((int)lowest.size() == b) lowest.push_back(kv.first);
+    class_bucket[kv.first] = b;
+    acc += kv.second;
+  }
+  if (lowest.empty()) lowest.push_back(0);
+  const int nb = (int)lowest.size();
+  for (int i = 0; i < count; i++) bucket_of[i] = n[i] > 0 ? class_bucket[NcritTuner::size_class(n[i])] : 0;
+  if (key) *key = lowest;
+  return nb;
+}
+
+}  // namespace
 
 // ================================================================ server
 namespace {
@@ -341,11 +435,116 @@ int exafmm_batch_set_ncrit_table(exafmm_batch *b, const int *pairs, int k) {
   return 0;
 }
 
+namespace {
+
+// Forest mode: every bucket's systems are one forest on one worker context;
+// buckets run concurrently, largest first.  The device time of the whole call
+// spans from an event that every context stream waits on to the last bucket's
+// copy out.
+int batch_solve_forest(exafmm_batch *b, int count, const long long *n, const double *const *xyzq,
+                       double *const *trg) {
+  cudaSetDevice(b->device);
+  std::vector<int> bucket(count);
+  std::vector<int> key;
+  const int nb = forest_buckets(count, n, b->forest_buckets, bucket.data(), &key);
+  std::vector<std::vector<int>> members(nb);
+  std::vector<long long> bodies(nb, 0);
+  for (int i = 0; i < count; i++) {
+    members[bucket[i]].push_back(i);
+    bodies[bucket[i]] += n[i];
+  }
+  std::vector<int> order(nb);
+  for (int i = 0; i < nb; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return bodies[x] > bodies[y]; });
+  const int nw = std::min(b->workers, nb);
+  if (!b->timing) {
+    if (cudaStreamCreateWithFlags(&b->timing, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->ev_start) != cudaSuccess || cudaEventCreate(&b->ev_end) != cudaSuccess) {
+      b->error = "timing stream or events";
+      return 1;
+    }
+  }
+  while ((int)b->ev_done.size() < nw) {
+    cudaEvent_t e;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      b->error = "cudaEventCreate";
+      return 1;
+    }
+    b->ev_done.push_back(e);
+  }
+  b->last_bucket = bucket;
+  b->last_bucket_ncrit.assign(nb, b->prm.ncrit);
+  if (cudaEventRecord(b->ev_start, b->timing) != cudaSuccess) {
+    b->error = "cudaEventRecord";
+    return 1;
+  }
+  std::atomic<int> next{0};
+  std::atomic<bool> failed{false};
+  std::mutex emu;
+  std::vector<char> used(nw, 0);
+  auto run = [&](int w) {
+    cudaSetDevice(b->device);
+    for (;;) {
+      const int i = next.fetch_add(1);
+      if (i >= nb || failed.load()) return;
+      const int k = order[i];
+      const std::vector<int> &mem = members[k];
+      std::vector<long long> nn(mem.size());
+      std::vector<const double *> in(mem.size());
+      std::vector<double *> out(mem.size());
+      for (size_t j = 0; j < mem.size(); j++) {
+        nn[j] = n[mem[j]];
+        in[j] = xyzq[mem[j]];
+        out[j] = trg[mem[j]];
+      }
+      SolveParams p = b->prm;
+      p.ncrit = b->tuner.pick_class(key[k], b->prm.ncrit);
+      b->last_bucket_ncrit[k] = p.ncrit;
+      try {
+        const double ms = b->slots[w].solve_forest(b->device, p, &b->policy, (int)mem.size(), nn.data(), in.data(),
+                                                   out.data(), b->ev_start, b->ev_done[w]);
+        used[w] = 1;
+        for (size_t j = 0; j < mem.size(); j++)
+          b->last_ms[mem[j]] = bodies[k] > 0 ? ms * (double)nn[j] / (double)bodies[k] : 0.0;
+        if (bodies[k] > 0) b->tuner.report_class(key[k], p.ncrit, ms / (double)bodies[k]);
+      } catch (const std::exception &e) {
+        std::lock_guard<std::mutex> lk(emu);
+        if (!failed.exchange(true)) b->error = std::string("forest bucket ") + std::to_string(k) + ": " + e.what();
+        b->slots[w].release();
+        return;
+      }
+    }
+  };
+  std::vector<std::thread> th;
+  for (int w = 1; w < nw; w++) th.emplace_back(run, w);
+  run(0);
+  for (auto &t : th) t.join();
+  if (failed.load()) return 1;
+  for (int w = 0; w < nw; w++)
+    if (used[w] && cudaStreamWaitEvent(b->timing, b->ev_done[w], 0) != cudaSuccess) {
+      b->error = "cudaStreamWaitEvent";
+      return 1;
+    }
+  float ms = 0.f;
+  if (cudaEventRecord(b->ev_end, b->timing) != cudaSuccess || cudaEventSynchronize(b->ev_end) != cudaSuccess ||
+      cudaEventElapsedTime(&ms, b->ev_start, b->ev_end) != cudaSuccess) {
+    b->error = "timing events";
+    return 1;
+  }
+  b->last_elapsed_ms = ms;
+  return 0;
+}
+
+}  // namespace
+
 int exafmm_batch_solve(exafmm_batch *b, int count, const long long *n, const double *const *xyzq, double *const *trg) {
   if (!b) return 2;
   if (count < 0 || (count > 0 && (!n || !xyzq || !trg))) return 2;
+  for (int i = 0; i < count; i++)
+    if (n[i] < 0) return 2;
   b->error.clear();
   b->last_ms.assign(count, 0.0);
+  if (b->forest_buckets > 0 && count > 0) return batch_solve_forest(b, count, n, xyzq, trg);
   std::vector<int> order(count);
   for (int i = 0; i < count; i++) order[i] = i;
   // largest first: the long solves start early and the short ones fill in
@@ -362,7 +561,7 @@ int exafmm_batch_solve(exafmm_batch *b, int count, const long long *n, const dou
       SolveParams p = b->prm;
       p.ncrit = b->tuner.pick(n[k], b->prm.ncrit);
       try {
-        const double ms = b->slots[w].solve(b->device, p, xyzq[k], n[k], trg[k]);
+        const double ms = b->slots[w].solve(b->device, p, xyzq[k], n[k], trg[k], &b->policy);
         b->last_ms[k] = ms;
         b->tuner.report(n[k], p.ncrit, ms);
       } catch (const std::exception &e) {
@@ -385,6 +584,44 @@ int exafmm_batch_times(exafmm_batch *b, double *ms) {
   if (!b || !ms) return 2;
   std::copy(b->last_ms.begin(), b->last_ms.end(), ms);
   return 0;
+}
+
+int exafmm_batch_set_forest(exafmm_batch *b, int buckets) {
+  if (!b || buckets < 0 || buckets > 64) return 2;
+  b->forest_buckets = buckets;
+  return 0;
+}
+
+int exafmm_batch_set_mixed_policy(exafmm_batch *b, int m2l_fp32, int p2p_fp32, int min_level, int max_dl) {
+  if (!b || m2l_fp32 < 0 || m2l_fp32 > 5 || min_level < 0 || max_dl < 0) return 2;
+  b->policy.set = true;
+  b->policy.m2l_fp32 = m2l_fp32;
+  b->policy.p2p_fp32 = p2p_fp32;
+  b->policy.min_level = min_level;
+  b->policy.max_dl = max_dl;
+  return 0;
+}
+
+int exafmm_batch_elapsed(exafmm_batch *b, double *ms) {
+  if (!b || !ms) return 2;
+  *ms = b->last_elapsed_ms;
+  return 0;
+}
+
+int exafmm_batch_buckets(exafmm_batch *b, int *bucket_of, int *bucket_ncrit, int cap) {
+  if (!b) return -1;
+  const int nb = (int)b->last_bucket_ncrit.size();
+  if (bucket_of) std::copy(b->last_bucket.begin(), b->last_bucket.end(), bucket_of);
+  if (bucket_ncrit)
+    for (int i = 0; i < nb && i < cap; i++) bucket_ncrit[i] = b->last_bucket_ncrit[i];
+  return nb;
+}
+
+int exafmm_forest_buckets(int count, const long long *n, int buckets, int *bucket_of) {
+  if (count < 0 || buckets < 1 || (count > 0 && (!n || !bucket_of))) return -1;
+  for (int i = 0; i < count; i++)
+    if (n[i] < 0) return -1;
+  return forest_buckets(count, n, buckets, bucket_of, nullptr);
 }
 
 // ---------------------------------------------------------------- server entry points

@@ -103,6 +103,14 @@ int exafmm_set_systems_device(exafmm_ctx *ctx, int count, const long long *n, co
  * (count + 1) and each system's bounds (count x 6, as exafmm_get_bounds);
  * any output may be NULL (body_off is known before a build). */
 int exafmm_get_systems(exafmm_ctx *ctx, long long *cell_base, long long *body_off, double *bounds);
+/* The same forest with one pointer per system instead of the concatenation:
+ * xyzq[s] holds system s's n[s] x 4 doubles, trg[s] receives its n[s] x 4
+ * results, in host or device memory (each copied with cudaMemcpyDefault, so
+ * host pointers must be addressable by CUDA: any pageable or pinned memory).
+ * A NULL pointer is allowed only for an empty system.  No counterpart in the
+ * reference (one system per process, examples/fmm.cxx:163-179). */
+int exafmm_set_systems_list(exafmm_ctx *ctx, int count, const long long *n, const double *const *xyzq);
+int exafmm_get_results_list(exafmm_ctx *ctx, double *const *trg);
 
 /* BoundBox::getBounds(Bodies&) (include/bound_box.h:11-25), including its
  * sequential 1e-5 drift, evaluated on the device in closed form; with separate
@@ -254,6 +262,31 @@ int exafmm_batch_ncrit_table(exafmm_batch *b, int *pairs, int cap);
 /* Replaces the table with k (size class, ncrit) pairs and freezes it (so two
  * batches can solve on the same trees). */
 int exafmm_batch_set_ncrit_table(exafmm_batch *b, const int *pairs, int k);
+/* Forest mode (buckets > 0): the systems of one call are cut into at most
+ * `buckets` groups of whole size classes with about equal bodies each
+ * (exafmm_forest_buckets), and every group is solved as one forest
+ * (exafmm_set_systems_list) on one worker context: every phase launches once
+ * per group, not once per system, and the groups run concurrently.  Each
+ * system's results are the bits of its solo solve at the group's ncrit.  The
+ * autotuner keys a group by the lowest size class it holds and tries one
+ * candidate per call.  In forest mode xyzq[i] and trg[i] may be host or device
+ * pointers.  buckets == 0 (the default) solves one system per context. */
+int exafmm_batch_set_forest(exafmm_batch *b, int buckets);
+/* exafmm_set_mixed_policy for every context of the batch (mixed precision). */
+int exafmm_batch_set_mixed_policy(exafmm_batch *b, int m2l_fp32, int p2p_fp32, int min_level, int max_dl);
+/* Forest mode: device time (ms) of the last call, from an event every worker
+ * stream waits on before its first copy in to the last group's copy out. */
+int exafmm_batch_elapsed(exafmm_batch *b, double *ms);
+/* Forest mode: the group of each system of the last call (bucket_of[count])
+ * and each group's ncrit (up to cap); returns the number of groups. */
+int exafmm_batch_buckets(exafmm_batch *b, int *bucket_of, int *bucket_ncrit, int cap);
+/* The grouping itself (host only): non-empty systems' size classes
+ * floor(log2 n) in increasing order, cut into at most `buckets` runs of whole
+ * classes; group b's share of the bodies ends at (b + 1) / buckets of the
+ * total, and the next group starts before a class whose bodies would overshoot
+ * that mark by more than stopping short of it falls below.  Empty systems join
+ * group 0.  Returns the number of groups, -1 on bad input. */
+int exafmm_forest_buckets(int count, const long long *n, int buckets, int *bucket_of);
 
 typedef struct exafmm_server exafmm_server;
 /* Request server: submitted systems wait in a FIFO queue and start when their

@@ -79,3 +79,29 @@ def test_kernel_entry_points_fail_loudly_without_gpu(ex):
         pytest.skip("a GPU is present")
     with pytest.raises(ex.FmmError):
         ex.p2p(np.zeros((2, 4)), np.ones((3, 4)))
+
+
+def test_forest_grouping_cuts_whole_size_classes(ex):
+    """The batch's forest groups: whole size classes (floor(log2 n)) in increasing
+    order, at most the asked number of groups, each near its share of the bodies;
+    empty systems go to group 0."""
+    rng = np.random.default_rng(7)
+    sizes = np.exp(rng.uniform(np.log(2000), np.log(200_000), 512)).astype(np.int64)
+    sizes[[3, 40]] = 0
+    for k in (1, 2, 3, 4, 8):
+        g = ex.forest_buckets(sizes, k)
+        assert g.shape == sizes.shape and g.min() == 0 and g.max() < k
+        cls = np.floor(np.log2(np.maximum(sizes, 1))).astype(int)
+        live = sizes > 0
+        for c in np.unique(cls[live]):          # a class is never split
+            assert len(np.unique(g[live & (cls == c)])) == 1
+        order = np.argsort(sizes[live], kind="stable")   # groups follow size order
+        assert np.all(np.diff(g[live][order]) >= 0)
+        assert np.all(g[~live] == 0)
+    assert list(ex.forest_buckets([2000, 0, 200_000, 5000, 70_000, 3000, 150_000], 3)) == [0, 0, 1, 0, 0, 0, 1]
+    assert list(ex.forest_buckets([0, 0], 4)) == [0, 0]
+    assert len(ex.forest_buckets([], 2)) == 0
+    with pytest.raises(ex.FmmError):
+        ex.forest_buckets([5, -1], 2)
+    with pytest.raises(ex.FmmError):
+        ex.forest_buckets([5], 0)

@@ -98,3 +98,53 @@ def test_server_admission_serializes_under_tiny_budget(ex, datasets):
     st = s.stats()
     assert st["completed"] == len(xs) and st["held"] == 0 and st["in_flight"] == 0
     s.close()
+
+
+def test_forest_batch_matches_single_solves(ex, datasets):
+    """Forest mode: the systems of a call are grouped by size into forests, one
+    context each; every system still gets the bits of its solo solve at its
+    group's ncrit, through host or device pointers, and again on a second call."""
+    import torch
+    xs = _systems(datasets, 14, 500, 60000, 700) + [np.zeros((0, 4)), datasets.cube(1, seed=11)]
+    kw = dict(P=8, theta=0.4, precision=ex.MIXED)
+    b = ex.Batch(ncrit=64, workers=3, forest=3, **kw)
+    b.set_mixed_policy(m2l_fp32=1, min_level=2)
+    outs = b.solve(xs)
+    group, ncrit = b.buckets(len(xs))
+    assert len(ncrit) == group.max() + 1 <= 3
+    assert b.elapsed_ms() > 0
+    for x, o, gi in zip(xs, outs, group):
+        f = ex.Fmm(ncrit=int(ncrit[gi]), **kw)
+        f.set_mixed_policy(m2l_fp32=1, min_level=2)
+        f.set_bodies(x)
+        f.solve()
+        assert np.array_equal(o, f.results())
+        f.close()
+    dev = [torch.from_numpy(x.copy()).cuda() for x in xs]
+    dout = [torch.zeros_like(d) for d in dev]
+    b.solve_device([len(x) for x in xs], [d.data_ptr() for d in dev], [d.data_ptr() for d in dout])
+    torch.cuda.synchronize()
+    assert all(np.array_equal(o, d.cpu().numpy()) for o, d in zip(outs, dout))
+    b.close()
+
+
+def test_forest_batch_autotune_per_group(ex, datasets):
+    xs = _systems(datasets, 10, 1000, 40000, 800)
+    b = ex.Batch(P=6, theta=0.4, ncrit=64, workers=2, forest=2)
+    b.autotune(True)
+    for _ in range(3):                 # one candidate per call
+        b.solve(xs)
+    b.autotune(False)
+    table = b.ncrit_table()
+    group, ncrit = b.buckets(len(xs))
+    assert len(table) == group.max() + 1 and all(v in (32, 64, 128) for v in table.values())
+    o1 = b.solve(xs)
+    group, ncrit = b.buckets(len(xs))
+    assert sorted(ncrit.tolist()) == sorted(table.values())
+    for x, o, gi in zip(xs, o1, group):
+        assert np.array_equal(o, _alone(ex, x, P=6, theta=0.4, ncrit=int(ncrit[gi])))
+    b2 = ex.Batch(P=6, theta=0.4, ncrit=64, workers=2, forest=2)   # a loaded table gives the same trees
+    b2.set_ncrit_table(table)
+    assert all(np.array_equal(a, c) for a, c in zip(o1, b2.solve(xs)))
+    b2.close()
+    b.close()
