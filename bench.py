@@ -441,7 +441,7 @@ def main():
 # ---------------------------------------------------------------- batched and served workloads
 BATCH = dict(name="batch_512_p10", count=512, lo=2000, hi=200_000, P=10, theta=0.4, ncrit=64, nspawn=5000)
 SERVE = dict(name="serve_poisson_p6_8_10", count=60, lo=1000, hi=1_000_000, theta=0.4, ncrit=64, nspawn=5000,
-             budget=150e9, repeat_frac=0.2, repeat_steps=50, loads=(0.5, 0.8))
+             budget=150e9, repeat_frac=0.2, repeat_steps=50, loads=(0.5, 0.8), replays=3)
 
 
 def _three_way(ex, datasets, xs, mixed, plain, sample=256, take=None):
@@ -673,54 +673,122 @@ def _run_batch(args, pkg, datasets, workloads, prec, rank, world, local_rank):
     return line
 
 
+def _request_errors(pkg, datasets, workloads, trace, mixed_samples, plain_samples):
+    """Per request (the final step of each job): rel-L2 of the potential on its
+    sampled targets, mixed vs an FP64 direct sum over all its bodies, plain vs the
+    same, and mixed vs plain."""
+    rows = []
+    for k, job in enumerate(trace.jobs):
+        if k not in mixed_samples:
+            continue
+        idx, mres, final = mixed_samples[k]
+        x = final if final is not None else workloads.job_bodies(job)
+        d = pkg.direct(x[idx], x)
+        row = {"job": k, "n": job.n, "P": job.P, "kind": job.kind, "steps": job.steps,
+               "mixed_vs_direct": datasets.rel_l2(mres[:, 0], d[:, 0])}
+        if k in plain_samples:
+            pidx, pres, pfinal = plain_samples[k]
+            if np.array_equal(pidx, idx) and (pfinal is None) == (final is None) and \
+                    (final is None or np.array_equal(pfinal, final)):
+                row["plain_vs_direct"] = datasets.rel_l2(pres[:, 0], d[:, 0])
+                row["mixed_vs_plain"] = datasets.rel_l2(mres[:, 0], pres[:, 0])
+        rows.append(row)
+    return rows
+
+
 def _run_serve(args, pkg, datasets, workloads, prec, rank, world, local_rank):
+    """Served request stream: a saturated replay (everything queued at once) gives
+    the capacity; the same trace replayed with the plain FP64 method gives the
+    mixed/plain ratio in bodies/s; Poisson traces at 0.5 and 0.8 of capacity,
+    three replays each, give p50/p99 as medians with their spread.  Repeat
+    chains stay on the device (server sessions)."""
     import torch
     cfg = SERVE
     srv = pkg.Server(device=local_rank, workers=args.workers, hbm_budget_bytes=cfg["budget"])
-    # warm-up: one request per order, then a saturated replay measures the service rate
+    # warm-up: one request per order and precision
     for P in (6, 8, 10):
-        srv.wait(srv.submit(datasets.cube(20000, seed=P), P=P, theta=cfg["theta"], ncrit=cfg["ncrit"],
-                            precision=prec))
+        for pr in {prec, pkg.FP64}:
+            srv.wait(srv.submit(datasets.cube(20000, seed=P), P=P, theta=cfg["theta"], ncrit=cfg["ncrit"],
+                                precision=pr))
     sat = workloads.make_trace(cfg["count"], rate=1e6, lo=cfg["lo"], hi=cfg["hi"], repeat_frac=cfg["repeat_frac"],
                                repeat_steps=cfg["repeat_steps"], seed=4000 + 1000 * rank, theta=cfg["theta"])
+    def pinned(shape):
+        return torch.empty(shape, dtype=torch.float64).pin_memory().numpy()
+
     launches0 = pkg.launch_count()
+    mixed_samples, plain_samples = {}, {}
     with ClockSampler(local_rank) as clocks:
         done, wall = workloads.replay(srv, sat, precision=prec, ncrit=cfg["ncrit"], nspawn=cfg["nspawn"],
-                                      deadline_s=240.0)
+                                      deadline_s=300.0, samples=mixed_samples, host_alloc=pinned)
         capacity = len(sat.jobs) / wall  # jobs per second with everything queued at once
         saturated = workloads.latency_summary(done, wall)
+        saturated["while_saturated"] = workloads.saturated_throughput(done)
         rates = {}
         for load in cfg["loads"]:
-            tr = workloads.make_trace(cfg["count"], rate=load * capacity, lo=cfg["lo"], hi=cfg["hi"],
-                                      repeat_frac=cfg["repeat_frac"], repeat_steps=cfg["repeat_steps"],
-                                      seed=5000 + int(100 * load) + 1000 * rank, theta=cfg["theta"])
-            d, w = workloads.replay(srv, tr, precision=prec, ncrit=cfg["ncrit"], nspawn=cfg["nspawn"],
-                                    deadline_s=240.0)
-            rates[f"{load:.2f}"] = dict(workloads.latency_summary(d, w), rate_jobs_per_s=load * capacity)
+            reps = []
+            for r in range(cfg["replays"]):
+                tr = workloads.make_trace(cfg["count"], rate=load * capacity, lo=cfg["lo"], hi=cfg["hi"],
+                                          repeat_frac=cfg["repeat_frac"], repeat_steps=cfg["repeat_steps"],
+                                          seed=5000 + int(100 * load) + 10 * r + 1000 * rank, theta=cfg["theta"])
+                d, w = workloads.replay(srv, tr, precision=prec, ncrit=cfg["ncrit"], nspawn=cfg["nspawn"],
+                                        deadline_s=300.0, host_alloc=pinned)
+                reps.append(workloads.latency_summary(d, w))
+            med = lambda key: float(np.median([x[key] for x in reps]))
+            rates[f"{load:.2f}"] = {"rate_jobs_per_s": load * capacity, "replays": len(reps),
+                                    "p50_ms": med("p50_ms"), "p99_ms": med("p99_ms"), "mean_ms": med("mean_ms"),
+                                    "bodies_per_s": med("bodies_per_s"),
+                                    "p50_ms_range": [min(x["p50_ms"] for x in reps), max(x["p50_ms"] for x in reps)],
+                                    "p99_ms_range": [min(x["p99_ms"] for x in reps), max(x["p99_ms"] for x in reps)],
+                                    "requests": reps[0]["requests"], "wall_s": med("wall_s")}
         torch.cuda.synchronize()
     clk = clocks.summary()
     launches = pkg.launch_count() - launches0
+    plain = None
+    if not args.no_plain and prec == pkg.MIXED:
+        pd, pw = workloads.replay(srv, sat, precision=pkg.FP64, ncrit=cfg["ncrit"], nspawn=cfg["nspawn"],
+                                  deadline_s=600.0, samples=plain_samples, host_alloc=pinned)
+        psat = workloads.latency_summary(pd, pw)
+        psat["while_saturated"] = workloads.saturated_throughput(pd)
+        plain = {"value": psat["while_saturated"]["bodies_per_s"],
+                 "unit": "bodies/s (saturated replay of the same trace, until its last single solve)",
+                 "capacity_jobs_per_s": len(sat.jobs) / pw, "saturated": psat,
+                 "speedup_of_mixed": saturated["while_saturated"]["bodies_per_s"] /
+                 psat["while_saturated"]["bodies_per_s"],
+                 "speedup_of_mixed_whole_trace": saturated["bodies_per_s"] / psat["bodies_per_s"]}
+    errs = _request_errors(pkg, datasets, workloads, sat, mixed_samples, plain_samples)
     st = srv.stats()
     srv.close()
     top = rates[f"{max(cfg['loads']):.2f}"]
-    return {
+    err_summary = {k: {"max": max(r[k] for r in errs if k in r), "median": float(np.median([r[k] for r in errs
+                                                                                           if k in r]))}
+                   for k in ("mixed_vs_direct", "plain_vs_direct", "mixed_vs_plain") if any(k in r for r in errs)}
+    line = {
         "metric": "served p99 latency (Poisson arrivals at 0.8 of capacity; N log-uniform [1e3, 1e6], "
                   "P in {6, 8, 10}, theta=0.4)",
-        "value": top["p99_ms"], "unit": "ms", "n_gpus": world, "steps": 1, "warmup": 1,
+        "value": top["p99_ms"], "unit": "ms", "n_gpus": world, "steps": cfg["replays"], "warmup": 1,
         "ms_per_step": top["mean_ms"], "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if prec == pkg.FP64 else "f32+kahan", "data": "synthetic",
         "config": {"workload": cfg["name"], "jobs_per_trace": cfg["count"], "repeat_fraction": cfg["repeat_frac"],
                    "repeat_steps": cfg["repeat_steps"], "hbm_budget_bytes": cfg["budget"],
                    "workers": args.workers, "precision": args.precision, "parallelism": f"replicas{world}",
-                   "timing": "host wall clock: scheduled arrival (or the previous chain step's return) to "
-                             "results in host memory",
-                   "l2": "requests stream their bodies in and results out"},
+                   "chains": "device-resident sessions: bodies moved and tree rebuilt on the device each step",
+                   "timing": "host clock: scheduled arrival (or the previous chain step's return) to results "
+                             "in host memory; p50/p99 are medians over the replays, with their ranges",
+                   "l2": "requests stream their bodies in and results out",
+                   "host_buffers": "each request's bodies and results in pinned host memory, generated and "
+                                   "allocated before the replay's clock starts"},
         "saturated": saturated, "capacity_jobs_per_s": capacity, "loads": rates,
+        "served_bodies_per_s": saturated["while_saturated"]["bodies_per_s"],
+        "request_rel_l2_pot": err_summary, "requests_checked": len(errs),
+        "per_request": [{k: (float(f"{v:.3e}") if isinstance(v, float) else v) for k, v in r.items()} for r in errs],
         "server_stats": st,
         "e2e": {"value": top["p99_ms"], "unit": "ms", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
         "gpu_launches": int(launches), "clocks": clk, "roofline": None,
         "_time": top["wall_s"], "_units": top["requests"],
     }
+    if plain is not None:
+        line["plain_fp64"] = plain
+    return line
 
 
 PERIODIC = dict(name="water_1m_images3_p10", waters=333_333, P=10, theta=0.4, ncrit=64, nspawn=5000, images=3,

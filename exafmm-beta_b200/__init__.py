@@ -127,6 +127,17 @@ def lib() -> ctypes.CDLL:
         "exafmm_server_wait": (_c_int, [_vp, _c_ll, _vp]),
         "exafmm_server_stats": (_c_int, [_vp, _vp]),
         "exafmm_server_error": (ctypes.c_char_p, []),
+        "exafmm_server_open_session": (_c_int, [_vp, _vp, _c_ll, _c_int, _c_double, _c_int, _c_int, _c_int,
+                                                ctypes.POINTER(_c_ll)]),
+        "exafmm_server_submit_step": (_c_int, [_vp, _c_ll, _c_double, ctypes.c_ulonglong, _vp, _vp,
+                                               ctypes.POINTER(_c_ll)]),
+        "exafmm_server_session_bodies": (_c_int, [_vp, _c_ll, _vp]),
+        "exafmm_server_close_session": (_c_int, [_vp, _c_ll]),
+        "exafmm_server_set_grouping": (_c_int, [_vp, _c_int, _c_ll, _c_ll]),
+        "exafmm_server_grouped": (_c_int, [_vp, ctypes.POINTER(_c_ll)]),
+        "exafmm_displace_bodies": (_c_int, [_vp, _c_double, ctypes.c_ulonglong]),
+        "exafmm_get_bodies": (_c_int, [_vp, _vp]),
+        "exafmm_get_bodies_device": (_c_int, [_vp, _vp]),
         "exafmm_ewald": (_c_int, [_vp, _c_ll, _c_int, _c_double, _c_double, _c_double, _c_double, _vp]),
         "exafmm_ewald_error": (ctypes.c_char_p, []),
         "exafmm_dipole_correction": (_c_int, [_vp, _vp, _c_ll]),
@@ -317,6 +328,17 @@ class Fmm:
         r = self.results(out)
         off = np.concatenate([[0], np.cumsum(self._sizes)])
         return [r[off[i]:off[i + 1]] for i in range(self.nsys)]
+
+    def displace_bodies(self, sigma: float, seed: int):
+        """Move every body in place on the device by sigma times three standard normals
+        (a counter-based stream keyed by seed and body index); the next solve rebuilds."""
+        self._check(lib().exafmm_displace_bodies(self._h, float(sigma), int(seed) & (2**64 - 1)))
+
+    def bodies(self) -> np.ndarray:
+        """The context's current bodies (caller order)."""
+        x = np.zeros((self.n, 4))
+        self._check(lib().exafmm_get_bodies(self._h, _p(x)))
+        return x
 
     def get_bounds(self) -> np.ndarray:
         b = np.zeros(6)
@@ -663,8 +685,55 @@ class Server:
             raise FmmError(lib().exafmm_server_error().decode())
         return o, t
 
+    # ---- device-resident repeat chains ----
+    def open_session(self, xyzq, P=10, theta=0.4, ncrit=64, nspawn=5000, precision=FP64) -> int:
+        """A chain of solves of one system kept on the device between steps."""
+        x = _f64(xyzq, 4)
+        sid = _c_ll()
+        rc = lib().exafmm_server_open_session(self._h, _p(x), len(x), P, theta, ncrit, nspawn, precision,
+                                              ctypes.byref(sid))
+        if rc != 0:
+            raise FmmError(f"exafmm_server_open_session failed ({rc})")
+        self._live[("session", sid.value)] = x
+        return sid.value
+
+    def submit_step(self, session: int, sigma=0.0, seed=0, d_xyzq: int | None = None, out=None) -> int:
+        """The session's next step: the first solves the opened bodies, later ones
+        move them on the device (to d_xyzq, or by a Gaussian step of sigma drawn from
+        seed) and solve again."""
+        n = len(self._live[("session", session)])
+        o = np.zeros((n, 4)) if out is None else out
+        assert o.dtype == np.float64 and o.shape == (n, 4) and o.flags.c_contiguous
+        t = _c_ll()
+        rc = lib().exafmm_server_submit_step(self._h, session, float(sigma), int(seed) & (2**64 - 1),
+                                             _vp(d_xyzq) if d_xyzq else None, _p(o), ctypes.byref(t))
+        if rc != 0:
+            raise FmmError(lib().exafmm_server_error().decode() or f"exafmm_server_submit_step failed ({rc})")
+        self._live[t.value] = (None, o)
+        return t.value
+
+    def session_bodies(self, session: int) -> np.ndarray:
+        x = np.zeros_like(self._live[("session", session)])
+        if lib().exafmm_server_session_bodies(self._h, session, _p(x)) != 0:
+            raise FmmError(lib().exafmm_server_error().decode())
+        return x
+
+    def close_session(self, session: int):
+        if lib().exafmm_server_close_session(self._h, session) != 0:
+            raise FmmError(lib().exafmm_server_error().decode())
+        self._live.pop(("session", session), None)
+
+    def set_grouping(self, max_requests=64, max_request_bodies=262144, max_group_bodies=4 << 20):
+        """Continuous batching of small queued requests with equal parameters into
+        one forest solve (max_requests=1: off)."""
+        if lib().exafmm_server_set_grouping(self._h, int(max_requests), int(max_request_bodies),
+                                            int(max_group_bodies)) != 0:
+            raise FmmError("invalid grouping limits")
+
     def stats(self) -> dict:
         v = np.zeros(6)
         lib().exafmm_server_stats(self._h, _p(v))
+        g = _c_ll()
+        lib().exafmm_server_grouped(self._h, ctypes.byref(g))
         return dict(in_flight=v[0], held=v[1], peak_admitted=v[2], completed=int(v[3]), queued=int(v[4]),
-                    budget=v[5])
+                    budget=v[5], grouped=int(g.value))

@@ -1,5 +1,6 @@
 // extern "C" surface of the engine (include/exafmm_b200.h) and the solve driver.
 #include <atomic>
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -451,6 +452,8 @@ struct Engine {
   }
 
   void results(double *dst, cudaMemcpyKind kind, double *const *parts = nullptr);
+  void displace(double sigma, unsigned long long seed);
+  void bodies(double *dst, cudaMemcpyKind kind);
 
   void get_dipole(const double *X0, double *dipole3) {
     const double zero[3] = {0.0, 0.0, 0.0};
@@ -473,7 +476,52 @@ __global__ void k_unsort(const double4 *trg, const int *perm, long long n, doubl
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     out[perm[i]] = trg[i];
 }
+
+// SplitMix64 (Steele, Lea and Flood 2014; Vigna's constants): a counter-based
+// stream, one 64-bit word per (seed, counter).
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+// uniform in (0, 1]: the top 53 bits, plus one ulp
+__device__ __forceinline__ double unit53(unsigned long long w) { return ((w >> 11) + 1) * 0x1.0p-53; }
+
+// Body i moves by sigma times three standard normals drawn by the Box-Muller
+// transform from four uniforms of the stream at counters 4i..4i+3 (the fourth
+// normal is dropped), so a displacement depends only on (seed, i).
+__global__ void k_displace(double4 *x, long long n, double sigma, unsigned long long seed) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const unsigned long long c = seed * 0x2545f4914f6cdd1dull + 4ull * (unsigned long long)i;
+    const double u0 = unit53(splitmix64(c)), u1 = unit53(splitmix64(c + 1));
+    const double u2 = unit53(splitmix64(c + 2)), u3 = unit53(splitmix64(c + 3));
+    const double r0 = sqrt(-2.0 * log(u0)), r1 = sqrt(-2.0 * log(u2));
+    double s0, c0, s1, c1;
+    sincospi(2.0 * u1, &s0, &c0);
+    sincospi(2.0 * u3, &s1, &c1);
+    double4 b = x[i];
+    b.x += sigma * r0 * c0;
+    b.y += sigma * r0 * s0;
+    b.z += sigma * r1 * c1;
+    x[i] = b;
+  }
+}
 }  // namespace
+
+void Engine::displace(double sigma, unsigned long long seed) {
+  const long long n = C.tree.n;
+  if (n) {
+    k_displace<<<kNumSMs * 4, 256, 0, C.stream>>>(C.tree.xyzq.p, n, sigma, seed);
+    EXA_CHECK_LAUNCH();
+  }
+  tree_ok = up_ok = lists_ok = false;
+}
+
+void Engine::bodies(double *dst, cudaMemcpyKind kind) {
+  if (C.tree.n) EXA_CUDA(cudaMemcpyAsync(dst, C.tree.xyzq.p, C.tree.n * sizeof(double4), kind, C.stream));
+  EXA_CUDA(cudaStreamSynchronize(C.stream));
+}
 
 // parts (a forest only): one destination per system, host or device memory.
 void Engine::results(double *dst, cudaMemcpyKind kind, double *const *parts) {
@@ -718,6 +766,28 @@ int exafmm_set_systems_device(exafmm_ctx *ctx, int count, const long long *n, co
   return guarded(ctx, [&] {
     cudaSetDevice(ctx->E.C.device);
     ctx->E.set_systems(count, n, d_xyzq, cudaMemcpyDeviceToDevice);
+  });
+}
+
+int exafmm_displace_bodies(exafmm_ctx *ctx, double sigma, unsigned long long seed) {
+  return guarded(ctx, [&] {
+    if (!(sigma >= 0) || !std::isfinite(sigma)) throw std::runtime_error("sigma must be finite and >= 0");
+    cudaSetDevice(ctx->E.C.device);
+    ctx->E.displace(sigma, seed);
+  });
+}
+
+int exafmm_get_bodies(exafmm_ctx *ctx, double *xyzq) {
+  return guarded(ctx, [&] {
+    cudaSetDevice(ctx->E.C.device);
+    ctx->E.bodies(xyzq, cudaMemcpyDeviceToHost);
+  });
+}
+
+int exafmm_get_bodies_device(exafmm_ctx *ctx, double *d_xyzq) {
+  return guarded(ctx, [&] {
+    cudaSetDevice(ctx->E.C.device);
+    ctx->E.bodies(d_xyzq, cudaMemcpyDeviceToDevice);
   });
 }
 

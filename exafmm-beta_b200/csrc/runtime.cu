@@ -163,11 +163,11 @@ struct Slot {
                       const double *const *xyzq, double *const *trg, cudaEvent_t start, cudaEvent_t done) {
     prepare(device, p, pol);
     cudaStream_t st = (cudaStream_t)exafmm_stream(ctx);
-    if (cudaStreamWaitEvent(st, start, 0) != cudaSuccess) throw std::runtime_error("cudaStreamWaitEvent");
+    if (start && cudaStreamWaitEvent(st, start, 0) != cudaSuccess) throw std::runtime_error("cudaStreamWaitEvent");
     check(exafmm_set_systems_list(ctx, count, n, xyzq));
     check(exafmm_solve(ctx));
     check(exafmm_get_results_list(ctx, trg));
-    if (cudaEventRecord(done, st) != cudaSuccess) throw std::runtime_error("cudaEventRecord");
+    if (done && cudaEventRecord(done, st) != cudaSuccess) throw std::runtime_error("cudaEventRecord");
     double ms[8];
     check(exafmm_phase_times(ctx, ms));
     return ms[7];
@@ -265,12 +265,34 @@ int forest_buckets(int count, const long long *n, int buckets, int *bucket_of, s
 // ================================================================ server
 namespace {
 
+// A repeat chain kept on the device: one context holds the chain's bodies,
+// tree and expansions between steps; each step after the first moves the
+// bodies in place on the device (or takes new positions from device memory)
+// and solves again, so no step uploads bodies from the host.
+struct Session {
+  long long id = 0;
+  SolveParams prm;
+  const double *xyzq0 = nullptr;  // the first step's bodies (host)
+  long long n = 0;
+  exafmm_ctx *ctx = nullptr;
+  long long held = 0;             // the context's device bytes while no step runs
+  bool busy = false;              // a step is queued or running
+  int steps = 0;                  // steps completed
+  ~Session() {
+    if (ctx) exafmm_destroy(ctx);
+  }
+};
+
 struct Request {
   long long id = 0;
   SolveParams prm;
   const double *xyzq = nullptr;
   long long n = 0;
   double *trg = nullptr;
+  Session *sess = nullptr;        // a chain step (prm and n are the session's)
+  double sigma = 0;
+  unsigned long long seed = 0;
+  const double *d_xyzq = nullptr; // a chain step's new positions in device memory (or null)
   long long est_bytes = 0;   // estimate at submission, then the bytes charged while in flight
   Clock::time_point t_submit, t_start, t_end;
   double device_ms = 0;
@@ -293,10 +315,20 @@ struct exafmm_server {
   std::unordered_map<long long, std::unique_ptr<Request>> reqs;
   std::vector<Slot> slots;
   std::vector<long long> held;     // device bytes held by each worker's idle context
+  std::unordered_map<long long, std::unique_ptr<Session>> sessions;
+  long long session_held = 0;      // device bytes held by sessions between steps
+  long long next_session = 1;
   long long in_flight = 0;         // bytes charged to the requests being solved
   int running = 0;                 // requests being solved
   long long peak_admitted = 0;
   long long next_id = 1, completed = 0;
+  // continuous batching: queued requests of at most group_max_n bodies with
+  // the same parameters are solved together as one forest, up to group_max
+  // requests and group_bodies bodies (group_max <= 1: one request per solve)
+  int group_max = 64;
+  long long group_max_n = 262144;
+  long long group_bodies = 4LL << 20;
+  long long grouped = 0;           // requests solved inside a group of two or more
   bool stop = false;
   std::vector<std::thread> threads;
 
@@ -311,22 +343,55 @@ struct exafmm_server {
   }
 
   long long held_total(int except) const {
-    long long s = 0;
+    long long s = session_held;
     for (int w = 0; w < (int)held.size(); w++)
       if (w != except) s += held[w];
     return s;
   }
 
+  // What a request brings onto the device: a chain step its session's context
+  // (which it then no longer holds idle), any other request the estimate or
+  // the worker context it will use.
+  long long charge_of(const Request *r, int w) const {
+    return r->sess ? std::max(r->est_bytes, r->sess->held) : std::max(r->est_bytes, held[w]);
+  }
+
   // Head-of-line admission: the request fits beside what the other workers
-  // hold and what is in flight; with nothing in flight it is always admitted,
-  // so a request larger than the budget still runs (alone).
+  // and the idle sessions hold and what is in flight; with nothing in flight
+  // it is always admitted, so a request larger than the budget still runs
+  // (alone).
   bool admissible(const Request *r, int w) const {
     if (running == 0) return true;
-    return (double)(held_total(w) + in_flight + std::max(r->est_bytes, held[w])) <= budget;
+    const long long others = held_total(w) - (r->sess ? r->sess->held : 0) + (r->sess ? held[w] : 0);
+    return (double)(others + in_flight + charge_of(r, w)) <= budget;
+  }
+
+  // One chain step on the session's own context.
+  double run_step(Request *r) {
+    Session *q = r->sess;
+    auto check = [&](int rc) {
+      if (rc != 0) throw std::runtime_error(exafmm_last_error(q->ctx));
+    };
+    if (!q->ctx) {
+      if (exafmm_create(&q->ctx, q->prm.P, q->prm.theta, q->prm.ncrit, q->prm.nspawn, q->prm.images, q->prm.cycle,
+                        q->prm.precision, device) != 0) {
+        q->ctx = nullptr;
+        throw std::runtime_error(exafmm_create_error());
+      }
+    }
+    if (q->steps == 0) check(exafmm_set_bodies(q->ctx, q->xyzq0, q->n));
+    else if (r->d_xyzq) check(exafmm_set_bodies_device(q->ctx, r->d_xyzq, q->n));
+    else check(exafmm_displace_bodies(q->ctx, r->sigma, r->seed));
+    check(exafmm_solve(q->ctx));
+    check(exafmm_get_results(q->ctx, r->trg));
+    double ms[8];
+    check(exafmm_phase_times(q->ctx, ms));
+    return ms[7];
   }
 
   void worker(int w) {
     cudaSetDevice(device);
+    std::vector<Request *> grp;
     for (;;) {
       Request *r = nullptr;
       {
@@ -335,47 +400,116 @@ struct exafmm_server {
         if (queue.empty()) return;
         r = queue.front();
         queue.pop_front();
-        const long long charge = std::max(r->est_bytes, held[w]);
+        grp.assign(1, r);
+        long long charge = charge_of(r, w);
+        if (!r->sess && group_max > 1 && r->n <= group_max_n) {
+          // the queued requests that can share this solve, in queue order,
+          // each joining only if the group still fits the budget (the head
+          // request alone is admitted as before)
+          long long bodies = r->n, est = r->est_bytes;
+          for (auto it = queue.begin(); it != queue.end() && (int)grp.size() < group_max;) {
+            Request *q = *it;
+            const long long est2 = est + q->est_bytes;
+            const long long charge2 = std::max(est2, held[w]);
+            if (!q->sess && q->n <= group_max_n && bodies + q->n <= group_bodies && same_params(q->prm, r->prm) &&
+                (double)(held_total(w) + in_flight + charge2) <= budget) {
+              grp.push_back(q);
+              bodies += q->n;
+              est = est2;
+              charge = charge2;
+              it = queue.erase(it);
+            } else {
+              ++it;
+            }
+          }
+        }
         in_flight += charge;
         running++;
-        held[w] = 0;
-        peak_admitted = std::max(peak_admitted, in_flight + held_total(w));
-        r->est_bytes = charge;
-        r->t_start = Clock::now();
+        if (r->sess) {
+          session_held -= r->sess->held;
+          r->sess->held = 0;
+        } else {
+          held[w] = 0;
+        }
+        peak_admitted = std::max(peak_admitted, in_flight + held_total(w) + held[w]);
+        r->est_bytes = charge;  // what is charged while the solve runs (the group's, on its first request)
+        const auto t = Clock::now();
+        for (Request *q : grp) q->t_start = t;
+        if (grp.size() > 1) grouped += (long long)grp.size();
       }
       int status = 0;
       std::string err;
       double dev_ms = 0;
       try {
-        dev_ms = slots[w].solve(device, r->prm, r->xyzq, r->n, r->trg);
+        if (r->sess) {
+          dev_ms = run_step(r);
+        } else if (grp.size() == 1) {
+          dev_ms = slots[w].solve(device, r->prm, r->xyzq, r->n, r->trg);
+        } else {
+          std::vector<long long> nn(grp.size());
+          std::vector<const double *> in(grp.size());
+          std::vector<double *> out(grp.size());
+          for (size_t j = 0; j < grp.size(); j++) {
+            nn[j] = grp[j]->n;
+            in[j] = grp[j]->xyzq;
+            out[j] = grp[j]->trg;
+          }
+          dev_ms = slots[w].solve_forest(device, r->prm, nullptr, (int)grp.size(), nn.data(), in.data(), out.data(),
+                                         nullptr, nullptr);
+        }
       } catch (const std::exception &e) {
         status = 1;
         err = e.what();
-        slots[w].release();
+        if (r->sess) {
+          if (r->sess->ctx) exafmm_destroy(r->sess->ctx);
+          r->sess->ctx = nullptr;
+        } else {
+          slots[w].release();
+        }
       }
-      const long long now_held = slots[w].bytes();
+      long long sess_bytes = 0;
+      if (r->sess && r->sess->ctx) exafmm_device_bytes(r->sess->ctx, &sess_bytes);
+      const long long now_held = r->sess ? 0 : slots[w].bytes();
       bool release = false;
       {
         std::lock_guard<std::mutex> lk(mu);
         in_flight -= r->est_bytes;
         running--;
-        // keep the context for reuse unless idle contexts crowd the budget
-        release = (double)(held_total(w) + now_held) > 0.5 * budget;
-        held[w] = release ? 0 : now_held;
+        if (r->sess) {
+          r->sess->held = sess_bytes;
+          session_held += sess_bytes;
+          if (status == 0) r->sess->steps++;
+          r->sess->busy = false;
+        } else {
+          // keep the context for reuse unless idle contexts crowd the budget
+          release = (double)(held_total(w) + now_held) > 0.5 * budget;
+          held[w] = release ? 0 : now_held;
+        }
       }
       if (release) slots[w].release();
       {
         std::lock_guard<std::mutex> lk(mu);
-        r->t_end = Clock::now();
-        r->device_ms = dev_ms;
-        r->status = status;
-        r->err = err;
-        r->done = true;
-        completed++;
+        const auto t = Clock::now();
+        long long bodies = 0;
+        for (Request *q : grp) bodies += q->n;
+        for (Request *q : grp) {
+          q->t_end = t;
+          // a group's device time is shared in proportion to the bodies
+          q->device_ms = grp.size() == 1 ? dev_ms : (bodies > 0 ? dev_ms * (double)q->n / (double)bodies : 0.0);
+          q->status = status;
+          q->err = err;
+          q->done = true;
+          completed++;
+        }
       }
       cv_done.notify_all();
       cv_work.notify_all();
     }
+  }
+
+  static bool same_params(const SolveParams &a, const SolveParams &b) {
+    return a.P == b.P && a.theta == b.theta && a.ncrit == b.ncrit && a.nspawn == b.nspawn && a.images == b.images &&
+           a.cycle == b.cycle && a.precision == b.precision;
   }
 };
 
@@ -650,6 +784,7 @@ int exafmm_server_destroy(exafmm_server *s) {
   }
   s->cv_work.notify_all();
   for (auto &t : s->threads) t.join();
+  cudaSetDevice(s->device);  // the sessions' contexts are released with it
   delete s;
   return 0;
 }
@@ -679,6 +814,104 @@ int exafmm_server_submit(exafmm_server *s, const double *xyzq, long long n, doub
     s->reqs.emplace(r->id, std::move(r));
   }
   s->cv_work.notify_all();
+  return 0;
+}
+
+int exafmm_server_open_session(exafmm_server *s, const double *xyzq, long long n, int P, double theta, int ncrit,
+                               int nspawn, int precision, long long *session) {
+  if (!s || !session || n < 0 || (n > 0 && !xyzq)) return 2;
+  if (P < 2 || P > 20 || ncrit < 1 || !(theta > 0)) return 2;
+  if (precision != EXAFMM_FP64 && precision != EXAFMM_MIXED) return 2;
+  auto q = std::make_unique<Session>();
+  q->prm.P = P;
+  q->prm.theta = theta;
+  q->prm.ncrit = ncrit;
+  q->prm.nspawn = nspawn;
+  q->prm.precision = precision;
+  q->xyzq0 = xyzq;
+  q->n = n;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->stop) return 1;
+  q->id = s->next_session++;
+  *session = q->id;
+  s->sessions.emplace(q->id, std::move(q));
+  return 0;
+}
+
+int exafmm_server_submit_step(exafmm_server *s, long long session, double sigma, unsigned long long seed,
+                              const double *d_xyzq, double *trg, long long *ticket) {
+  if (!s || !ticket || !(sigma >= 0) || !std::isfinite(sigma)) return 2;
+  auto r = std::make_unique<Request>();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) return 1;
+    auto it = s->sessions.find(session);
+    if (it == s->sessions.end()) {
+      g_server_error = "unknown session";
+      return 2;
+    }
+    Session *q = it->second.get();
+    if (q->busy) {
+      g_server_error = "the session's previous step has not completed";
+      return 2;
+    }
+    if (q->n > 0 && !trg) return 2;
+    q->busy = true;
+    r->sess = q;
+    r->prm = q->prm;
+    r->n = q->n;
+    r->trg = trg;
+    r->sigma = sigma;
+    r->seed = seed;
+    r->d_xyzq = d_xyzq;
+    r->t_submit = Clock::now();
+    r->id = s->next_id++;
+    r->est_bytes = s->estimate(q->n, q->prm.P);
+    *ticket = r->id;
+    s->queue.push_back(r.get());
+    s->reqs.emplace(r->id, std::move(r));
+  }
+  s->cv_work.notify_all();
+  return 0;
+}
+
+int exafmm_server_session_bodies(exafmm_server *s, long long session, double *xyzq) {
+  if (!s || !xyzq) return 2;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->sessions.find(session);
+  if (it == s->sessions.end() || it->second->busy || !it->second->ctx) {
+    g_server_error = "no such idle session with a completed step";
+    return 2;
+  }
+  cudaSetDevice(s->device);
+  if (exafmm_get_bodies(it->second->ctx, xyzq) != 0) {
+    g_server_error = exafmm_last_error(it->second->ctx);
+    return 1;
+  }
+  return 0;
+}
+
+int exafmm_server_close_session(exafmm_server *s, long long session) {
+  if (!s) return 2;
+  std::unique_ptr<Session> q;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->sessions.find(session);
+    if (it == s->sessions.end()) {
+      g_server_error = "unknown session";
+      return 2;
+    }
+    if (it->second->busy) {
+      g_server_error = "the session has a step in flight";
+      return 2;
+    }
+    s->session_held -= it->second->held;
+    q = std::move(it->second);
+    s->sessions.erase(it);
+  }
+  cudaSetDevice(s->device);
+  q.reset();
+  s->cv_work.notify_all();  // its bytes are free for queued requests
   return 0;
 }
 
@@ -728,6 +961,23 @@ int exafmm_server_stats(exafmm_server *s, double *stats6) {
   stats6[3] = (double)s->completed;
   stats6[4] = (double)s->queue.size();
   stats6[5] = s->budget;
+  return 0;
+}
+
+int exafmm_server_set_grouping(exafmm_server *s, int max_requests, long long max_request_bodies,
+                               long long max_group_bodies) {
+  if (!s || max_requests < 1 || max_requests > 4096 || max_request_bodies < 0 || max_group_bodies < 1) return 2;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->group_max = max_requests;
+  s->group_max_n = max_request_bodies;
+  s->group_bodies = max_group_bodies;
+  return 0;
+}
+
+int exafmm_server_grouped(exafmm_server *s, long long *requests) {
+  if (!s || !requests) return 2;
+  std::lock_guard<std::mutex> lk(s->mu);
+  *requests = s->grouped;
   return 0;
 }
 

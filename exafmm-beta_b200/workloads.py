@@ -96,17 +96,53 @@ class Completion:
     P: int
     latency_ms: float             # scheduled arrival (or previous step's return) to results on the host
     times: np.ndarray = field(default_factory=lambda: np.zeros(4))
+    end_s: float = 0.0            # completion, seconds from the start of the replay
+    steps: int = 1                # steps of its job (1: a single solve)
+
+
+def chain_seed(job: Job, step: int) -> int:
+    """Seed of a chain step's device-side displacement (the same in every replay)."""
+    return job.seed * 1_000_003 + step
 
 
 def replay(server, trace: Trace, precision: int, ncrit: int = 64, nspawn: int = 5000, poll_s: float = 2e-4,
-           clock=time.perf_counter, sleep=time.sleep, deadline_s: float | None = None):
+           clock=time.perf_counter, sleep=time.sleep, deadline_s: float | None = None,
+           device_chains: bool | None = None, samples: dict | None = None, sample_size: int = 256,
+           host_alloc=None):
     """Replays the trace against `server` (submit(x, P=, theta=, ncrit=, nspawn=, precision=) -> ticket,
     done(ticket) -> bool, wait(ticket) -> (results, times)).  Returns the completions and the wall time.
-    With deadline_s, a replay that runs longer raises instead of waiting on."""
+    With deadline_s, a replay that runs longer raises instead of waiting on.
+
+    Chains run device-resident when the server has sessions (open_session / submit_step /
+    session_bodies / close_session; device_chains=None means whenever it does): the first step
+    uploads the bodies, every later step moves them on the device by a Gaussian step of the
+    job's sigma (seed chain_seed(job, step)) and solves again.  Otherwise each step is displaced
+    on the host and submitted as a new request.
+
+    samples (a dict) receives, per job, the final step's results on `sample_size` strided
+    targets: {job: (target indices, results there, final bodies or None when they are the
+    job's initial bodies)}.
+
+    host_alloc(shape) -> float64 array, if given, allocates the requests' host
+    buffers (pinned memory, for instance); they are filled before the clock starts."""
+    if device_chains is None:
+        device_chains = hasattr(server, "open_session")
+    # the requests' inputs exist before the replay starts (generating them is
+    # not the server's work): every job's bodies, and a result buffer whose
+    # pages are already touched
+    alloc = host_alloc or (lambda shape: np.empty(shape))
+    inputs, outputs = {}, {}
+    for k, j in enumerate(trace.jobs):
+        x = alloc((j.n, 4))
+        x[:] = job_bodies(j)
+        o = alloc((j.n, 4))
+        o.fill(0.0)
+        inputs[k], outputs[k] = x, o
     events = [(j.arrival, k, 0) for k, j in enumerate(trace.jobs)]  # (due time, job, step)
     heapq.heapify(events)
     pending = {}           # ticket -> (job, step, due)
-    bodies = {}            # job -> current bodies (chains)
+    bodies = {}            # job -> current bodies (chains displaced on the host)
+    sessions = {}          # job -> session (device-resident chains)
     rngs = {}
     done = []
     t0 = clock()
@@ -117,26 +153,46 @@ def replay(server, trace: Trace, precision: int, ncrit: int = 64, nspawn: int = 
         while events and events[0][0] <= now:
             due, k, step = heapq.heappop(events)
             job = trace.jobs[k]
-            if step == 0:
-                x = job_bodies(job)
-                rngs[k] = np.random.default_rng(job.seed + 7)
+            if job.steps > 1 and device_chains:
+                if step == 0:
+                    sessions[k] = server.open_session(inputs[k], P=job.P, theta=trace.theta, ncrit=ncrit,
+                                                      nspawn=nspawn, precision=precision)
+                    tk = server.submit_step(sessions[k], out=outputs[k])
+                else:
+                    tk = server.submit_step(sessions[k], sigma=job.sigma, seed=chain_seed(job, step), out=outputs[k])
             else:
-                x = displace(bodies[k], job.sigma, rngs[k])
-            bodies[k] = x
-            tk = server.submit(x, P=job.P, theta=trace.theta, ncrit=ncrit, nspawn=nspawn, precision=precision)
+                if step == 0:
+                    x = inputs[k]
+                    rngs[k] = np.random.default_rng(job.seed + 7)
+                else:
+                    x = displace(bodies[k], job.sigma, rngs[k])
+                bodies[k] = x
+                tk = server.submit(x, P=job.P, theta=trace.theta, ncrit=ncrit, nspawn=nspawn, precision=precision,
+                                   out=outputs[k])
             pending[tk] = (k, step, due)
         finished = [tk for tk in pending if server.done(tk)]
         for tk in finished:
             k, step, due = pending.pop(tk)
-            _, times = server.wait(tk)
+            res, times = server.wait(tk)
             end = clock() - t0
             job = trace.jobs[k]
-            done.append(Completion(job=k, step=step, n=job.n, P=job.P, latency_ms=1e3 * (end - due), times=times))
+            done.append(Completion(job=k, step=step, n=job.n, P=job.P, latency_ms=1e3 * (end - due), times=times,
+                                   end_s=end, steps=job.steps))
             if step + 1 < job.steps:
                 heapq.heappush(events, (end, k, step + 1))
             else:
+                if samples is not None:
+                    idx = datasets.strided_sample(job.n, sample_size)
+                    final = None
+                    if job.steps > 1:
+                        final = server.session_bodies(sessions[k]) if k in sessions else bodies[k]
+                    samples[k] = (idx, np.array(res[idx]), final)
+                if k in sessions:
+                    server.close_session(sessions.pop(k))
                 bodies.pop(k, None)
                 rngs.pop(k, None)
+                inputs.pop(k, None)
+                outputs.pop(k, None)
         if not finished:
             if events and not pending:
                 sleep(max(0.0, min(events[0][0] - (clock() - t0), 0.01)))
@@ -148,6 +204,25 @@ def replay(server, trace: Trace, precision: int, ncrit: int = 64, nspawn: int = 
 def latency_summary(done, wall_s: float) -> dict:
     lat = np.array([c.latency_ms for c in done]) if done else np.zeros(1)
     bodies = sum(c.n for c in done)
-    return {"requests": len(done), "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-            "mean_ms": float(lat.mean()), "bodies_per_s": bodies / wall_s if wall_s > 0 else 0.0,
-            "wall_s": wall_s}
+    out = {"requests": len(done), "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+           "mean_ms": float(lat.mean()), "bodies_per_s": bodies / wall_s if wall_s > 0 else 0.0,
+           "wall_s": wall_s}
+    chain = [c.latency_ms for c in done if c.steps > 1 and c.step > 0]
+    if chain:
+        out["chain_step_p50_ms"] = float(np.percentile(chain, 50))
+        out["chain_step_p99_ms"] = float(np.percentile(chain, 99))
+    return out
+
+
+def saturated_throughput(done) -> dict:
+    """Bodies/s while a saturated replay still has single solves to run: every
+    completion up to the last single solve's, over that time.  After it only the
+    repeat chains' remaining steps are left, one step at a time each, which
+    measures their sequential latency rather than the server's throughput."""
+    singles = [c.end_s for c in done if c.steps == 1]
+    if not singles:
+        return {"bodies_per_s": 0.0, "window_s": 0.0, "requests": 0}
+    t = max(singles)
+    inside = [c for c in done if c.end_s <= t]
+    return {"bodies_per_s": sum(c.n for c in inside) / t if t > 0 else 0.0, "window_s": t,
+            "requests": len(inside), "bodies": sum(c.n for c in inside)}

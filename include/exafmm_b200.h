@@ -112,6 +112,19 @@ int exafmm_get_systems(exafmm_ctx *ctx, long long *cell_base, long long *body_of
 int exafmm_set_systems_list(exafmm_ctx *ctx, int count, const long long *n, const double *const *xyzq);
 int exafmm_get_results_list(exafmm_ctx *ctx, double *const *trg);
 
+/* Repeated MD-style solves without a host round trip (no counterpart in the
+ * reference, whose MD wrappers re-partition and re-upload every step,
+ * wrappers/gromacs.cxx:139-190): every body's position moves in place on the
+ * device by sigma times three standard normals drawn from a counter-based
+ * stream (SplitMix64 words by (seed, body index), Box-Muller), so the move
+ * depends only on (seed, sigma, body index); the next solve rebuilds the tree
+ * on the device.  An MD code that integrates on the GPU passes its new
+ * positions with exafmm_set_bodies_device instead. */
+int exafmm_displace_bodies(exafmm_ctx *ctx, double sigma, unsigned long long seed);
+/* The context's current bodies (caller order, n x 4), to host or device memory. */
+int exafmm_get_bodies(exafmm_ctx *ctx, double *xyzq);
+int exafmm_get_bodies_device(exafmm_ctx *ctx, double *d_xyzq);
+
 /* BoundBox::getBounds(Bodies&) (include/bound_box.h:11-25), including its
  * sequential 1e-5 drift, evaluated on the device in closed form; with separate
  * sources, extended by them as getBounds(jbodies, bounds) does
@@ -301,6 +314,27 @@ int exafmm_server_destroy(exafmm_server *s);
 int exafmm_server_submit(exafmm_server *s, const double *xyzq, long long n, double *trg, int P, double theta,
                          int ncrit, int nspawn, int precision, long long *ticket);
 int exafmm_server_poll(exafmm_server *s, long long ticket, int *done);
+/* Device-resident repeat chains (an MD trajectory: one system solved step
+ * after step while its bodies move; no counterpart in the reference, whose MD
+ * wrappers rebuild from host data every step, wrappers/gromacs.cxx:139-190).
+ * A session owns one context that keeps the chain's bodies, tree and
+ * expansions on the device between steps; between steps its device bytes
+ * count against the budget as held.  xyzq (host, n x 4) must stay valid until
+ * the first step completes. */
+int exafmm_server_open_session(exafmm_server *s, const double *xyzq, long long n, int P, double theta, int ncrit,
+                               int nspawn, int precision, long long *session);
+/* Queues the session's next step (one at a time per session; status 2 while
+ * the previous one is in flight).  The first step solves the opened bodies;
+ * each later step first moves them on the device, to d_xyzq (device memory,
+ * n x 4) when it is not NULL, else by exafmm_displace_bodies(sigma, seed),
+ * and rebuilds the tree there.  Results go to trg (host, n x 4); wait / poll
+ * take the ticket as for exafmm_server_submit. */
+int exafmm_server_submit_step(exafmm_server *s, long long session, double sigma, unsigned long long seed,
+                              const double *d_xyzq, double *trg, long long *ticket);
+/* The session's current bodies (host, n x 4); the session must be idle. */
+int exafmm_server_session_bodies(exafmm_server *s, long long session, double *xyzq);
+/* Releases the session's context (status 2 while a step is in flight). */
+int exafmm_server_close_session(exafmm_server *s, long long session);
 /* Blocks until the request is done and releases its ticket.  times4: queue
  * wait, start to results on the host, submit to results on the host (ms), and
  * the solve's device time (ms).  Returns the request's status. */
@@ -308,6 +342,17 @@ int exafmm_server_wait(exafmm_server *s, long long ticket, double *times4);
 /* stats6: bytes in flight, bytes held by idle contexts, peak admitted bytes,
  * completed requests, queued requests, budget. */
 int exafmm_server_stats(exafmm_server *s, double *stats6);
+/* Continuous batching: a worker that takes a request of at most
+ * max_request_bodies bodies also takes the queued requests (in queue order)
+ * of at most that size with the same parameters, up to max_requests requests
+ * and max_group_bodies bodies in all, each admitted against the budget as it
+ * joins, and solves them as one forest (exafmm_set_systems_list): every
+ * request gets the bits of its solo solve.  Chain steps are never grouped.
+ * max_requests = 1 turns grouping off.  Defaults: 64, 262144, 4194304. */
+int exafmm_server_set_grouping(exafmm_server *s, int max_requests, long long max_request_bodies,
+                               long long max_group_bodies);
+/* Requests solved so far inside a group of two or more. */
+int exafmm_server_grouped(exafmm_server *s, long long *requests);
 /* Error text of the last failed exafmm_server_wait on this thread. */
 const char *exafmm_server_error(void);
 

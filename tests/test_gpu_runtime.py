@@ -148,3 +148,74 @@ def test_forest_batch_autotune_per_group(ex, datasets):
     assert all(np.array_equal(a, c) for a, c in zip(o1, b2.solve(xs)))
     b2.close()
     b.close()
+
+
+def test_server_chain_steps_stay_on_the_device(ex, datasets):
+    """A session's step k (bodies moved on the device, tree rebuilt there) gives
+    the bits of a fresh solve of the same positions, alone or beside other
+    requests; the first step solves the opened bodies."""
+    s = ex.Server(workers=3, hbm_budget_bytes=40e9)
+    x = datasets.plummer(20000, seed=21)
+    kw = dict(P=8, theta=0.4, ncrit=64, precision=ex.MIXED)
+    sid = s.open_session(x, **kw)
+    r0, _ = s.wait(s.submit_step(sid))
+    assert np.array_equal(r0, _alone(ex, x, **kw))
+    assert np.array_equal(s.session_bodies(sid), x)
+    sigma = 1e-3 * (4 / 3 * np.pi / len(x)) ** (1 / 3)
+    prev = x
+    for k in range(1, 4):
+        other = s.submit(datasets.cube(30000, seed=k), P=6, theta=0.4, ncrit=32)
+        rk, _ = s.wait(s.submit_step(sid, sigma=sigma, seed=1000 + k))
+        s.wait(other)
+        xk = s.session_bodies(sid)
+        moved = xk[:, :3] - prev[:, :3]
+        assert np.array_equal(xk[:, 3], x[:, 3]) and 0 < np.abs(moved).max() < 20 * sigma
+        assert abs(np.std(moved) / sigma - 1) < 0.05
+        assert np.array_equal(rk, _alone(ex, xk, **kw))
+        prev = xk
+    # the displacement depends only on (seed, sigma, body index)
+    f = ex.Fmm(**kw)
+    f.set_bodies(x)
+    f.displace_bodies(sigma, 1001)
+    sid2 = s.open_session(x, **kw)
+    s.wait(s.submit_step(sid2))
+    s.wait(s.submit_step(sid2, sigma=sigma, seed=1001))
+    assert np.array_equal(f.bodies(), s.session_bodies(sid2))
+    f.close()
+    with pytest.raises(ex.FmmError):        # one step at a time per session
+        t = s.submit_step(sid, sigma=sigma, seed=7)
+        s.submit_step(sid, sigma=sigma, seed=8)
+    s.wait(t)
+    s.close_session(sid)
+    s.close_session(sid2)
+    st = s.stats()
+    assert st["queued"] == 0 and st["in_flight"] == 0
+    s.close()
+
+
+def test_server_groups_small_queued_requests_into_one_forest(ex, datasets):
+    """Continuous batching: small requests with equal parameters that queue behind
+    a running one are solved together as a forest; each still gets its solo bits,
+    and requests with other parameters are not mixed in."""
+    s = ex.Server(workers=1, hbm_budget_bytes=40e9)
+    big = s.submit(datasets.plummer(400000, seed=3), P=8, theta=0.4, ncrit=64, precision=ex.MIXED)
+    kw = dict(P=8, theta=0.4, ncrit=64, precision=ex.MIXED)
+    xs = _systems(datasets, 12, 1000, 30000, 900)
+    tickets = [s.submit(x, **kw) for x in xs]
+    odd = datasets.cube(5000, seed=5)
+    t_odd = s.submit(odd, P=6, theta=0.4, ncrit=64, precision=ex.MIXED)
+    s.wait(big)
+    outs = [s.wait(t)[0] for t in tickets]
+    r_odd, _ = s.wait(t_odd)
+    assert s.stats()["grouped"] >= 2
+    for x, o in zip(xs, outs):
+        assert np.array_equal(o, _alone(ex, x, **kw))
+    assert np.array_equal(r_odd, _alone(ex, odd, P=6, theta=0.4, ncrit=64, precision=ex.MIXED))
+    s.set_grouping(max_requests=1)     # off: one request per solve
+    g0 = s.stats()["grouped"]
+    big = s.submit(datasets.plummer(400000, seed=3), **kw)
+    tickets = [s.submit(x, **kw) for x in xs[:4]]
+    s.wait(big)
+    assert all(np.array_equal(s.wait(t)[0], o) for t, o in zip(tickets, outs[:4]))
+    assert s.stats()["grouped"] == g0
+    s.close()
