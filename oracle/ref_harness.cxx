@@ -41,8 +41,11 @@ namespace exafmm_laplace {
     C_iter C0;    // first target cell
     C_iter Cj0;   // first source cell (C0 unless the sources have their own tree)
     Kernel(int P, real_t eps2, complex_t wavek) : RefKernelBase(P, eps2, wavek) {}
+    // the traversal's tasks call these from several threads when threads > 1
+    std::mutex log_mutex;
     void M2L(C_iter Ci, C_iter Cj) {
       if (log) {
+        std::lock_guard<std::mutex> lock(log_mutex);
         log->m2l.push_back(int(Ci - C0));
         log->m2l.push_back(int(Cj - Cj0));
       }
@@ -50,6 +53,7 @@ namespace exafmm_laplace {
     }
     void P2P(C_iter Ci, C_iter Cj) {
       if (log) {
+        std::lock_guard<std::mutex> lock(log_mutex);
         log->p2p.push_back(int(Ci - C0));
         log->p2p.push_back(int(Cj - Cj0));
       }

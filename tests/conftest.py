@@ -61,7 +61,8 @@ def golden_cases():
     the MD ABI are separate)."""
     other = ("kernel_kat.npz", "records.npz", "md_gromacs.npz", "md_distributed.npz", "datasets_reference.npz")
     return sorted(p for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if os.path.basename(p) not in other and not os.path.basename(p).startswith(("periodic_", "inej_")))
+                  if os.path.basename(p) not in other
+                  and not os.path.basename(p).startswith(("periodic_", "inej_", "large_")))
 
 
 def periodic_golden_cases():

@@ -10,7 +10,7 @@ and the GPU engine to the reference's behaviour.
 Run from the repository root, with EXAFMM_REFERENCE_ROOT naming the
 exafmm-beta source tree (read only):
 
-    EXAFMM_REFERENCE_ROOT=/root/reference python tests/golden/make_golden.py [solve periodic kat records md inej datasets]
+    EXAFMM_REFERENCE_ROOT=/root/reference python tests/golden/make_golden.py [solve periodic kat records md inej datasets large]
 """
 from __future__ import annotations
 
@@ -283,7 +283,37 @@ def make_datasets():
     print("datasets_reference:", ", ".join(f"{k} {v.shape}" for k, v in data.items()))
 
 
-def main(which=("solve", "periodic", "kat", "records", "md", "inej", "datasets")):
+# Large all-positive case (the single large adaptive solve's distribution at a
+# size the reference finishes in about a minute on a few cores): the bodies are
+# regenerated from the seed at test time (their SHA-256 is stored to check
+# that), and the reference's results are kept on 4,096 strided targets plus
+# whole-run sums.
+# (name, generator, n, seed, P, theta, ncrit, nspawn, sample)
+LARGE_CASES = [
+    ("large_plummer_n1048576_p8", "plummer", 1 << 20, 77, 8, 0.35, 64, 5000, 4096),
+]
+
+
+def make_large(ref: Reference, name, gen, n, seed, P, theta, ncrit, nspawn, sample):
+    import hashlib
+    import time
+    x = getattr(datasets, gen)(n, seed)
+    t0 = time.perf_counter()
+    run = ref.solve(x, P=P, theta=theta, ncrit=ncrit, nspawn=nspawn, threads=os.cpu_count() or 1,
+                    record_lists=True)
+    dt = time.perf_counter() - t0
+    idx = datasets.strided_sample(n, sample)
+    data = dict(params=np.array([P, theta, ncrit, nspawn], dtype=np.float64), n=np.int64(n), seed=np.int64(seed),
+                generator=np.array(gen), xyzq_sha256=np.array(hashlib.sha256(x.tobytes()).hexdigest()),
+                bounds=run.bounds, ncells=np.int64(len(run.cells_int)), n_m2l=np.int64(len(run.m2l)),
+                n_p2p=np.int64(len(run.p2p)), idx=idx, trg=run.trg[idx],
+                pot_sum=np.float64(run.trg[:, 0].sum()), pot_sq_sum=np.float64((run.trg[:, 0] ** 2).sum()),
+                acc_sq_sum=np.float64((run.trg[:, 1:] ** 2).sum()))
+    np.savez_compressed(os.path.join(OUT, name + ".npz"), **data)
+    print(f"{name}: cells={len(run.cells_int)} m2l={len(run.m2l)} p2p={len(run.p2p)} ({dt:.1f} s)")
+
+
+def main(which=("solve", "periodic", "kat", "records", "md", "inej", "datasets", "large")):
     root = os.environ.get("EXAFMM_REFERENCE_ROOT")
     if not root or not os.path.isdir(os.path.join(root, "include")):
         raise SystemExit("set EXAFMM_REFERENCE_ROOT to the exafmm-beta source tree")
@@ -307,8 +337,11 @@ def main(which=("solve", "periodic", "kat", "records", "md", "inej", "datasets")
             make_inej(ref, *c)
     if "datasets" in which:
         make_datasets()
+    if "large" in which:
+        for c in LARGE_CASES:
+            make_large(ref, *c)
 
 
 if __name__ == "__main__":
-    # optional arguments: a subset of solve, periodic, kat, records, md, inej, datasets
-    main(tuple(sys.argv[1:]) or ("solve", "periodic", "kat", "records", "md", "inej", "datasets"))
+    # optional arguments: a subset of solve, periodic, kat, records, md, inej, datasets, large
+    main(tuple(sys.argv[1:]) or ("solve", "periodic", "kat", "records", "md", "inej", "datasets", "large"))

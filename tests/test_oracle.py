@@ -140,3 +140,22 @@ def test_oracle_ewald_matches_reference(oracle, reference):
         b = reference.ewald(x, ncrit=16, **kw)
         assert rel_l2(a[:, 0], b[:, 0]) < 1e-12
         assert rel_l2(a[:, 1:], b[:, 1:]) < 1e-12
+
+
+def test_restatement_matches_the_reference_on_the_large_fixture(oracle):
+    """The CPU restatement against the compiled reference's 1,048,576-body
+    all-positive Plummer run (sampled targets, whole-run sums and list sizes)."""
+    import hashlib
+    from conftest import GOLDEN, load_golden, load_package
+    load_package()
+    import exafmm_b200.datasets as datasets
+    g = load_golden(os.path.join(GOLDEN, "large_plummer_n1048576_p8.npz"))
+    x = getattr(datasets, str(g["generator"]))(int(g["n"]), int(g["seed"]))
+    assert hashlib.sha256(x.tobytes()).hexdigest() == str(g["xyzq_sha256"])
+    P, theta, ncrit, nspawn = g["params"]
+    a = oracle.solve(x, P=int(P), theta=float(theta), ncrit=int(ncrit), nspawn=int(nspawn))
+    assert np.array_equal(a.bounds, g["bounds"])
+    assert (len(a.cells_int), len(a.m2l), len(a.p2p)) == (int(g["ncells"]), int(g["n_m2l"]), int(g["n_p2p"]))
+    idx = g["idx"]
+    assert rel_l2(a.trg[idx], g["trg"]) < 1e-12
+    assert abs(a.trg[:, 0].sum() / g["pot_sum"] - 1) < 1e-12
