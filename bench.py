@@ -11,7 +11,9 @@ pass, results scattered back to input order.
   value : N * steps / device time of the steps (CUDA events on the solver's stream)
   e2e   : the same through the public API from pinned host buffers: the host->device
           copy of the bodies and the device->host copy of the results are timed
-  roofline : the dominant kernel (M2L) timed live with CUDA events
+  roofline : the dominant kernel timed live with CUDA events; rooflines: every
+             north-star kernel (P2P against the FP32 FMA peak, M2L and the
+             upward / downward passes against the measured HBM bandwidth)
   cpu_baseline : the reference's own CPU FMM (its headers compiled in place),
           all host threads, on a bounded sample of the same workload
 
@@ -225,6 +227,64 @@ def check_world(gpus: int, env=None) -> str:
     return "run"
 
 
+P2P_FLOPS_PER_INTERACTION = 20   # the canonical count for a Laplace potential + gradient pair
+
+
+def fp32_fma_peak_tflops(sm_mhz: float) -> float:
+    """CUDA-core FP32 peak: 148 SMs x 128 FMA lanes x 2 flop per clock (no measured figure exists)."""
+    return 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+
+
+def kernel_rooflines(P, mixed, n, info, phases, interactions, hbm_peak, peak_kind, sm_mhz):
+    """One entry per north-star kernel of a solve, from its phase time (CUDA events
+    over the timed steps) and its algorithmic work:
+      p2p      20 flop per pair interaction (sum over the P2P list of n_i n_j, counted
+               on the device) against the CUDA-core FP32 FMA peak;
+      m2l      per pair the source's expansion (NTERM x 8 B in FP32, 16 B in FP64) and an
+               8-byte list entry, per cell the local expansion read and written, against
+               the measured HBM copy bandwidth (also its flop rate, 8 NTERM P^2 per pair);
+      upward   the bodies read by P2M (32 B each), every cell's multipole written and
+               every non-root cell's read by its parent's M2M (NTERM x 16 B each);
+      downward every non-root cell's parent local expansion read and its own read and
+               written by L2L (3 x NTERM x 16 B), the bodies read and their results read
+               and written by L2P (96 B each)."""
+    nt = P * (P + 1) // 2
+    C, n_m2l = info["ncells"], info["n_m2l"]
+    cplx = 8 if mixed else 16
+    fp32_peak = fp32_fma_peak_tflops(sm_mhz)
+    out = []
+
+    def hbm(kernel, ms, nbytes, note, **extra):
+        a = nbytes / (ms / 1e3) / 1e9 if ms > 0 else 0.0
+        d = {"kernel": kernel, "bound": "hbm", "achieved": a, "peak": hbm_peak, "unit": "GB/s",
+             "frac": a / hbm_peak, "traffic": None, "peak_kind": peak_kind, "ms_per_launch": ms,
+             "algorithmic_bytes": int(nbytes), "note": note}
+        d.update(extra)
+        out.append(d)
+
+    p2p_ms = phases["p2p"]
+    flops = P2P_FLOPS_PER_INTERACTION * interactions
+    a = flops / (p2p_ms / 1e3) / 1e12 if p2p_ms > 0 else 0.0
+    out.append({"kernel": "p2p", "bound": "fp32", "achieved": a, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": a / fp32_peak, "traffic": None,
+                "peak_kind": f"nominal CUDA-core FP32 (148 SMs x 128 lanes x 2 flop x {sm_mhz:.0f} MHz)",
+                "ms_per_launch": p2p_ms, "interactions": int(interactions),
+                "flops_per_interaction": P2P_FLOPS_PER_INTERACTION,
+                "note": "both P2P launches of a solve (FP32 in the mixed form, FP64 in the plain one)"})
+    m2l_ms = phases["m2l"]
+    alg_flops = n_m2l * 8 * nt * P * P
+    hbm("m2l", m2l_ms, n_m2l * (nt * cplx + 8) + C * 2 * nt * cplx,
+        "the M2L phase: class hashing and sorting, the per-class products (tensor cores in the mixed "
+        "form), their per-target sums, the pair-by-pair FP32 launches and the FP64 root-level pairs",
+        algorithmic_flops=int(alg_flops), achieved_tflops=alg_flops / (m2l_ms / 1e3) / 1e12 if m2l_ms else 0.0,
+        traffic=(M2L_DRAM_BYTES_PER_PAIR * n_m2l if mixed and P == 8 else None))
+    hbm("upward", phases["upward"], n * 32 + C * nt * 16 + max(C - 1, 0) * nt * 16,
+        "P2M at the leaves and M2M level by level (FP64)")
+    hbm("downward", phases["downward"], 3 * max(C - 1, 0) * nt * 16 + n * 96,
+        "L2L level by level and L2P at the leaves (FP64)")
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -382,29 +442,14 @@ def main():
                             "direct_sample": 4096}}
         f64.close()
 
-    # ---- roofline of the dominant kernel (M2L), from the timed steps ----
+    # ---- rooflines of the north-star kernels, from the timed steps; the dominant one is `roofline`
     hbm_peak, bf16_peak, peak_kind = _peaks()
     P = wl["P"]
-    nterm = P * (P + 1) // 2
-    m2l_ms = phase_acc["m2l"] / args.steps
-    n_m2l = info["n_m2l"]
-    cplx = 16 if prec == pkg.FP64 else 8
-    alg_bytes = n_m2l * (nterm * cplx + 8) + info["ncells"] * 2 * nterm * cplx
-    alg_flops = n_m2l * 8 * nterm * P * P
-    achieved = alg_bytes / (m2l_ms / 1e3) / 1e9
-    traffic = M2L_DRAM_BYTES_PER_PAIR * n_m2l if prec == pkg.MIXED and P == 8 else None
-    roofline = {
-        "kernel": "m2l", "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-        "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
-        "ms_per_launch": m2l_ms, "algorithmic_bytes": alg_bytes, "algorithmic_flops": alg_flops,
-        "achieved_tflops": alg_flops / (m2l_ms / 1e3) / 1e12,
-        "note": "the M2L phase: per-offset-class dense products on the tensor cores (tcgen05, bf16x3 "
-                "pieces, 6 x 4,096 multiply-adds per pair at P=8, FP32 accumulation in TMEM) plus a "
-                "per-target FP64 pass over their contributions, the class hashing and sorting, and the "
-                "FP64 pairs of the root levels; frac is its distance from the memory roof, "
-                "achieved_tflops its rate by the reference's per-pair count (8 NTERM P^2), and traffic "
-                "above the algorithmic bytes is the contributions' round trip through HBM",
-    }
+    phases = {k: v / args.steps for k, v in phase_acc.items()}
+    interactions = fmm.p2p_interactions()
+    rooflines = kernel_rooflines(P, prec == pkg.MIXED, n, info, phases, interactions, hbm_peak, peak_kind,
+                                 clk.get("sm_max_mhz") or 1965.0)
+    roofline = max(rooflines, key=lambda r: r["ms_per_launch"])
 
     line = {
         "metric": METRIC, "value": value, "unit": "bodies/s", "n_gpus": world, "steps": args.steps,
@@ -414,9 +459,10 @@ def main():
                    "P": P, "theta": wl["theta"], "ncrit": ncrit, "ncrit_tuning_ms": tuned, "nspawn": wl["nspawn"],
                    "precision": args.precision, "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (134 MB of bodies per solve)",
-                   "cells": info["ncells"], "depth": info["depth"], "m2l_pairs": n_m2l, "p2p_pairs": info["n_p2p"]},
-        "phases_ms": {k: v / args.steps for k, v in phase_acc.items()},
+                   "cells": info["ncells"], "depth": info["depth"], "m2l_pairs": info["n_m2l"], "p2p_pairs": info["n_p2p"]},
+        "phases_ms": phases,
         "roofline": roofline,
+        "rooflines": rooflines,
         "e2e": {"value": e2e_value, "unit": "bodies/s", "h2d_bytes_per_step": int(n * 32),
                 "d2h_bytes_per_step": int(n * 32)},
         "gpu_launches": int(launches),

@@ -134,6 +134,7 @@ def lib() -> ctypes.CDLL:
         "exafmm_server_session_bodies": (_c_int, [_vp, _c_ll, _vp]),
         "exafmm_server_close_session": (_c_int, [_vp, _c_ll]),
         "exafmm_server_set_grouping": (_c_int, [_vp, _c_int, _c_ll, _c_ll]),
+        "exafmm_list_work": (_c_int, [_vp, ctypes.POINTER(_c_ll)]),
         "exafmm_server_grouped": (_c_int, [_vp, ctypes.POINTER(_c_ll)]),
         "exafmm_displace_bodies": (_c_int, [_vp, _c_double, ctypes.c_ulonglong]),
         "exafmm_get_bodies": (_c_int, [_vp, _vp]),
@@ -398,6 +399,12 @@ class Fmm:
         self._check(lib().exafmm_tree_info(self._h, ctypes.byref(nc), ctypes.byref(d), ctypes.byref(nm),
                                            ctypes.byref(npp)))
         return {"ncells": nc.value, "depth": d.value, "n_m2l": nm.value, "n_p2p": npp.value}
+
+    def p2p_interactions(self) -> int:
+        """Sum over the P2P list of NBODY(target) * NBODY(source), counted on the device."""
+        v = _c_ll()
+        self._check(lib().exafmm_list_work(self._h, ctypes.byref(v)))
+        return int(v.value)
 
     def cells(self):
         nc = self.info()["ncells"]

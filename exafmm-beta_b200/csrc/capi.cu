@@ -453,6 +453,7 @@ struct Engine {
 
   void results(double *dst, cudaMemcpyKind kind, double *const *parts = nullptr);
   void displace(double sigma, unsigned long long seed);
+  long long p2p_interactions();
   void bodies(double *dst, cudaMemcpyKind kind);
 
   void get_dipole(const double *X0, double *dipole3) {
@@ -508,6 +509,47 @@ __global__ void k_displace(double4 *x, long long n, double sigma, unsigned long 
   }
 }
 }  // namespace
+
+namespace {
+// Pair interactions of the P2P lists, sum over list entries (i, j) of
+// NBODY(i) * NBODY(j): each block sums its target cells and adds once.
+__global__ void k_list_work(const int *off, const int *src, long long nc, const int4 *cell_b,
+                            const int4 *src_cell_b, unsigned long long *out) {
+  unsigned long long acc = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nc; i += (long long)gridDim.x * blockDim.x) {
+    unsigned long long nj = 0;
+    for (int q = off[i]; q < off[i + 1]; q++) nj += (unsigned)src_cell_b[src[q] & 0x3ffffff].y;
+    acc += nj * (unsigned)cell_b[i].y;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  __shared__ unsigned long long part[32];
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += part[w];
+    atomicAdd(out, t);
+  }
+}
+}  // namespace
+
+long long Engine::p2p_interactions() {
+  if (!lists_ok) throw std::runtime_error("no interaction lists (solve first)");
+  const long long nc = C.tree.ncells;
+  dip.ensure(1);  // one word of the dipole scratch
+  unsigned long long *d = (unsigned long long *)dip.p;
+  EXA_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned long long), C.stream));
+  if (nc > 0) {
+    const int4 *sb = jsrc ? jsrc->C.tree.cell_b.p : C.tree.cell_b.p;
+    const int grid = (int)std::max<long long>(1, std::min<long long>(kNumSMs * 4, (nc + 255) / 256));
+    k_list_work<<<grid, 256, 0, C.stream>>>(lists.p2p_off.p, lists.p2p_src.p, nc, C.tree.cell_b.p, sb, d);
+    EXA_CHECK_LAUNCH();
+  }
+  unsigned long long h = 0;
+  EXA_CUDA(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, C.stream));
+  EXA_CUDA(cudaStreamSynchronize(C.stream));
+  return (long long)h;
+}
 
 void Engine::displace(double sigma, unsigned long long seed) {
   const long long n = C.tree.n;
@@ -899,6 +941,14 @@ int exafmm_tree_info(exafmm_ctx *ctx, long long *ncells, int *depth, long long *
     if (depth) *depth = ctx->E.C.tree.depth;
     if (n_m2l) *n_m2l = ctx->E.lists_ok ? ctx->E.lists.n_m2l : -1;
     if (n_p2p) *n_p2p = ctx->E.lists_ok ? ctx->E.lists.n_p2p : -1;
+  });
+}
+
+int exafmm_list_work(exafmm_ctx *ctx, long long *p2p_interactions) {
+  return guarded(ctx, [&] {
+    if (!p2p_interactions) throw std::runtime_error("null output");
+    cudaSetDevice(ctx->E.C.device);
+    *p2p_interactions = ctx->E.p2p_interactions();
   });
 }
 

@@ -168,6 +168,12 @@ int exafmm_get_results_device(exafmm_ctx *ctx, double *d_trg);
 
 /* Tree and list inspection for parity checks. */
 int exafmm_tree_info(exafmm_ctx *ctx, long long *ncells, int *depth, long long *n_m2l, long long *n_p2p);
+/* Pair interactions of the last solve's P2P lists: the sum over list entries
+ * (target cell i, source cell j) of NBODY(i) * NBODY(j), self pairs included
+ * (the work the P2P kernels do; kernels/laplace.h:150-235 per call).  Counted
+ * on the device from the lists.  No counterpart in the reference (its
+ * EXAFMM_COUNT_KERNEL build counts calls, include/traversal.h:396-410). */
+int exafmm_list_work(exafmm_ctx *ctx, long long *p2p_interactions);
 int exafmm_get_cells(exafmm_ctx *ctx, int *ints, double *reals);
 /* perm[i] = caller index of the body in tree slot i (Body::IBODY after buildTree). */
 int exafmm_get_perm(exafmm_ctx *ctx, int *perm);

@@ -238,3 +238,22 @@ def test_gpu_context_reuse_with_growing_systems(ex, datasets):
             assert np.array_equal(reused, g.results())
             g.close()
         f.close()
+
+
+def test_p2p_interaction_count_matches_the_lists(ex, datasets):
+    """exafmm_list_work: the sum over P2P list entries of NBODY(target) * NBODY(source),
+    recomputed here from the cell table and the lists (free space, periodic, forest)."""
+    for kw, systems in ((dict(P=6, theta=0.4, ncrit=32), None), (dict(P=6, theta=0.4, ncrit=32, images=1), None),
+                        (dict(P=6, theta=0.4, ncrit=16), [datasets.cube(3000, seed=8), datasets.plummer(2000, seed=9)])):
+        f = ex.Fmm(**kw)
+        if systems is None:
+            f.set_bodies(datasets.plummer(20000, seed=7) if not kw.get("images") else datasets.cube(5000, seed=7))
+        else:
+            f.set_systems(systems)
+        f.solve()
+        ints, _ = f.cells()
+        _, p2p = f.lists()
+        nb = ints[:, 4].astype(np.int64)
+        expect = int(np.sum(nb[p2p[:, 0]] * nb[p2p[:, 1]]))
+        assert f.p2p_interactions() == expect
+        f.close()
