@@ -1,6 +1,7 @@
 // extern "C" surface of the engine (include/exafmm_b200.h) and the solve driver.
 #include <atomic>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -36,15 +37,16 @@ namespace {
 
 // Phase events of the last solve: ev[0..7] bound bounds, tree, upward, lists,
 // m2l, p2p, downward; link splits the tree build (growTree / linkTree), lat
-// brackets the periodic lattice.  After each complete solve (pending) the times
-// are added under the reference's logger event names to `timer`, which
-// exafmm_write_time writes out and clears (logger::writeTime).
+// brackets the periodic lattice.  Each phase, once complete, is flagged in
+// `done`; fold() adds the flagged phases' times under the reference's logger
+// event names to `timer` (before their events are recorded again), which
+// exafmm_write_time writes out and exafmm_take_timers hands to the caller.
 struct Timing {
+  enum : unsigned { kBounds = 1, kGrow = 2, kLink = 4, kUp = 8, kTrav = 16, kPer = 32, kDown = 64 };
   cudaEvent_t ev[8] = {};
   cudaEvent_t link = nullptr, lat[2] = {};
   bool live = false;
-  bool pending = false;    // a complete solve whose times are not in `timer` yet
-  bool periodic = false;   // that solve ran the periodic lattice
+  unsigned done = 0;       // phases complete whose times are not in `timer` yet
   std::map<std::string, double> timer;
   void init() {
     if (live) return;
@@ -54,6 +56,7 @@ struct Timing {
     live = true;
   }
   double seconds(cudaEvent_t a, cudaEvent_t b) {
+    EXA_CUDA(cudaEventSynchronize(b));
     float ms = 0.f;
     EXA_CUDA(cudaEventElapsedTime(&ms, a, b));
     return 1e-3 * ms;
@@ -61,16 +64,19 @@ struct Timing {
   // Event names of include/bound_box.h:12, build_tree.h:187-207, up_down_pass.h:50-74,
   // traversal.h:234-350 ("Traverse" includes "Traverse periodic", as there).
   void fold() {
-    if (!pending) return;
-    EXA_CUDA(cudaEventSynchronize(ev[7]));
-    timer["Get bounds"] += seconds(ev[0], ev[1]);
-    timer["Grow tree"] += seconds(ev[1], link);
-    timer["Link tree"] += seconds(link, ev[2]);
-    timer["Upward pass"] += seconds(ev[2], ev[3]);
-    timer["Traverse"] += seconds(ev[3], ev[6]);
-    if (periodic) timer["Traverse periodic"] += seconds(lat[0], lat[1]);
-    timer["Downward pass"] += seconds(ev[6], ev[7]);
-    pending = false;
+    if (!done) return;
+    if (done & kBounds) timer["Get bounds"] += seconds(ev[0], ev[1]);
+    if (done & kGrow) timer["Grow tree"] += seconds(ev[1], link);
+    if (done & kLink) timer["Link tree"] += seconds(link, ev[2]);
+    if (done & kUp) timer["Upward pass"] += seconds(ev[2], ev[3]);
+    if (done & kTrav) timer["Traverse"] += seconds(ev[3], ev[6]);
+    if (done & kPer) timer["Traverse periodic"] += seconds(lat[0], lat[1]);
+    if (done & kDown) timer["Downward pass"] += seconds(ev[6], ev[7]);
+    done = 0;
+  }
+  // Before a phase records its events again, the last run of it is folded.
+  void reuse(unsigned phases) {
+    if (done & phases) fold();
   }
   ~Timing() {
     if (live) {
@@ -288,6 +294,7 @@ struct Engine {
     grow_tree();
     if (jsrc) jsrc->build_sources(C.tree.bounds.p, C.prm);
     EXA_CUDA(cudaEventRecord(tm.ev[2], C.stream));
+    tm.done |= Timing::kBounds | Timing::kGrow | Timing::kLink;
     tree_ok = true;
     up_ok = lists_ok = false;
   }
@@ -338,7 +345,9 @@ struct Engine {
       for (int l = C.tree.depth - 1; l >= 0; l--) m2m_fp64(a, l, C.tree.lvl_host[l]);
     }
     if (jsrc) jsrc->upward();  // examples/fmm.cxx:70
+    tm.reuse(Timing::kUp | Timing::kTrav);
     EXA_CUDA(cudaEventRecord(tm.ev[3], C.stream));
+    tm.done |= Timing::kUp;
     up_ok = true;
   }
 
@@ -369,6 +378,7 @@ struct Engine {
     if (!up_ok) throw std::runtime_error("traverse before the upward pass");
     const long long nc = C.tree.ncells;
     const int NT = tri(C.prm.P);
+    tm.reuse(Timing::kTrav | Timing::kPer | Timing::kDown);
     trg.ensure(C.tree.n);
     if (C.tree.n) EXA_CUDA(cudaMemsetAsync(trg.p, 0, C.tree.n * sizeof(double4), C.stream));
     if (nc > 0 && jsrc) {
@@ -435,6 +445,7 @@ struct Engine {
       EXA_CUDA(cudaEventRecord(tm.ev[5], C.stream));
     }
     EXA_CUDA(cudaEventRecord(tm.ev[6], C.stream));
+    tm.done |= Timing::kTrav | (C.prm.images > 0 ? Timing::kPer : 0u);
     lists_ok = true;
   }
 
@@ -446,9 +457,9 @@ struct Engine {
       for (int l = 1; l <= C.tree.depth; l++) l2l_fp64(a, l, C.tree.lvl_host[l]);
       l2p_fp64(a);
     }
+    tm.reuse(Timing::kDown);
     EXA_CUDA(cudaEventRecord(tm.ev[7], C.stream));
-    tm.pending = true;
-    tm.periodic = C.prm.images > 0;
+    tm.done |= Timing::kDown;
   }
 
   void results(double *dst, cudaMemcpyKind kind, double *const *parts = nullptr);
@@ -1058,6 +1069,24 @@ int exafmm_write_time(exafmm_ctx *ctx, const char *path, int rank) {
     cudaSetDevice(E.C.device);
     E.tm.fold();
     write_time_file(path, rank, E.tm.timer);
+    E.tm.timer.clear();
+  });
+}
+
+int exafmm_take_timers(exafmm_ctx *ctx, int cap, char *names, double *seconds, int *count) {
+  return guarded(ctx, [&] {
+    if (!count) throw std::runtime_error("null count");
+    Engine &E = ctx->E;
+    cudaSetDevice(E.C.device);
+    E.tm.fold();
+    *count = (int)E.tm.timer.size();
+    if (!names || !seconds) return;  // the count only
+    if (cap < *count) throw std::runtime_error("timer arrays too short");
+    int k = 0;
+    for (auto &kv : E.tm.timer) {
+      std::snprintf(names + 32 * k, 32, "%s", kv.first.c_str());
+      seconds[k++] = kv.second;
+    }
     E.tm.timer.clear();
   });
 }

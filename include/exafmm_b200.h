@@ -200,6 +200,12 @@ int exafmm_phase_times(exafmm_ctx *ctx, double *ms8);
  * prefix ending in '/' ("./" if null). */
 int exafmm_write_list(exafmm_ctx *ctx, const char *path, int rank);
 int exafmm_write_time(exafmm_ctx *ctx, const char *path, int rank);
+/* The same events handed to the caller instead of a file (what the reference's
+ * logger::timer holds after these calls, include/logger.h:39-53): *count is
+ * the number of events; with names (cap x 32 chars, NUL-terminated) and
+ * seconds given, cap >= *count, they are filled in the name order and the
+ * engine's timers are cleared.  Waits for the phases timed so far. */
+int exafmm_take_timers(exafmm_ctx *ctx, int cap, char *names, double *seconds, int *count);
 int exafmm_write_time_events(const char *path, int rank, int count, const char *const *names, const double *seconds);
 /* BuildTree::getKey (include/build_tree.h:111-120) of center X at level, cube
  * corner Xmin and cell diameter, with the compiled reference's 32-bit shift

@@ -28,8 +28,12 @@
  *    next traverse (examples/fmm.cxx -j: cells, jcells), in FP64;
  *  - the periodic solve needs cycle[0] == cycle[1] == cycle[2];
  *  - Kernel's eps2 must be 0 and wavek is not used (Laplace);
- *  - Args (the command line) is not provided; logger keeps host wall-clock
- *    timers and the time file, not PAPI counters or traces.
+ *  - num_threads sizes nothing (the work runs on the GPU); logger keeps
+ *    wall-clock timers (the engine's phases timed on the device) and the time
+ *    file, not PAPI counters or traces.
+ * With include/exafmm_compat/ first on the include path, the reference's own
+ * examples (fmm.cxx, kernel.cxx, tree.cxx) compile unchanged: its headers
+ * there (args.h, bound_box.h, build_tree.h, ...) all lead here. 
  * Errors throw std::runtime_error with the engine's message. */
 #ifndef EXAFMM_B200_HPP
 #define EXAFMM_B200_HPP
@@ -45,13 +49,29 @@
 #include <iomanip>
 #include <iostream>
 #include <map>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <vector>
 
+#include <getopt.h>
+
 #include "exafmm_b200.h"
 
-namespace exafmm_laplace {
+#if (defined(EXAFMM_HELMHOLTZ) && EXAFMM_HELMHOLTZ) || (defined(EXAFMM_BIOTSAVART) && EXAFMM_BIOTSAVART)
+#error "the B200 engine evaluates the Laplace kernel only (EXAFMM_LAPLACE)"
+#endif
+// include/namespace.h: the drivers say `using namespace EXAFMM_NAMESPACE`.
+#ifndef EXAFMM_NAMESPACE
+#define EXAFMM_NAMESPACE exafmm_laplace
+#endif
+// The engine's precision for the facade's solves: EXAFMM_FP64 (the plain
+// method, the default) or EXAFMM_MIXED.
+#ifndef EXAFMM_B200_PRECISION
+#define EXAFMM_B200_PRECISION EXAFMM_FP64
+#endif
+
+namespace EXAFMM_NAMESPACE {
 
 typedef double real_t;
 typedef std::complex<real_t> complex_t;
@@ -131,7 +151,7 @@ struct Engine {
   exafmm_ctx *ctx = nullptr;
   int P = 10, ncrit = 64, nspawn = 5000, images = 0;
   double theta = 0.4, cycle = 2 * M_PI;
-  int precision = EXAFMM_FP64;
+  int precision = EXAFMM_B200_PRECISION;
   Bodies *targets = nullptr, *sources = nullptr;  // the bodies of the last trees
   std::vector<int> perm, jperm;                   // tree slot -> caller index at buildTree
   bool evaluated = false;
@@ -188,6 +208,269 @@ inline Cells cells_of(std::vector<int> &ci, std::vector<double> &cr, long long n
 }
 
 }  // namespace facade_detail
+
+// include/logger.h:39-138: event timers (host wall clock) and the time file.
+// The engine's phases (Get bounds, Grow tree, Link tree, Upward pass,
+// Traverse, Traverse periodic, Downward pass) join `timer` after each facade
+// call that runs them, as the reference's own phases time themselves there;
+// writeTime writes path + "time%06d.dat" from `timer` and clears it.  The
+// PAPI, tracer and DAG hooks do nothing here.
+namespace logger {
+inline int stringLength = 20;
+inline int decimal = 7;
+inline bool verbose = false;
+inline const char *path = "./";
+inline std::map<std::string, double> timer, beginTimer;
+
+inline double get_time() {
+  struct timespec ts;
+  clock_gettime(CLOCK_REALTIME, &ts);
+  return double(ts.tv_sec) + double(ts.tv_nsec) * 1e-9;
+}
+inline void printTitle(std::string title) {
+  if (verbose) {
+    title += " ";
+    std::cout << "--- " << std::setw(stringLength) << std::left << std::setfill('-') << title << std::setw(10) << "-"
+              << std::setfill(' ') << std::endl;
+  }
+}
+inline void startTimer(std::string event) { beginTimer[event] = get_time(); }
+inline void printTime(std::string event) {
+  if (verbose)
+    std::cout << std::setw(stringLength) << std::left << event << " : " << std::setprecision(decimal) << std::fixed
+              << timer[event] << " s" << std::endl;
+}
+inline double stopTimer(std::string event, int print = 1) {
+  const double t = get_time() - beginTimer[event];
+  timer[event] += t;
+  if (verbose && print) printTime(event);
+  return t;
+}
+// The engine's phase times since the last take, added to `timer` (and
+// printed when verbose, as the reference's stopTimer prints its phases).
+inline void takeEngineTimers() {
+  facade_detail::Engine &e = facade_detail::engine();
+  if (!e.ctx) return;
+  int n = 0;
+  e.check(exafmm_take_timers(e.ctx, 0, nullptr, nullptr, &n), "take_timers");
+  if (n == 0) return;
+  std::vector<char> names(32 * (size_t)n);
+  std::vector<double> secs(n);
+  e.check(exafmm_take_timers(e.ctx, n, names.data(), secs.data(), &n), "take_timers");
+  for (int k = 0; k < n; k++) {
+    const std::string ev(names.data() + 32 * k);
+    timer[ev] += secs[k];
+    printTime(ev);
+  }
+}
+inline void writeTime(int mpirank = 0) {
+  takeEngineTimers();
+  std::ostringstream name;
+  name << path << "time" << std::setfill('0') << std::setw(6) << mpirank << ".dat";
+  std::ofstream f(name.str().c_str());
+  for (auto &kv : timer) f << std::setw(stringLength) << std::left << kv.first << " " << kv.second << std::endl;
+  if (!f) throw std::runtime_error("exafmm: cannot write " + name.str());
+  timer.clear();
+}
+inline void resetTimer(std::string event) { timer.erase(event); }
+inline void resetTimer() { timer.clear(); }
+inline void startPAPI() {}
+inline void stopPAPI() {}
+inline void printPAPI() {}
+inline void initTracer() {}
+inline void writeTracer(int = 0) {}
+inline void startDAG() {}
+inline void stopDAG() {}
+inline void writeDAG() {}
+}  // namespace logger
+
+// include/thread.h: the reference sizes its host thread pool here; the
+// engine's work runs on the GPU, so there is nothing to size.
+inline void num_threads(int) {}
+
+// include/args.h:14-274: the examples' command line, with the same long and
+// short options, defaults and getKey layout (the key names the records of the
+// regression files).  -P sets the order, as in the reference's parser.
+class Args {
+ public:
+  int accuracy = 0;
+  int ncrit = 64;
+  double cutoff = 0.0;
+  const char *distribution = "cube";
+  int dual = 0;
+  int graft = 0;
+  int getMatrix = 0;
+  int images = 0;
+  int IneJ = 0;
+  int numBodies = 1000000;
+  const char *path = "./";
+  int P = 10;
+  int repeat = 1;
+  int nspawn = 5000;
+  double theta = 0.4;
+  int threads = 16;
+  int verbose = 0;
+  int write = 0;
+
+  Args(int argc = 0, char **argv = nullptr) {
+    static const struct option opts[] = {
+        {"accuracy", no_argument, 0, 'a'},     {"ncrit", required_argument, 0, 'c'},
+        {"cutoff", required_argument, 0, 'C'}, {"distribution", required_argument, 0, 'd'},
+        {"dual", no_argument, 0, 'D'},         {"graft", no_argument, 0, 'g'},
+        {"getMatrix", no_argument, 0, 'G'},    {"help", no_argument, 0, 'h'},
+        {"images", required_argument, 0, 'i'}, {"IneJ", no_argument, 0, 'j'},
+        {"numBodies", required_argument, 0, 'n'}, {"path", required_argument, 0, 'p'},
+        {"P", required_argument, 0, 'P'},      {"repeat", required_argument, 0, 'r'},
+        {"nspawn", required_argument, 0, 's'}, {"theta", required_argument, 0, 't'},
+        {"threads", required_argument, 0, 'T'}, {"verbose", no_argument, 0, 'v'},
+        {"write", no_argument, 0, 'w'},        {0, 0, 0, 0}};
+    // the reference's short-option string, letters it does not handle included
+    // (they end in the usage message, as there)
+    const char *shorts = "ab:c:d:De:gGhi:jmMn:op:P:r:s:t:T:vwx";
+    if (argc <= 0 || !argv) return;
+    optind = 1;
+    for (;;) {
+      int index = 0;
+      const int c = getopt_long(argc, argv, shorts, opts, &index);
+      if (c == -1) break;
+      switch (c) {
+        case 'a': accuracy = 1; break;
+        case 'c': ncrit = std::atoi(optarg); break;
+        case 'C': cutoff = std::atof(optarg); break;
+        case 'd': distribution = distribution_name(optarg); break;
+        case 'D': dual = 1; break;
+        case 'g': graft = 1; break;
+        case 'G': getMatrix = 1; break;
+        case 'i': images = std::atoi(optarg); break;
+        case 'j': IneJ = 1; break;
+        case 'n': numBodies = std::atoi(optarg); break;
+        case 'p': path = optarg; break;
+        case 'P': P = std::atoi(optarg); break;
+        case 'r': repeat = std::atoi(optarg); break;
+        case 's': nspawn = std::atoi(optarg); break;
+        case 't': theta = std::atof(optarg); break;
+        case 'T': threads = std::atoi(optarg); break;
+        case 'v': verbose = 1; break;
+        case 'w': write = 1; break;
+        default:  // 'h' and anything unknown
+          usage(argv[0]);
+          std::abort();
+      }
+    }
+  }
+
+  // Bit fields of the reference's key: log2 ncrit, distribution, dual, kernel
+  // (Laplace = 0), graft, images, IneJ, log10 N, P, log10 nspawn, 14 theta,
+  // log2 threads, build switches, log2 ranks.
+  uint64_t getKey(int mpisize = 1) {
+    auto lg = [](double v, double b) { return uint64_t(std::round(std::log(v) / std::log(b))); };
+    uint64_t key = lg(ncrit, 2);
+    key |= distribution_code(distribution) << 4;
+    key |= uint64_t(dual) << 7;
+    key |= uint64_t(graft) << 11;
+    key |= uint64_t(images) << 12;
+    key |= uint64_t(IneJ) << 14;
+    key |= lg(numBodies, 10) << 15;
+    key |= uint64_t(P) << 19;
+    key |= lg(nspawn, 10) << 25;
+    key |= uint64_t(theta * 14) << 28;
+    key |= lg(threads, 2) << 31;
+    key |= build_code() << 34;
+    key |= lg(mpisize, 2) << 37;
+    return key;
+  }
+
+  void print(int stringLength) {
+    if (!verbose) return;
+    auto row = [&](const char *name) -> std::ostream & {
+      return std::cout << std::setw(stringLength) << std::fixed << std::left << name << " : ";
+    };
+    row("accuracy") << accuracy << std::endl;
+    row("ncrit") << ncrit << std::endl;
+    row("cutoff") << cutoff << std::endl;
+    row("distribution") << distribution << std::endl;
+    row("dual") << dual << std::endl;
+    row("graft") << graft << std::endl;
+    row("getMatrix") << getMatrix << std::endl;
+    row("images") << images << std::endl;
+    row("IneJ") << IneJ << std::endl;
+    row("numBodies") << numBodies << std::endl;
+    row("path") << path << std::endl;
+    row("P") << P << std::endl;
+    row("repeat") << repeat << std::endl;
+    row("nspawn") << nspawn << std::endl;
+    row("theta") << theta << std::endl;
+    row("threads") << threads << std::endl;
+    row("verbose") << verbose << std::endl;
+    row("write") << write << std::endl;
+  }
+
+ private:
+  static const char *distribution_name(const char *a) {
+    switch (a[0]) {
+      case 'c': return "cube";
+      case 'l': return "lattice";
+      case 'o': return "octant";
+      case 'p': return "plummer";
+      case 's': return "sphere";
+    }
+    std::fprintf(stderr, "invalid distribution %s\n", a);
+    std::abort();
+  }
+  static uint64_t distribution_code(const char *d) {
+    switch (d[0]) {
+      case 'c': return 0;
+      case 'l': return 1;
+      case 'o': return 2;
+      case 'p': return 3;
+      case 's': return 4;
+      case 'e': return 7;
+    }
+    std::fprintf(stderr, "invalid distribution %s\n", d);
+    std::abort();
+  }
+  // EXAFMM_SINGLE, EXAFMM_USE_SIMD and EXAFMM_USE_KAHAN as the reference's build sets them
+  static uint64_t build_code() {
+    uint64_t k = 0;
+#if defined(EXAFMM_SINGLE) && EXAFMM_SINGLE
+    k |= 1;
+#endif
+#if defined(EXAFMM_USE_SIMD) && EXAFMM_USE_SIMD
+    k |= 2;
+#endif
+#if defined(EXAFMM_USE_KAHAN) && EXAFMM_USE_KAHAN
+    k |= 4;
+#endif
+    return k;
+  }
+  void usage(const char *name) {
+    std::fprintf(stderr,
+                 "Usage: %s [options]\n"
+                 "Long option (short option)       : Description (Default value)\n"
+                 " --accuracy (-a)                 : Regression for accuracy only (%d)\n"
+                 " --ncrit (-c)                    : Number of bodies per leaf cell (%d)\n"
+                 " --cutoff (-C)                   : Cutoff distance of interaction (%f)\n"
+                 " --distribution (-d) [c/l/o/p/s] : lattice, cube, sphere, octant, plummer (%s)\n"
+                 " --dual (-D)                     : Use dual tree traversal (%d)\n"
+                 " --graft (-g)                    : Graft remote trees to global tree (%d)\n"
+                 " --getMatrix (-G)                : Write G matrix to file (%d)\n"
+                 " --help (-h)                     : Show this help document\n"
+                 " --images (-i)                   : Number of periodic image levels (%d)\n"
+                 " --IneJ (-j)                     : Use different sources & targets (%d)\n"
+                 " --numBodies (-n)                : Number of bodies (%d)\n"
+                 " --path (-p)                     : Path to save files (%s)\n"
+                 " --P (-P)                        : Order of expansion (%d)\n"
+                 " --repeat (-r)                   : Number of iteration loops (%d)\n"
+                 " --nspawn (-s)                   : Threshold for stopping task creation during recursion (%d)\n"
+                 " --theta (-t)                    : Multipole acceptance criterion (%f)\n"
+                 " --threads (-T)                  : Number of threads (%d)\n"
+                 " --verbose (-v)                  : Print information to screen (%d)\n"
+                 " --write (-w)                    : Write timings to file (%d)\n",
+                 name, accuracy, ncrit, cutoff, distribution, dual, graft, getMatrix, images, IneJ, numBodies, path, P,
+                 repeat, nspawn, theta, threads, verbose, write);
+  }
+};
+
 
 // kernels/laplace.h:116-148 and the per-cell operators (:150-388), each on the
 // device through exafmm_kernel_*, accumulating into the cells' M, L and the
@@ -275,6 +558,22 @@ class Kernel {
 class BoundBox {
  public:
   Bounds getBounds(Bodies &bodies) {
+    logger::startTimer("Get bounds");
+    Bounds b = bounds_of(bodies);
+    logger::stopTimer("Get bounds");
+    return b;
+  }
+  // getBounds(jbodies, getBounds(bodies)): the bounds of bodies extended by
+  // jbodies as the reference's running update does (examples/fmm.cxx:62-64).
+  Bounds getBounds(Bodies &jbodies, Bounds bounds) {
+    logger::startTimer("Get bounds");
+    Bounds b = extended(jbodies, bounds);
+    logger::stopTimer("Get bounds");
+    return b;
+  }
+
+ private:
+  Bounds bounds_of(Bodies &bodies) {
     Bounds b;
     if (bodies.empty()) {
       b.Xmin = b.Xmax = 0;
@@ -290,9 +589,7 @@ class BoundBox {
     last_ = &bodies;
     return to_bounds(g);
   }
-  // getBounds(jbodies, getBounds(bodies)): the bounds of bodies extended by
-  // jbodies as the reference's running update does (examples/fmm.cxx:62-64).
-  Bounds getBounds(Bodies &jbodies, Bounds bounds) {
+  Bounds extended(Bodies &jbodies, Bounds bounds) {
     facade_detail::Engine &e = facade_detail::engine();
     if (!last_) throw std::runtime_error("exafmm: getBounds(jbodies, bounds) extends the last getBounds(bodies)");
     std::vector<double> x = facade_detail::pack(*last_), jx = facade_detail::pack(jbodies);
@@ -305,7 +602,6 @@ class BoundBox {
     return to_bounds(g);
   }
 
- private:
   Bodies *last_ = nullptr;
   static Bounds to_bounds(const double *g) {
     Bounds b;
@@ -322,7 +618,19 @@ class BoundBox {
 // reference's order with BODY into them.  buffer is not used.
 class BuildTree {
  public:
+  int numLevels = 0;  // depth of the last tree
   explicit BuildTree(int ncrit) { facade_detail::engine().ncrit = ncrit; }
+
+  // include/build_tree.h:212-222 (verbose only).
+  void printTreeData(Cells &cells) {
+    if (logger::verbose && !cells.empty()) {
+      logger::printTitle("Tree stats");
+      std::cout << std::setw(logger::stringLength) << std::left << "Bodies" << " : " << cells.front().NBODY
+                << std::endl
+                << std::setw(logger::stringLength) << std::left << "Cells" << " : " << cells.size() << std::endl
+                << std::setw(logger::stringLength) << std::left << "Tree depth" << " : " << numLevels << std::endl;
+    }
+  }
 
   Cells buildTree(Bodies &bodies, Bodies &buffer, Bounds bounds) {
     (void)buffer;
@@ -347,7 +655,7 @@ class BuildTree {
       e.check(exafmm_set_sources(e.context(), nullptr, 0), "set_sources");
       e.check(exafmm_set_bodies(e.context(), x.data(), (long long)bodies.size()), "set_bodies");
       e.check(exafmm_build_tree(e.context(), b6), "build_tree");
-      e.check(exafmm_tree_info(e.context(), &nc, nullptr, nullptr, nullptr), "tree_info");
+      e.check(exafmm_tree_info(e.context(), &nc, &numLevels, nullptr, nullptr), "tree_info");
       ci.resize(5 * nc);
       cr.resize(4 * nc);
       e.perm.resize(bodies.size());
@@ -358,6 +666,7 @@ class BuildTree {
       e.sources = nullptr;
     }
     e.evaluated = false;
+    logger::takeEngineTimers();
     return facade_detail::cells_of(ci, cr, nc, bodies);
   }
 };
@@ -371,6 +680,7 @@ class UpDownPass {
     facade_detail::Engine &e = facade_detail::engine();
     if (cells.empty()) return;
     e.check(exafmm_upward(e.context()), "upward");  // the targets' tree and, once built, the sources'
+    logger::takeEngineTimers();
   }
   void downwardPass(Cells &cells) {
     facade_detail::Engine &e = facade_detail::engine();
@@ -378,6 +688,7 @@ class UpDownPass {
     e.check(exafmm_downward(e.context()), "downward");
     std::vector<double> trg(4 * e.targets->size());
     e.check(exafmm_get_results(e.context(), trg.data()), "get_results");
+    logger::takeEngineTimers();
     Bodies &b = *e.targets;
     for (size_t i = 0; i < b.size(); i++)  // results come in the caller's order of buildTree
       for (int k = 0; k < 4; k++) b[i].TRG[k] += trg[4 * e.perm[i] + k];
@@ -427,6 +738,7 @@ class Traversal {
     e.params();
     e.check(exafmm_traverse(e.context()), "traverse");
     e.evaluated = true;
+    logger::takeEngineTimers();
   }
   // include/traversal.h:355-377: all of jbodies onto bodies over the image
   // range of the traversal's images and theta, added to bodies' TRG.
@@ -439,10 +751,44 @@ class Traversal {
     for (size_t i = 0; i < bodies.size(); i++)
       for (int k = 0; k < 4; k++) bodies[i].TRG[k] += trg[4 * i + k];
   }
-  // include/traversal.h:412-421 (list%06d.dat of the last traversal).
+  // include/traversal.h:380-393: path + "matrix.dat", the Green's function
+  // 1/|Xi - Xj| (0 at r = 0) of every target and source body, one line per target.
+  void writeMatrix(Bodies &bodies, Bodies &jbodies) {
+    std::ofstream f((path_ + "matrix.dat").c_str());
+    for (B_iter Bi = bodies.begin(); Bi != bodies.end(); Bi++) {
+      for (B_iter Bj = jbodies.begin(); Bj != jbodies.end(); Bj++) {
+        const real_t R2 = norm(Bi->X - Bj->X) + kernel_.eps2;
+        f << (R2 == 0 ? 0.0 : 1.0 / std::sqrt(R2)) << " ";
+      }
+      f << std::endl;
+    }
+  }
+  // include/traversal.h:396-410: the P2P and M2L calls of the last traversal
+  // (one per list entry), printed when verbose in a build with
+  // EXAFMM_COUNT_KERNEL, as there.
+  void printTraversalData() {
+#if defined(EXAFMM_COUNT_KERNEL) && EXAFMM_COUNT_KERNEL
+    facade_detail::Engine &e = facade_detail::engine();
+    if (logger::verbose && e.ctx) {
+      long long m2l = 0, p2p = 0;
+      e.check(exafmm_tree_info(e.ctx, nullptr, nullptr, &m2l, &p2p), "tree_info");
+      std::cout << "--- Traversal stats --------------" << std::endl
+                << std::setw(logger::stringLength) << std::left << "P2P calls" << " : " << std::max(p2p, 0LL)
+                << std::endl
+                << std::setw(logger::stringLength) << std::left << "M2L calls" << " : " << std::max(m2l, 0LL)
+                << std::endl;
+    }
+#endif
+  }
+  // include/traversal.h:411-424: list%06d.dat of the last traversal in a
+  // build with EXAFMM_COUNT_LIST; without it the call does nothing, as there.
   void writeList(Cells &, int mpirank) {
+#if defined(EXAFMM_COUNT_LIST) && EXAFMM_COUNT_LIST
     facade_detail::Engine &e = facade_detail::engine();
     e.check(exafmm_write_list(e.context(), path_.c_str(), mpirank), "write_list");
+#else
+    (void)mpirank;
+#endif
   }
 
  private:
@@ -450,81 +796,6 @@ class Traversal {
   std::string path_;
 };
 
-// include/logger.h:39-138: event timers (host wall clock) and the time file.
-// writeTime writes path + "time%06d.dat" with the driver's timers and the
-// engine's phases since the last write (Get bounds, Grow tree, Link tree,
-// Upward pass, Traverse, Traverse periodic, Downward pass), as the
-// reference's file holds its own phases; the PAPI, tracer and DAG hooks do
-// nothing here.
-namespace logger {
-inline int stringLength = 20;
-inline int decimal = 7;
-inline bool verbose = false;
-inline const char *path = "./";
-inline std::map<std::string, double> timer, beginTimer;
-
-inline double get_time() {
-  struct timespec ts;
-  clock_gettime(CLOCK_REALTIME, &ts);
-  return double(ts.tv_sec) + double(ts.tv_nsec) * 1e-9;
-}
-inline void printTitle(std::string title) {
-  if (verbose) {
-    title += " ";
-    std::cout << "--- " << std::setw(stringLength) << std::left << std::setfill('-') << title << std::setw(10) << "-"
-              << std::setfill(' ') << std::endl;
-  }
-}
-inline void startTimer(std::string event) { beginTimer[event] = get_time(); }
-inline void printTime(std::string event) {
-  if (verbose)
-    std::cout << std::setw(stringLength) << std::left << event << " : " << std::setprecision(decimal) << std::fixed
-              << timer[event] << " s" << std::endl;
-}
-inline double stopTimer(std::string event, int print = 1) {
-  const double t = get_time() - beginTimer[event];
-  timer[event] += t;
-  if (verbose && print) printTime(event);
-  return t;
-}
-inline void writeTime(int mpirank = 0) {
-  std::map<std::string, double> all = timer;
-  facade_detail::Engine &e = facade_detail::engine();
-  char name[32];
-  std::snprintf(name, sizeof(name), "time%06d.dat", mpirank);
-  if (e.ctx && exafmm_write_time(e.ctx, path, mpirank) == 0) {  // the engine's phases, then merged
-    std::ifstream f((std::string(path) + name).c_str());
-    std::string line;
-    while (std::getline(f, line)) {
-      if (line.size() <= (size_t)stringLength) continue;
-      std::string ev = line.substr(0, stringLength);
-      ev.erase(ev.find_last_not_of(' ') + 1);
-      all[ev] += std::atof(line.c_str() + stringLength + 1);
-    }
-  }
-  std::vector<std::string> names;
-  std::vector<const char *> cnames;
-  std::vector<double> secs;
-  for (auto &kv : all) {
-    names.push_back(kv.first);
-    secs.push_back(kv.second);
-  }
-  for (auto &n : names) cnames.push_back(n.c_str());
-  if (exafmm_write_time_events(path, mpirank, (int)names.size(), cnames.data(), secs.data()) != 0)
-    throw std::runtime_error("exafmm: cannot write the time file");
-  timer.clear();
-}
-inline void resetTimer(std::string event) { timer.erase(event); }
-inline void resetTimer() { timer.clear(); }
-inline void startPAPI() {}
-inline void stopPAPI() {}
-inline void printPAPI() {}
-inline void initTracer() {}
-inline void writeTracer(int = 0) {}
-inline void startDAG() {}
-inline void stopDAG() {}
-inline void writeDAG() {}
-}  // namespace logger
 
 // include/dataset.h:29-298 for Laplace: the generators with the same drand48
 // streams and arithmetic, initSource, initTarget and sampleBodies.
@@ -772,6 +1043,6 @@ class Verify {
   std::string path_;
 };
 
-}  // namespace exafmm_laplace
+}  // namespace EXAFMM_NAMESPACE
 
 #endif

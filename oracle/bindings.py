@@ -23,12 +23,19 @@ REF_SO = os.path.join(HERE, "_ref", "libexafmm_ref.so")
 _c_int, _c_double, _vp = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
 
 
-def build(reference_root: str | None = None) -> None:
+EXAMPLES_DIR = os.path.join(HERE, "_ref", "examples")
+
+
+def build(reference_root: str | None = None, examples: bool = True) -> None:
     """Compile liboracle.so and, when reference_root names an exafmm-beta
-    source tree that exists, the reference harness compiled in place from it."""
+    source tree that exists, the reference harness compiled in place from it
+    and (examples=True, the engine library built first) the reference's own
+    example drivers compiled against the facade into _ref/examples/."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
     if reference_root and os.path.isdir(os.path.join(reference_root, "include")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE_ROOT={reference_root}"], check=True)
+        if examples:
+            subprocess.run(["make", "-s", "-C", HERE, "examples", f"REFERENCE_ROOT={reference_root}"], check=True)
 
 
 def _ptr(a: np.ndarray | None):

@@ -317,7 +317,7 @@ def main(which=("solve", "periodic", "kat", "records", "md", "inej", "datasets",
     root = os.environ.get("EXAFMM_REFERENCE_ROOT")
     if not root or not os.path.isdir(os.path.join(root, "include")):
         raise SystemExit("set EXAFMM_REFERENCE_ROOT to the exafmm-beta source tree")
-    build(reference_root=root)
+    build(reference_root=root, examples=False)
     ref = Reference()
     if "solve" in which:
         for c in CASES:

@@ -14,9 +14,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 
 
-def compile_facade(src, out, ex):
+def compile_facade(src, out, ex, defines=()):
     pkg = os.path.dirname(ex.LIB_PATH)
     cmd = ["/usr/bin/g++", "-O2", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+           *[f"-D{d}" for d in defines],
            os.path.join(HERE, "facade", src), "-L", pkg, "-lexafmm_b200", f"-Wl,-rpath,{pkg}", "-o", out]
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
@@ -93,3 +94,65 @@ def test_facade_logger_time_file(ex, tmp_path):
     assert names == ["Direct sum", "Total FMM"]
     assert 0.015 < vals[0] < 0.5 and 0.05 < vals[1] < 1.0
     assert (tmp_path / "time000003.dat").read_text() == ""
+    # another name width: the file follows logger::stringLength, as the reference's does
+    wide = tmp_path / "wide"
+    wide.mkdir()
+    subprocess.run([exe, str(wide) + "/", "26"], check=True)
+    lines = (wide / "time000002.dat").read_text().splitlines()
+    assert [ln[:26].rstrip() for ln in lines] == ["Direct sum", "Total FMM"]
+    assert all(ln[26] == " " and float(ln[27:]) > 0 for ln in lines)
+
+
+EXAMPLES = ("fmm", "kernel", "tree")
+
+
+def reference_examples(ex):
+    """The reference's examples/{fmm,kernel,tree}.cxx compiled unchanged against the
+    facade (oracle/Makefile `examples`): built here when EXAFMM_REFERENCE_ROOT names
+    the exafmm-beta tree, else taken as built by the build step; None if absent."""
+    sys_path = os.path.join(ROOT, "oracle")
+    root = os.environ.get("EXAFMM_REFERENCE_ROOT")
+    if root and os.path.isdir(os.path.join(root, "examples")):
+        subprocess.run(["make", "-s", "-C", sys_path, "examples", f"REFERENCE_ROOT={root}"], check=True)
+    paths = {e: os.path.join(sys_path, "_ref", "examples", e) for e in EXAMPLES}
+    return paths if all(os.path.exists(p) for p in paths.values()) else None
+
+
+def test_reference_examples_build_against_the_facade(ex):
+    """examples/fmm.cxx, kernel.cxx and tree.cxx, unmodified, compile against
+    include/exafmm_compat/ + the facade and link only the engine library."""
+    paths = reference_examples(ex)
+    if paths is None:
+        pytest.skip("the reference tree was not available to the build step")
+    for name, p in paths.items():
+        assert os.access(p, os.X_OK), name
+        libs = subprocess.run(["ldd", p], capture_output=True, text=True).stdout
+        assert "libexafmm_b200.so" in libs and "not found" not in libs, (name, libs)
+
+
+def test_facade_args_match_the_reference_command_line(ex, tmp_path):
+    """Args: the reference's options, defaults and getKey, exercised by a driver."""
+    exe = compile_facade("args_driver.cpp", str(tmp_path / "args_driver"), ex)
+    out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
+    d = dict(zip(out[0::2], out[1::2]))
+    assert d == {"ncrit": "64", "P": "10", "theta": "0.4", "numBodies": "1000000", "distribution": "cube",
+                 "images": "0", "nspawn": "5000", "threads": "16", "repeat": "1", "dual": "0", "IneJ": "0",
+                 "path": "./", "verbose": "0", "key": str(_reference_key(64, "c", 0, 0, 0, 1000000, 10, 5000, 0.4, 16))}
+    argv = ["-n", "20000", "-P", "8", "-t", "0.35", "-c", "32", "-d", "p", "-i", "2", "-s", "1000", "-j", "-D", "-r",
+            "3", "-T", "4", "-v", "--path", "out/"]
+    out = subprocess.run([exe, *argv], capture_output=True, text=True, check=True).stdout.split()
+    d = dict(zip(out[0::2], out[1::2]))
+    assert (d["numBodies"], d["P"], d["theta"], d["ncrit"], d["distribution"], d["images"], d["nspawn"], d["IneJ"],
+            d["dual"], d["repeat"], d["threads"], d["verbose"], d["path"]) == \
+        ("20000", "8", "0.35", "32", "plummer", "2", "1000", "1", "1", "3", "4", "1", "out/")
+    assert d["key"] == str(_reference_key(32, "p", 1, 2, 1, 20000, 8, 1000, 0.35, 4))
+    bad = subprocess.run([exe, "-x"], capture_output=True, text=True)
+    assert bad.returncode != 0 and "Usage" in bad.stderr
+
+
+def _reference_key(ncrit, dist, dual, images, inej, n, P, nspawn, theta, threads):
+    """include/args.h getKey bit layout (Laplace, no build switches, one rank)."""
+    lg = lambda v, b: int(round(np.log(v) / np.log(b)))
+    code = {"c": 0, "l": 1, "o": 2, "p": 3, "s": 4}[dist]
+    return (lg(ncrit, 2) | code << 4 | dual << 7 | images << 12 | inej << 14 | lg(n, 10) << 15 | P << 19
+            | lg(nspawn, 10) << 25 | int(theta * 14) << 28 | lg(threads, 2) << 31)
