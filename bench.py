@@ -305,7 +305,9 @@ def main():
     ap.add_argument("--buckets", type=int, default=3,
                     help="batch: size groups solved as one forest each (0: one context per system)")
     ap.add_argument("--min-level", type=int, default=None,
-                    help="mixed form: lowest target level of the FP32 M2L (batch default 2, solve default 4)")
+                    help="mixed form: lowest target level of the FP32 M2L (default 2: levels 0 and 1 in FP64)")
+    ap.add_argument("--ncrit-candidates", default="32,64,128",
+                    help="batch: the ncrit values the autotuner tries per size group")
     args = ap.parse_args()
     if check_world(args.gpus) == "spawn":
         r = subprocess.run(["timeout", "-k", "60", "3600"] + torchrun_command(sys.argv[1:], args.gpus, _free_port()))
@@ -345,8 +347,8 @@ def main():
     def make(precision, ncrit):
         f = pkg.Fmm(P=wl["P"], theta=wl["theta"], ncrit=ncrit, nspawn=wl["nspawn"], precision=precision,
                     device=local_rank)
-        if precision == pkg.MIXED and args.m2l_policy != 1:
-            f.set_mixed_policy(m2l_fp32=args.m2l_policy)
+        if precision == pkg.MIXED and (args.m2l_policy != 1 or args.min_level is not None):
+            f.set_mixed_policy(m2l_fp32=args.m2l_policy, min_level=2 if args.min_level is None else args.min_level)
         return f
 
     def solve_device(f, out):
@@ -613,12 +615,14 @@ def _run_batch(args, pkg, datasets, workloads, prec, rank, world, local_rank):
 
     b = make(prec)
     forest = args.buckets > 0
-    if forest:  # the tuner tries one ncrit per call: three untimed tuning calls, then the table is frozen
+    cands = [int(v) for v in args.ncrit_candidates.split(",") if v]
+    if forest:  # the tuner tries one ncrit per call: untimed tuning calls, then the table is frozen
+        b.set_ncrit_candidates(cands)
         b.autotune(True)
-        for _ in range(3):
+        for _ in range(len(cands)):
             step(b)
         b.autotune(False)
-        warm = max(1, args.warmup - 3)
+        warm = max(1, args.warmup - len(cands))
     else:
         b.autotune(True)
         step(b)
@@ -742,6 +746,33 @@ def _request_errors(pkg, datasets, workloads, trace, mixed_samples, plain_sample
     return rows
 
 
+def _saturated_replays(srv, trace, precision, cfg, workloads, pinned, samples):
+    """The trace with every job queued at once, replayed cfg["replays"] times: the
+    medians of bodies/s (whole trace and until its last single solve), capacity and
+    latencies, with their ranges; samples from the first replay."""
+    reps = []
+    for r in range(cfg["replays"]):
+        done, wall = workloads.replay(srv, trace, precision=precision, ncrit=cfg["ncrit"], nspawn=cfg["nspawn"],
+                                      deadline_s=600.0, samples=samples if r == 0 else None, host_alloc=pinned)
+        s = workloads.latency_summary(done, wall)
+        s["while_saturated"] = workloads.saturated_throughput(done)
+        s["capacity_jobs_per_s"] = len(trace.jobs) / wall
+        reps.append(s)
+    med = lambda f: float(np.median([f(x) for x in reps]))
+    out = {k: med(lambda x, k=k: x[k]) for k in ("p50_ms", "p99_ms", "mean_ms", "bodies_per_s", "wall_s",
+                                                  "capacity_jobs_per_s")}
+    out["requests"] = reps[0]["requests"]
+    out["replays"] = len(reps)
+    out["bodies_per_s_range"] = [min(x["bodies_per_s"] for x in reps), max(x["bodies_per_s"] for x in reps)]
+    ws = [x["while_saturated"]["bodies_per_s"] for x in reps]
+    out["while_saturated"] = {"bodies_per_s": float(np.median(ws)), "range": [min(ws), max(ws)],
+                              "window_s": med(lambda x: x["while_saturated"]["window_s"])}
+    if "chain_step_p50_ms" in reps[0]:
+        out["chain_step_p50_ms"] = med(lambda x: x["chain_step_p50_ms"])
+        out["chain_step_p99_ms"] = med(lambda x: x["chain_step_p99_ms"])
+    return out
+
+
 def _run_serve(args, pkg, datasets, workloads, prec, rank, world, local_rank):
     """Served request stream: a saturated replay (everything queued at once) gives
     the capacity; the same trace replayed with the plain FP64 method gives the
@@ -751,6 +782,8 @@ def _run_serve(args, pkg, datasets, workloads, prec, rank, world, local_rank):
     import torch
     cfg = SERVE
     srv = pkg.Server(device=local_rank, workers=args.workers, hbm_budget_bytes=cfg["budget"])
+    if args.min_level is not None:
+        srv.set_mixed_policy(min_level=args.min_level)
     # warm-up: one request per order and precision
     for P in (6, 8, 10):
         for pr in {prec, pkg.FP64}:
@@ -764,11 +797,8 @@ def _run_serve(args, pkg, datasets, workloads, prec, rank, world, local_rank):
     launches0 = pkg.launch_count()
     mixed_samples, plain_samples = {}, {}
     with ClockSampler(local_rank) as clocks:
-        done, wall = workloads.replay(srv, sat, precision=prec, ncrit=cfg["ncrit"], nspawn=cfg["nspawn"],
-                                      deadline_s=300.0, samples=mixed_samples, host_alloc=pinned)
-        capacity = len(sat.jobs) / wall  # jobs per second with everything queued at once
-        saturated = workloads.latency_summary(done, wall)
-        saturated["while_saturated"] = workloads.saturated_throughput(done)
+        saturated = _saturated_replays(srv, sat, prec, cfg, workloads, pinned, mixed_samples)
+        capacity = saturated["capacity_jobs_per_s"]
         rates = {}
         for load in cfg["loads"]:
             reps = []
@@ -791,13 +821,10 @@ def _run_serve(args, pkg, datasets, workloads, prec, rank, world, local_rank):
     launches = pkg.launch_count() - launches0
     plain = None
     if not args.no_plain and prec == pkg.MIXED:
-        pd, pw = workloads.replay(srv, sat, precision=pkg.FP64, ncrit=cfg["ncrit"], nspawn=cfg["nspawn"],
-                                  deadline_s=600.0, samples=plain_samples, host_alloc=pinned)
-        psat = workloads.latency_summary(pd, pw)
-        psat["while_saturated"] = workloads.saturated_throughput(pd)
+        psat = _saturated_replays(srv, sat, pkg.FP64, cfg, workloads, pinned, plain_samples)
         plain = {"value": psat["while_saturated"]["bodies_per_s"],
                  "unit": "bodies/s (saturated replay of the same trace, until its last single solve)",
-                 "capacity_jobs_per_s": len(sat.jobs) / pw, "saturated": psat,
+                 "capacity_jobs_per_s": psat["capacity_jobs_per_s"], "saturated": psat,
                  "speedup_of_mixed": saturated["while_saturated"]["bodies_per_s"] /
                  psat["while_saturated"]["bodies_per_s"],
                  "speedup_of_mixed_whole_trace": saturated["bodies_per_s"] / psat["bodies_per_s"]}
@@ -817,6 +844,7 @@ def _run_serve(args, pkg, datasets, workloads, prec, rank, world, local_rank):
         "config": {"workload": cfg["name"], "jobs_per_trace": cfg["count"], "repeat_fraction": cfg["repeat_frac"],
                    "repeat_steps": cfg["repeat_steps"], "hbm_budget_bytes": cfg["budget"],
                    "workers": args.workers, "precision": args.precision, "parallelism": f"replicas{world}",
+                   "mixed_min_level": 2 if args.min_level is None else args.min_level,
                    "chains": "device-resident sessions: bodies moved and tree rebuilt on the device each step",
                    "timing": "host clock: scheduled arrival (or the previous chain step's return) to results "
                              "in host memory; p50/p99 are medians over the replays, with their ranges",
@@ -860,6 +888,8 @@ def _run_periodic(args, pkg, datasets, prec, rank, world, local_rank):
         f.results_device(out.data_ptr())
 
     fmm = pkg.Fmm(precision=prec, **kw)
+    if prec == pkg.MIXED and args.min_level is not None:
+        fmm.set_mixed_policy(min_level=args.min_level)
     for _ in range(max(3, args.warmup)):
         solve(fmm, dout)
     torch.cuda.synchronize()
@@ -898,6 +928,7 @@ def _run_periodic(args, pkg, datasets, prec, rank, world, local_rank):
         "vs_baseline": None, "dtype": "f64" if prec == pkg.FP64 else "f32+kahan", "data": "synthetic",
         "config": {"workload": cfg["name"], "charges": n, "box_edge_A": L, "P": cfg["P"], "theta": cfg["theta"],
                    "ncrit": cfg["ncrit"], "images": cfg["images"], "precision": args.precision,
+                   "mixed_min_level": (2 if args.min_level is None else args.min_level) if prec == pkg.MIXED else None,
                    "parallelism": f"replicas{world}", "cells": info["ncells"], "m2l_pairs": info["n_m2l"],
                    "p2p_pairs": info["n_p2p"],
                    "ewald": {"alpha": alpha, "cutoff_A": cfg["cutoff"], "ksize": ksize, "sigma": 0.25 / np.pi,

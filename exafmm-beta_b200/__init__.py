@@ -136,6 +136,8 @@ def lib() -> ctypes.CDLL:
         "exafmm_server_set_grouping": (_c_int, [_vp, _c_int, _c_ll, _c_ll]),
         "exafmm_list_work": (_c_int, [_vp, ctypes.POINTER(_c_ll)]),
         "exafmm_server_grouped": (_c_int, [_vp, ctypes.POINTER(_c_ll)]),
+        "exafmm_server_set_mixed_policy": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int]),
+        "exafmm_batch_set_ncrit_candidates": (_c_int, [_vp, _vp, _c_int]),
         "exafmm_displace_bodies": (_c_int, [_vp, _c_double, ctypes.c_ulonglong]),
         "exafmm_get_bodies": (_c_int, [_vp, _vp]),
         "exafmm_get_bodies_device": (_c_int, [_vp, _vp]),
@@ -225,7 +227,7 @@ class Fmm:
         self._check(lib().exafmm_set_params(self._h, P, theta, ncrit, nspawn, images, cycle))
         self.P, self.theta, self.ncrit, self.nspawn, self.images, self.cycle = P, theta, ncrit, nspawn, images, cycle
 
-    def set_mixed_policy(self, m2l_fp32=1, p2p_fp32=True, min_level=4, max_dl=3):
+    def set_mixed_policy(self, m2l_fp32=1, p2p_fp32=True, min_level=2, max_dl=3):
         """Mixed form: which operators run in FP32 and which M2L pairs may.
         m2l_fp32: 0 FP64; 1 FP32 with per-class products on the tensor cores (bf16x3
         pieces, FP32 accumulation) where they pay; 2 FP32 pair by pair; 3 as 1 with the
@@ -568,10 +570,16 @@ class Batch:
         if lib().exafmm_batch_set_forest(self._h, int(buckets)) != 0:
             raise FmmError("invalid forest bucket count")
 
-    def set_mixed_policy(self, m2l_fp32=1, p2p_fp32=True, min_level=4, max_dl=3):
+    def set_mixed_policy(self, m2l_fp32=1, p2p_fp32=True, min_level=2, max_dl=3):
         """Fmm.set_mixed_policy for every context of the batch."""
         if lib().exafmm_batch_set_mixed_policy(self._h, int(m2l_fp32), int(p2p_fp32), min_level, max_dl) != 0:
             raise FmmError("invalid mixed policy")
+
+    def set_ncrit_candidates(self, candidates):
+        """The ncrit values the autotuner tries, in order (default 32, 64, 128)."""
+        c = np.ascontiguousarray(candidates, dtype=np.int32)
+        if lib().exafmm_batch_set_ncrit_candidates(self._h, _p(c), len(c)) != 0:
+            raise FmmError("invalid ncrit candidates")
 
     def elapsed_ms(self) -> float:
         """Forest mode: device time of the last call (first copy in to last copy out)."""
@@ -729,6 +737,11 @@ class Server:
         if lib().exafmm_server_close_session(self._h, session) != 0:
             raise FmmError(lib().exafmm_server_error().decode())
         self._live.pop(("session", session), None)
+
+    def set_mixed_policy(self, m2l_fp32=1, p2p_fp32=True, min_level=2, max_dl=3):
+        """Fmm.set_mixed_policy for the server's mixed-precision requests."""
+        if lib().exafmm_server_set_mixed_policy(self._h, int(m2l_fp32), int(p2p_fp32), min_level, max_dl) != 0:
+            raise FmmError("invalid mixed policy")
 
     def set_grouping(self, max_requests=64, max_request_bodies=262144, max_group_bodies=4 << 20):
         """Continuous batching of small queued requests with equal parameters into

@@ -20,7 +20,7 @@ struct Params {
   // and source/target level difference) may; the rest stays FP64.
   int mixed_m2l = 1;
   int mixed_p2p = 1;
-  int mixed_min_level = 4;
+  int mixed_min_level = 2;
   int mixed_max_dl = 3;
   int mixed_gemm = 1;     // per-class products for frequent offset classes: 0 off, 1 where they pay, 2 always
   int mixed_gemm_tc = 1;  // ... on the tensor cores (bf16x3), else FP32 on the CUDA cores

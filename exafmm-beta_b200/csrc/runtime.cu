@@ -45,6 +45,14 @@ class NcritTuner {
  public:
   explicit NcritTuner(std::vector<int> cand) : cand_(std::move(cand)) {}
 
+  // New candidates start the tuning over (the table found so far is kept
+  // until a class has tried them all).
+  void set_candidates(std::vector<int> cand) {
+    std::lock_guard<std::mutex> lk(mu_);
+    cand_ = std::move(cand);
+    cls_.clear();
+  }
+
   int pick(long long n, int fallback) { return pick_class(size_class(n), fallback); }
 
   void report(long long n, int ncrit, double ms) {
@@ -127,7 +135,7 @@ struct SolveParams {
 // exafmm_set_mixed_policy's arguments, applied to every context a batch uses.
 struct MixedPolicy {
   bool set = false;
-  int m2l_fp32 = 1, p2p_fp32 = 1, min_level = 4, max_dl = 3;
+  int m2l_fp32 = 1, p2p_fp32 = 1, min_level = 2, max_dl = 3;
 };
 
 // One worker's context, created on first use and re-parameterized per system.
@@ -309,6 +317,7 @@ struct exafmm_server {
   int device = 0;
   int workers = 1;
   double budget = 0;
+  MixedPolicy policy;              // for the mixed-precision requests
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<Request *> queue;
@@ -378,6 +387,8 @@ struct exafmm_server {
         q->ctx = nullptr;
         throw std::runtime_error(exafmm_create_error());
       }
+      if (policy.set && q->prm.precision == EXAFMM_MIXED)
+        check(exafmm_set_mixed_policy(q->ctx, policy.m2l_fp32, policy.p2p_fp32, policy.min_level, policy.max_dl));
     }
     if (q->steps == 0) check(exafmm_set_bodies(q->ctx, q->xyzq0, q->n));
     else if (r->d_xyzq) check(exafmm_set_bodies_device(q->ctx, r->d_xyzq, q->n));
@@ -444,7 +455,7 @@ struct exafmm_server {
         if (r->sess) {
           dev_ms = run_step(r);
         } else if (grp.size() == 1) {
-          dev_ms = slots[w].solve(device, r->prm, r->xyzq, r->n, r->trg);
+          dev_ms = slots[w].solve(device, r->prm, r->xyzq, r->n, r->trg, &policy);
         } else {
           std::vector<long long> nn(grp.size());
           std::vector<const double *> in(grp.size());
@@ -454,7 +465,7 @@ struct exafmm_server {
             in[j] = grp[j]->xyzq;
             out[j] = grp[j]->trg;
           }
-          dev_ms = slots[w].solve_forest(device, r->prm, nullptr, (int)grp.size(), nn.data(), in.data(), out.data(),
+          dev_ms = slots[w].solve_forest(device, r->prm, &policy, (int)grp.size(), nn.data(), in.data(), out.data(),
                                          nullptr, nullptr);
         }
       } catch (const std::exception &e) {
@@ -736,6 +747,14 @@ int exafmm_batch_set_mixed_policy(exafmm_batch *b, int m2l_fp32, int p2p_fp32, i
   return 0;
 }
 
+int exafmm_batch_set_ncrit_candidates(exafmm_batch *b, const int *ncrit, int k) {
+  if (!b || k < 1 || k > 16 || !ncrit) return 2;
+  for (int i = 0; i < k; i++)
+    if (ncrit[i] < 1 || ncrit[i] > 1024) return 2;
+  b->tuner.set_candidates(std::vector<int>(ncrit, ncrit + k));
+  return 0;
+}
+
 int exafmm_batch_elapsed(exafmm_batch *b, double *ms) {
   if (!b || !ms) return 2;
   *ms = b->last_elapsed_ms;
@@ -971,6 +990,17 @@ int exafmm_server_set_grouping(exafmm_server *s, int max_requests, long long max
   s->group_max = max_requests;
   s->group_max_n = max_request_bodies;
   s->group_bodies = max_group_bodies;
+  return 0;
+}
+
+int exafmm_server_set_mixed_policy(exafmm_server *s, int m2l_fp32, int p2p_fp32, int min_level, int max_dl) {
+  if (!s || m2l_fp32 < 0 || m2l_fp32 > 5 || min_level < 0 || max_dl < 0) return 2;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->policy.set = true;
+  s->policy.m2l_fp32 = m2l_fp32;
+  s->policy.p2p_fp32 = p2p_fp32;
+  s->policy.min_level = min_level;
+  s->policy.max_dl = max_dl;
   return 0;
 }
 

@@ -61,8 +61,9 @@ int exafmm_set_params(exafmm_ctx *ctx, int P, double theta, int ncrit, int nspaw
  * enough for that to pay (P = 8 or 10); 2 = FP32 pair by pair only; 3 = as 1
  * with the per-class products at any size; 4 and 5 = as 1 and 3 with the
  * per-class products in FP32 on the CUDA cores.  p2p_fp32: 0 or 1.
- * Defaults: 1, 1, 4, 3.  No counterpart in the reference (its precision is a
- * compile-time switch, EXAFMM_SINGLE). */
+ * Defaults: 1, 1, 2, 3 (levels 0 and 1, the root levels, stay FP64).  No
+ * counterpart in the reference (its precision is a compile-time switch,
+ * EXAFMM_SINGLE). */
 int exafmm_set_mixed_policy(exafmm_ctx *ctx, int m2l_fp32, int p2p_fp32, int min_level, int max_dl);
 
 /* Separate source bodies (examples/fmm.cxx -j IneJ, :37-47, :61-73): the next
@@ -299,6 +300,9 @@ int exafmm_batch_set_ncrit_table(exafmm_batch *b, const int *pairs, int k);
 int exafmm_batch_set_forest(exafmm_batch *b, int buckets);
 /* exafmm_set_mixed_policy for every context of the batch (mixed precision). */
 int exafmm_batch_set_mixed_policy(exafmm_batch *b, int m2l_fp32, int p2p_fp32, int min_level, int max_dl);
+/* The autotuner's ncrit candidates (k of them, tried in this order; default
+ * 32, 64, 128); setting them restarts the tuning of every class. */
+int exafmm_batch_set_ncrit_candidates(exafmm_batch *b, const int *ncrit, int k);
 /* Forest mode: device time (ms) of the last call, from an event every worker
  * stream waits on before its first copy in to the last group's copy out. */
 int exafmm_batch_elapsed(exafmm_batch *b, double *ms);
@@ -363,6 +367,9 @@ int exafmm_server_stats(exafmm_server *s, double *stats6);
  * max_requests = 1 turns grouping off.  Defaults: 64, 262144, 4194304. */
 int exafmm_server_set_grouping(exafmm_server *s, int max_requests, long long max_request_bodies,
                                long long max_group_bodies);
+/* exafmm_set_mixed_policy for the server's mixed-precision requests (solves,
+ * groups and sessions opened afterwards). */
+int exafmm_server_set_mixed_policy(exafmm_server *s, int m2l_fp32, int p2p_fp32, int min_level, int max_dl);
 /* Requests solved so far inside a group of two or more. */
 int exafmm_server_grouped(exafmm_server *s, long long *requests);
 /* Error text of the last failed exafmm_server_wait on this thread. */

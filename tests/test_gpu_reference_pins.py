@@ -25,7 +25,7 @@ PLAIN_TOL = 1e-10
 ENGINES = (1, 2, 3, 5)
 
 
-def _solve(ex, x, precision, policy=None, min_level=4, **kw):
+def _solve(ex, x, precision, policy=None, min_level=2, **kw):
     f = ex.Fmm(precision=precision, **kw)
     if policy is not None:
         f.set_mixed_policy(m2l_fp32=policy, min_level=min_level)
