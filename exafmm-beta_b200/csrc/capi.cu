@@ -99,7 +99,7 @@ struct Engine {
   M2LGemmBufs gemm;         // class-grouped tile M2L (mixed form)
   DBuf<double2> lat;        // periodic lattice: supercell multipoles and warp partials
   DBuf<double> dip;         // dipole reduction scratch and result
-  DBuf<unsigned long long> work;  // work counter of persistent kernels
+  P2PWork p2pw;               // work counters and order of the mixed P2P kernels
   DBuf<double4> trg, out;
   Timing tm;
   bool tree_ok = false, up_ok = false, lists_ok = false;
@@ -433,8 +433,7 @@ struct Engine {
       if (mixed && C.prm.mixed_p2p) {
         x32.ensure(2 * C.tree.n);  // hi and lo float4 per body
         rel_bodies32(a, x32.p);
-        work.ensure(2);  // work counters of the two P2P kernels
-        p2p_mixed(a, x32.p, C.prm.images > 0, work.p);
+        p2p_mixed(C, a, x32.p, C.prm.images > 0, p2pw);
       } else {
         p2p_fp64(a);
       }

@@ -106,8 +106,15 @@ void dipole_correction_fp64(const double4 *xt, double4 *trg, long long n, double
 // Mixed-precision P2P (p2p32.cu): bodies as two-float pairs relative to the
 // root center; periodic selects the form that tests every pair for r = 0.
 void rel_bodies32(const FmmArgs &a, float4 *x32);
-// counter: one device word of scratch (the kernel's work counter).
-void p2p_mixed(const FmmArgs &a, const float4 *x32, bool periodic, unsigned long long *counter);
+// Scratch of the mixed P2P: the persistent kernels' work counters and their
+// work order (target leaves by kind, longest first).
+struct P2PWork {
+  DBuf<unsigned long long> next;   // [2] work counters
+  DBuf<unsigned> key, key_alt;     // order keys
+  DBuf<int> order, order_alt;      // cells in work order
+  DBuf<int> count;                 // [3] leaves of each kind: two targets per lane, three, no P2P list
+};
+void p2p_mixed(Context &C, const FmmArgs &a, const float4 *x32, bool periodic, P2PWork &w);
 
 // Interaction lists of the dual tree traversal (traverse.cu).
 struct ListBufs {

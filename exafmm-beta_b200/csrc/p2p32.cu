@@ -340,24 +340,52 @@ __device__ __forceinline__ bool three_per_lane(int n) {
   return (n > 8 && n <= 12) || (n > 16 && n <= 24) || (n > 32 && n <= 48) || (n > 64 && n <= 96);
 }
 
-// Persistent one-warp blocks, as many as fit on the GPU; each takes target
-// cells in order from a counter until none is left, so leaves of very
-// different cost balance out without the launch of one block per cell.  Each
-// kernel evaluates the leaves of its kind and skips the others.
+// Work order: each cell's kind (0: a leaf of two targets per lane, 1: three,
+// 2: no P2P list) above its cost (its bodies times the bodies of its list,
+// capped), reversed so that an ascending sort puts the costliest leaf of
+// each kind first.  count[kind] receives the cells of each kind.
+constexpr int kCostBits = 22;
+constexpr unsigned kCostMax = (1u << kCostBits) - 1;
+
+__global__ void k_p2p_keys(const int *off, const int *src, long long ncells, const int4 *cell_b, unsigned *key,
+                           int *val, int *count) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncells;
+       c += (long long)gridDim.x * blockDim.x) {
+    const int b = off[c], e = off[c + 1];
+    unsigned kind = 2, cost = 0;
+    if (b < e) {
+      const int nb = cell_b[c].y;
+      unsigned long long s = 0;
+      for (int q = b; q < e; q++) s += (unsigned)cell_b[src[q] & 0x3ffffff].y;
+      kind = three_per_lane(nb) ? 1u : 0u;
+      cost = (unsigned)min((unsigned long long)kCostMax, s * (unsigned long long)nb);
+    }
+    key[c] = (kind << kCostBits) | (kCostMax - cost);
+    val[c] = (int)c;
+    atomicAdd(&count[kind], 1);
+  }
+}
+
+// Persistent one-warp blocks, as many as fit on the GPU; each takes the next
+// target leaf of its kind from a counter, in the work order above (longest
+// first), until none is left, so leaves of very different cost balance out
+// and the warps finish together.  A leaf's result does not depend on when or
+// by which warp it is evaluated.
 template <bool PERIODIC, int TPL>
 __global__ void __launch_bounds__(32, TPL == 2 ? 16 : 12)
-k_p2p32(const int *off, const int *src, long long ncells, const int4 *cell_b, const float4 *x32, double4 *trg,
-        double cycle, unsigned long long *next) {
+k_p2p32(const int *off, const int *src, const int *order, const int *count, const int4 *cell_b, const float4 *x32,
+        double4 *trg, double cycle, unsigned long long *next) {
   __shared__ Stage sm;
+  const long long items = count[TPL == 2 ? 0 : 1];
+  const int *mine = order + (TPL == 2 ? 0 : count[0]);
   for (;;) {
-    unsigned long long c = 0;
-    if (threadIdx.x == 0) c = atomicAdd(next, 1ull);
-    c = __shfl_sync(kFull, c, 0);
-    if ((long long)c >= ncells) return;
+    unsigned long long k = 0;
+    if (threadIdx.x == 0) k = atomicAdd(next, 1ull);
+    k = __shfl_sync(kFull, k, 0);
+    if ((long long)k >= items) return;
+    const int c = mine[k];
     const int b = off[c], e = off[c + 1];
-    if (b == e) continue;
     const int4 cb = cell_b[c];
-    if (three_per_lane(cb.y) != (TPL == 3)) continue;
     if (cb.y <= 4 * TPL)
       p2p_leaf<4, TPL, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
     else if (cb.y <= 8 * TPL)
@@ -381,23 +409,38 @@ void rel_bodies32(const FmmArgs &a, float4 *x32) {
   EXA_CHECK_LAUNCH();
 }
 
-void p2p_mixed(const FmmArgs &a, const float4 *x32, bool periodic, unsigned long long *counter) {
-  if (a.ncells <= 0) return;
-  EXA_CUDA(cudaMemsetAsync(counter, 0, 2 * sizeof(unsigned long long), a.stream));
-  const unsigned g2 = (unsigned)std::min<long long>(a.ncells, (long long)kNumSMs * 16);
-  const unsigned g3 = (unsigned)std::min<long long>(a.ncells, (long long)kNumSMs * 12);
+void p2p_mixed(Context &C, const FmmArgs &a, const float4 *x32, bool periodic, P2PWork &w) {
+  const long long nc = a.ncells;
+  if (nc <= 0) return;
+  cudaStream_t st = a.stream;
+  w.next.ensure(2);
+  w.count.ensure(3);
+  w.key.ensure(nc);
+  w.key_alt.ensure(nc);
+  w.order.ensure(nc);
+  w.order_alt.ensure(nc);
+  EXA_CUDA(cudaMemsetAsync(w.next.p, 0, 2 * sizeof(unsigned long long), st));
+  EXA_CUDA(cudaMemsetAsync(w.count.p, 0, 3 * sizeof(int), st));
+  const int kg = (int)std::max<long long>(1, std::min<long long>((long long)kNumSMs * 8, (nc + 255) / 256));
+  k_p2p_keys<<<kg, 256, 0, st>>>(a.p2p_off, a.p2p_src, nc, a.cell_b, w.key.p, w.order.p, w.count.p);
+  EXA_CHECK_LAUNCH();
+  const bool alt = radix_sort_u32(w.key.p, w.order.p, w.key_alt.p, w.order_alt.p, nc, 0, kCostBits + 2, C.sort,
+                                  C.err.p, st);
+  const int *order = alt ? w.order_alt.p : w.order.p;
+  const unsigned g2 = (unsigned)std::min<long long>(nc, (long long)kNumSMs * 16);
+  const unsigned g3 = (unsigned)std::min<long long>(nc, (long long)kNumSMs * 12);
   if (periodic) {
-    k_p2p32<true, 2><<<g2, 32, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b, x32, a.trg64, a.cycle,
-                                              counter);
+    k_p2p32<true, 2><<<g2, 32, 0, st>>>(a.p2p_off, a.p2p_src, order, w.count.p, a.cell_b, x32, a.trg64, a.cycle,
+                                        w.next.p);
     EXA_CHECK_LAUNCH();
-    k_p2p32<true, 3><<<g3, 32, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b, x32, a.trg64, a.cycle,
-                                              counter + 1);
+    k_p2p32<true, 3><<<g3, 32, 0, st>>>(a.p2p_off, a.p2p_src, order, w.count.p, a.cell_b, x32, a.trg64, a.cycle,
+                                        w.next.p + 1);
   } else {
-    k_p2p32<false, 2><<<g2, 32, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b, x32, a.trg64, a.cycle,
-                                               counter);
+    k_p2p32<false, 2><<<g2, 32, 0, st>>>(a.p2p_off, a.p2p_src, order, w.count.p, a.cell_b, x32, a.trg64, a.cycle,
+                                         w.next.p);
     EXA_CHECK_LAUNCH();
-    k_p2p32<false, 3><<<g3, 32, 0, a.stream>>>(a.p2p_off, a.p2p_src, a.ncells, a.cell_b, x32, a.trg64, a.cycle,
-                                               counter + 1);
+    k_p2p32<false, 3><<<g3, 32, 0, st>>>(a.p2p_off, a.p2p_src, order, w.count.p, a.cell_b, x32, a.trg64, a.cycle,
+                                         w.next.p + 1);
   }
   EXA_CHECK_LAUNCH();
 }
