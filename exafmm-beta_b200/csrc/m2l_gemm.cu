@@ -20,10 +20,12 @@
 // adds them to L: deterministic, no atomics.  The 4,096 multiply-adds per pair
 // (at P = 8) replace the 9,216 of the pair-by-pair complex contraction.
 //
-// Classes used by fewer than kMinClassPairs pairs and pairs through periodic
-// images stay with the pair-by-pair FP32 kernel, which then runs on a compacted
-// list of just those pairs (left_off / left_src); pairs outside the mixed
-// policy stay with the FP64 kernel as before.
+// Pairs through periodic images form classes of their own (the image and the
+// target level join the key, since the shift is not a multiple of the radii).
+// Classes used by fewer than kMinClassPairs pairs stay with the pair-by-pair
+// FP32 kernel, which then runs on a compacted list of just those pairs
+// (left_off / left_src); pairs outside the mixed policy stay with the FP64
+// kernel as before.
 //
 // Two engines form the products.  The tensor-core one (k_m2l_class_mma) splits
 // every operand entry into three bf16 pieces, x = hi + mid + lo (24 significant
@@ -106,6 +108,19 @@ __device__ __forceinline__ unsigned long long class_key(int dl, long long dx, lo
          ((unsigned long long)(dy + 32768) << 16) | (unsigned long long)(dz + 32768);
 }
 
+// A pair through a periodic image: the source sits at its cell's center plus
+// the image shift (a multiple of the cycle, not of the radii), so the offset
+// in units of the target radius is the integer offset of the two cells minus
+// shift / R_t, which depends on the target level too.  Key: bit 63 set, the
+// target level at bits 58-62, dl + 16 at 53-57, the image at 48-52, then the
+// cells' integer offset as in class_key (whose keys keep bit 63 clear).
+__device__ __forceinline__ unsigned long long class_key_image(int lt, int dl, int img, long long dx, long long dy,
+                                                              long long dz) {
+  return (1ull << 63) | ((unsigned long long)lt << 58) | ((unsigned long long)(dl + 16) << 53) |
+         ((unsigned long long)img << 48) | ((unsigned long long)(dx + 32768) << 32) |
+         ((unsigned long long)(dy + 32768) << 16) | (unsigned long long)(dz + 32768);
+}
+
 // 1. Per pair of the target-grouped list: its class's hash slot, or -1.
 __global__ void k_pair_class(const int *off, const int *src, long long ncells, const double4 *cell_x,
                              const int2 *cell_pl, int min_level, int max_dl, unsigned long long *hk, unsigned *hc,
@@ -123,12 +138,14 @@ __global__ void k_pair_class(const int *off, const int *src, long long ncells, c
       const int ls = cell_pl[cj].y;
       const int dl = ls - lt;
       int slot = -1;
-      if (img == 13 && lt >= min_level && dl <= max_dl && dl >= -max_dl) {
+      if (lt >= min_level && lt < 32 && dl <= max_dl && dl >= -max_dl) {
         const double4 Xs = cell_x[cj];
         const double rmin = fmin(Xt.w, Xs.w);
         const double fx = rint((Xt.x - Xs.x) / rmin), fy = rint((Xt.y - Xs.y) / rmin), fz = rint((Xt.z - Xs.z) / rmin);
         if (fabs(fx) < 32767 && fabs(fy) < 32767 && fabs(fz) < 32767) {
-          const unsigned long long key = class_key(dl, (long long)fx, (long long)fy, (long long)fz);
+          const unsigned long long key =
+              img == 13 ? class_key(dl, (long long)fx, (long long)fy, (long long)fz)
+                        : class_key_image(lt, dl, img, (long long)fx, (long long)fy, (long long)fz);
           long long h = (long long)(mix64(key) & (unsigned long long)hmask);
           for (int p = 0; p < kProbe; p++) {
             // a slot's key, once set, never changes: read it at L2 and CAS only
@@ -170,18 +187,29 @@ __global__ void k_class_ids(const int *cs_sorted, int ncls, int *hid) {
 // 3. Operator of each class: FP32 k-major, Kt[class][input dof][output dof]
 // (CUDA-core engine), or three bf16 pieces of it per class, each an operand
 // image of NDP output rows x NDP inputs in the core_off layout (tensor cores).
+// cell_x[0].w (the root radius) and cycle place the image shifts of
+// class_key_image keys (one system, never a forest, has image pairs).
 __global__ void k_build_K(DevTables t, const unsigned long long *ck, int P, float *Kt, unsigned short *Kb,
-                          bool swizzled) {
+                          bool swizzled, const double4 *cell_x, double cycle) {
   extern __shared__ double2 S[];  // S'_p^q, q >= 0, at d / R_t
   const int NT = t.nterm, ND = nd_of(P), NDP = ndp_of(P);
   const unsigned long long key = ck[blockIdx.x];
-  const int dl = (int)((key >> 48) & 0xffff) - 16;
+  const bool image = (key >> 63) != 0;
+  const int dl = image ? (int)((key >> 53) & 31) - 16 : (int)((key >> 48) & 0xffff) - 16;
   const double ux = (double)(long long)((key >> 32) & 0xffff) - 32768.0;
   const double uy = (double)(long long)((key >> 16) & 0xffff) - 32768.0;
   const double uz = (double)(long long)(key & 0xffff) - 32768.0;
   const double to_rt = dl > 0 ? ldexp(1.0, -dl) : 1.0;  // min(R_s, R_t) / R_t
+  double sx = 0.0, sy = 0.0, sz = 0.0;                    // image shift / R_t
+  if (image) {
+    const int lt = (int)((key >> 58) & 31), img = (int)((key >> 48) & 31);
+    const double inv_rt = 1.0 / ldexp(cell_x[0].w, -lt);
+    sx = (double)(img / 9 - 1) * cycle * inv_rt;
+    sy = (double)((img / 3) % 3 - 1) * cycle * inv_rt;
+    sz = (double)(img % 3 - 1) * cycle * inv_rt;
+  }
   if ((int)threadIdx.x < 2 * P - 1)
-    singular_column(t, threadIdx.x, 2 * P - 1, ux * to_rt, uy * to_rt, uz * to_rt, t.ainv, S);
+    singular_column(t, threadIdx.x, 2 * P - 1, ux * to_rt - sx, uy * to_rt - sy, uz * to_rt - sz, t.ainv, S);
   __syncthreads();
   const int KB = (NDP + 63) / 64;  // 128-byte K-blocks of the swizzled image
   const int img = swizzled ? KB * NDP * 64 : NDP * NDP;
@@ -1124,7 +1152,7 @@ bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int
   EXA_CUDA(cudaStreamSynchronize(st));
   if (ncls <= 0) return false;
   if (ncls > ccap) ncls = ccap;  // the overflow classes' pairs stay per-pair
-  bool alt = radix_sort_u64((uint64_t *)g.ck.p, g.cs.p, (uint64_t *)g.ck_alt.p, g.cs_alt.p, ncls, 0, 56, C.sort,
+  bool alt = radix_sort_u64((uint64_t *)g.ck.p, g.cs.p, (uint64_t *)g.ck_alt.p, g.cs_alt.p, ncls, 0, 64, C.sort,
                             C.err.p, st);
   unsigned long long *ck = alt ? g.ck_alt.p : g.ck.p;
   int *cs = alt ? g.cs_alt.p : g.cs.p;
@@ -1140,7 +1168,8 @@ bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int
   else g.K.ensure((long long)ncls * NDP * NDP);
   {
     const size_t smem = tri(2 * P - 1) * sizeof(double2);
-    k_build_K<<<ncls, 256, smem, st>>>(t, ck, P, tc ? nullptr : g.K.p, tc ? g.Kb.p : nullptr, use_tma);
+    k_build_K<<<ncls, 256, smem, st>>>(t, ck, P, tc ? nullptr : g.K.p, tc ? g.Kb.p : nullptr, use_tma, a.cell_x,
+                                       a.cycle);
     EXA_CHECK_LAUNCH();
   }
   if (tc) g.Msb.ensure(nc * 3 * NDP);

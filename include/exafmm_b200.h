@@ -58,7 +58,8 @@ int exafmm_set_params(exafmm_ctx *ctx, int P, double theta, int ncrit, int nspaw
  * FP64.  m2l_fp32: 0 = FP64; 1 = FP32, with the pairs of frequent offset
  * classes evaluated as dense per-class products on the tensor cores (three
  * bf16 pieces per operand, FP32 accumulation) when the system is large
- * enough for that to pay (P = 8 or 10); 2 = FP32 pair by pair only; 3 = as 1
+ * enough for that to pay (P = 8 or 10) or periodic (images > 0, any size and
+ * P = 4, 6, 8, 10, for accuracy); 2 = FP32 pair by pair only; 3 = as 1
  * with the per-class products at any size; 4 and 5 = as 1 and 3 with the
  * per-class products in FP32 on the CUDA cores.  p2p_fp32: 0 or 1.
  * Defaults: 1, 1, 2, 3 (levels 0 and 1, the root levels, stay FP64).  No

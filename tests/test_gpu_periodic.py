@@ -84,3 +84,37 @@ def test_periodic_oracle_matches_fresh_inputs(ex, oracle, datasets):
     assert rel_l2(trg[:, 0], o.trg[:, 0]) < 1e-10
     assert rel_l2(trg[:, 1:], o.trg[:, 1:]) < 1e-10
     f.close()
+
+
+@pytest.mark.parametrize("P", [8, 10])
+def test_periodic_class_products_through_images(ex, datasets, P):
+    """Pairs through periodic images take the per-class products too (their class
+    key adds the image and the target level): every mixed M2L engine on a water
+    box with images = 3 against the plain FP64 method on the same trees, and the
+    class products against the pair-by-pair FP32 kernel."""
+    x, L = datasets.water_box(12000, seed=17)
+    kw = dict(P=P, theta=0.4, ncrit=32, nspawn=5000, images=3, cycle=L)
+    res = {}
+    for name, prec, pol in (("plain", ex.FP64, None), ("default", ex.MIXED, 1), ("tc", ex.MIXED, 3),
+                            ("cc", ex.MIXED, 5), ("pair", ex.MIXED, 2)):
+        f = ex.Fmm(precision=prec, **kw)
+        if pol is not None:
+            f.set_mixed_policy(m2l_fp32=pol)
+        f.set_bodies(x)
+        f.solve()
+        res[name] = f.results()
+        m2l, _ = f.lists()
+        f.close()
+    assert np.mean(m2l[:, 2] != 13) > 0.2  # image pairs are a large share of this box's M2L
+    err = {}
+    for name in ("default", "tc", "cc", "pair"):
+        err[name] = (rel_l2(res[name][:, 0], res["plain"][:, 0]), rel_l2(res[name][:, 1:], res["plain"][:, 1:]))
+        print(f"P={P} {name}: pot {err[name][0]:.2e} acc {err[name][1]:.2e}")
+    # the default takes the class products in a periodic box, at any size
+    assert np.array_equal(res["default"], res["tc"])
+    for name in ("tc", "cc"):
+        assert err[name][0] < 1e-6 and err[name][1] < 1e-6, name
+    # pair by pair, the FP32 sums over a lane's sources lose more on this
+    # neutral box (which is why periodic solves default to the products)
+    assert err["pair"][0] < 5e-6 and err["pair"][1] < 1e-6
+    assert rel_l2(res["tc"][:, 0], res["pair"][:, 0]) < 5e-6
