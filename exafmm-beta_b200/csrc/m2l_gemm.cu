@@ -38,6 +38,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <stdexcept>
 
 #include "fmm.h"
@@ -980,64 +981,73 @@ k_m2l_class_mma_tma(const __grid_constant__ CUtensorMap msb_map, const int4 *chu
   }
 }
 
-// 7. Per target: its taken pairs' contributions summed in list order in FP64,
-// scaled by (-1)^j A_j^k R_t^{-(j+1)}, added to L.  Lane l holds entries
-// 2l, 2l + 1 (+ 64 u) of the column and loads them as one 8-byte word.
+// 7. Per target cell, in list order: the sum of its taken pairs' columns of
+// Y (FP64), scaled by (-1)^j A_j^k R_t^{-(j+1)}, added to L.  Lane l holds
+// entries VEC l .. VEC l + VEC - 1 of a column (VEC = 4 floats, one 16-byte
+// load per lane and pair, for NDP > 64; else 2).  A group's rows are loaded
+// together with its taken flags (the rows of pairs not taken hold whatever is
+// there and are dropped by a select, so the loads do not wait for the flags),
+// and the next group's loads are in flight while this one is added.
 template <int NDP>
 __global__ void k_m2l_class_reduce(const int *off, long long ncells, const unsigned char *taken, const float *Y,
                                    const double4 *cell_x, DevTables t, int P, double2 *L) {
-  constexpr int PER = (NDP + 63) / 64;
+  constexpr int VEC = NDP > 64 ? 4 : 2;
+  constexpr int LANES = NDP / VEC;  // lanes that hold entries
+  static_assert(NDP % VEC == 0 && LANES <= 32, "one row per warp-wide load");
+  constexpr int G = 8;
+  using V = typename std::conditional<VEC == 4, float4, float2>::type;
   const int lane = threadIdx.x & 31;
+  const bool active = lane < LANES;
   const int NT = t.nterm, ND = nd_of(P);
   const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  auto load = [&](int q, int e, bool &tk, V &v) {
+    tk = false;
+    v = V{};
+    if (q < e) {
+      tk = taken[q] != 0;
+      if (active) v = reinterpret_cast<const V *>(Y + (long long)q * NDP)[lane];
+    }
+  };
   for (long long c = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < ncells; c += warps) {
     const int b = off[c], e = off[c + 1];
-    double acc[PER][2];
+    double acc[VEC];
+#pragma unroll
+    for (int i = 0; i < VEC; i++) acc[i] = 0.0;
     bool any = false;
+    bool tk[G], tk2[G];
+    V v[G], v2[G];
 #pragma unroll
-    for (int u = 0; u < PER; u++) acc[u][0] = acc[u][1] = 0.0;
-    // G pairs' flags and columns loaded before they are added (in list order)
-    constexpr int G = NDP > 64 ? 8 : 16;
+    for (int i = 0; i < G; i++) load(b + i, e, tk[i], v[i]);
     for (int q0 = b; q0 < e; q0 += G) {
-      bool tk[G];
-      float2 v[G][PER];
 #pragma unroll
-      for (int i = 0; i < G; i++) tk[i] = q0 + i < e && taken[q0 + i];
-#pragma unroll
-      for (int i = 0; i < G; i++) {
-        const float2 *y = reinterpret_cast<const float2 *>(Y + (long long)(q0 + i) * NDP);
-#pragma unroll
-        for (int u = 0; u < PER; u++)
-          v[i][u] = (tk[i] && 2 * lane + 64 * u < NDP) ? y[lane + 32 * u] : make_float2(0.f, 0.f);
-      }
+      for (int i = 0; i < G; i++) load(q0 + G + i, e, tk2[i], v2[i]);  // the next group, in flight
 #pragma unroll
       for (int i = 0; i < G; i++) {
         if (!tk[i]) continue;
         any = true;
+        const float *f = reinterpret_cast<const float *>(&v[i]);
 #pragma unroll
-        for (int u = 0; u < PER; u++)
-          if (2 * lane + 64 * u < NDP) {
-            acc[u][0] += (double)v[i][u].x;
-            acc[u][1] += (double)v[i][u].y;
-          }
+        for (int k = 0; k < VEC; k++) acc[k] += (double)f[k];
+      }
+#pragma unroll
+      for (int i = 0; i < G; i++) {
+        tk[i] = tk2[i];
+        v[i] = v2[i];
       }
     }
-    if (!any) continue;
+    if (!any || !active) continue;
     const double rt = cell_x[c].w;
 #pragma unroll
-    for (int u = 0; u < PER; u++) {
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const int d = 2 * lane + 64 * u + h;
-        if (d >= ND) continue;
-        int j, k, part;
-        dof_decode(d, NT, j, k, part);
-        const int o = tri(j) + k;
-        const double v = acc[u][h] * sgn_pow(j) * t.anm[o] * pow(rt, -(double)(j + 1));
-        double2 *dst = &L[c * NT + o];
-        if (part == 0) dst->x += v;
-        else dst->y += v;
-      }
+    for (int h = 0; h < VEC; h++) {
+      const int d = VEC * lane + h;
+      if (d >= ND) continue;
+      int j, k, part;
+      dof_decode(d, NT, j, k, part);
+      const int o = tri(j) + k;
+      const double val = acc[h] * sgn_pow(j) * t.anm[o] * pow(rt, -(double)(j + 1));
+      double2 *dst = &L[c * NT + o];
+      if (part == 0) dst->x += val;
+      else dst->y += val;
     }
   }
 }
