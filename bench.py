@@ -306,6 +306,10 @@ def main():
                     help="batch: size groups solved as one forest each (0: one context per system)")
     ap.add_argument("--min-level", type=int, default=None,
                     help="mixed form: lowest target level of the FP32 M2L (default 2: levels 0 and 1 in FP64)")
+    ap.add_argument("--orders", default="6,8,10",
+                    help="serve: the expansion orders requests draw from (10 alone: the north star's P = 10 stream)")
+    ap.add_argument("--group-max-n", type=int, default=262144,
+                    help="serve: requests of at most this many bodies are grouped into forests")
     ap.add_argument("--ncrit-candidates", default="32,64,128",
                     help="batch: the ncrit values the autotuner tries per size group")
     args = ap.parse_args()
@@ -760,7 +764,7 @@ def _saturated_replays(srv, trace, precision, cfg, workloads, pinned, samples):
         reps.append(s)
     med = lambda f: float(np.median([f(x) for x in reps]))
     out = {k: med(lambda x, k=k: x[k]) for k in ("p50_ms", "p99_ms", "mean_ms", "bodies_per_s", "wall_s",
-                                                  "capacity_jobs_per_s")}
+                                                  "capacity_jobs_per_s", "device_ms_sum")}
     out["requests"] = reps[0]["requests"]
     out["replays"] = len(reps)
     out["bodies_per_s_range"] = [min(x["bodies_per_s"] for x in reps), max(x["bodies_per_s"] for x in reps)]
@@ -784,12 +788,15 @@ def _run_serve(args, pkg, datasets, workloads, prec, rank, world, local_rank):
     srv = pkg.Server(device=local_rank, workers=args.workers, hbm_budget_bytes=cfg["budget"])
     if args.min_level is not None:
         srv.set_mixed_policy(min_level=args.min_level)
+    srv.set_grouping(max_request_bodies=args.group_max_n)
     # warm-up: one request per order and precision
-    for P in (6, 8, 10):
+    for P in sorted(set(int(v) for v in args.orders.split(",") if v)):
         for pr in {prec, pkg.FP64}:
             srv.wait(srv.submit(datasets.cube(20000, seed=P), P=P, theta=cfg["theta"], ncrit=cfg["ncrit"],
                                 precision=pr))
-    sat = workloads.make_trace(cfg["count"], rate=1e6, lo=cfg["lo"], hi=cfg["hi"], repeat_frac=cfg["repeat_frac"],
+    orders = tuple(int(v) for v in args.orders.split(",") if v)
+    sat = workloads.make_trace(cfg["count"], rate=1e6, lo=cfg["lo"], hi=cfg["hi"], orders=orders,
+                               repeat_frac=cfg["repeat_frac"],
                                repeat_steps=cfg["repeat_steps"], seed=4000 + 1000 * rank, theta=cfg["theta"])
     def pinned(shape):
         return torch.empty(shape, dtype=torch.float64).pin_memory().numpy()
@@ -803,7 +810,7 @@ def _run_serve(args, pkg, datasets, workloads, prec, rank, world, local_rank):
         for load in cfg["loads"]:
             reps = []
             for r in range(cfg["replays"]):
-                tr = workloads.make_trace(cfg["count"], rate=load * capacity, lo=cfg["lo"], hi=cfg["hi"],
+                tr = workloads.make_trace(cfg["count"], rate=load * capacity, lo=cfg["lo"], hi=cfg["hi"], orders=orders,
                                           repeat_frac=cfg["repeat_frac"], repeat_steps=cfg["repeat_steps"],
                                           seed=5000 + int(100 * load) + 10 * r + 1000 * rank, theta=cfg["theta"])
                 d, w = workloads.replay(srv, tr, precision=prec, ncrit=cfg["ncrit"], nspawn=cfg["nspawn"],
@@ -837,7 +844,7 @@ def _run_serve(args, pkg, datasets, workloads, prec, rank, world, local_rank):
                    for k in ("mixed_vs_direct", "plain_vs_direct", "mixed_vs_plain") if any(k in r for r in errs)}
     line = {
         "metric": "served p99 latency (Poisson arrivals at 0.8 of capacity; N log-uniform [1e3, 1e6], "
-                  "P in {6, 8, 10}, theta=0.4)",
+                  f"P in {{{', '.join(str(o) for o in orders)}}}, theta=0.4)",
         "value": top["p99_ms"], "unit": "ms", "n_gpus": world, "steps": cfg["replays"], "warmup": 1,
         "ms_per_step": top["mean_ms"], "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if prec == pkg.FP64 else "f32+kahan", "data": "synthetic",
@@ -845,6 +852,7 @@ def _run_serve(args, pkg, datasets, workloads, prec, rank, world, local_rank):
                    "repeat_steps": cfg["repeat_steps"], "hbm_budget_bytes": cfg["budget"],
                    "workers": args.workers, "precision": args.precision, "parallelism": f"replicas{world}",
                    "mixed_min_level": 2 if args.min_level is None else args.min_level,
+                   "group_max_request_bodies": args.group_max_n, "orders": list(orders),
                    "chains": "device-resident sessions: bodies moved and tree rebuilt on the device each step",
                    "timing": "host clock: scheduled arrival (or the previous chain step's return) to results "
                              "in host memory; p50/p99 are medians over the replays, with their ranges",

@@ -41,6 +41,7 @@ struct TreeBufs {
   DBuf<int> nd_begin, nd_count, nd_nchild, nd_childbeg, nd_nnode, nd_cell, nd_pcell, nd_ichild;
   DBuf<double4> nd_x;
   DBuf<long long> lvl;       // [0, L]: node count per level; [L+1, 2L+1]: level start
+  DBuf<int> split_level;     // deepest level with a node of more than ncrit bodies (-1: none)
   // cells (reference layout)
   long long cell_cap = 0;
   DBuf<int4> cell_b;         // ibody, nbody, ichild, nchild

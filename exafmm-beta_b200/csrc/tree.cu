@@ -177,6 +177,36 @@ __global__ void k_keys(const double4 *x, long long n, const double *box, unsigne
   }
 }
 
+// The deepest level whose nodes split, from the sorted keys alone: bodies i
+// and i + ncrit lie in one node of level l exactly when their keys share the
+// digits of levels 0..l-1 (and, in a forest, their system), and that node then
+// holds more than ncrit bodies; so the deepest splitting level is the largest
+// number of shared leading digits over i (kMaxLevels when the keys are equal).
+// sys_off (a forest, else null) places each body's caller index in its system.
+__device__ __forceinline__ int system_of(const long long *sys_off, int nsys, long long i) {
+  int lo = 0, hi = nsys - 1;  // last s with sys_off[s] <= i
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (sys_off[mid] <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void k_split_level(const unsigned long long *keys, const int *perm, long long n, int ncrit,
+                              const long long *sys_off, int nsys, int *out) {
+  int best = -1;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i + ncrit < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    if (sys_off && system_of(sys_off, nsys, perm[i]) != system_of(sys_off, nsys, perm[i + ncrit])) continue;
+    const unsigned long long x = keys[i] ^ keys[i + ncrit];
+    const int shared = x == 0 ? kMaxLevels : kMaxLevels - 1 - (63 - __clzll((long long)x)) / 3;
+    best = max(best, shared);
+  }
+  for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+  if ((threadIdx.x & 31) == 0 && best >= 0) atomicMax(out, best);
+}
+
 __global__ void k_tree_root(long long n, long long *lvl, int *nd_begin, int *nd_count, double4 *nd_x,
                             const double *box, int *nd_cell, int *nd_pcell, int *nd_ichild) {
   if (threadIdx.x != 0) return;
@@ -781,11 +811,27 @@ void build_tree(Context &C) {
                                   T.nd_pcell.p, T.nd_ichild.p);
   }
   EXA_CHECK_LAUNCH();
+  // The level kernels run down to one level below the deepest splitting one
+  // (its nodes are leaves), so a shallow tree costs a few launches per
+  // level, not kMaxLevels of them; the deepest splitting level is read back
+  // from the sorted keys first (one small transfer).
+  int last = 0;
+  if (n > ncrit) {
+    T.split_level.ensure(1);
+    EXA_CUDA(cudaMemsetAsync(T.split_level.p, 0xff, sizeof(int), st));
+    k_split_level<<<grid_for(n, 256), 256, 0, st>>>(T.keys.p, T.perm.p, n, ncrit, forest ? T.sys_off.p : nullptr,
+                                                   T.nsys, T.split_level.p);
+    EXA_CHECK_LAUNCH();
+    int deepest = -1;
+    EXA_CUDA(cudaMemcpyAsync(&deepest, T.split_level.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    EXA_CUDA(cudaStreamSynchronize(st));
+    last = std::min(deepest + 1, kMaxLevels);
+  }
   // per-level kernels: eight threads per node at most node_cap nodes
   const int node_grid = (int)std::max<long long>(1, std::min<long long>(kNumSMs * 4, (8 * T.node_cap + 255) / 256));
   long long *lvl_n = T.lvl.p + 2 * (kMaxLevels + 1);
   long long *lvl_s = lvl_n + 1;
-  for (int l = 0; l <= kMaxLevels; l++) {
+  for (int l = 0; l <= last; l++) {
     k_expand<<<node_grid, 256, 0, st>>>(a, l);
     EXA_CHECK_LAUNCH();
     if (l == kMaxLevels) break;  // deepest level: only the too-deep check runs
@@ -797,7 +843,7 @@ void build_tree(Context &C) {
     EXA_CHECK_LAUNCH();
   }
   if (C.ev_link) EXA_CUDA(cudaEventRecord(C.ev_link, st));  // BuildTree: growTree done, linkTree next
-  for (int l = kMaxLevels; l >= 0; l--) {
+  for (int l = last; l >= 0; l--) {
     k_nnode<<<node_grid, 256, 0, st>>>(a, l);
     EXA_CHECK_LAUNCH();
   }
@@ -806,7 +852,7 @@ void build_tree(Context &C) {
                                       T.sys_cell.p, T.cell_cap, C.err.p);
     EXA_CHECK_LAUNCH();
   }
-  for (int l = 0; l <= kMaxLevels; l++) {
+  for (int l = 0; l <= last; l++) {
     k_cells<<<node_grid, 256, 0, st>>>(a, l);
     EXA_CHECK_LAUNCH();
   }

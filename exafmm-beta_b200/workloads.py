@@ -207,6 +207,7 @@ def latency_summary(done, wall_s: float) -> dict:
     out = {"requests": len(done), "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
            "mean_ms": float(lat.mean()), "bodies_per_s": bodies / wall_s if wall_s > 0 else 0.0,
            "wall_s": wall_s}
+    out["device_ms_sum"] = float(sum(float(c.times[3]) for c in done))
     chain = [c.latency_ms for c in done if c.steps > 1 and c.step > 0]
     if chain:
         out["chain_step_p50_ms"] = float(np.percentile(chain, 50))
