@@ -44,9 +44,9 @@ METRIC = "FMM bodies/s (full mixed-precision solve, Plummer N=4,194,304, P=8, th
 CPU_SAMPLE_N = 262_144
 # DRAM bytes per M2L pair of the mixed M2L phase at P = 8: the per-class products write each
 # pair's contribution (256 B) and the per-target pass reads it back; dram__bytes_read.sum +
-# dram__bytes_write.sum of those two kernels in the ncu capture of the 1M-body case (4.41 GB
-# for 8,233,680 pairs), scaled by pairs
-M2L_DRAM_BYTES_PER_PAIR = 535.0
+# dram__bytes_write.sum of those two kernels in the ncu capture of the 1M-body case (4.43 GB
+# for 8,233,680 pairs, profiles/m2l_traffic_plummer_1m_p8_mixed_ncrit128.txt), scaled by pairs
+M2L_DRAM_BYTES_PER_PAIR = 538.0
 
 
 def _package():
