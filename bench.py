@@ -312,6 +312,8 @@ def main():
                     help="serve: requests of at most this many bodies are grouped into forests")
     ap.add_argument("--ncrit-candidates", default="32,64,128",
                     help="batch: the ncrit values the autotuner tries per size group")
+    ap.add_argument("--p2p-candidates", default="0,2,3",
+                    help="batch: the P2P targets-per-lane settings tried with every ncrit (mixed form)")
     args = ap.parse_args()
     if check_world(args.gpus) == "spawn":
         r = subprocess.run(["timeout", "-k", "60", "3600"] + torchrun_command(sys.argv[1:], args.gpus, _free_port()))
@@ -620,13 +622,15 @@ def _run_batch(args, pkg, datasets, workloads, prec, rank, world, local_rank):
     b = make(prec)
     forest = args.buckets > 0
     cands = [int(v) for v in args.ncrit_candidates.split(",") if v]
-    if forest:  # the tuner tries one ncrit per call: untimed tuning calls, then the table is frozen
+    p2p_cands = [int(v) for v in args.p2p_candidates.split(",") if v] if prec == pkg.MIXED else [0]
+    if forest:  # the tuner tries one configuration per call: untimed tuning calls, then the table is frozen
         b.set_ncrit_candidates(cands)
+        b.set_p2p_candidates(p2p_cands)
         b.autotune(True)
-        for _ in range(len(cands)):
+        for _ in range(len(cands) * len(p2p_cands)):
             step(b)
         b.autotune(False)
-        warm = max(1, args.warmup - len(cands))
+        warm = max(1, args.warmup - len(cands) * len(p2p_cands))
     else:
         b.autotune(True)
         step(b)
@@ -684,6 +688,8 @@ def _run_batch(args, pkg, datasets, workloads, prec, rank, world, local_rank):
                    "distribution": "even systems uniform in [-1,1]^3, odd on the unit sphere; q U[-1,1]",
                    "P": cfg["P"], "theta": cfg["theta"], "forest_groups": int(len(group_ncrit)),
                    "group_ncrit": [int(v) for v in group_ncrit], "ncrit_table": b.ncrit_table(),
+                   "group_p2p_targets_per_lane": [int(v) for v in b.bucket_p2p()] if forest else None,
+                   "tuned": {"ncrit": cands, "p2p_targets_per_lane": p2p_cands},
                    "group_bodies": [int(sum(n for n, gi in zip(sizes, group) if gi == k))
                                     for k in range(len(group_ncrit))],
                    "mixed_min_level": min_level if prec == pkg.MIXED else None,

@@ -138,6 +138,11 @@ def lib() -> ctypes.CDLL:
         "exafmm_server_grouped": (_c_int, [_vp, ctypes.POINTER(_c_ll)]),
         "exafmm_server_set_mixed_policy": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int]),
         "exafmm_batch_set_ncrit_candidates": (_c_int, [_vp, _vp, _c_int]),
+        "exafmm_batch_set_p2p_candidates": (_c_int, [_vp, _vp, _c_int]),
+        "exafmm_batch_config_table": (_c_int, [_vp, _vp, _c_int]),
+        "exafmm_batch_set_config_table": (_c_int, [_vp, _vp, _c_int]),
+        "exafmm_batch_bucket_p2p": (_c_int, [_vp, _vp, _c_int]),
+        "exafmm_set_p2p_targets_per_lane": (_c_int, [_vp, _c_int]),
         "exafmm_displace_bodies": (_c_int, [_vp, _c_double, ctypes.c_ulonglong]),
         "exafmm_get_bodies": (_c_int, [_vp, _vp]),
         "exafmm_get_bodies_device": (_c_int, [_vp, _vp]),
@@ -234,6 +239,10 @@ class Fmm:
         per-class products at any size; 4 and 5 as 1 and 3 with the per-class products in
         FP32 on the CUDA cores."""
         self._check(lib().exafmm_set_mixed_policy(self._h, int(m2l_fp32), int(p2p_fp32), min_level, max_dl))
+
+    def set_p2p_targets_per_lane(self, tpl: int):
+        """Mixed P2P: targets per lane, 0 by leaf size (two or three), or 2 / 3 for every leaf."""
+        self._check(lib().exafmm_set_p2p_targets_per_lane(self._h, int(tpl)))
 
     # ---- solve steps (examples/fmm.cxx:163-179) ----
     def set_sources(self, xyzq=None):
@@ -575,6 +584,24 @@ class Batch:
         if lib().exafmm_batch_set_mixed_policy(self._h, int(m2l_fp32), int(p2p_fp32), min_level, max_dl) != 0:
             raise FmmError("invalid mixed policy")
 
+    def set_p2p_candidates(self, candidates):
+        """P2P targets-per-lane settings the autotuner tries with every ncrit (default [0])."""
+        c = np.ascontiguousarray(candidates, dtype=np.int32)
+        if lib().exafmm_batch_set_p2p_candidates(self._h, _p(c), len(c)) != 0:
+            raise FmmError("invalid P2P candidates")
+
+    def config_table(self) -> dict:
+        """The tuned table: size class -> (ncrit, P2P targets per lane)."""
+        buf = np.zeros(3 * 64, dtype=np.int32)
+        k = lib().exafmm_batch_config_table(self._h, _p(buf), 64)
+        return {int(buf[3 * i]): (int(buf[3 * i + 1]), int(buf[3 * i + 2])) for i in range(k)}
+
+    def set_config_table(self, table: dict):
+        t = np.ascontiguousarray([v for c, (n, tp) in sorted(table.items()) for v in (c, n, tp)] or [0],
+                                 dtype=np.int32)
+        if lib().exafmm_batch_set_config_table(self._h, _p(t), len(table)) != 0:
+            raise FmmError("invalid config table")
+
     def set_ncrit_candidates(self, candidates):
         """The ncrit values the autotuner tries, in order (default 32, 64, 128)."""
         c = np.ascontiguousarray(candidates, dtype=np.int32)
@@ -593,6 +620,12 @@ class Batch:
         nc = np.zeros(64, dtype=np.int32)
         k = lib().exafmm_batch_buckets(self._h, _p(of), _p(nc), 64)
         return of[:count], nc[:max(0, k)]
+
+    def bucket_p2p(self) -> np.ndarray:
+        """Forest mode: each group's P2P targets per lane in the last call."""
+        t = np.zeros(64, dtype=np.int32)
+        k = lib().exafmm_batch_bucket_p2p(self._h, _p(t), 64)
+        return t[:max(0, k)]
 
     def close(self):
         if getattr(self, "_h", None):

@@ -795,6 +795,14 @@ int exafmm_set_mixed_policy(exafmm_ctx *ctx, int m2l_fp32, int p2p_fp32, int min
   });
 }
 
+int exafmm_set_p2p_targets_per_lane(exafmm_ctx *ctx, int tpl) {
+  return guarded(ctx, [&] {
+    if (tpl != 0 && tpl != 2 && tpl != 3) throw std::runtime_error("targets per lane: 0 (by leaf size), 2 or 3");
+    ctx->E.C.prm.p2p_tpl = tpl;
+    ctx->E.lists_ok = false;
+  });
+}
+
 int exafmm_set_bodies(exafmm_ctx *ctx, const double *xyzq, long long n) {
   return guarded(ctx, [&] {
     cudaSetDevice(ctx->E.C.device);

@@ -24,6 +24,7 @@ struct Params {
   int mixed_max_dl = 3;
   int mixed_gemm = 1;     // per-class products for frequent offset classes: 0 off, 1 where they pay, 2 always
   int mixed_gemm_tc = 1;  // ... on the tensor cores (bf16x3), else FP32 on the CUDA cores
+  int p2p_tpl = 0;        // mixed P2P targets per lane: 0 by leaf size (two or three), 2 or 3 for every leaf
 };
 
 // Level-ordered octree nodes plus the reference-layout cell table.

@@ -341,14 +341,15 @@ __device__ __forceinline__ bool three_per_lane(int n) {
 }
 
 // Work order: each cell's kind (0: a leaf of two targets per lane, 1: three,
-// 2: no P2P list) above its cost (its bodies times the bodies of its list,
+// 2: no P2P list; tpl 2 or 3 gives every leaf that kind, tpl 0 chooses by the
+// leaf's size) above its cost (its bodies times the bodies of its list,
 // capped), reversed so that an ascending sort puts the costliest leaf of
 // each kind first.  count[kind] receives the cells of each kind.
 constexpr int kCostBits = 22;
 constexpr unsigned kCostMax = (1u << kCostBits) - 1;
 
-__global__ void k_p2p_keys(const int *off, const int *src, long long ncells, const int4 *cell_b, unsigned *key,
-                           int *val, int *count) {
+__global__ void k_p2p_keys(const int *off, const int *src, long long ncells, const int4 *cell_b, int tpl,
+                           unsigned *key, int *val, int *count) {
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncells;
        c += (long long)gridDim.x * blockDim.x) {
     const int b = off[c], e = off[c + 1];
@@ -357,7 +358,7 @@ __global__ void k_p2p_keys(const int *off, const int *src, long long ncells, con
       const int nb = cell_b[c].y;
       unsigned long long s = 0;
       for (int q = b; q < e; q++) s += (unsigned)cell_b[src[q] & 0x3ffffff].y;
-      kind = three_per_lane(nb) ? 1u : 0u;
+      kind = (tpl == 0 ? three_per_lane(nb) : tpl == 3) ? 1u : 0u;
       cost = (unsigned)min((unsigned long long)kCostMax, s * (unsigned long long)nb);
     }
     key[c] = (kind << kCostBits) | (kCostMax - cost);
@@ -422,7 +423,8 @@ void p2p_mixed(Context &C, const FmmArgs &a, const float4 *x32, bool periodic, P
   EXA_CUDA(cudaMemsetAsync(w.next.p, 0, 2 * sizeof(unsigned long long), st));
   EXA_CUDA(cudaMemsetAsync(w.count.p, 0, 3 * sizeof(int), st));
   const int kg = (int)std::max<long long>(1, std::min<long long>((long long)kNumSMs * 8, (nc + 255) / 256));
-  k_p2p_keys<<<kg, 256, 0, st>>>(a.p2p_off, a.p2p_src, nc, a.cell_b, w.key.p, w.order.p, w.count.p);
+  k_p2p_keys<<<kg, 256, 0, st>>>(a.p2p_off, a.p2p_src, nc, a.cell_b, C.prm.p2p_tpl, w.key.p, w.order.p,
+                                 w.count.p);
   EXA_CHECK_LAUNCH();
   const bool alt = radix_sort_u32(w.key.p, w.order.p, w.key_alt.p, w.order_alt.p, nc, 0, kCostBits + 2, C.sort,
                                   C.err.p, st);

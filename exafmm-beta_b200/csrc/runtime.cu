@@ -130,7 +130,13 @@ struct SolveParams {
   int images = 0;
   double cycle = 6.283185307179586;
   int precision = EXAFMM_FP64;
+  int p2p_tpl = 0;  // exafmm_set_p2p_targets_per_lane
 };
+
+// A tuned configuration packed in one int: ncrit and the P2P targets per lane.
+inline int pack_config(int ncrit, int tpl) { return ncrit * 4 + (tpl == 2 ? 1 : tpl == 3 ? 2 : 0); }
+inline int config_ncrit(int cfg) { return cfg / 4; }
+inline int config_tpl(int cfg) { return cfg % 4 == 1 ? 2 : cfg % 4 == 2 ? 3 : 0; }
 
 // exafmm_set_mixed_policy's arguments, applied to every context a batch uses.
 struct MixedPolicy {
@@ -189,6 +195,7 @@ struct Slot {
         throw std::runtime_error(exafmm_create_error());
       }
       cur = p;
+      ctx_tpl = 0;
     } else if (p.P != cur.P || p.theta != cur.theta || p.ncrit != cur.ncrit || p.nspawn != cur.nspawn ||
                p.images != cur.images || p.cycle != cur.cycle) {
       check(exafmm_set_params(ctx, p.P, p.theta, p.ncrit, p.nspawn, p.images, p.cycle));
@@ -196,7 +203,12 @@ struct Slot {
     }
     if (pol && pol->set && p.precision == EXAFMM_MIXED)
       check(exafmm_set_mixed_policy(ctx, pol->m2l_fp32, pol->p2p_fp32, pol->min_level, pol->max_dl));
+    if (p.p2p_tpl != ctx_tpl) {
+      check(exafmm_set_p2p_targets_per_lane(ctx, p.p2p_tpl));
+      ctx_tpl = p.p2p_tpl;
+    }
   }
+  int ctx_tpl = 0;  // the context's P2P targets per lane
   void check(int rc) {
     if (rc != 0) throw std::runtime_error(exafmm_last_error(ctx));
   }
@@ -212,11 +224,20 @@ struct exafmm_batch {
   MixedPolicy policy;
   int forest_buckets = 0;       // 0: one context per system; k > 0: up to k forests by size
   std::vector<Slot> slots;
-  NcritTuner tuner{{32, 64, 128}};
+  // the autotuner's candidates: every ncrit with every P2P targets-per-lane
+  // setting, packed (pack_config); the table maps a size class to one of them
+  std::vector<int> ncrit_cands{32, 64, 128}, tpl_cands{0};
+  NcritTuner tuner{{pack_config(32, 0), pack_config(64, 0), pack_config(128, 0)}};
+  void retune() {
+    std::vector<int> c;
+    for (int t : tpl_cands)
+      for (int n : ncrit_cands) c.push_back(pack_config(n, t));
+    tuner.set_candidates(c);
+  }
   std::vector<double> last_ms;  // per system of the last call, device ms
   double last_elapsed_ms = 0;   // the last forest call, first copy in to last copy out, on the device
   std::vector<int> last_bucket; // bucket of each system in the last forest call
-  std::vector<int> last_bucket_ncrit;
+  std::vector<int> last_bucket_ncrit, last_bucket_tpl;
   cudaStream_t timing = nullptr;
   cudaEvent_t ev_start = nullptr, ev_end = nullptr;
   std::vector<cudaEvent_t> ev_done;
@@ -567,16 +588,54 @@ int exafmm_batch_ncrit_table(exafmm_batch *b, int *pairs, int cap) {
   const int k = (int)t.size() / 2;
   for (int i = 0; i < k && i < cap; i++) {
     pairs[2 * i] = t[2 * i];
-    pairs[2 * i + 1] = t[2 * i + 1];
+    pairs[2 * i + 1] = config_ncrit(t[2 * i + 1]);
   }
   return k;
 }
 
 int exafmm_batch_set_ncrit_table(exafmm_batch *b, const int *pairs, int k) {
   if (!b || k < 0 || (k > 0 && !pairs)) return 2;
-  for (int i = 0; i < k; i++)
+  std::vector<int> packed(2 * (size_t)k);
+  for (int i = 0; i < k; i++) {
     if (pairs[2 * i + 1] < 1 || pairs[2 * i + 1] > 1024) return 2;
-  b->tuner.load(pairs, k);
+    packed[2 * i] = pairs[2 * i];
+    packed[2 * i + 1] = pack_config(pairs[2 * i + 1], 0);
+  }
+  b->tuner.load(packed.data(), k);
+  return 0;
+}
+
+int exafmm_batch_config_table(exafmm_batch *b, int *triples, int cap) {
+  if (!b) return -1;
+  std::vector<int> t = b->tuner.table();
+  const int k = (int)t.size() / 2;
+  for (int i = 0; i < k && i < cap; i++) {
+    triples[3 * i] = t[2 * i];
+    triples[3 * i + 1] = config_ncrit(t[2 * i + 1]);
+    triples[3 * i + 2] = config_tpl(t[2 * i + 1]);
+  }
+  return k;
+}
+
+int exafmm_batch_set_config_table(exafmm_batch *b, const int *triples, int k) {
+  if (!b || k < 0 || (k > 0 && !triples)) return 2;
+  std::vector<int> packed(2 * (size_t)k);
+  for (int i = 0; i < k; i++) {
+    const int nc = triples[3 * i + 1], tpl = triples[3 * i + 2];
+    if (nc < 1 || nc > 1024 || (tpl != 0 && tpl != 2 && tpl != 3)) return 2;
+    packed[2 * i] = triples[3 * i];
+    packed[2 * i + 1] = pack_config(nc, tpl);
+  }
+  b->tuner.load(packed.data(), k);
+  return 0;
+}
+
+int exafmm_batch_set_p2p_candidates(exafmm_batch *b, const int *tpl, int k) {
+  if (!b || k < 1 || k > 3 || !tpl) return 2;
+  for (int i = 0; i < k; i++)
+    if (tpl[i] != 0 && tpl[i] != 2 && tpl[i] != 3) return 2;
+  b->tpl_cands.assign(tpl, tpl + k);
+  b->retune();
   return 0;
 }
 
@@ -619,6 +678,7 @@ int batch_solve_forest(exafmm_batch *b, int count, const long long *n, const dou
   }
   b->last_bucket = bucket;
   b->last_bucket_ncrit.assign(nb, b->prm.ncrit);
+  b->last_bucket_tpl.assign(nb, 0);
   if (cudaEventRecord(b->ev_start, b->timing) != cudaSuccess) {
     b->error = "cudaEventRecord";
     return 1;
@@ -643,15 +703,18 @@ int batch_solve_forest(exafmm_batch *b, int count, const long long *n, const dou
         out[j] = trg[mem[j]];
       }
       SolveParams p = b->prm;
-      p.ncrit = b->tuner.pick_class(key[k], b->prm.ncrit);
+      const int cfg = b->tuner.pick_class(key[k], pack_config(b->prm.ncrit, 0));
+      p.ncrit = config_ncrit(cfg);
+      p.p2p_tpl = config_tpl(cfg);
       b->last_bucket_ncrit[k] = p.ncrit;
+      b->last_bucket_tpl[k] = p.p2p_tpl;
       try {
         const double ms = b->slots[w].solve_forest(b->device, p, &b->policy, (int)mem.size(), nn.data(), in.data(),
                                                    out.data(), b->ev_start, b->ev_done[w]);
         used[w] = 1;
         for (size_t j = 0; j < mem.size(); j++)
           b->last_ms[mem[j]] = bodies[k] > 0 ? ms * (double)nn[j] / (double)bodies[k] : 0.0;
-        if (bodies[k] > 0) b->tuner.report_class(key[k], p.ncrit, ms / (double)bodies[k]);
+        if (bodies[k] > 0) b->tuner.report_class(key[k], cfg, ms / (double)bodies[k]);
       } catch (const std::exception &e) {
         std::lock_guard<std::mutex> lk(emu);
         if (!failed.exchange(true)) b->error = std::string("forest bucket ") + std::to_string(k) + ": " + e.what();
@@ -704,11 +767,13 @@ int exafmm_batch_solve(exafmm_batch *b, int count, const long long *n, const dou
       if (i >= count || failed.load()) return;
       const int k = order[i];
       SolveParams p = b->prm;
-      p.ncrit = b->tuner.pick(n[k], b->prm.ncrit);
+      const int cfg = b->tuner.pick(n[k], pack_config(b->prm.ncrit, 0));
+      p.ncrit = config_ncrit(cfg);
+      p.p2p_tpl = config_tpl(cfg);
       try {
         const double ms = b->slots[w].solve(b->device, p, xyzq[k], n[k], trg[k], &b->policy);
         b->last_ms[k] = ms;
-        b->tuner.report(n[k], p.ncrit, ms);
+        b->tuner.report(n[k], cfg, ms);
       } catch (const std::exception &e) {
         std::lock_guard<std::mutex> lk(emu);
         if (!failed.exchange(true)) b->error = std::string("system ") + std::to_string(k) + ": " + e.what();
@@ -751,7 +816,8 @@ int exafmm_batch_set_ncrit_candidates(exafmm_batch *b, const int *ncrit, int k) 
   if (!b || k < 1 || k > 16 || !ncrit) return 2;
   for (int i = 0; i < k; i++)
     if (ncrit[i] < 1 || ncrit[i] > 1024) return 2;
-  b->tuner.set_candidates(std::vector<int>(ncrit, ncrit + k));
+  b->ncrit_cands.assign(ncrit, ncrit + k);
+  b->retune();
   return 0;
 }
 
@@ -767,6 +833,14 @@ int exafmm_batch_buckets(exafmm_batch *b, int *bucket_of, int *bucket_ncrit, int
   if (bucket_of) std::copy(b->last_bucket.begin(), b->last_bucket.end(), bucket_of);
   if (bucket_ncrit)
     for (int i = 0; i < nb && i < cap; i++) bucket_ncrit[i] = b->last_bucket_ncrit[i];
+  return nb;
+}
+
+int exafmm_batch_bucket_p2p(exafmm_batch *b, int *bucket_tpl, int cap) {
+  if (!b) return -1;
+  const int nb = (int)b->last_bucket_tpl.size();
+  if (bucket_tpl)
+    for (int i = 0; i < nb && i < cap; i++) bucket_tpl[i] = b->last_bucket_tpl[i];
   return nb;
 }
 

@@ -66,6 +66,14 @@ int exafmm_set_params(exafmm_ctx *ctx, int P, double theta, int ncrit, int nspaw
  * counterpart in the reference (its precision is a compile-time switch,
  * EXAFMM_SINGLE). */
 int exafmm_set_mixed_policy(exafmm_ctx *ctx, int m2l_fp32, int p2p_fp32, int min_level, int max_dl);
+/* Mixed form: how many targets each lane of the FP32 P2P holds (the lanes of
+ * a warp split into groups of 4, 8, 16 or 32 by leaf size; each lane takes
+ * tpl targets of its group's slice): 0 (default) chooses 2 or 3 per leaf by
+ * which fills the slots better, 2 or 3 use that for every leaf.  A tuning
+ * parameter (the batch autotuner tries it); results stay within the precision
+ * bar either way, though their bits differ.  No counterpart in the reference
+ * (its P2P is a SIMD loop over targets, kernels/laplace.h:150-235). */
+int exafmm_set_p2p_targets_per_lane(exafmm_ctx *ctx, int tpl);
 
 /* Separate source bodies (examples/fmm.cxx -j IneJ, :37-47, :61-73): the next
  * solves evaluate the field of these n sources (n x 4: x, y, z, q, caller
@@ -304,6 +312,17 @@ int exafmm_batch_set_mixed_policy(exafmm_batch *b, int m2l_fp32, int p2p_fp32, i
 /* The autotuner's ncrit candidates (k of them, tried in this order; default
  * 32, 64, 128); setting them restarts the tuning of every class. */
 int exafmm_batch_set_ncrit_candidates(exafmm_batch *b, const int *ncrit, int k);
+/* The autotuner's P2P targets-per-lane candidates (exafmm_set_p2p_targets_per_lane:
+ * 0, 2, 3; default 0 alone): it tries every ncrit candidate with each of them
+ * (one per call), and keeps the fastest pair per class. */
+int exafmm_batch_set_p2p_candidates(exafmm_batch *b, const int *tpl, int k);
+/* The tuned table as (size class, ncrit, targets per lane) triples; returns
+ * the number of classes.  The _set form loads such a table and freezes it. */
+int exafmm_batch_config_table(exafmm_batch *b, int *triples, int cap);
+int exafmm_batch_set_config_table(exafmm_batch *b, const int *triples, int k);
+/* Forest mode: each group's targets per lane in the last call (up to cap);
+ * returns the number of groups. */
+int exafmm_batch_bucket_p2p(exafmm_batch *b, int *bucket_tpl, int cap);
 /* Forest mode: device time (ms) of the last call, from an event every worker
  * stream waits on before its first copy in to the last group's copy out. */
 int exafmm_batch_elapsed(exafmm_batch *b, double *ms);

@@ -78,3 +78,27 @@ def test_tile_m2l_matches_pair_by_pair(ex, datasets, P):
         print(f"P={P} {gen}: " + " ".join(f"{k} {v[0]:.2e}/{v[1]:.2e}" for k, v in errs.items()))
         for i in range(2):
             assert errs["tc-plain"][i] < 10 * errs["cc-plain"][i] + 1e-8
+
+
+@pytest.mark.parametrize("dist,n", [("plummer", 60000), ("cube", 40000)])
+def test_p2p_targets_per_lane_settings_agree(ex, datasets, dist, n):
+    """The mixed P2P's targets per lane (by leaf size, two, three for every leaf)
+    is a tuning parameter: each setting stays within the precision bar of the
+    plain method on the same tree, and of the others."""
+    x = getattr(datasets, dist)(n, seed=77)
+    kw = dict(P=8, theta=0.4, ncrit=64)
+    plain, _ = _run(ex, x, ex.FP64, **kw)
+    outs = {}
+    for tpl in (0, 2, 3):
+        f = ex.Fmm(precision=ex.MIXED, **kw)
+        f.set_p2p_targets_per_lane(tpl)
+        f.set_bodies(x)
+        f.solve()
+        outs[tpl] = f.results()
+        f.close()
+        assert rel_l2(outs[tpl][:, 0], plain[:, 0]) < PRECISION_TOL
+        assert rel_l2(outs[tpl][:, 1:], plain[:, 1:]) < PRECISION_TOL
+    assert rel_l2(outs[2][:, 1:], outs[3][:, 1:]) < PRECISION_TOL
+    with pytest.raises(ex.FmmError):
+        f = ex.Fmm(precision=ex.MIXED, **kw)
+        f.set_p2p_targets_per_lane(4)

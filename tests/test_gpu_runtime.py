@@ -219,3 +219,39 @@ def test_server_groups_small_queued_requests_into_one_forest(ex, datasets):
     assert all(np.array_equal(s.wait(t)[0], o) for t, o in zip(tickets, outs[:4]))
     assert s.stats()["grouped"] == g0
     s.close()
+
+
+def test_forest_batch_tunes_ncrit_and_targets_per_lane(ex, datasets):
+    """The autotuner tries every ncrit with every P2P targets-per-lane setting,
+    one pair per call, and keeps the fastest per group; each system then has the
+    bits of its solo solve with its group's pair, and a loaded table reproduces
+    them."""
+    xs = _systems(datasets, 10, 2000, 40000, 900)
+    kw = dict(P=8, theta=0.4, precision=ex.MIXED)
+    b = ex.Batch(ncrit=64, workers=2, forest=2, **kw)
+    b.set_ncrit_candidates([32, 64])
+    b.set_p2p_candidates([0, 2, 3])
+    b.autotune(True)
+    for _ in range(6):
+        b.solve(xs)
+    b.autotune(False)
+    table = b.config_table()
+    group, ncrit = b.buckets(len(xs))
+    assert len(table) == group.max() + 1
+    assert all(nc in (32, 64) and tp in (0, 2, 3) for nc, tp in table.values())
+    outs = b.solve(xs)
+    group, ncrit = b.buckets(len(xs))
+    tpl = b.bucket_p2p()
+    for x, o, gi in zip(xs, outs, group):
+        f = ex.Fmm(ncrit=int(ncrit[gi]), **kw)
+        f.set_p2p_targets_per_lane(int(tpl[gi]))
+        f.set_bodies(x)
+        f.solve()
+        assert np.array_equal(o, f.results())
+        f.close()
+    b2 = ex.Batch(ncrit=64, workers=2, forest=2, **kw)
+    b2.set_config_table(table)
+    assert b2.config_table() == table
+    assert all(np.array_equal(a, c) for a, c in zip(outs, b2.solve(xs)))
+    b2.close()
+    b.close()
