@@ -247,7 +247,7 @@ class Fmm:
     # ---- solve steps (examples/fmm.cxx:163-179) ----
     def set_sources(self, xyzq=None):
         """Separate source bodies (examples/fmm.cxx -j IneJ): later solves evaluate the field
-        of these sources at this context's bodies (free space, FP64).  None: sources are
+        of these sources at this context's bodies (free space; FP64 or mixed).  None: sources are
         the bodies again."""
         if xyzq is None:
             self._check(lib().exafmm_set_sources(self._h, None, 0))

@@ -96,6 +96,7 @@ struct Engine {
   DBuf<unsigned char> Ms;  // scaled multipoles for the unrolled M2L (FP32 or FP64)
   DBuf<unsigned char> Ms64;  // FP64 scaled multipoles for the FP64 part of the mixed form
   DBuf<float4> x32;        // bodies as two-float pairs relative to the root center (mixed P2P)
+  DBuf<float4> x32j;       // the same for separate source bodies
   M2LGemmBufs gemm;         // class-grouped tile M2L (mixed form)
   DBuf<double2> lat;        // periodic lattice: supercell multipoles and warp partials
   DBuf<double> dip;         // dipole reduction scratch and result
@@ -351,9 +352,12 @@ struct Engine {
     up_ok = true;
   }
 
-  // Traversal::traverse(cells, jcells) and the FP64 operators across the two trees.
+  // Traversal::traverse(cells, jcells) and the operators across the two trees:
+  // FP64, or in the mixed form the FP32 pair-by-pair M2L for the pairs of the
+  // mixed policy (the source tree's scaled multipoles), FP64 for the rest, and
+  // the FP32 P2P over the source tree's bodies (two-float offsets from the
+  // common root center: both trees are built on the same bounds).
   void traverse_separate_sources() {
-    if (C.prm.precision != kFP64) throw std::runtime_error("separate sources: FP64 precision only");
     if (C.prm.images != 0) throw std::runtime_error("separate sources: free space only (images = 0)");
     const long long nc = C.tree.ncells;
     const int NT = tri(C.prm.P);
@@ -364,14 +368,33 @@ struct Engine {
     EXA_CUDA(cudaMemsetAsync(L.p, 0, nc * NT * sizeof(double2), C.stream));
     FmmArgs a = args();
     a.src_cell_b = jsrc->C.tree.cell_b.p;
+    a.src_cell_pl = jsrc->C.tree.cell_pl.p;
     a.src_cell_x = jsrc->C.tree.cell_x.p;
     a.src_xt = jsrc->C.tree.xyzq_tree.p;
     a.src_M64 = jsrc->M.p;
-    m2l_fp64(a);
+    const bool mixed = C.prm.precision == kMixed;
+    if (mixed && C.prm.mixed_m2l && m2l_fast_supported(C.prm.P, true)) {
+      const long long ncj = jsrc->C.tree.ncells;
+      Ms.ensure(std::max<long long>(1, ncj) * NT * sizeof(float2));
+      scale_multipoles(C.prm.P, jsrc->M.p, jsrc->C.tree.cell_x.p, ncj, true, Ms.p, C.stream);
+      m2l_fast(a, true, Ms.p, C.prm.mixed_min_level, C.prm.mixed_max_dl);
+      m2l_fp64(a, C.prm.mixed_min_level, C.prm.mixed_max_dl);  // the pairs outside the policy
+    } else {
+      m2l_fp64(a);
+    }
     EXA_CUDA(cudaEventRecord(tm.lat[0], C.stream));
     EXA_CUDA(cudaEventRecord(tm.lat[1], C.stream));
     EXA_CUDA(cudaEventRecord(tm.ev[5], C.stream));
-    p2p_fp64(a);
+    if (mixed && C.prm.mixed_p2p) {
+      const long long ns = jsrc->C.tree.n;
+      x32.ensure(2 * C.tree.n);
+      x32j.ensure(std::max<long long>(1, 2 * ns));
+      rel_bodies32(a, x32.p);
+      rel_bodies32(a, jsrc->C.tree.xyzq_tree.p, ns, x32j.p);
+      p2p_mixed(C, a, x32.p, false, p2pw, x32j.p);
+    } else {
+      p2p_fp64(a);
+    }
   }
 
   void traverse_and_evaluate() {

@@ -24,6 +24,7 @@ struct FmmArgs {
   // separate source bodies (their own tree): the source side of M2L and P2P
   // (null: the sources are the targets)
   const int4 *src_cell_b = nullptr;
+  const int2 *src_cell_pl = nullptr;
   const double4 *src_cell_x = nullptr;
   const double4 *src_xt = nullptr;
   const double2 *src_M64 = nullptr;
@@ -51,8 +52,11 @@ constexpr int kMixedMaxDl = 3;
 
 // Register-resident unrolled M2L (m2l.cu) for the orders it is built for.
 bool m2l_fast_supported(int P, bool mixed);
-// Ms = A_n^m M_n^m / R^n per cell, FP32 (mixed) or FP64.
+// Ms = A_n^m M_n^m / R^n per cell, FP32 (mixed) or FP64: of the cells of a,
+// or of any cell table (a separate source tree's).
 void scale_multipoles(const FmmArgs &a, bool mixed, void *Ms);
+void scale_multipoles(int P, const double2 *M, const double4 *cell_x, long long ncells, bool mixed, void *Ms,
+                      cudaStream_t st);
 // In mixed mode only pairs with target level >= min_level and |level difference|
 // <= max_dl are taken (FP64 takes the rest, compacted by m2l_complement).
 // taken: pairs another kernel evaluates (skipped here), or null.
@@ -106,6 +110,8 @@ void dipole_correction_fp64(const double4 *xt, double4 *trg, long long n, double
 // Mixed-precision P2P (p2p32.cu): bodies as two-float pairs relative to the
 // root center; periodic selects the form that tests every pair for r = 0.
 void rel_bodies32(const FmmArgs &a, float4 *x32);
+// The same for other bodies (a separate source tree's) about the root center of a.
+void rel_bodies32(const FmmArgs &a, const double4 *xt, long long n, float4 *x32);
 // Scratch of the mixed P2P: the persistent kernels' work counters and their
 // work order (target leaves by kind, longest first).
 struct P2PWork {
@@ -114,7 +120,9 @@ struct P2PWork {
   DBuf<int> order, order_alt;      // cells in work order
   DBuf<int> count;                 // [3] leaves of each kind: two targets per lane, three, no P2P list
 };
-void p2p_mixed(Context &C, const FmmArgs &a, const float4 *x32, bool periodic, P2PWork &w);
+// x32j (null: x32) holds the source bodies, whose cells are a.src_cell_b when set.
+void p2p_mixed(Context &C, const FmmArgs &a, const float4 *x32, bool periodic, P2PWork &w,
+               const float4 *x32j = nullptr);
 
 // Interaction lists of the dual tree traversal (traverse.cu).
 struct ListBufs {

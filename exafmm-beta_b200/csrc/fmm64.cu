@@ -228,7 +228,7 @@ __device__ __forceinline__ void m2l_accumulate(const DevTables &t, const int (&o
 template <int MAXO>
 __global__ void k_m2l(DevTables t, const int *off, const int *src, long long ncells, const double4 *cell_x,
                       const double4 *cell_xj, const double2 *M, double2 *L, double cycle, const int2 *cell_pl,
-                      int skip_min_level, int skip_max_dl) {
+                      const int2 *cell_plj, int skip_min_level, int skip_max_dl) {
   extern __shared__ double2 sh[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int P = t.P, NT = t.nterm, NS = tri(2 * P - 1);
@@ -254,7 +254,7 @@ __global__ void k_m2l(DevTables t, const int *off, const int *src, long long nce
       const int cj = packed & 0x3ffffff, img = packed >> 26;
       if (cell_pl) {
         // pairs the mixed-precision kernel takes are skipped here
-        const int dl = lt - cell_pl[cj].y;
+        const int dl = lt - cell_plj[cj].y;
         if (lt >= skip_min_level && dl <= skip_max_dl && dl >= -skip_max_dl) continue;
       }
       double sx, sy, sz;
@@ -674,11 +674,12 @@ void m2l_fp64(const FmmArgs &a, int skip_min_level, int skip_max_dl) {
   const DevTables &t = device_tables(a.P);
   size_t smem = kWarpsPerBlock * (t.nterm + tri(2 * a.P - 1)) * sizeof(double2);
   const int2 *pl = skip_min_level >= 0 ? a.cell_pl : nullptr;
+  const int2 *plj = skip_min_level >= 0 ? (a.src_cell_pl ? a.src_cell_pl : a.cell_pl) : nullptr;
   EXA_MAXO_SWITCH(maxo_for(a.P), {
     set_smem(k_m2l<MO>, smem);
     k_m2l<MO><<<blocks_for(a.ncells), 32 * kWarpsPerBlock, smem, a.stream>>>(
         t, a.m2l_off, a.m2l_src, a.ncells, a.cell_x, a.src_cell_x ? a.src_cell_x : a.cell_x,
-        a.src_M64 ? a.src_M64 : a.M64, a.L64, a.cycle, pl, skip_min_level, skip_max_dl);
+        a.src_M64 ? a.src_M64 : a.M64, a.L64, a.cycle, pl, plj, skip_min_level, skip_max_dl);
   });
   EXA_CHECK_LAUNCH();
 }

@@ -93,6 +93,8 @@ struct M2LCtx {
   long long ncells;
   const double4 *cell_x;
   const int2 *cell_pl;
+  const double4 *cell_xj;  // source cells: the same table, or a separate source tree's
+  const int2 *cell_plj;
   const void *Ms;
   double cycle;
   int mode;  // 0: every pair; 1: mixed-regular pairs only
@@ -142,14 +144,14 @@ k_m2l_part(M2LCtx g, DevTables t, double2 *L) {
         const int packed = g.src[q];
         cj = packed & 0x3ffffff;
         img = packed >> 26;
-        ls = g.cell_pl[cj].y;
+        ls = g.cell_plj[cj].y;
         if (g.mode == 1 && !mixed_regular(g, lt, ls)) live = false;
         if (g.taken && g.taken[q]) live = false;
       }
       if (!__any_sync(0xffffffffu, live)) continue;  // warp-uniform: a batch with nothing to add
       T x = T(1), y = T(0), z = T(0);
       if (live) {
-        const double4 Xs = g.cell_x[cj];
+        const double4 Xs = g.cell_xj[cj];
         const double sx = (double)(img / 9 - 1) * g.cycle, sy = (double)((img / 3) % 3 - 1) * g.cycle,
                      sz = (double)(img % 3 - 1) * g.cycle;
         x = (T)((Xt.x - Xs.x - sx) * inv_rt);
@@ -273,13 +275,18 @@ bool m2l_fast_supported(int P, bool mixed) {
 }
 
 void scale_multipoles(const FmmArgs &a, bool mixed, void *Ms) {
-  const DevTables &t = device_tables(a.P);
-  const long long total = a.ncells * t.nterm;
+  scale_multipoles(a.P, a.M64, a.cell_x, a.ncells, mixed, Ms, a.stream);
+}
+
+void scale_multipoles(int P, const double2 *M, const double4 *cell_x, long long ncells, bool mixed, void *Ms,
+                      cudaStream_t st) {
+  const DevTables &t = device_tables(P);
+  const long long total = ncells * t.nterm;
   int grid = (int)((total + 255) / 256);
   if (grid > kNumSMs * 16) grid = kNumSMs * 16;
   if (grid < 1) grid = 1;
-  if (mixed) k_scale_M<float><<<grid, 256, 0, a.stream>>>(t, a.M64, a.cell_x, a.ncells, (Cx<float> *)Ms);
-  else k_scale_M<double><<<grid, 256, 0, a.stream>>>(t, a.M64, a.cell_x, a.ncells, (Cx<double> *)Ms);
+  if (mixed) k_scale_M<float><<<grid, 256, 0, st>>>(t, M, cell_x, ncells, (Cx<float> *)Ms);
+  else k_scale_M<double><<<grid, 256, 0, st>>>(t, M, cell_x, ncells, (Cx<double> *)Ms);
   EXA_CHECK_LAUNCH();
 }
 
@@ -293,6 +300,8 @@ bool m2l_fast(const FmmArgs &a, bool mixed, const void *Ms, int min_level, int m
   g.ncells = a.ncells;
   g.cell_x = a.cell_x;
   g.cell_pl = a.cell_pl;
+  g.cell_xj = a.src_cell_x ? a.src_cell_x : a.cell_x;
+  g.cell_plj = a.src_cell_pl ? a.src_cell_pl : a.cell_pl;
   g.Ms = Ms;
   g.cycle = a.cycle;
   g.mode = mixed ? 1 : 0;

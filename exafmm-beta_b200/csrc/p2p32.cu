@@ -286,8 +286,8 @@ __device__ __forceinline__ void p2p_stream(Stage &sm, const int *src, const int4
 }
 
 template <int S, int TPL, bool PERIODIC>
-__device__ __forceinline__ void p2p_leaf(Stage &sm, int4 cb, int b, int e, const int *src, const int4 *cell_b,
-                                         const float4 *x32, double4 *trg, double cycle) {
+__device__ __forceinline__ void p2p_leaf(Stage &sm, int4 cb, int b, int e, const int *src, const int4 *cell_bj,
+                                         const float4 *x32, const float4 *x32j, double4 *trg, double cycle) {
   const int lane = threadIdx.x & 31, g = lane / S, j = lane % S;
   for (int tb = 0; tb < cb.y; tb += S * TPL) {
     Targets<TPL> T;
@@ -307,7 +307,7 @@ __device__ __forceinline__ void p2p_leaf(Stage &sm, int4 cb, int b, int e, const
       T.t[u][5] = pk2(l.z, l.z);
     }
     Sums<TPL> acc;
-    p2p_stream<S, TPL, PERIODIC>(sm, src, cell_b, x32, cycle, b, e, T, acc);
+    p2p_stream<S, TPL, PERIODIC>(sm, src, cell_bj, x32j, cycle, b, e, T, acc);
     // combine the groups (lanes j, j + S, j + 2S, ... hold the same targets) in FP64
 #pragma unroll
     for (int u = 0; u < TPL; u++) {
@@ -348,8 +348,8 @@ __device__ __forceinline__ bool three_per_lane(int n) {
 constexpr int kCostBits = 22;
 constexpr unsigned kCostMax = (1u << kCostBits) - 1;
 
-__global__ void k_p2p_keys(const int *off, const int *src, long long ncells, const int4 *cell_b, int tpl,
-                           unsigned *key, int *val, int *count) {
+__global__ void k_p2p_keys(const int *off, const int *src, long long ncells, const int4 *cell_b,
+                           const int4 *cell_bj, int tpl, unsigned *key, int *val, int *count) {
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncells;
        c += (long long)gridDim.x * blockDim.x) {
     const int b = off[c], e = off[c + 1];
@@ -357,7 +357,7 @@ __global__ void k_p2p_keys(const int *off, const int *src, long long ncells, con
     if (b < e) {
       const int nb = cell_b[c].y;
       unsigned long long s = 0;
-      for (int q = b; q < e; q++) s += (unsigned)cell_b[src[q] & 0x3ffffff].y;
+      for (int q = b; q < e; q++) s += (unsigned)cell_bj[src[q] & 0x3ffffff].y;
       kind = (tpl == 0 ? three_per_lane(nb) : tpl == 3) ? 1u : 0u;
       cost = (unsigned)min((unsigned long long)kCostMax, s * (unsigned long long)nb);
     }
@@ -374,8 +374,9 @@ __global__ void k_p2p_keys(const int *off, const int *src, long long ncells, con
 // by which warp it is evaluated.
 template <bool PERIODIC, int TPL>
 __global__ void __launch_bounds__(32, TPL == 2 ? 16 : 12)
-k_p2p32(const int *off, const int *src, const int *order, const int *count, const int4 *cell_b, const float4 *x32,
-        double4 *trg, double cycle, unsigned long long *next) {
+k_p2p32(const int *off, const int *src, const int *order, const int *count, const int4 *cell_b,
+        const int4 *cell_bj, const float4 *x32, const float4 *x32j, double4 *trg, double cycle,
+        unsigned long long *next) {
   __shared__ Stage sm;
   const long long items = count[TPL == 2 ? 0 : 1];
   const int *mine = order + (TPL == 2 ? 0 : count[0]);
@@ -388,29 +389,33 @@ k_p2p32(const int *off, const int *src, const int *order, const int *count, cons
     const int b = off[c], e = off[c + 1];
     const int4 cb = cell_b[c];
     if (cb.y <= 4 * TPL)
-      p2p_leaf<4, TPL, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
+      p2p_leaf<4, TPL, PERIODIC>(sm, cb, b, e, src, cell_bj, x32, x32j, trg, cycle);
     else if (cb.y <= 8 * TPL)
-      p2p_leaf<8, TPL, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
+      p2p_leaf<8, TPL, PERIODIC>(sm, cb, b, e, src, cell_bj, x32, x32j, trg, cycle);
     else if (cb.y <= 16 * TPL)
-      p2p_leaf<16, TPL, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
+      p2p_leaf<16, TPL, PERIODIC>(sm, cb, b, e, src, cell_bj, x32, x32j, trg, cycle);
     else
-      p2p_leaf<32, TPL, PERIODIC>(sm, cb, b, e, src, cell_b, x32, trg, cycle);
+      p2p_leaf<32, TPL, PERIODIC>(sm, cb, b, e, src, cell_bj, x32, x32j, trg, cycle);
     __syncwarp();  // the stage buffer is free before the next cell's first fill
   }
 }
 
 }  // namespace
 
-void rel_bodies32(const FmmArgs &a, float4 *x32) {
-  if (a.n <= 0) return;
-  long long g = (a.n + 255) / 256;
+void rel_bodies32(const FmmArgs &a, float4 *x32) { rel_bodies32(a, a.xt, a.n, x32); }
+
+void rel_bodies32(const FmmArgs &a, const double4 *xt, long long n, float4 *x32) {
+  if (n <= 0) return;
+  long long g = (n + 255) / 256;
   if (g > kNumSMs * 16) g = kNumSMs * 16;
-  if (a.nsys) k_abs32_forest<<<(int)g, 256, 0, a.stream>>>(a.xt, a.n, a.sys_off, a.nsys, a.sys_box, x32);
-  else k_abs32<<<(int)g, 256, 0, a.stream>>>(a.xt, a.n, a.cell_x, x32);
+  if (a.nsys) k_abs32_forest<<<(int)g, 256, 0, a.stream>>>(xt, n, a.sys_off, a.nsys, a.sys_box, x32);
+  else k_abs32<<<(int)g, 256, 0, a.stream>>>(xt, n, a.cell_x, x32);
   EXA_CHECK_LAUNCH();
 }
 
-void p2p_mixed(Context &C, const FmmArgs &a, const float4 *x32, bool periodic, P2PWork &w) {
+void p2p_mixed(Context &C, const FmmArgs &a, const float4 *x32, bool periodic, P2PWork &w, const float4 *x32j) {
+  const int4 *cell_bj = a.src_cell_b ? a.src_cell_b : a.cell_b;
+  if (!x32j) x32j = x32;
   const long long nc = a.ncells;
   if (nc <= 0) return;
   cudaStream_t st = a.stream;
@@ -423,7 +428,7 @@ void p2p_mixed(Context &C, const FmmArgs &a, const float4 *x32, bool periodic, P
   EXA_CUDA(cudaMemsetAsync(w.next.p, 0, 2 * sizeof(unsigned long long), st));
   EXA_CUDA(cudaMemsetAsync(w.count.p, 0, 3 * sizeof(int), st));
   const int kg = (int)std::max<long long>(1, std::min<long long>((long long)kNumSMs * 8, (nc + 255) / 256));
-  k_p2p_keys<<<kg, 256, 0, st>>>(a.p2p_off, a.p2p_src, nc, a.cell_b, C.prm.p2p_tpl, w.key.p, w.order.p,
+  k_p2p_keys<<<kg, 256, 0, st>>>(a.p2p_off, a.p2p_src, nc, a.cell_b, cell_bj, C.prm.p2p_tpl, w.key.p, w.order.p,
                                  w.count.p);
   EXA_CHECK_LAUNCH();
   const bool alt = radix_sort_u32(w.key.p, w.order.p, w.key_alt.p, w.order_alt.p, nc, 0, kCostBits + 2, C.sort,
@@ -432,17 +437,17 @@ void p2p_mixed(Context &C, const FmmArgs &a, const float4 *x32, bool periodic, P
   const unsigned g2 = (unsigned)std::min<long long>(nc, (long long)kNumSMs * 16);
   const unsigned g3 = (unsigned)std::min<long long>(nc, (long long)kNumSMs * 12);
   if (periodic) {
-    k_p2p32<true, 2><<<g2, 32, 0, st>>>(a.p2p_off, a.p2p_src, order, w.count.p, a.cell_b, x32, a.trg64, a.cycle,
-                                        w.next.p);
+    k_p2p32<true, 2><<<g2, 32, 0, st>>>(a.p2p_off, a.p2p_src, order, w.count.p, a.cell_b, cell_bj, x32, x32j,
+                                        a.trg64, a.cycle, w.next.p);
     EXA_CHECK_LAUNCH();
-    k_p2p32<true, 3><<<g3, 32, 0, st>>>(a.p2p_off, a.p2p_src, order, w.count.p, a.cell_b, x32, a.trg64, a.cycle,
-                                        w.next.p + 1);
+    k_p2p32<true, 3><<<g3, 32, 0, st>>>(a.p2p_off, a.p2p_src, order, w.count.p, a.cell_b, cell_bj, x32, x32j,
+                                        a.trg64, a.cycle, w.next.p + 1);
   } else {
-    k_p2p32<false, 2><<<g2, 32, 0, st>>>(a.p2p_off, a.p2p_src, order, w.count.p, a.cell_b, x32, a.trg64, a.cycle,
-                                         w.next.p);
+    k_p2p32<false, 2><<<g2, 32, 0, st>>>(a.p2p_off, a.p2p_src, order, w.count.p, a.cell_b, cell_bj, x32, x32j,
+                                         a.trg64, a.cycle, w.next.p);
     EXA_CHECK_LAUNCH();
-    k_p2p32<false, 3><<<g3, 32, 0, st>>>(a.p2p_off, a.p2p_src, order, w.count.p, a.cell_b, x32, a.trg64, a.cycle,
-                                         w.next.p + 1);
+    k_p2p32<false, 3><<<g3, 32, 0, st>>>(a.p2p_off, a.p2p_src, order, w.count.p, a.cell_b, cell_bj, x32, x32j,
+                                         a.trg64, a.cycle, w.next.p + 1);
   }
   EXA_CHECK_LAUNCH();
 }

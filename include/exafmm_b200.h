@@ -80,8 +80,9 @@ int exafmm_set_p2p_targets_per_lane(exafmm_ctx *ctx, int tpl);
  * order) at the context's bodies.  As there, the bounds are the targets'
  * extended by the sources (BoundBox::getBounds(jbodies, bounds)), each set gets
  * a tree on those bounds and its upward pass, and the traversal runs target
- * cells against source cells.  Free space, FP64 precision.  xyzq == NULL
- * returns to sources == targets. */
+ * cells against source cells.  Free space; FP64, or the mixed form (FP32 P2P
+ * and pair-by-pair FP32 M2L across the two trees, FP64 at the root levels).
+ * xyzq == NULL returns to sources == targets. */
 int exafmm_set_sources(exafmm_ctx *ctx, const double *xyzq, long long n);
 /* The source tree of the last build: cell count, cell table (as
  * exafmm_get_cells) and the sources' tree-order permutation; any output may be NULL. */

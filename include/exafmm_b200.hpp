@@ -25,7 +25,7 @@
  *    of a body's potential and gradient to Body::TRG at once (the reference
  *    adds P2P during traverse and L2P in downwardPass);
  *  - a second buildTree on other bodies makes them the source tree of the
- *    next traverse (examples/fmm.cxx -j: cells, jcells), in FP64;
+ *    next traverse (examples/fmm.cxx -j: cells, jcells), in the context's precision;
  *  - the periodic solve needs cycle[0] == cycle[1] == cycle[2];
  *  - Kernel's eps2 must be 0 and wavek is not used (Laplace);
  *  - num_threads sizes nothing (the work runs on the GPU); logger keeps

@@ -69,17 +69,41 @@ def test_separate_sources_against_direct_and_reset(ex, datasets):
     g.close()
 
 
-def test_separate_sources_need_fp64_free_space(ex, datasets):
+def test_separate_sources_need_free_space(ex, datasets):
     x = datasets.cube(500, seed=1)
-    f = ex.Fmm(P=6, precision=ex.MIXED)
-    f.set_bodies(x)
-    f.set_sources(x[:100])
-    with pytest.raises(ex.FmmError, match="FP64"):
-        f.solve()
-    f.close()
     f = ex.Fmm(P=6, images=1)
     f.set_bodies(x)
     f.set_sources(x[:100])
     with pytest.raises(ex.FmmError, match="free space"):
         f.solve()
     f.close()
+
+
+@pytest.mark.parametrize("path", inej_golden_cases(), ids=lambda p: os.path.basename(p)[:-4])
+def test_separate_sources_mixed_form(ex, datasets, path):
+    """The mixed form across two trees (FP32 P2P over the source tree's bodies,
+    pair-by-pair FP32 M2L from its multipoles, FP64 at the root levels): the same
+    trees and lists as the FP64 solve, results within the precision bar of it and
+    of the reference's, on the reference fixtures and on a larger pair of sets."""
+    g = load_golden(path)
+    P, theta, ncrit, nspawn = g["params"]
+    kw = dict(P=int(P), theta=float(theta), ncrit=int(ncrit), nspawn=int(nspawn))
+    cases = [(g["xyzq"], g["jxyzq"], g["trg"])]
+    x = datasets.cube(40000, seed=12)
+    jx = datasets.plummer(50000, seed=13)
+    x[:, 0] = (x[:, 0] + np.pi) * 0.5   # examples/fmm.cxx's -j shifts
+    jx[:, 0] = (jx[:, 0] - np.pi) * 0.5
+    cases.append((x, jx, None))
+    for xi, xj, ref in cases:
+        out = {}
+        for prec in (ex.FP64, ex.MIXED):
+            f = ex.Fmm(precision=prec, **kw)
+            f.set_bodies(xi)
+            f.set_sources(xj)
+            f.solve()
+            out[prec] = (f.results(), f.lists())
+            f.close()
+        (plain, (m2l64, p2p64)), (mixed, (m2l32, p2p32)) = out[ex.FP64], out[ex.MIXED]
+        assert np.array_equal(m2l64, m2l32) and np.array_equal(p2p64, p2p32)
+        for a, b in ((mixed, plain),) + (((mixed, ref),) if ref is not None else ()):
+            assert rel_l2(a[:, 0], b[:, 0]) < 1e-6 and rel_l2(a[:, 1:], b[:, 1:]) < 1e-6
