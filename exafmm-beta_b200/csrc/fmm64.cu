@@ -9,7 +9,6 @@ namespace exafmm_b200 {
 namespace {
 
 constexpr int kWarpsPerBlock = 4;
-constexpr int kM2MBatchedMaxP = 12;  // 16 NTERM complex values per warp fit a 4-warp block's shared memory
 
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
@@ -194,53 +193,6 @@ __global__ void k_m2m(DevTables t, const long long *lvl, int level, const int *n
       const int o = lane + 32 * u;
       if (o < NT) M[(long long)c * NT + o] = acc[u];
     }
-  }
-}
-
-// The same with the parent's children taken together: the lanes first form
-// every child's regular harmonics (a work item per child and column) and
-// stage every child's multipoles, then each lane adds the children's
-// contributions to its coefficients in child order, so the sums are the same
-// as the child-by-child kernel's with one warp barrier per parent instead of
-// two per child.  Shared memory: 16 NTERM complex values per warp.
-template <int MAXO>
-__global__ void k_m2m_batched(DevTables t, const long long *lvl, int level, const int *nd_cell, const int4 *cell_b,
-                              const double4 *cell_x, double2 *M) {
-  extern __shared__ double2 sh[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int P = t.P, NT = t.nterm;
-  double2 *Y = sh + warp * 16 * NT;  // child i's harmonics at Y + i NT
-  double2 *Mc = Y + 8 * NT;          // child i's multipoles at Mc + i NT
-  const long long cnt = lvl[level], start = lvl[kMaxLevels + 1 + level];
-  int oj[MAXO], ok[MAXO];
-#pragma unroll
-  for (int u = 0; u < MAXO; u++) {
-    const int o = lane + 32 * u;
-    if (o < NT) tri_decode(o, oj[u], ok[u]);
-    else oj[u] = ok[u] = -1;
-  }
-  for (long long i = (long long)blockIdx.x * kWarpsPerBlock + warp; i < cnt; i += (long long)gridDim.x * kWarpsPerBlock) {
-    const int c = nd_cell[start + i];
-    const int4 cb = cell_b[c];
-    if (cb.w == 0) continue;
-    const double4 Xp = cell_x[c];
-    for (int w = lane; w < cb.w * P; w += 32) {
-      const int ch = w / P, m = w - ch * P;
-      const double4 Xc = cell_x[cb.z + ch];
-      regular_column(t, m, P, Xp.x - Xc.x, Xp.y - Xc.y, Xp.z - Xc.z, true, Y + ch * NT);
-    }
-    for (int o = lane; o < cb.w * NT; o += 32) Mc[o] = M[(long long)cb.z * NT + o];  // children are consecutive cells
-    __syncwarp();
-    double2 acc[MAXO];
-#pragma unroll
-    for (int u = 0; u < MAXO; u++) acc[u] = make_double2(0.0, 0.0);
-    for (int ch = 0; ch < cb.w; ch++) m2m_accumulate<MAXO>(t, oj, ok, Y + ch * NT, Mc + ch * NT, acc);
-#pragma unroll
-    for (int u = 0; u < MAXO; u++) {
-      const int o = lane + 32 * u;
-      if (o < NT) M[(long long)c * NT + o] = acc[u];
-    }
-    __syncwarp();
   }
 }
 
@@ -709,21 +661,12 @@ void p2m_fp64(const FmmArgs &a) {
 
 void m2m_fp64(const FmmArgs &a, int level, long long nodes_at_level) {
   const DevTables &t = device_tables(a.P);
-  if (a.P <= kM2MBatchedMaxP) {  // all children at once: 16 NTERM complex values of shared memory per warp
-    const size_t smem = kWarpsPerBlock * 16 * t.nterm * sizeof(double2);
-    EXA_MAXO_SWITCH(maxo_for(a.P), {
-      set_smem(k_m2m_batched<MO>, smem);
-      k_m2m_batched<MO><<<blocks_for(nodes_at_level), 32 * kWarpsPerBlock, smem, a.stream>>>(
-          t, a.lvl, level, a.nd_cell, a.cell_b, a.cell_x, a.M64);
-    });
-  } else {
-    const size_t smem = kWarpsPerBlock * 2 * t.nterm * sizeof(double2);
-    EXA_MAXO_SWITCH(maxo_for(a.P), {
-      set_smem(k_m2m<MO>, smem);
-      k_m2m<MO><<<blocks_for(nodes_at_level), 32 * kWarpsPerBlock, smem, a.stream>>>(t, a.lvl, level, a.nd_cell,
-                                                                                     a.cell_b, a.cell_x, a.M64);
-    });
-  }
+  size_t smem = kWarpsPerBlock * 2 * t.nterm * sizeof(double2);
+  EXA_MAXO_SWITCH(maxo_for(a.P), {
+    set_smem(k_m2m<MO>, smem);
+    k_m2m<MO><<<blocks_for(nodes_at_level), 32 * kWarpsPerBlock, smem, a.stream>>>(t, a.lvl, level, a.nd_cell,
+                                                                                   a.cell_b, a.cell_x, a.M64);
+  });
   EXA_CHECK_LAUNCH();
 }
 
