@@ -564,13 +564,24 @@ __global__ void k_lattice_m2m(DevTables t, const double2 *Msup, double cycle, in
   }
 }
 
-// out[o] = (base ? base[o] : out[o]) + sum_w part[w][o], w in order.
-__global__ void k_part_sum(const double2 *part, int nparts, int NT, const double2 *base, double2 *out) {
-  for (int o = threadIdx.x; o < NT; o += blockDim.x) {
-    double2 v = base ? base[o] : out[o];
-    for (int w = 0; w < nparts; w++) v = cadd(v, part[(long long)w * NT + o]);
-    out[o] = v;
+// out[o] = (base ? base[o] : out[o]) + sum_w part[w][o]: one block per
+// coefficient o; thread i sums the parts w = i (mod kPartThreads) in order,
+// then a shared-memory tree adds the threads' sums in a fixed order, so the
+// result does not depend on timing.
+constexpr int kPartThreads = 256;
+__global__ void __launch_bounds__(kPartThreads)
+k_part_sum(const double2 *part, int nparts, int NT, const double2 *base, double2 *out) {
+  __shared__ double2 sh[kPartThreads];
+  const int o = blockIdx.x;
+  double2 v = make_double2(0.0, 0.0);
+  for (int w = threadIdx.x; w < nparts; w += kPartThreads) v = cadd(v, part[(long long)w * NT + o]);
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int h = kPartThreads / 2; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) sh[threadIdx.x] = cadd(sh[threadIdx.x], sh[threadIdx.x + h]);
+    __syncthreads();
   }
+  if (threadIdx.x == 0) out[o] = cadd(base ? base[o] : out[o], sh[0]);
 }
 
 // ---------------------------------------------------------------- dipole
@@ -744,7 +755,7 @@ void lattice_fp64(const FmmArgs &a, int images, double theta, double2 *scratch) 
       k_lattice_m2l<MO><<<grid_l, 32 * kWarpsPerBlock, smem, a.stream>>>(t, cur, cycle, prange, part);
     });
     EXA_CHECK_LAUNCH();
-    k_part_sum<<<1, 64, 0, a.stream>>>(part, grid_l * kWarpsPerBlock, NT, nullptr, a.L64);
+    k_part_sum<<<NT, kPartThreads, 0, a.stream>>>(part, grid_l * kWarpsPerBlock, NT, nullptr, a.L64);
     EXA_CHECK_LAUNCH();
     EXA_MAXO_SWITCH(maxo_for(a.P), {
       const size_t smem = kWarpsPerBlock * 2 * NT * sizeof(double2);
@@ -752,7 +763,7 @@ void lattice_fp64(const FmmArgs &a, int images, double theta, double2 *scratch) 
       k_lattice_m2m<MO><<<grid_m, 32 * kWarpsPerBlock, smem, a.stream>>>(t, cur, cycle, prange, part);
     });
     EXA_CHECK_LAUNCH();
-    k_part_sum<<<1, 64, 0, a.stream>>>(part, grid_m * kWarpsPerBlock, NT, cur, nxt);
+    k_part_sum<<<NT, kPartThreads, 0, a.stream>>>(part, grid_m * kWarpsPerBlock, NT, cur, nxt);
     EXA_CHECK_LAUNCH();
     cycle *= nb;
   }

@@ -211,6 +211,13 @@ __global__ void k_build_K(DevTables t, const unsigned long long *ck, int P, floa
   }
   if ((int)threadIdx.x < 2 * P - 1)
     singular_column(t, threadIdx.x, 2 * P - 1, ux * to_rt - sx, uy * to_rt - sy, uz * to_rt - sz, t.ainv, S);
+  // (n, m, part) of every real degree of freedom, decoded once per block
+  __shared__ int dof_nmp[128];
+  for (int d = threadIdx.x; d < ND && d < 128; d += blockDim.x) {
+    int n, m, part;
+    dof_decode(d, NT, n, m, part);
+    dof_nmp[d] = n | (m << 8) | (part << 16);
+  }
   __syncthreads();
   const int KB = (NDP + 63) / 64;  // 128-byte K-blocks of the swizzled image
   const int img = swizzled ? KB * NDP * 64 : NDP * NDP;
@@ -230,9 +237,9 @@ __global__ void k_build_K(DevTables t, const unsigned long long *ck, int P, floa
     }
     double val = 0.0;
     if (r < ND && c < ND) {
-      int j, k, rp, n, mp, cp;
-      dof_decode(r, NT, j, k, rp);
-      dof_decode(c, NT, n, mp, cp);
+      const int er = dof_nmp[r], ec = dof_nmp[c];
+      const int j = er & 0xff, k = (er >> 8) & 0xff, rp = er >> 16;
+      const int n = ec & 0xff, mp = (ec >> 8) & 0xff, cp = ec >> 16;
       const double fn = ldexp(1.0, -dl * n);  // (R_s / R_t)^n
       double sr = 0.0, si = 0.0;
       for (int side = 0; side < (mp > 0 ? 2 : 1); side++) {
