@@ -372,8 +372,14 @@ __global__ void k_p2p_keys(const int *off, const int *src, long long ncells, con
 // first), until none is left, so leaves of very different cost balance out
 // and the warps finish together.  A leaf's result does not depend on when or
 // by which warp it is evaluated.
+// Resident warps per SM: the register budgets (96 and 126 registers, no
+// spills) at which the two kinds measured fastest on a 512-system batch at
+// P = 10 (P2P 55.3 -> 54.5 ms against 16 and 12 warps; the same on one 4M
+// solve).
+constexpr int kWarps2 = 20, kWarps3 = 16;
+
 template <bool PERIODIC, int TPL>
-__global__ void __launch_bounds__(32, TPL == 2 ? 16 : 12)
+__global__ void __launch_bounds__(32, TPL == 2 ? kWarps2 : kWarps3)
 k_p2p32(const int *off, const int *src, const int *order, const int *count, const int4 *cell_b,
         const int4 *cell_bj, const float4 *x32, const float4 *x32j, double4 *trg, double cycle,
         unsigned long long *next) {
@@ -434,8 +440,8 @@ void p2p_mixed(Context &C, const FmmArgs &a, const float4 *x32, bool periodic, P
   const bool alt = radix_sort_u32(w.key.p, w.order.p, w.key_alt.p, w.order_alt.p, nc, 0, kCostBits + 2, C.sort,
                                   C.err.p, st);
   const int *order = alt ? w.order_alt.p : w.order.p;
-  const unsigned g2 = (unsigned)std::min<long long>(nc, (long long)kNumSMs * 16);
-  const unsigned g3 = (unsigned)std::min<long long>(nc, (long long)kNumSMs * 12);
+  const unsigned g2 = (unsigned)std::min<long long>(nc, (long long)kNumSMs * kWarps2);
+  const unsigned g3 = (unsigned)std::min<long long>(nc, (long long)kNumSMs * kWarps3);
   if (periodic) {
     k_p2p32<true, 2><<<g2, 32, 0, st>>>(a.p2p_off, a.p2p_src, order, w.count.p, a.cell_b, cell_bj, x32, x32j,
                                         a.trg64, a.cycle, w.next.p);
