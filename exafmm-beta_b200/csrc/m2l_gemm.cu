@@ -623,7 +623,8 @@ __host__ __device__ constexpr int mma_ctas_per_sm(int NDP) {
 // (2^-8 and 2^-16 of it) another: the large one sees NDP / 16 additions, and
 // the epilogue adds the two in FP32.
 // Per chunk j: thread 0 issues the 6 x NDP / 16 MMAs and commits them to an
-// mbarrier; every thread loads chunk j+1's indices meanwhile; once the
+// mbarrier; every thread loads chunk j+2's indices meanwhile (those of j+1
+// were loaded during chunk j-1's products); once the
 // products are done, all threads start the cp.async gather of chunk j+1's
 // source pieces (lane pairs fetch whole 32-byte sectors) and, while it is in
 // flight, read chunk j's accumulators (warp w: TMEM lanes 32w..32w+31) and
@@ -725,6 +726,15 @@ k_m2l_class_mma(const int4 *chunks, const int *nchunks, const int *sval, const i
   tc_fence_after();
   const unsigned tmem = s_tmem;
   mma_gather<NDP>(sA, sB, s_src, ch.z, ch.x, cur_cls, Kb, Msb);
+  // the next chunk's descriptor, list positions and sources, loaded one chunk
+  // ahead of their use
+  int4 chn = ch;
+  int qn = -1, scn = -1;
+  if (j0 + 1 < j1) {
+    chn = chunks[j0 + 1];
+    qn = (int)threadIdx.x < chn.z ? sval[chn.y + threadIdx.x] : -1;
+    scn = (int)threadIdx.x < chn.z ? ssrc[chn.y + threadIdx.x] : -1;
+  }
   mma_tiles_ready();
   for (int j = j0; j < j1; j++) {
     const int cnt = ch.z, qc = q;
@@ -743,11 +753,16 @@ k_m2l_class_mma(const int4 *chunks, const int *nchunks, const int *sval, const i
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
                    : "memory");
     }
-    int sc = -1;  // the next chunk's indices while the products run
+    int sc = -1;
     if (j + 1 < j1) {
-      ch = chunks[j + 1];
-      q = (int)threadIdx.x < ch.z ? sval[ch.y + threadIdx.x] : -1;
-      sc = q >= 0 ? ssrc[ch.y + threadIdx.x] : -1;
+      ch = chn;
+      q = qn;
+      sc = scn;
+    }
+    if (j + 2 < j1) {  // the chunk after, while the products run
+      chn = chunks[j + 2];
+      qn = (int)threadIdx.x < chn.z ? sval[chn.y + threadIdx.x] : -1;
+      scn = (int)threadIdx.x < chn.z ? ssrc[chn.y + threadIdx.x] : -1;
     }
     bool done = true;  // one poller per warp
     if ((threadIdx.x & 31) == 0) done = mbar_wait_bounded(bar, (unsigned)((j - j0) & 1));
@@ -906,6 +921,16 @@ k_m2l_class_mma_tma(const __grid_constant__ CUtensorMap msb_map, const int4 *chu
     }
   };
   issue_loads(ch.x, ch.z);
+  // the next chunk's descriptor, list positions and sources, loaded one chunk
+  // ahead of their use (so the three dependent loads are not waited for
+  // between the products and the next gather)
+  int4 chn = ch;
+  int qn = -1, scn = -1;
+  if (j0 + 1 < j1) {
+    chn = chunks[j0 + 1];
+    qn = (int)threadIdx.x < chn.z ? sval[chn.y + threadIdx.x] : -1;
+    scn = (int)threadIdx.x < chn.z ? ssrc[chn.y + threadIdx.x] : -1;
+  }
   bool ok = true;
   for (int j = j0; j < j1; j++) {
     const int cnt = ch.z, qc = q, it = j - j0;
@@ -939,9 +964,14 @@ k_m2l_class_mma_tma(const __grid_constant__ CUtensorMap msb_map, const int4 *chu
     }
     int sc = -1;
     if (j + 1 < j1) {
-      ch = chunks[j + 1];
-      q = (int)threadIdx.x < ch.z ? sval[ch.y + threadIdx.x] : -1;
-      sc = q >= 0 ? ssrc[ch.y + threadIdx.x] : -1;
+      ch = chn;
+      q = qn;
+      sc = scn;
+    }
+    if (j + 2 < j1) {  // the chunk after, while the products run
+      chn = chunks[j + 2];
+      qn = (int)threadIdx.x < chn.z ? sval[chn.y + threadIdx.x] : -1;
+      scn = (int)threadIdx.x < chn.z ? ssrc[chn.y + threadIdx.x] : -1;
     }
     bool done = true;
     if ((threadIdx.x & 31) == 0) done = mbar_wait_bounded(bar, (unsigned)(it & 1));
