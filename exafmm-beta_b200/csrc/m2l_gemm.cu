@@ -1239,7 +1239,7 @@ bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int
                                             max_dl, g.taken.p, g.left_cnt.p, g.skey.p, g.pval.p);
   EXA_CHECK_LAUNCH();
   LeftScan ls{g.left_cnt.p, g.left_off.p, nc};
-  launch_scan<256, 8>(ls, nullptr, nc, nc, C.scan, C.err.p, st);
+  launch_scan<1024, 8>(ls, nullptr, nc, nc, C.scan, C.err.p, st);
   k_left_fill<<<kNumSMs * 8, 256, 0, st>>>(a.m2l_off, a.m2l_src, nc, g.taken.p, a.cell_pl, min_level, max_dl,
                                            g.left_off.p, g.left_src.p);
   EXA_CHECK_LAUNCH();
@@ -1252,7 +1252,7 @@ bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int
   k_class_ranges<<<(ncls + 256) / 256, 256, 0, st>>>(sk, n_m2l, ncls, g.cstart.p);
   EXA_CHECK_LAUNCH();
   ChunkScan cs2{g.cstart.p, g.cbase.p, ncls};
-  launch_scan<256, 8>(cs2, nullptr, ncls, ncls, C.scan, C.err.p, st);
+  launch_scan<1024, 8>(cs2, nullptr, ncls, ncls, C.scan, C.err.p, st);
   const long long chunks_max = n_m2l / kChunk + ncls + 1;
   if (tc) {
     g.chunks.ensure(chunks_max);
@@ -1307,7 +1307,7 @@ long long m2l_complement(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long
   k_complement_count<<<grid, 256, 0, st>>>(a.m2l_off, a.m2l_src, nc, a.cell_pl, min_level, max_dl, g.comp_cnt.p);
   EXA_CHECK_LAUNCH();
   LeftScan ls{g.comp_cnt.p, g.comp_off.p, nc};
-  launch_scan<256, 8>(ls, nullptr, nc, nc, C.scan, C.err.p, st);
+  launch_scan<1024, 8>(ls, nullptr, nc, nc, C.scan, C.err.p, st);
   k_complement_fill<<<grid, 256, 0, st>>>(a.m2l_off, a.m2l_src, nc, a.cell_pl, min_level, max_dl, g.comp_off.p,
                                           g.comp_src.p);
   EXA_CHECK_LAUNCH();

@@ -205,7 +205,7 @@ void radix_pass(const K *kin, const int *vin, K *kout, int *vout, long long n, i
   EXA_CHECK_LAUNCH();
   CountScan cs{w.counts.p};
   const long long cells = (long long)(1 << BITS) * ntiles;
-  launch_scan<256, 8>(cs, nullptr, cells, cells, w.scan, err, st);
+  launch_scan<1024, 8>(cs, nullptr, cells, cells, w.scan, err, st);
   constexpr size_t smem = scatter_smem_bytes<K, BITS>();
   scatter_smem_optin<K, BITS>();
   radix_scatter<K, BITS><<<ntiles, kSortThreads, smem, st>>>(kin, vin, kout, vout, n, shift, mask, w.counts.p,

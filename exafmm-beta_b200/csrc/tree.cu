@@ -838,7 +838,7 @@ void build_tree(Context &C) {
     k_scan_prep<<<1, 1, 0, st>>>(T.lvl.p, l, lvl_n, lvl_s);
     EXA_CHECK_LAUNCH();
     LevelScan ls{a, l, lvl_s};
-    launch_scan<256, 4>(ls, lvl_n, 0, T.node_cap, C.scan, C.err.p, st);
+    launch_scan<1024, 8>(ls, lvl_n, 0, T.node_cap, C.scan, C.err.p, st);
     k_emit<<<node_grid, 256, 0, st>>>(a, l);
     EXA_CHECK_LAUNCH();
   }
