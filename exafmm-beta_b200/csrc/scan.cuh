@@ -59,6 +59,19 @@ __device__ __forceinline__ T warp_inclusive_scan(T v) {
 
 template <typename T> __device__ __forceinline__ T zero_value() { return T{}; }
 
+// A value another block published: read from L2 (ld.global.cg), never from
+// a line this SM's L1 may hold from before it was written.
+template <typename T>
+__device__ __forceinline__ T load_cg(const T *p) {
+  static_assert(sizeof(T) % 4 == 0, "whole 32-bit words");
+  T v;
+  unsigned *d = reinterpret_cast<unsigned *>(&v);
+  const unsigned *src = reinterpret_cast<const unsigned *>(p);
+#pragma unroll
+  for (int i = 0; i < (int)(sizeof(T) / 4); i++) d[i] = __ldcg(src + i);
+  return v;
+}
+
 // Bounded spin: about a second of polling before giving up.
 constexpr unsigned kSpinLimit = 1u << 22;
 
@@ -106,36 +119,67 @@ scan_kernel(Producer prod, const long long *n_ptr, long long n_const, ScanScratc
     }
     T thread_excl = wexcl + shfl_up_any(winc, 1);
     if (lane == 0) thread_excl = wexcl;
-    if (threadIdx.x == 0) {
+    if (warp == 0) {
+      // Look-back by the whole warp: lane l reads the flag of tile p - l, so
+      // 32 predecessors are examined per round trip to memory.  Once every
+      // tile of the window has published something, the lanes up to the
+      // nearest inclusive prefix add their values (aggregates, or that
+      // inclusive prefix); with no inclusive prefix in the window, the next
+      // 32 tiles follow.  The values are integer counts, so the order of the
+      // additions does not matter.
       T excl = zero_value<T>();
       if (t == 0) {
-        incl[0] = agg;
-        __threadfence();
-        flags[0] = (epoch << 2) | 2u;
+        if (lane == 0) {
+          incl[0] = agg;
+          __threadfence();
+          flags[0] = (epoch << 2) | 2u;
+        }
       } else {
-        aggs[t] = agg;
-        __threadfence();
-        flags[t] = (epoch << 2) | 1u;
+        if (lane == 0) {
+          aggs[t] = agg;
+          __threadfence();
+          flags[t] = (epoch << 2) | 1u;
+        }
         long long p = t - 1;
         unsigned spins = 0;
-        while (p >= 0) {
-          unsigned f = flags[p];
-          if ((f >> 2) != epoch || (f & 3u) == 0) {
-            if (++spins > kSpinLimit) { atomicOr(s.error, 16); break; }
+        bool failed = false;
+        while (true) {
+          const long long q = p - lane;
+          unsigned f = 0;
+          while (true) {
+            f = q >= 0 ? flags[q] : 0u;
+            const bool ready = q < 0 || ((f >> 2) == epoch && (f & 3u) != 0);
+            if (__all_sync(0xffffffffu, ready)) break;
+            if (++spins > kSpinLimit) {
+              failed = true;
+              break;
+            }
             if (spins > 64) __nanosleep(64);  // short waits poll at full rate
-            continue;
+          }
+          if (failed) {
+            if (lane == 0) atomicOr(s.error, 16);
+            break;
           }
           __threadfence();
-          if ((f & 3u) == 2u) { excl = incl[p] + excl; break; }
-          excl = aggs[p] + excl;
-          p--;
+          const unsigned inc = __ballot_sync(0xffffffffu, q >= 0 && (f & 3u) == 2u);
+          const int stop = inc ? __ffs((int)inc) - 1 : 31;
+          T v = zero_value<T>();
+          if (q >= 0 && lane <= stop) v = (f & 3u) == 2u ? load_cg(incl + q) : load_cg(aggs + q);
+          v = warp_inclusive_scan(v);
+          excl = excl + shfl_any(v, 31);
+          if (inc || p < 32) break;  // an inclusive prefix, or tile 0 reached
+          p -= 32;
         }
-        incl[t] = excl + agg;
-        __threadfence();
-        flags[t] = (epoch << 2) | 2u;
+        if (lane == 0) {
+          incl[t] = excl + agg;
+          __threadfence();
+          flags[t] = (epoch << 2) | 2u;
+        }
       }
-      tile_excl = excl;
-      if ((t + 1) * TILE >= n) prod.total(excl + agg);
+      if (lane == 0) {
+        tile_excl = excl;
+        if ((t + 1) * TILE >= n) prod.total(excl + agg);
+      }
     }
     __syncthreads();
     T acc = tile_excl + thread_excl;
