@@ -5,6 +5,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <vector>
 
@@ -107,10 +108,10 @@ struct Engine {
   // Separate source bodies (examples/fmm.cxx -j IneJ, :61-73): their own tree
   // and multipoles, on the same stream as the targets.
   std::unique_ptr<Engine> jsrc;
-  bool is_source = false;  // this engine is another one's source tree (owns its pinned error word)
+  bool is_source = false;  // this engine is another one's source tree
 
   ~Engine() {
-    if (is_source && C.err_host) cudaFreeHost(C.err_host);
+    if (C.pin) pinned_block_release(C.pin);  // its copies ended with the call that made them
   }
 
   FmmArgs args() {
@@ -259,7 +260,8 @@ struct Engine {
         e->C.stream = C.stream;
         e->C.err.ensure(1);
         EXA_CUDA(cudaMemsetAsync(e->C.err.p, 0, sizeof(int), C.stream));
-        EXA_CUDA(cudaMallocHost((void **)&e->C.err_host, sizeof(int)));
+        e->C.pin = pinned_block_acquire();
+        e->C.err_host = reinterpret_cast<int *>(e->C.pin);
         jsrc = std::move(e);
       }
       jsrc->C.prm = C.prm;
@@ -637,6 +639,30 @@ struct exafmm_ctx {
 namespace exafmm_b200 {
 thread_local long long *g_dbuf_account = nullptr;
 thread_local cudaStream_t g_dbuf_stream = nullptr;
+
+namespace {
+std::mutex g_pin_mutex;
+std::vector<unsigned char *> g_pin_free;  // blocks of kPinBytes in pinned slabs that live until exit
+}  // namespace
+
+unsigned char *pinned_block_acquire() {
+  std::lock_guard<std::mutex> lock(g_pin_mutex);
+  if (g_pin_free.empty()) {
+    constexpr int kBlocks = 64;
+    unsigned char *slab = nullptr;
+    EXA_CUDA(cudaMallocHost((void **)&slab, kBlocks * kPinBytes));
+    for (int i = kBlocks - 1; i >= 0; i--) g_pin_free.push_back(slab + (size_t)i * kPinBytes);
+  }
+  unsigned char *p = g_pin_free.back();
+  g_pin_free.pop_back();
+  return p;
+}
+
+void pinned_block_release(unsigned char *p) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lock(g_pin_mutex);
+  g_pin_free.push_back(p);
+}
 }
 
 namespace {
@@ -755,7 +781,8 @@ int exafmm_create(exafmm_ctx **out, int P, double theta, int ncrit, int nspawn, 
     g_dbuf_stream = C.stream;
     C.err.ensure(1);
     EXA_CUDA(cudaMemsetAsync(C.err.p, 0, sizeof(int), C.stream));
-    EXA_CUDA(cudaMallocHost((void **)&C.err_host, sizeof(int)));
+    C.pin = pinned_block_acquire();
+    C.err_host = reinterpret_cast<int *>(C.pin);
     device_tables(P);
     *out = c.release();
     return 0;
@@ -769,7 +796,6 @@ int exafmm_destroy(exafmm_ctx *ctx) {
   if (!ctx) return 0;
   cudaSetDevice(ctx->E.C.device);
   cudaStreamSynchronize(ctx->E.C.stream);
-  if (ctx->E.C.err_host) cudaFreeHost(ctx->E.C.err_host);
   cudaStream_t st = ctx->E.C.stream;
   delete ctx;
   if (st) cudaStreamDestroy(st);

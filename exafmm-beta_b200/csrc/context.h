@@ -89,12 +89,24 @@ struct Context {
   cudaEvent_t ev_link = nullptr;  // when set, recorded between growing the octree and linking the cells
   int device = 0;
   DBuf<int> err;               // device error word
-  int *err_host = nullptr;     // pinned mirror
+  unsigned char *pin = nullptr;  // pinned block (pinned_block_acquire): the error word, then readback staging
+  int *err_host = nullptr;     // pinned mirror of the error word (the start of pin)
   TreeBufs tree;
   ScanWork scan;
   SortWork sort;
   std::string last_error;
 };
+
+// Pinned host block of a context: its error word at offset 0 and, from
+// kPinScratch on, the staging area of a solve's small device-to-host readbacks
+// (level counts, traversal counts, the class count), so that a solve copies
+// nothing into pageable memory.  Blocks come from a process-wide pinned slab
+// and return to it when the context is destroyed: creating and destroying
+// contexts neither pins nor unpins host memory (cudaFreeHost waits for the
+// whole device, which stalls every other context's stream in a server).
+constexpr size_t kPinBytes = 4096, kPinScratch = 64;
+unsigned char *pinned_block_acquire();
+void pinned_block_release(unsigned char *p);
 
 // Tree construction (tree.cu).
 void compute_bounds(Context &C);

@@ -1194,9 +1194,10 @@ bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int
   g.cs_alt.ensure(ccap);
   k_class_compact<<<kNumSMs * 4, 256, 0, st>>>(g.hk.p, g.hc.p, hcap, g.ck.p, g.cs.p, g.cnt.p, ccap);
   EXA_CHECK_LAUNCH();
-  int ncls = 0;
-  EXA_CUDA(cudaMemcpyAsync(&ncls, g.cnt.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  int *ncls_h = reinterpret_cast<int *>(C.pin + kPinScratch);  // the context's pinned staging
+  EXA_CUDA(cudaMemcpyAsync(ncls_h, g.cnt.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   EXA_CUDA(cudaStreamSynchronize(st));
+  int ncls = *ncls_h;
   if (ncls <= 0) return false;
   if (ncls > ccap) ncls = ccap;  // the overflow classes' pairs stay per-pair
   bool alt = radix_sort_u64((uint64_t *)g.ck.p, g.cs.p, (uint64_t *)g.ck_alt.p, g.cs_alt.p, ncls, 0, 64, C.sort,

@@ -262,8 +262,10 @@ bool traverse(Context &C, ListBufs &lb, const TreeBufs *sources) {
     // on a 4M-body solve against 2048-pair tiles of 256 threads
     launch_scan<1024, 8>(ps, lb.cnt.p + 3 * s, 0, lb.q_cap, C.scan, C.err.p, st);
   }
-  long long cnt[3 * (kMaxSweeps + 1)];
-  EXA_CUDA(cudaMemcpyAsync(cnt, lb.cnt.p, 3 * (nsw + 1) * sizeof(long long), cudaMemcpyDeviceToHost, st));
+  static_assert(kPinScratch + 3 * (kMaxSweeps + 1) * sizeof(long long) <= kPinBytes, "pinned staging layout");
+  const long long *cnt = reinterpret_cast<const long long *>(C.pin + kPinScratch);
+  EXA_CUDA(cudaMemcpyAsync(C.pin + kPinScratch, lb.cnt.p, 3 * (nsw + 1) * sizeof(long long), cudaMemcpyDeviceToHost,
+                           st));
   EXA_CUDA(cudaMemcpyAsync(C.err_host, C.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   EXA_CUDA(cudaStreamSynchronize(st));
   long long qmax = 0;

@@ -12,6 +12,7 @@
 // a leaf the reference keeps input order (its partitions are stable), so a final
 // per-leaf sort restores ascending input index there.
 #include <algorithm>
+#include <cstring>
 
 #include "context.h"
 #include "drift.cuh"
@@ -822,9 +823,10 @@ void build_tree(Context &C) {
     k_split_level<<<grid_for(n, 256), 256, 0, st>>>(T.keys.p, T.perm.p, n, ncrit, forest ? T.sys_off.p : nullptr,
                                                    T.nsys, T.split_level.p);
     EXA_CHECK_LAUNCH();
-    int deepest = -1;
-    EXA_CUDA(cudaMemcpyAsync(&deepest, T.split_level.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int *deepest_h = reinterpret_cast<int *>(C.pin + kPinScratch);
+    EXA_CUDA(cudaMemcpyAsync(deepest_h, T.split_level.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     EXA_CUDA(cudaStreamSynchronize(st));
+    const int deepest = *deepest_h;
     last = std::min(deepest + 1, kMaxLevels);
   }
   // per-level kernels: eight threads per node at most node_cap nodes
@@ -869,18 +871,30 @@ void build_tree(Context &C) {
 
 void sync_tree(Context &C) {
   TreeBufs &T = C.tree;
-  EXA_CUDA(cudaMemcpyAsync(T.lvl_host, T.lvl.p, sizeof(T.lvl_host), cudaMemcpyDeviceToHost, C.stream));
-  int nn = 0;
+  // staging in the context's pinned block: level counts, then the cell count
+  // (or a forest's per-system cell offsets, when they fit)
+  static_assert(kPinScratch + sizeof(T.lvl_host) + sizeof(int) <= 1024, "pinned staging layout");
+  long long *lvl_h = reinterpret_cast<long long *>(C.pin + kPinScratch);
+  int *nn_h = reinterpret_cast<int *>(C.pin + 1024);
+  const bool sys_pinned = (size_t)(T.nsys + 1) * sizeof(int) <= kPinBytes - 1024;
+  EXA_CUDA(cudaMemcpyAsync(lvl_h, T.lvl.p, sizeof(T.lvl_host), cudaMemcpyDeviceToHost, C.stream));
   if (T.nsys) {
     T.sys_cell_host.assign(T.nsys + 1, 0);
-    EXA_CUDA(cudaMemcpyAsync(T.sys_cell_host.data(), T.sys_cell.p, (T.nsys + 1) * sizeof(int),
-                             cudaMemcpyDeviceToHost, C.stream));
+    EXA_CUDA(cudaMemcpyAsync(sys_pinned ? (void *)nn_h : (void *)T.sys_cell_host.data(), T.sys_cell.p,
+                             (T.nsys + 1) * sizeof(int), cudaMemcpyDeviceToHost, C.stream));
   } else if (T.n > 0) {
-    EXA_CUDA(cudaMemcpyAsync(&nn, T.nd_nnode.p, sizeof(int), cudaMemcpyDeviceToHost, C.stream));
+    EXA_CUDA(cudaMemcpyAsync(nn_h, T.nd_nnode.p, sizeof(int), cudaMemcpyDeviceToHost, C.stream));
   }
   EXA_CUDA(cudaMemcpyAsync(C.err_host, C.err.p, sizeof(int), cudaMemcpyDeviceToHost, C.stream));
   EXA_CUDA(cudaStreamSynchronize(C.stream));
-  if (T.nsys) nn = T.sys_cell_host[T.nsys];
+  std::memcpy(T.lvl_host, lvl_h, sizeof(T.lvl_host));
+  int nn = 0;
+  if (T.nsys) {
+    if (sys_pinned) std::memcpy(T.sys_cell_host.data(), nn_h, (T.nsys + 1) * sizeof(int));
+    nn = T.sys_cell_host[T.nsys];
+  } else if (T.n > 0) {
+    nn = *nn_h;
+  }
   T.ncells = (T.n > 0) ? nn : 0;
   T.depth = 0;
   for (int l = 0; l <= kMaxLevels; l++)
