@@ -285,11 +285,13 @@ __device__ __forceinline__ void p2p_stream(Stage &sm, const int *src, const int4
   }
 }
 
+// One pass over the leaf's source stream for its targets [tb, tb + S * TPL).
 template <int S, int TPL, bool PERIODIC>
-__device__ __forceinline__ void p2p_leaf(Stage &sm, int4 cb, int b, int e, const int *src, const int4 *cell_bj,
-                                         const float4 *x32, const float4 *x32j, double4 *trg, double cycle) {
+__device__ __forceinline__ void p2p_pass(Stage &sm, int4 cb, int tb, int b, int e, const int *src,
+                                         const int4 *cell_bj, const float4 *x32, const float4 *x32j, double4 *trg,
+                                         double cycle) {
   const int lane = threadIdx.x & 31, g = lane / S, j = lane % S;
-  for (int tb = 0; tb < cb.y; tb += S * TPL) {
+  {
     Targets<TPL> T;
 #pragma unroll
     for (int u = 0; u < TPL; u++) {
@@ -331,14 +333,29 @@ __device__ __forceinline__ void p2p_leaf(Stage &sm, int4 cb, int b, int e, const
   }
 }
 
-// Target slots of a leaf: S lanes x TPL targets per lane.  Leaves of 9-12,
-// 17-24, 33-48 and 65-96 bodies fill three targets per lane (12, 24, 48, 96
-// slots) better than two (16, 32, 64, 128); the rest take two.  The two
-// kinds run as separate kernels, so the three-target code's registers do not
-// lower the occupancy of the two-target one.
-__device__ __forceinline__ bool three_per_lane(int n) {
-  return (n > 8 && n <= 12) || (n > 16 && n <= 24) || (n > 32 && n <= 48) || (n > 64 && n <= 96);
+// Target slots of a leaf: passes of S lanes x TPL targets per lane, each pass
+// taking the narrowest group that holds the targets still left (S = 32 while
+// more than 16 TPL remain).  A 70-body leaf at two per lane: 64 + 8 slots in
+// two passes, rather than 96 at three per lane or 128 in two full passes.
+// Every pass streams the leaf's sources again, which costs about as much as
+// a few more target slots, so a leaf takes three targets per lane when that
+// costs fewer slots plus passes.  The two kinds run as separate kernels, so
+// the three-target code's registers do not lower the occupancy of the
+// two-target one.
+__host__ __device__ __forceinline__ int pass_lanes(int left, int tpl) {
+  return left <= 4 * tpl ? 4 : left <= 8 * tpl ? 8 : left <= 16 * tpl ? 16 : 32;
 }
+constexpr int kPassCharge = 4;  // target slots one more stream of the sources costs
+__host__ __device__ __forceinline__ int pass_cost(int n, int tpl) {
+  int cost = 0;
+  for (int tb = 0; tb < n;) {
+    const int w = pass_lanes(n - tb, tpl) * tpl;
+    cost += w + kPassCharge;
+    tb += w;
+  }
+  return cost;
+}
+__device__ __forceinline__ bool three_per_lane(int n) { return pass_cost(n, 3) < pass_cost(n, 2); }
 
 // Work order: each cell's kind (0: a leaf of two targets per lane, 1: three,
 // 2: no P2P list; tpl 2 or 3 gives every leaf that kind, tpl 0 chooses by the
@@ -394,15 +411,23 @@ k_p2p32(const int *off, const int *src, const int *order, const int *count, cons
     const int c = mine[k];
     const int b = off[c], e = off[c + 1];
     const int4 cb = cell_b[c];
-    if (cb.y <= 4 * TPL)
-      p2p_leaf<4, TPL, PERIODIC>(sm, cb, b, e, src, cell_bj, x32, x32j, trg, cycle);
-    else if (cb.y <= 8 * TPL)
-      p2p_leaf<8, TPL, PERIODIC>(sm, cb, b, e, src, cell_bj, x32, x32j, trg, cycle);
-    else if (cb.y <= 16 * TPL)
-      p2p_leaf<16, TPL, PERIODIC>(sm, cb, b, e, src, cell_bj, x32, x32j, trg, cycle);
-    else
-      p2p_leaf<32, TPL, PERIODIC>(sm, cb, b, e, src, cell_bj, x32, x32j, trg, cycle);
-    __syncwarp();  // the stage buffer is free before the next cell's first fill
+    for (int tb = 0; tb < cb.y;) {
+      const int left = cb.y - tb;
+      if (left <= 4 * TPL) {
+        p2p_pass<4, TPL, PERIODIC>(sm, cb, tb, b, e, src, cell_bj, x32, x32j, trg, cycle);
+        tb += 4 * TPL;
+      } else if (left <= 8 * TPL) {
+        p2p_pass<8, TPL, PERIODIC>(sm, cb, tb, b, e, src, cell_bj, x32, x32j, trg, cycle);
+        tb += 8 * TPL;
+      } else if (left <= 16 * TPL) {
+        p2p_pass<16, TPL, PERIODIC>(sm, cb, tb, b, e, src, cell_bj, x32, x32j, trg, cycle);
+        tb += 16 * TPL;
+      } else {
+        p2p_pass<32, TPL, PERIODIC>(sm, cb, tb, b, e, src, cell_bj, x32, x32j, trg, cycle);
+        tb += 32 * TPL;
+      }
+      __syncwarp();  // the stage buffer is free before the next pass's first fill
+    }
   }
 }
 
