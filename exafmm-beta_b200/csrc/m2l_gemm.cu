@@ -190,10 +190,21 @@ __global__ void k_class_ids(const int *cs_sorted, int ncls, int *hid) {
 // image of NDP output rows x NDP inputs in the core_off layout (tensor cores).
 // cell_x[0].w (the root radius) and cycle place the image shifts of
 // class_key_image keys (one system, never a forest, has image pairs).
-__global__ void k_build_K(DevTables t, const unsigned long long *ck, int P, float *Kt, unsigned short *Kb,
-                          bool swizzled, const double4 *cell_x, double cycle) {
+// Operand layouts of k_build_K: FP32 k-major Kt[class][input][output] (CUDA
+// cores), three bf16 pieces in the core_off image, or in the 128-byte-swizzled
+// image (TMA).  NDP and the layout are template parameters so that mapping an
+// entry's position to its (output, input) pair is shifts and constant
+// divisions, not runtime divisions (the build was bound by integer work).
+enum KLayout : int { kKFp32 = 0, kKCore = 1, kKSwizzled = 2 };
+
+template <int NDP, int LAYOUT>
+__global__ void __launch_bounds__(256)
+k_build_K(DevTables t, const unsigned long long *ck, int P, float *Kt, unsigned short *Kb, const double4 *cell_x,
+          double cycle) {
   extern __shared__ double2 S[];  // S'_p^q, q >= 0, at d / R_t
-  const int NT = t.nterm, ND = nd_of(P), NDP = ndp_of(P);
+  constexpr int KB = (NDP + 63) / 64;  // 128-byte K-blocks of the swizzled image
+  constexpr int IMG = LAYOUT == kKSwizzled ? KB * NDP * 64 : NDP * NDP;
+  const int NT = t.nterm, ND = nd_of(P);
   const unsigned long long key = ck[blockIdx.x];
   const bool image = (key >> 63) != 0;
   const int dl = image ? (int)((key >> 53) & 31) - 16 : (int)((key >> 48) & 0xffff) - 16;
@@ -211,23 +222,24 @@ __global__ void k_build_K(DevTables t, const unsigned long long *ck, int P, floa
   }
   if ((int)threadIdx.x < 2 * P - 1)
     singular_column(t, threadIdx.x, 2 * P - 1, ux * to_rt - sx, uy * to_rt - sy, uz * to_rt - sz, t.ainv, S);
-  // (n, m, part) of every real degree of freedom, decoded once per block
+  // (n, m, part) of every real degree of freedom, decoded once per block, and
+  // (R_s / R_t)^n for every source degree n
   __shared__ int dof_nmp[128];
+  __shared__ double fn_of[32];
   for (int d = threadIdx.x; d < ND && d < 128; d += blockDim.x) {
     int n, m, part;
     dof_decode(d, NT, n, m, part);
     dof_nmp[d] = n | (m << 8) | (part << 16);
   }
+  if ((int)threadIdx.x < P) fn_of[threadIdx.x] = ldexp(1.0, -dl * (int)threadIdx.x);
   __syncthreads();
-  const int KB = (NDP + 63) / 64;  // 128-byte K-blocks of the swizzled image
-  const int img = swizzled ? KB * NDP * 64 : NDP * NDP;
-  for (int e = threadIdx.x; e < img; e += blockDim.x) {
+  for (int e = threadIdx.x; e < IMG; e += blockDim.x) {
     int c, r;  // input and output dof; with Kb, e walks the operand image so the stores are contiguous
-    if (Kb && swizzled) {  // 128-byte-swizzled image: K-block c / 64, row r, 16-byte chunk ((c % 64) / 8) ^ (r % 8)
+    if constexpr (LAYOUT == kKSwizzled) {  // K-block c / 64, row r, 16-byte chunk ((c % 64) / 8) ^ (r % 8)
       const int kb = e / (NDP * 64), w = e - kb * NDP * 64;
       r = w >> 6;
       c = kb * 64 + (((((w >> 3) & 7) ^ (r & 7))) << 3) + (w & 7);
-    } else if (Kb) {
+    } else if constexpr (LAYOUT == kKCore) {
       const int ci = e >> 6, w = e & 63;
       r = (ci / (NDP >> 3)) * 8 + (w >> 3);
       c = (ci % (NDP >> 3)) * 8 + (w & 7);
@@ -240,7 +252,7 @@ __global__ void k_build_K(DevTables t, const unsigned long long *ck, int P, floa
       const int er = dof_nmp[r], ec = dof_nmp[c];
       const int j = er & 0xff, k = (er >> 8) & 0xff, rp = er >> 16;
       const int n = ec & 0xff, mp = (ec >> 8) & 0xff, cp = ec >> 16;
-      const double fn = ldexp(1.0, -dl * n);  // (R_s / R_t)^n
+      const double fn = fn_of[n];  // (R_s / R_t)^n
       double sr = 0.0, si = 0.0;
       for (int side = 0; side < (mp > 0 ? 2 : 1); side++) {
         const int m = side == 0 ? mp : -mp;
@@ -264,13 +276,14 @@ __global__ void k_build_K(DevTables t, const unsigned long long *ck, int P, floa
       }
       val = fn * (rp == 0 ? sr : si);
     }
-    if (Kt) Kt[(long long)blockIdx.x * NDP * NDP + c * NDP + r] = (float)val;
-    if (Kb) {
+    if constexpr (LAYOUT == kKFp32) {
+      Kt[(long long)blockIdx.x * NDP * NDP + c * NDP + r] = (float)val;
+    } else {
       unsigned short h[3];
       split_bf16x3(val, h);
-      unsigned short *dst = Kb + (long long)blockIdx.x * 3 * img + e;  // e == the operand offset of (r, c)
+      unsigned short *dst = Kb + (long long)blockIdx.x * 3 * IMG + e;  // e == the operand offset of (r, c)
 #pragma unroll
-      for (int p = 0; p < 3; p++) dst[p * img] = h[p];
+      for (int p = 0; p < 3; p++) dst[p * IMG] = h[p];
     }
   }
 }
@@ -1216,9 +1229,26 @@ bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int
   else g.K.ensure((long long)ncls * NDP * NDP);
   {
     const size_t smem = tri(2 * P - 1) * sizeof(double2);
-    k_build_K<<<ncls, 256, smem, st>>>(t, ck, P, tc ? nullptr : g.K.p, tc ? g.Kb.p : nullptr, use_tma, a.cell_x,
-                                       a.cycle);
-    EXA_CHECK_LAUNCH();
+    float *Kt = tc ? nullptr : g.K.p;
+    unsigned short *Kb = tc ? g.Kb.p : nullptr;
+    auto build = [&](auto kernel) {
+      kernel<<<ncls, 256, smem, st>>>(t, ck, P, Kt, Kb, a.cell_x, a.cycle);
+      EXA_CHECK_LAUNCH();
+    };
+    switch (NDP) {
+#define EXA_BUILD_K_CASE(N)                                      \
+  case N:                                                        \
+    if (!tc) build(k_build_K<N, kKFp32>);                        \
+    else if (use_tma) build(k_build_K<N, kKSwizzled>);           \
+    else build(k_build_K<N, kKCore>);                            \
+    break;
+      EXA_BUILD_K_CASE(16)
+      EXA_BUILD_K_CASE(48)
+      EXA_BUILD_K_CASE(64)
+      EXA_BUILD_K_CASE(112)
+#undef EXA_BUILD_K_CASE
+      default: return false;
+    }
   }
   if (tc) g.Msb.ensure(nc * 3 * NDP);
   else g.Msr.ensure(nc * NDP);
