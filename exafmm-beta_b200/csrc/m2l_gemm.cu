@@ -12,7 +12,7 @@
 // Im of those with m > 0: 2 NTERM - P of them, 64 at P = 8), a class's map is
 // one ND x ND real matrix K (built once per solve from FP64 harmonics).
 //
-// The pairs of each frequent class are sorted together; one block takes up to
+// The pairs of each class are sorted together; one block takes up to
 // 128 of them and forms Y = K x [Ms of their sources] as a dense product in
 // FP32 (the operator loaded once per block, 8 x 8 outputs per thread), writing
 // each pair's column of Y at the pair's position in the target-grouped list.
@@ -22,10 +22,14 @@
 //
 // Pairs through periodic images form classes of their own (the image and the
 // target level join the key, since the shift is not a multiple of the radii).
-// Classes used by fewer than kMinClassPairs pairs stay with the pair-by-pair
-// FP32 kernel, which then runs on a compacted list of just those pairs
-// (left_off / left_src); pairs outside the mixed policy stay with the FP64
-// kernel as before.
+// Every class gets its operator, even one used by a single pair: leaving the
+// classes of fewer than 8, 16, 32 or 64 pairs to the pair-by-pair kernel
+// measured slower on a 4M-body solve, the 512-system batch and the periodic
+// water box alike (the build of one more operator costs less than a pair
+// through the pair-by-pair kernel's launches).  Pairs whose class found no
+// hash slot stay with the pair-by-pair FP32 kernel, which then runs on a
+// compacted list of just those pairs (left_off / left_src); pairs outside the
+// mixed policy stay with the FP64 kernel as before.
 //
 // Two engines form the products.  The tensor-core one (k_m2l_class_mma) splits
 // every operand entry into three bf16 pieces, x = hi + mid + lo (24 significant
@@ -49,7 +53,7 @@ namespace exafmm_b200 {
 namespace {
 
 constexpr unsigned long long kEmpty = ~0ull;
-constexpr int kMinClassPairs = 16;
+constexpr int kMinClassPairs = 1;  // pairs a class needs for an operator of its own
 constexpr int kClsBits = 20;      // class id field of the pair key
 constexpr int kProbe = 64;        // hash probe limit (a pair that finds no slot stays per-pair)
 
@@ -167,7 +171,7 @@ __global__ void k_pair_class(const int *off, const int *src, long long ncells, c
   }
 }
 
-// 2. Classes used often enough, in arbitrary order (sorted by key next).
+// 2. Classes used by at least kMinClassPairs pairs, in arbitrary order (sorted by key next).
 __global__ void k_class_compact(const unsigned long long *hk, const unsigned *hc, long long hcap,
                                 unsigned long long *ck, int *cs, int *ncls, int cap) {
   for (long long h = blockIdx.x * (long long)blockDim.x + threadIdx.x; h < hcap; h += (long long)gridDim.x * blockDim.x) {
@@ -316,7 +320,7 @@ __global__ void k_scale_M_real(DevTables t, const double2 *M, const double4 *cel
   }
 }
 
-// 4. Per target: flag the pairs of frequent classes (taken) and count the
+// 4. Per target: flag the pairs of classes with an operator (taken) and count the
 // leftover pairs of the mixed policy (for the pair-by-pair kernel).
 __device__ __forceinline__ bool policy_pair(int lt, int ls, int min_level, int max_dl) {
   const int dl = lt - ls;
@@ -1257,7 +1261,7 @@ bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int
   k_scale_M_real<<<kNumSMs * 8, 256, 0, st>>>(t, a.M64, a.cell_x, nc, P, tc ? nullptr : g.Msr.p,
                                               tc ? g.Msb.p : nullptr);
   EXA_CHECK_LAUNCH();
-  // ---- pairs of frequent classes, sorted by class
+  // ---- pairs of classes with an operator, sorted by class
   g.taken.ensure(n_m2l);
   g.left_cnt.ensure(nc);
   g.left_off.ensure(nc + 1);
