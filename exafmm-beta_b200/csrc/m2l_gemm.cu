@@ -1170,13 +1170,20 @@ void tma_launch(const CUtensorMap &map, M2LGemmBufs &g, const int *sv, long long
 bool m2l_gemm_supported(int P) { return P == 4 || P == 6 || P == 8 || P == 10; }
 
 // Where the class products beat the pair-by-pair kernel for one solve on a
-// B200: from about 1M pairs at P = 8 and 0.4M pairs at P = 10; at P <= 6 the
-// pair-by-pair code is small and fast enough that they never do.
+// B200, measured on cube and Plummer systems of 20K-1M bodies (theta 0.4,
+// ncrit 64): from about 0.15M pairs at P = 10, 1M at P = 8 and 8M at P = 6
+// (at P = 4 the pair-by-pair code always wins), and only when the classes
+// hold at least kMinPairsPerClass pairs on average, since every class costs
+// an operator build: a 50K-body Plummer system at P = 10 (510K pairs, 73 per
+// class) solved in 5.1 ms pair by pair and 6.6 ms with the products, a
+// 100K-body cube (597K pairs, 89 per class) in 5.9 and 5.4 ms.
 bool m2l_gemm_worthwhile(int P, long long n_m2l) {
+  if (P == 6) return n_m2l >= 8000000;
   if (P == 8) return n_m2l >= 1000000;
-  if (P == 10) return n_m2l >= 400000;
+  if (P == 10) return n_m2l >= 150000;
   return false;
 }
+constexpr long long kMinPairsPerClass = 80;
 
 bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int min_level, int max_dl) {
   const int P = a.P;
@@ -1216,6 +1223,7 @@ bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int
   EXA_CUDA(cudaStreamSynchronize(st));
   int ncls = *ncls_h;
   if (ncls <= 0) return false;
+  if (!g.force && n_m2l < kMinPairsPerClass * (long long)ncls) return false;  // too many classes for their pairs
   if (ncls > ccap) ncls = ccap;  // the overflow classes' pairs stay per-pair
   bool alt = radix_sort_u64((uint64_t *)g.ck.p, g.cs.p, (uint64_t *)g.ck_alt.p, g.cs_alt.p, ncls, 0, 64, C.sort,
                             C.err.p, st);
