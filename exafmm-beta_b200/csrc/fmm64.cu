@@ -327,53 +327,76 @@ __global__ void k_l2l(DevTables t, const long long *lvl, int level, const int *n
 //               - sum_{u=1..n-2} conj(L_n^u) conj(Y_{n-1}^{u+1}) s(n,-u) ],  s(n,m) = sqrt((n+m)(n+m-1)/2)
 //   dx  = -sqrt(2) Re L11,  dy = sqrt(2) Im L11
 // This has no 1/sin(theta) factor, so no offset of the body from the cell center is needed.
+// Per leaf, the products of its local expansion that do not depend on the
+// body are formed once in shared memory (per term o = (n, m)):
+//   W = w_m L_n^m,  G = gz_o L_{n+1}^m,  A = s1_o L_{n+1}^{m+1},
+//   B = s2_o L_{n+1}^0 (m = 1) or s2_o conj(L_{n+1}^{m-1}) (m >= 2),
+// so a body's pass over the terms is four complex products with its regular
+// harmonic and the recurrence, from shared memory only (the recurrence
+// coefficients are staged once per block).
 __global__ void k_l2p(DevTables t, const int4 *cell_b, const double4 *cell_x, const double4 *xt, const double2 *L,
                       double4 *trg, long long ncells) {
   extern __shared__ double2 sh[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int P = t.P, NT = t.nterm;
-  double2 *Lc = sh + warp * NT;
+  double *ra = reinterpret_cast<double *>(sh);  // block: a_n^m, b_n^m, then rd
+  double *rb = ra + NT;
+  double *rd = rb + NT;
+  double2 *Wc = sh + NT + (P + 1) / 2 + warp * 4 * NT;
+  double2 *Gc = Wc + NT, *Ac = Gc + NT, *Bc = Ac + NT;
+  for (int o = threadIdx.x; o < NT; o += blockDim.x) {
+    ra[o] = t.ra[o];
+    rb[o] = t.rb[o];
+  }
+  for (int m = threadIdx.x; m < P; m += blockDim.x) rd[m] = t.rd[m];
+  __syncthreads();
   for (long long c = (long long)blockIdx.x * kWarpsPerBlock + warp; c < ncells; c += (long long)gridDim.x * kWarpsPerBlock) {
     const int4 cb = cell_b[c];
     if (cb.w != 0) continue;
     const double4 X = cell_x[c];
-    for (int o = lane; o < NT; o += 32) Lc[o] = L[c * NT + o];
+    const double2 *Lg = L + c * NT;
+    for (int o = lane; o < NT; o += 32) {
+      int n, m;
+      tri_decode(o, n, m);
+      const double2 Lnm = Lg[o];
+      Wc[o] = m == 0 ? Lnm : cscale(Lnm, 2.0);
+      double2 g = make_double2(0.0, 0.0), a = g, b = g;
+      if (n + 1 < P) {
+        g = cscale(Lg[tri(n + 1) + m], t.l2p_gz[o]);
+        a = cscale(Lg[tri(n + 1) + m + 1], t.l2p_s1[o]);
+        if (m == 1) b = cscale(Lg[tri(n + 1)], t.l2p_s2[o]);
+        else if (m >= 2) b = cscale(cconj(Lg[tri(n + 1) + m - 1]), t.l2p_s2[o]);
+      }
+      Gc[o] = g;
+      Ac[o] = a;
+      Bc[o] = b;
+    }
     __syncwarp();
     for (int i = lane; i < cb.y; i += 32) {
-      const double4 b = xt[cb.x + i];
-      const double x = b.x - X.x, y = b.y - X.y, z = b.z - X.z;
+      const double4 bd = xt[cb.x + i];
+      const double x = bd.x - X.x, y = bd.y - X.y, z = bd.z - X.z;
       const double r2 = x * x + y * y + z * z;
       double pot = 0, gz = 0;
       double2 l11 = make_double2(0.0, 0.0);
       double2 diag = make_double2(1.0, 0.0);
       for (int m = 0; m < P; m++) {
         if (m > 0) {
-          const double f = -t.rd[m];
+          const double f = -rd[m];
           diag = make_double2(f * (diag.x * x - diag.y * y), f * (diag.x * y + diag.y * x));
         }
-        const double wm = (m == 0) ? 1.0 : 2.0;
         double2 prev = make_double2(0.0, 0.0), cur = diag;
         for (int n = m; n < P; n++) {
           // cur = Y_n^m
-          const double2 Lnm = Lc[tri(n) + m];
-          pot += wm * (Lnm.x * cur.x - Lnm.y * cur.y);
+          const int o = tri(n) + m;
+          const double2 w = Wc[o];
+          pot += w.x * cur.x - w.y * cur.y;
           if (n + 1 < P) {
-            const int o = tri(n) + m;
-            const double2 L1 = Lc[tri(n + 1) + m];
-            gz += t.l2p_gz[o] * (L1.x * cur.x - L1.y * cur.y);
-            if (m + 1 <= n + 1) {
-              const double2 L2 = Lc[tri(n + 1) + m + 1];
-              l11 = cfma(L2, cscale(cur, t.l2p_s1[o]), l11);
-            }
-            if (m == 1) {
-              const double2 L0 = Lc[tri(n + 1)];
-              l11 = cfma(L0, cscale(cconj(cur), t.l2p_s2[o]), l11);
-            } else if (m >= 2) {
-              const double2 Lu = cconj(Lc[tri(n + 1) + m - 1]);
-              l11 = cfma(Lu, cscale(cconj(cur), t.l2p_s2[o]), l11);
-            }
-            const double a = t.ra[tri(n) + m], bb = t.rb[tri(n) + m];
-            double2 nxt = make_double2(a * z * cur.x - bb * r2 * prev.x, a * z * cur.y - bb * r2 * prev.y);
+            const double2 g = Gc[o];
+            gz += g.x * cur.x - g.y * cur.y;
+            l11 = cfma(Ac[o], cur, l11);
+            if (m >= 1) l11 = cfma(Bc[o], cconj(cur), l11);
+            const double az = ra[o] * z, br = rb[o] * r2;
+            double2 nxt = make_double2(az * cur.x - br * prev.x, az * cur.y - br * prev.y);
             prev = cur;
             cur = nxt;
           }
@@ -708,7 +731,8 @@ void l2l_fp64(const FmmArgs &a, int level, long long nodes_at_level) {
 
 void l2p_fp64(const FmmArgs &a) {
   const DevTables &t = device_tables(a.P);
-  size_t smem = kWarpsPerBlock * t.nterm * sizeof(double2);
+  // recurrence tables (2 NT + P doubles), then W, G, A, B per warp
+  size_t smem = (t.nterm + (a.P + 1) / 2 + kWarpsPerBlock * 4 * t.nterm) * sizeof(double2);
   set_smem(k_l2p, smem);
   k_l2p<<<blocks_for(a.ncells), 32 * kWarpsPerBlock, smem, a.stream>>>(t, a.cell_b, a.cell_x, a.xt, a.L64,
                                                                        a.trg64, a.ncells);
