@@ -67,7 +67,16 @@ __global__ void k_p2m(DevTables t, const int4 *cell_b, const double4 *cell_x, co
   extern __shared__ double2 sh[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int P = t.P, NT = t.nterm;
-  double2 *acc = sh + warp * (NT + 32 * kP2mRow);  // (m, n) order
+  double *ra = reinterpret_cast<double *>(sh);  // block: the recurrence's a_n^m, b_n^m and rd
+  double *rb = ra + NT;
+  double *rd = rb + NT;
+  for (int o = threadIdx.x; o < NT; o += blockDim.x) {
+    ra[o] = t.ra[o];
+    rb[o] = t.rb[o];
+  }
+  for (int m = threadIdx.x; m < P; m += blockDim.x) rd[m] = t.rd[m];
+  __syncthreads();
+  double2 *acc = sh + NT + (P + 1) / 2 + warp * (NT + 32 * kP2mRow);  // (m, n) order
   double2 *stage = acc + NT;
   double2 *mine = stage + lane * kP2mRow;
   double *accd = reinterpret_cast<double *>(acc);
@@ -92,7 +101,7 @@ __global__ void k_p2m(DevTables t, const int4 *cell_b, const double4 *cell_x, co
       int k = 0, win = 0;
       for (int m = 0; m < P; m++) {
         if (m > 0) {
-          const double f = -t.rd[m];
+          const double f = -rd[m];
           w = make_double2(f * (w.x * x + w.y * y), f * (w.y * x - w.x * y));
         }
         double2 prev = make_double2(0.0, 0.0), cur = w;
@@ -104,7 +113,7 @@ __global__ void k_p2m(DevTables t, const int4 *cell_b, const double4 *cell_x, co
             k = 0;
           }
           if (n + 1 < P) {
-            const double a = t.ra[tri(n) + m], b = t.rb[tri(n) + m];
+            const double a = ra[tri(n) + m], b = rb[tri(n) + m];
             double2 nxt = make_double2(a * z * cur.x - b * r2 * prev.x, a * z * cur.y - b * r2 * prev.y);
             prev = cur;
             cur = nxt;
@@ -687,7 +696,7 @@ void set_smem(F f, size_t bytes) {
 
 void p2m_fp64(const FmmArgs &a) {
   const DevTables &t = device_tables(a.P);
-  size_t smem = kWarpsPerBlock * (t.nterm + 32 * kP2mRow) * sizeof(double2);
+  size_t smem = (t.nterm + (a.P + 1) / 2 + kWarpsPerBlock * (t.nterm + 32 * kP2mRow)) * sizeof(double2);
   set_smem(k_p2m, smem);
   k_p2m<<<blocks_for(a.ncells), 32 * kWarpsPerBlock, smem, a.stream>>>(t, a.cell_b, a.cell_x, a.xt, a.M64, a.ncells);
   EXA_CHECK_LAUNCH();
