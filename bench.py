@@ -12,7 +12,7 @@ pass, results scattered back to input order.
   e2e   : the same through the public API from pinned host buffers: the host->device
           copy of the bodies and the device->host copy of the results are timed
   roofline : the dominant kernel timed live with CUDA events; rooflines: every
-             north-star kernel (P2P against the FP32 FMA peak, M2L and the
+             hot-path kernel (P2P against the FP32 FMA peak, M2L and the
              upward / downward passes against the measured HBM bandwidth)
   cpu_baseline : the reference's own CPU FMM (its headers compiled in place),
           all host threads, on a bounded sample of the same workload
@@ -236,7 +236,7 @@ def fp32_fma_peak_tflops(sm_mhz: float) -> float:
 
 
 def kernel_rooflines(P, mixed, n, info, phases, interactions, hbm_peak, peak_kind, sm_mhz):
-    """One entry per north-star kernel of a solve, from its phase time (CUDA events
+    """One entry per hot-path kernel of a solve, from its phase time (CUDA events
     over the timed steps) and its algorithmic work:
       p2p      20 flop per pair interaction (sum over the P2P list of n_i n_j, counted
                on the device) against the CUDA-core FP32 FMA peak;
@@ -307,7 +307,7 @@ def main():
     ap.add_argument("--min-level", type=int, default=None,
                     help="mixed form: lowest target level of the FP32 M2L (default 2: levels 0 and 1 in FP64)")
     ap.add_argument("--orders", default="6,8,10",
-                    help="serve: the expansion orders requests draw from (10 alone: the north star's P = 10 stream)")
+                    help="serve: the expansion orders requests draw from (10 alone: a stream of P = 10 requests only)")
     ap.add_argument("--group-max-n", type=int, default=262144,
                     help="serve: requests of at most this many bodies are grouped into forests")
     ap.add_argument("--ncrit-candidates", default="32,64,128",
@@ -450,7 +450,7 @@ def main():
                             "direct_sample": 4096}}
         f64.close()
 
-    # ---- rooflines of the north-star kernels, from the timed steps; the dominant one is `roofline`
+    # ---- rooflines of the hot-path kernels, from the timed steps; the dominant one is `roofline`
     hbm_peak, bf16_peak, peak_kind = _peaks()
     P = wl["P"]
     phases = {k: v / args.steps for k, v in phase_acc.items()}
