@@ -176,8 +176,8 @@ __global__ void k_m2m(DevTables t, const long long *lvl, int level, const int *n
   int oj[MAXO], ok[MAXO];
 #pragma unroll
   for (int u = 0; u < MAXO; u++) {
-    const int o = lane + 32 * u;
-    if (o < NT) tri_decode(o, oj[u], ok[u]);
+    const int o = t.m2m_lane[lane * MAXO + u];
+    if (o >= 0) tri_decode(o, oj[u], ok[u]);
     else oj[u] = ok[u] = -1;
   }
   for (long long i = (long long)blockIdx.x * kWarpsPerBlock + warp; i < cnt; i += (long long)gridDim.x * kWarpsPerBlock) {
@@ -198,10 +198,8 @@ __global__ void k_m2m(DevTables t, const long long *lvl, int level, const int *n
       __syncwarp();
     }
 #pragma unroll
-    for (int u = 0; u < MAXO; u++) {
-      const int o = lane + 32 * u;
-      if (o < NT) M[(long long)c * NT + o] = acc[u];
-    }
+    for (int u = 0; u < MAXO; u++)
+      if (oj[u] >= 0) M[(long long)c * NT + tri(oj[u]) + ok[u]] = acc[u];
   }
 }
 
@@ -302,8 +300,8 @@ __global__ void k_l2l(DevTables t, const long long *lvl, int level, const int *n
   int oj[MAXO], ok[MAXO];
 #pragma unroll
   for (int u = 0; u < MAXO; u++) {
-    const int o = lane + 32 * u;
-    if (o < NT) tri_decode(o, oj[u], ok[u]);
+    const int o = t.l2l_lane[lane * MAXO + u];
+    if (o >= 0) tri_decode(o, oj[u], ok[u]);
     else oj[u] = ok[u] = -1;
   }
   for (long long i = (long long)blockIdx.x * kWarpsPerBlock + warp; i < cnt; i += (long long)gridDim.x * kWarpsPerBlock) {

@@ -4,6 +4,7 @@
 // the tables here are the unscaled values.
 #include <math.h>
 
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <utility>
@@ -127,6 +128,29 @@ const DevTables &device_tables(int P) {
   t.m2m_start = (const int *)upload_raw(m2m_start.data(), m2m_start.size() * sizeof(int));
   t.l2l_ops = (const TransOp *)upload_raw(l2l.data(), l2l.size() * sizeof(TransOp));
   t.l2l_start = (const int *)upload_raw(l2l_start.data(), l2l_start.size() * sizeof(int));
+  // Balanced lane assignment of the output coefficients (see DevTables).
+  auto balance = [&](const std::vector<int> &start) {
+    const int NT = tri(P), MO = (NT + 31) / 32;
+    std::vector<int> order(NT);
+    for (int o = 0; o < NT; o++) order[o] = o;
+    auto cost = [&](int o) { return start[o + 1] - start[o]; };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+    std::vector<long long> load(32, 0);
+    std::vector<int> used(32, 0);
+    std::vector<short> out((size_t)32 * MO, (short)-1);
+    for (int o : order) {
+      int best = -1;
+      for (int l = 0; l < 32; l++)
+        if (used[l] < MO && (best < 0 || load[l] < load[best])) best = l;
+      out[(size_t)best * MO + used[best]] = (short)o;
+      used[best]++;
+      load[best] += cost(o) + 1;
+    }
+    return out;
+  };
+  const std::vector<short> m2m_lane = balance(m2m_start), l2l_lane = balance(l2l_start);
+  t.m2m_lane = (const short *)upload_raw(m2m_lane.data(), m2m_lane.size() * sizeof(short));
+  t.l2l_lane = (const short *)upload_raw(l2l_lane.data(), l2l_lane.size() * sizeof(short));
   t.l2p_gz = upload(gz);
   t.l2p_s1 = upload(s1);
   t.l2p_s2 = upload(s2);
