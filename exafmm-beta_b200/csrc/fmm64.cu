@@ -288,21 +288,26 @@ __global__ void k_m2l(DevTables t, const int *off, const int *src, long long nce
 
 // ---------------------------------------------------------------- L2L
 // Child L from its parent (laplace.h:324-357), d = X_child - X_parent.
-template <int MAXO>
+template <int MI>
 __global__ void k_l2l(DevTables t, const long long *lvl, int level, const int *nd_cell, const int2 *cell_pl,
                       const double4 *cell_x, double2 *L) {
   extern __shared__ double2 sh[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int P = t.P, NT = t.nterm;
-  double2 *Y = sh + warp * 2 * NT;
+  double2 *Y = sh + warp * (2 * NT + 32 * MI);
   double2 *Lp = Y + NT;
+  double2 *part = Lp + NT;  // the warp's piece sums
   const long long cnt = lvl[level], start = lvl[kMaxLevels + 1 + level];
-  int oj[MAXO], ok[MAXO];
+  int pid[MI], pb[MI], pe[MI];
 #pragma unroll
-  for (int u = 0; u < MAXO; u++) {
-    const int o = t.l2l_lane[lane * MAXO + u];
-    if (o >= 0) tri_decode(o, oj[u], ok[u]);
-    else oj[u] = ok[u] = -1;
+  for (int u = 0; u < MI; u++) {
+    pid[u] = t.l2l_slot[lane * MI + u];
+    pb[u] = pe[u] = 0;
+    if (pid[u] >= 0) {
+      const int4 pc = t.l2l_piece[pid[u]];
+      pb[u] = pc.y;
+      pe[u] = pc.z;
+    }
   }
   for (long long i = (long long)blockIdx.x * kWarpsPerBlock + warp; i < cnt; i += (long long)gridDim.x * kWarpsPerBlock) {
     const int c = nd_cell[start + i];
@@ -313,13 +318,15 @@ __global__ void k_l2l(DevTables t, const long long *lvl, int level, const int *n
     for (int o = lane; o < NT; o += 32) Lp[o] = L[(long long)p * NT + o];
     __syncwarp();
 #pragma unroll
-    for (int u = 0; u < MAXO; u++) {
-      const int j = oj[u], k = ok[u];
-      if (j < 0) continue;
-      const int o = tri(j) + k;
-      const double2 a = trans_sum(t.l2l_ops, t.l2l_start[o], t.l2l_start[o + 1], Lp, Y, make_double2(0.0, 0.0));
+    for (int u = 0; u < MI; u++)
+      if (pid[u] >= 0) part[pid[u]] = trans_sum(t.l2l_ops, pb[u], pe[u], Lp, Y, make_double2(0.0, 0.0));
+    __syncwarp();
+    for (int o = lane; o < NT; o += 32) {
+      const int q0 = t.l2l_piece_start[o], q1 = t.l2l_piece_start[o + 1];
+      double2 v = part[q0];
+      for (int q = q0 + 1; q < q1; q++) v = cadd(v, part[q]);
       double2 *dst = &L[(long long)c * NT + o];
-      *dst = cadd(*dst, a);
+      *dst = cadd(*dst, v);
     }
     __syncwarp();
   }
@@ -727,8 +734,8 @@ void m2l_fp64(const FmmArgs &a, int skip_min_level, int skip_max_dl) {
 
 void l2l_fp64(const FmmArgs &a, int level, long long nodes_at_level) {
   const DevTables &t = device_tables(a.P);
-  size_t smem = kWarpsPerBlock * 2 * t.nterm * sizeof(double2);
-  EXA_MAXO_SWITCH(maxo_for(a.P), {
+  size_t smem = kWarpsPerBlock * (2 * t.nterm + 32 * t.l2l_slots) * sizeof(double2);
+  EXA_MAXO_SWITCH(t.l2l_slots, {
     set_smem(k_l2l<MO>, smem);
     k_l2l<MO><<<blocks_for(nodes_at_level), 32 * kWarpsPerBlock, smem, a.stream>>>(t, a.lvl, level, a.nd_cell,
                                                                                    a.cell_pl, a.cell_x, a.L64);

@@ -41,12 +41,22 @@ struct DevTables {
   const int *m2m_start;
   const TransOp *l2l_ops;
   const int *l2l_start;
-  // The output coefficients each lane of a warp sums in k_m2m and k_l2l:
-  // lane l takes entries [l * MAXO, l * MAXO + MAXO) (-1: none), MAXO =
-  // ceil(NT / 32), assigned longest first to the least loaded lane so that
-  // the lanes' term counts are about equal (the warp waits for its busiest).
+  // The output coefficients each lane of a warp sums in k_m2m: lane l takes
+  // entries [l * MAXO, l * MAXO + MAXO) (-1: none), MAXO = ceil(NT / 32),
+  // assigned longest first to the least loaded lane so that the lanes' term
+  // counts are about equal (the warp waits for its busiest).
   const short *m2m_lane;
-  const short *l2l_lane;
+  // Work split of k_l2l over the 32 lanes of a warp.  Each output
+  // coefficient's terms are cut into pieces of about the lanes' average share
+  // (piece q: int4 (o, first term, end term, 0), pieces of one output
+  // consecutive, [piece_start[o], piece_start[o + 1])); lane l sums the pieces
+  // slot[l * slots + u] (-1: none), assigned longest first to the least
+  // loaded lane, and an output is the sum of its pieces in order.  L2L needs
+  // it: its (0, 0) coefficient sums every term.
+  const int4 *l2l_piece;
+  const int *l2l_piece_start;
+  const short *l2l_slot;
+  int l2l_slots, l2l_pieces;
   // L2P factors per (n, m), index tri(n) + m, n + 1 < P (laplace.h:359-388 as
   // restated in k_l2p): w_m sqrt((n+1)^2 - m^2), sqrt((n+m+2)(n+m+1)/2), and
   // -sqrt((n+1)n/2) (m = 1) or -sqrt((n+2-m)(n+1-m)/2) (m >= 2).

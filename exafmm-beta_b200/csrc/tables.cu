@@ -128,29 +128,71 @@ const DevTables &device_tables(int P) {
   t.m2m_start = (const int *)upload_raw(m2m_start.data(), m2m_start.size() * sizeof(int));
   t.l2l_ops = (const TransOp *)upload_raw(l2l.data(), l2l.size() * sizeof(TransOp));
   t.l2l_start = (const int *)upload_raw(l2l_start.data(), l2l_start.size() * sizeof(int));
-  // Balanced lane assignment of the output coefficients (see DevTables).
-  auto balance = [&](const std::vector<int> &start) {
+  // Pieces of the translation terms and their lanes (see DevTables).
+  struct Split {
+    std::vector<int4> piece;
+    std::vector<int> piece_start;
+    std::vector<short> slot;
+    int slots = 0;
+  };
+  auto split = [&](const std::vector<int> &start) {
+    const int NT = tri(P);
+    const int total = start[NT] - start[0];
+    const int cap = std::max(1, (total + 31) / 32);  // about the lanes' average share
+    Split s;
+    for (int o = 0; o < NT; o++) {
+      s.piece_start.push_back((int)s.piece.size());
+      const int b = start[o], n = start[o + 1] - start[o];
+      const int k = std::max(1, (n + cap - 1) / cap);
+      for (int q = 0; q < k; q++) s.piece.push_back(make_int4(o, b + n * q / k, b + n * (q + 1) / k, 0));
+    }
+    s.piece_start.push_back((int)s.piece.size());
+    const int np = (int)s.piece.size();
+    s.slots = (np + 31) / 32;
+    std::vector<int> order(np);
+    for (int q = 0; q < np; q++) order[q] = q;
+    auto len = [&](int q) { return s.piece[q].z - s.piece[q].y; };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return len(a) > len(b); });
+    std::vector<long long> load(32, 0);
+    std::vector<int> used(32, 0);
+    s.slot.assign((size_t)32 * s.slots, (short)-1);
+    for (int q : order) {
+      int best = -1;
+      for (int l = 0; l < 32; l++)
+        if (used[l] < s.slots && (best < 0 || load[l] < load[best])) best = l;
+      s.slot[(size_t)best * s.slots + used[best]] = (short)q;
+      used[best]++;
+      load[best] += len(q) + 1;
+    }
+    return s;
+  };
+  // M2M's lanes: whole output coefficients, longest first to the least loaded
+  // lane (cutting them into pieces measured slower at P = 10).
+  {
     const int NT = tri(P), MO = (NT + 31) / 32;
     std::vector<int> order(NT);
     for (int o = 0; o < NT; o++) order[o] = o;
-    auto cost = [&](int o) { return start[o + 1] - start[o]; };
+    auto cost = [&](int o) { return m2m_start[o + 1] - m2m_start[o]; };
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
     std::vector<long long> load(32, 0);
     std::vector<int> used(32, 0);
-    std::vector<short> out((size_t)32 * MO, (short)-1);
+    std::vector<short> lane_out((size_t)32 * MO, (short)-1);
     for (int o : order) {
       int best = -1;
       for (int l = 0; l < 32; l++)
         if (used[l] < MO && (best < 0 || load[l] < load[best])) best = l;
-      out[(size_t)best * MO + used[best]] = (short)o;
+      lane_out[(size_t)best * MO + used[best]] = (short)o;
       used[best]++;
       load[best] += cost(o) + 1;
     }
-    return out;
-  };
-  const std::vector<short> m2m_lane = balance(m2m_start), l2l_lane = balance(l2l_start);
-  t.m2m_lane = (const short *)upload_raw(m2m_lane.data(), m2m_lane.size() * sizeof(short));
-  t.l2l_lane = (const short *)upload_raw(l2l_lane.data(), l2l_lane.size() * sizeof(short));
+    t.m2m_lane = (const short *)upload_raw(lane_out.data(), lane_out.size() * sizeof(short));
+  }
+  const Split sl = split(l2l_start);
+  t.l2l_piece = (const int4 *)upload_raw(sl.piece.data(), sl.piece.size() * sizeof(int4));
+  t.l2l_piece_start = (const int *)upload_raw(sl.piece_start.data(), sl.piece_start.size() * sizeof(int));
+  t.l2l_slot = (const short *)upload_raw(sl.slot.data(), sl.slot.size() * sizeof(short));
+  t.l2l_slots = sl.slots;
+  t.l2l_pieces = (int)sl.piece.size();
   t.l2p_gz = upload(gz);
   t.l2p_s1 = upload(s1);
   t.l2p_s2 = upload(s2);
