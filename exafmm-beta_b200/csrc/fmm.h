@@ -119,6 +119,20 @@ struct P2PWork {
   DBuf<unsigned> key, key_alt;     // order keys
   DBuf<int> order, order_alt;      // cells in work order
   DBuf<int> count;                 // [3] leaves of each kind: two targets per lane, three, no P2P list
+  // The three-target kind runs on a stream of its own, forked from and joined
+  // back to the solve's stream, so its blocks take the SMs that the
+  // two-target kind's last leaves leave idle (made on first use).
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  P2PWork() = default;
+  P2PWork(const P2PWork &) = delete;
+  P2PWork &operator=(const P2PWork &) = delete;
+  ~P2PWork() {
+    if (side) cudaStreamSynchronize(side);
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+    if (side) cudaStreamDestroy(side);
+  }
 };
 // x32j (null: x32) holds the source bodies, whose cells are a.src_cell_b when set.
 void p2p_mixed(Context &C, const FmmArgs &a, const float4 *x32, bool periodic, P2PWork &w,

@@ -467,20 +467,33 @@ void p2p_mixed(Context &C, const FmmArgs &a, const float4 *x32, bool periodic, P
   const int *order = alt ? w.order_alt.p : w.order.p;
   const unsigned g2 = (unsigned)std::min<long long>(nc, (long long)kNumSMs * kWarps2);
   const unsigned g3 = (unsigned)std::min<long long>(nc, (long long)kNumSMs * kWarps3);
+  if (!w.side) {
+    int dev = 0;
+    EXA_CUDA(cudaGetDevice(&dev));
+    EXA_CUDA(cudaStreamCreateWithFlags(&w.side, cudaStreamNonBlocking));
+    EXA_CUDA(cudaEventCreateWithFlags(&w.fork, cudaEventDisableTiming));
+    EXA_CUDA(cudaEventCreateWithFlags(&w.join, cudaEventDisableTiming));
+  }
+  // the two kinds write disjoint target leaves; the side stream starts after
+  // the work order is sorted and the solve's stream waits for it at the end
+  EXA_CUDA(cudaEventRecord(w.fork, st));
+  EXA_CUDA(cudaStreamWaitEvent(w.side, w.fork, 0));
   if (periodic) {
     k_p2p32<true, 2><<<g2, 32, 0, st>>>(a.p2p_off, a.p2p_src, order, w.count.p, a.cell_b, cell_bj, x32, x32j,
                                         a.trg64, a.cycle, w.next.p);
     EXA_CHECK_LAUNCH();
-    k_p2p32<true, 3><<<g3, 32, 0, st>>>(a.p2p_off, a.p2p_src, order, w.count.p, a.cell_b, cell_bj, x32, x32j,
-                                        a.trg64, a.cycle, w.next.p + 1);
+    k_p2p32<true, 3><<<g3, 32, 0, w.side>>>(a.p2p_off, a.p2p_src, order, w.count.p, a.cell_b, cell_bj, x32, x32j,
+                                            a.trg64, a.cycle, w.next.p + 1);
   } else {
     k_p2p32<false, 2><<<g2, 32, 0, st>>>(a.p2p_off, a.p2p_src, order, w.count.p, a.cell_b, cell_bj, x32, x32j,
                                          a.trg64, a.cycle, w.next.p);
     EXA_CHECK_LAUNCH();
-    k_p2p32<false, 3><<<g3, 32, 0, st>>>(a.p2p_off, a.p2p_src, order, w.count.p, a.cell_b, cell_bj, x32, x32j,
-                                         a.trg64, a.cycle, w.next.p + 1);
+    k_p2p32<false, 3><<<g3, 32, 0, w.side>>>(a.p2p_off, a.p2p_src, order, w.count.p, a.cell_b, cell_bj, x32, x32j,
+                                             a.trg64, a.cycle, w.next.p + 1);
   }
   EXA_CHECK_LAUNCH();
+  EXA_CUDA(cudaEventRecord(w.join, w.side));
+  EXA_CUDA(cudaStreamWaitEvent(st, w.join, 0));
 }
 
 }  // namespace exafmm_b200
