@@ -69,7 +69,6 @@ bool m2l_fast(const FmmArgs &a, bool mixed, const void *Ms, int min_level = 0, i
 // by target, for the pair-by-pair FP32 kernel.
 struct M2LGemmBufs {
   DBuf<unsigned long long> hk;        // class hash table: keys
-  DBuf<unsigned> hc;                  // pairs per slot
   DBuf<int> hid;                      // slot -> class id (or -1)
   DBuf<int> pair_slot;                // per list entry: hash slot (or -1)
   DBuf<unsigned long long> ck, ck_alt;

@@ -53,7 +53,6 @@ namespace exafmm_b200 {
 namespace {
 
 constexpr unsigned long long kEmpty = ~0ull;
-constexpr int kMinClassPairs = 1;  // pairs a class needs for an operator of its own
 constexpr int kClsBits = 20;      // class id field of the pair key
 constexpr int kProbe = 64;        // hash probe limit (a pair that finds no slot stays per-pair)
 
@@ -128,7 +127,7 @@ __device__ __forceinline__ unsigned long long class_key_image(int lt, int dl, in
 
 // 1. Per pair of the target-grouped list: its class's hash slot, or -1.
 __global__ void k_pair_class(const int *off, const int *src, long long ncells, const double4 *cell_x,
-                             const int2 *cell_pl, int min_level, int max_dl, unsigned long long *hk, unsigned *hc,
+                             const int2 *cell_pl, int min_level, int max_dl, unsigned long long *hk,
                              long long hmask, int *pair_slot) {
   const int lane = threadIdx.x & 31;
   const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
@@ -158,7 +157,6 @@ __global__ void k_pair_class(const int *off, const int *src, long long ncells, c
             unsigned long long old = __ldcg(&hk[h]);
             if (old == kEmpty) old = atomicCAS(&hk[h], kEmpty, key);
             if (old == kEmpty || old == key) {
-              atomicAdd(&hc[h], 1u);
               slot = (int)h;
               break;
             }
@@ -171,11 +169,11 @@ __global__ void k_pair_class(const int *off, const int *src, long long ncells, c
   }
 }
 
-// 2. Classes used by at least kMinClassPairs pairs, in arbitrary order (sorted by key next).
-__global__ void k_class_compact(const unsigned long long *hk, const unsigned *hc, long long hcap,
+// 2. The classes (every occupied slot), in arbitrary order (sorted by key next).
+__global__ void k_class_compact(const unsigned long long *hk, long long hcap,
                                 unsigned long long *ck, int *cs, int *ncls, int cap) {
   for (long long h = blockIdx.x * (long long)blockDim.x + threadIdx.x; h < hcap; h += (long long)gridDim.x * blockDim.x) {
-    if (hk[h] != kEmpty && hc[h] >= (unsigned)kMinClassPairs) {
+    if (hk[h] != kEmpty) {
       const int i = atomicAdd(ncls, 1);
       if (i < cap) {
         ck[i] = hk[h];
@@ -1200,23 +1198,21 @@ bool m2l_gemm(Context &C, const FmmArgs &a, M2LGemmBufs &g, long long n_m2l, int
   long long hcap = 1 << 14;
   while (hcap < n_m2l / 16 && hcap < (1LL << 20)) hcap <<= 1;
   g.hk.ensure(hcap);
-  g.hc.ensure(hcap);
   g.hid.ensure(hcap);
   g.pair_slot.ensure(n_m2l);
   g.cnt.ensure(4);
   EXA_CUDA(cudaMemsetAsync(g.hk.p, 0xff, hcap * sizeof(unsigned long long), st));
-  EXA_CUDA(cudaMemsetAsync(g.hc.p, 0, hcap * sizeof(unsigned), st));
   EXA_CUDA(cudaMemsetAsync(g.hid.p, 0xff, hcap * sizeof(int), st));
   EXA_CUDA(cudaMemsetAsync(g.cnt.p, 0, 4 * sizeof(int), st));
   k_pair_class<<<kNumSMs * 8, 256, 0, st>>>(a.m2l_off, a.m2l_src, nc, a.cell_x, a.cell_pl, min_level, max_dl, g.hk.p,
-                                            g.hc.p, hcap - 1, g.pair_slot.p);
+                                            hcap - 1, g.pair_slot.p);
   EXA_CHECK_LAUNCH();
   const int ccap = (int)std::min<long long>(hcap, (1LL << kClsBits) - 1);
   g.ck.ensure(ccap);
   g.ck_alt.ensure(ccap);
   g.cs.ensure(ccap);
   g.cs_alt.ensure(ccap);
-  k_class_compact<<<kNumSMs * 4, 256, 0, st>>>(g.hk.p, g.hc.p, hcap, g.ck.p, g.cs.p, g.cnt.p, ccap);
+  k_class_compact<<<kNumSMs * 4, 256, 0, st>>>(g.hk.p, hcap, g.ck.p, g.cs.p, g.cnt.p, ccap);
   EXA_CHECK_LAUNCH();
   int *ncls_h = reinterpret_cast<int *>(C.pin + kPinScratch);  // the context's pinned staging
   EXA_CUDA(cudaMemcpyAsync(ncls_h, g.cnt.p, sizeof(int), cudaMemcpyDeviceToHost, st));
